@@ -1,0 +1,274 @@
+/*
+ * rtt_spgemm.h - C ABI of the B200 (sm_100a) tiled FP64 SpGEMM.
+ *
+ * This library replaces the tiled SpGEMM path of for-the-juan/RTT-SpGEMM:
+ * CSR -> 16x16 tiles (csr2tile) -> three-step tile SpGEMM (C = A*B, A*A,
+ * A*A^T) -> tiles -> CSR (tile2csr).  Every entry point below does its work
+ * with hand-written CUDA kernels on one GPU; there is no CPU fallback.  When
+ * no usable GPU is present an entry point returns RTT_ERR_NO_DEVICE.
+ *
+ * Conventions kept from the reference so that existing callers drop in:
+ *   - SMatrix is byte-for-byte the struct of src/common.h:50-72
+ *     (MAT_VAL_TYPE = double, MAT_PTR_TYPE = int).
+ *   - Tile geometry is 16x16 (BLOCK_SIZE, src/common.h:30-33).
+ *   - Row-major tiles (csr2tile_row_major): tile_csr_Col holds the packed
+ *     byte (row << 4) | col, mask[tile*16 + row] has bit (15 - col) set,
+ *     tile_csr_Ptr holds exclusive per-row offsets inside the tile and
+ *     tile_nnz is the exclusive scan of per-tile counts (numtile + 1 entries).
+ *   - Column-major tiles (csr2tile_col_major): per-tile data stored in tile
+ *     CSC order, plain column bytes, rows past a partial edge padded with the
+ *     tile's entry count.
+ *   - Outputs are allocated with malloc() into the SMatrix and are owned by
+ *     the caller (free() them, or call rtt_matrix_destroy).
+ *
+ * Differences from the reference, all deliberate:
+ *   - Functions return an rtt_status code instead of void/bool and never
+ *     abort; on failure the output SMatrix is left unchanged.
+ *   - rtt_spgemm_tile reads A's in-tile column as (byte & 0xF).  The
+ *     reference spgemm_cpu uses the packed byte directly as a column
+ *     (src/spgemm-cpu.h:231, :324), which is wrong for every A row but row 0.
+ *   - rtt_spgemm_tile also fills C->m, C->n, C->tilem, C->tilen, C->mask and
+ *     C->tile_rowidx, which spgemm_cpu leaves untouched.
+ */
+#ifndef RTT_SPGEMM_H_
+#define RTT_SPGEMM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RTT_API __attribute__((visibility("default")))
+#else
+#define RTT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef MAT_VAL_TYPE
+#define MAT_VAL_TYPE double
+#endif
+#ifndef MAT_PTR_TYPE
+#define MAT_PTR_TYPE int
+#endif
+
+/* Edge of the legacy square tile (reference BLOCK_SIZE). */
+#define RTT_TILE_DIM 16
+/* Edge of the reference's native 8x8 output tile (DMMA_TILE_M/N). */
+#define RTT_OUTPUT_TILE_DIM 8
+
+#ifndef SMATRIX
+#define SMATRIX
+/* Identical layout to the reference SMatrix (src/common.h:50-72). */
+typedef struct
+{
+    int m;
+    int n;
+    int nnz;
+    int isSymmetric;
+    MAT_VAL_TYPE *value;
+    int *columnindex;
+    MAT_PTR_TYPE *rowpointer;
+    int tilem;
+    int tilen;
+    MAT_PTR_TYPE *tile_ptr;
+    int *tile_columnidx;
+    int *tile_rowidx;
+    int *tile_nnz;
+    int numtile;
+    MAT_VAL_TYPE *tile_csr_Value;
+    unsigned char *tile_csr_Col;
+    unsigned char *tile_csr_Ptr;
+    unsigned short *mask;
+    int *csc_tile_ptr;
+    int *csc_tile_rowidx;
+} SMatrix;
+#endif
+
+/* Status codes.  RTT_ERR_UNREPRESENTABLE mirrors the reference's
+ * WIDE_OUTPUT_UNREPRESENTABLE status (src/main.cu:2203-2219): the result does
+ * not fit the int32 fields of SMatrix / the int32 CSR of the device path. */
+typedef enum
+{
+    RTT_OK = 0,
+    RTT_ERR_INVALID_ARGUMENT = 1,
+    RTT_ERR_INVALID_CSR = 2,
+    RTT_ERR_SHAPE_MISMATCH = 3,
+    RTT_ERR_OUT_OF_MEMORY = 4,
+    RTT_ERR_CUDA = 5,
+    RTT_ERR_UNREPRESENTABLE = 6,
+    RTT_ERR_NO_DEVICE = 7,
+    RTT_ERR_DEVICE_CHECK = 8,
+    RTT_ERR_INVALID_PERMUTATION = 9,
+    RTT_ERR_TAIL_NONEMPTY = 10,
+    RTT_ERR_STATE = 11
+} rtt_status;
+
+/* Human-readable name of a status code. */
+RTT_API const char *rtt_status_string(int status);
+/* Message of the most recent failure on the calling thread ("" if none). */
+RTT_API const char *rtt_last_error(void);
+/* Library version string. */
+RTT_API const char *rtt_version(void);
+
+/* ------------------------------------------------------------------------
+ * Host-buffer drop-ins.  SMatrix arrays live in host memory; the work runs on
+ * the current CUDA device (device 0 unless rtt_set_device was called).
+ * ------------------------------------------------------------------------ */
+
+/* Select the CUDA device used by the host-buffer entry points. */
+RTT_API int rtt_set_device(int device);
+
+/* Replaces csr2tile_row_major(SMatrix*) (src/csr2tile.h:196-259).
+ * Reads m, n, nnz, rowpointer, columnindex, value; allocates and fills
+ * tilem, tilen, numtile, tile_ptr, tile_columnidx, tile_rowidx, tile_nnz,
+ * tile_csr_Ptr, tile_csr_Col, tile_csr_Value, mask. */
+RTT_API int rtt_csr2tile_row_major(SMatrix *matrix);
+
+/* Replaces csr2tile_col_major(SMatrix*) (src/csr2tile.h:261-478).
+ * Additionally fills csc_tile_ptr and csc_tile_rowidx; the per-tile arrays
+ * (tile_nnz, tile_csr_*, mask) are in tile-CSC order, tile_rowidx is zeroed
+ * as in the reference. */
+RTT_API int rtt_csr2tile_col_major(SMatrix *matrix);
+
+/* Replaces spgemm_cpu(SMatrix*A, SMatrix*B, SMatrix*C) (src/spgemm-cpu.h:369-455).
+ * A: output of csr2tile_row_major; B: output of csr2tile_col_major (B may
+ * describe A itself for C = A*A, or A^T for C = A*A^T).  C receives the
+ * legacy 16x16 tile CSR: tile_ptr, tile_columnidx, tile_nnz, tile_csr_Ptr,
+ * tile_csr_Col (plain column), tile_csr_Value, nnz, numtile, plus m, n,
+ * tilem, tilen, tile_rowidx and mask (bit 15 - col). */
+RTT_API int rtt_spgemm_tile(SMatrix *A, SMatrix *B, SMatrix *C);
+
+/* Replaces tile2csr(SMatrix*, bool canonical) (src/tile2csr.h:232-329) for
+ * square tiles of edge tile_dim (8: the reference's native output tiles;
+ * 16: the legacy tiles produced by rtt_spgemm_tile).  Fills rowpointer,
+ * columnindex, value and nnz.  Entries with an out-of-range column are
+ * dropped and row bounds are clamped exactly as the reference does.  With
+ * canonical == 0 each row is sorted by column (stable). */
+RTT_API int rtt_tile2csr(SMatrix *matrix, int tile_dim, int canonical);
+
+/* Replaces tile2csr_restore_rows (src/tile2csr.h:337-523): tile2csr that
+ * writes reordered row new_row of C to original row row_new_to_old[new_row]
+ * for new_row < permutation_size.  Rows at or past permutation_size must be
+ * empty (RTT_ERR_TAIL_NONEMPTY otherwise); an illegal permutation returns
+ * RTT_ERR_INVALID_PERMUTATION. */
+RTT_API int rtt_tile2csr_restore_rows(SMatrix *matrix, const int *row_new_to_old,
+                              int permutation_size, int tile_dim,
+                              int canonical);
+
+/* Split a legacy 16x16 tile C (as produced by rtt_spgemm_tile) into the
+ * reference's native 8x8 output layout: the SMatrix that dmma_tilespgemm
+ * exports (src/dmma_spgemm.h:6399-6488) - tile_ptr over 8-row tile rows,
+ * tile_columnidx over 8-column tile columns, tile_nnz offsets, 8 row-offset
+ * bytes per tile, column byte = col % 8.  Empty 8x8 quadrants are dropped. */
+RTT_API int rtt_tile16_to_tile8(const SMatrix *c16, SMatrix *c8);
+
+/* Frees every array the library allocated into matrix (tile fields, the csc
+ * fields and, when owned_csr != 0, rowpointer/columnindex/value) and sets the
+ * pointers to NULL.  The reference matrix_destroy (src/csr2tile.h:481-492)
+ * frees the tile fields only. */
+RTT_API void rtt_matrix_destroy(SMatrix *matrix, int owned_csr);
+
+/* ------------------------------------------------------------------------
+ * Device-resident product: device CSR(A) [, CSR(B)] in -> device CSR(C) out,
+ * through 16x16 tiles.  This is the path the reference times
+ * (src/main.cu:2171-2382: B csr2tile + symbolic + allocation + numeric),
+ * extended with csr2tile of A and tile2csr of C.
+ * ------------------------------------------------------------------------ */
+
+typedef struct rtt_context_s *rtt_context;
+
+/* C = A * B (B == NULL means B = A), C = A * A^T. */
+enum
+{
+    RTT_OP_AB = 0,
+    RTT_OP_AAT = 1
+};
+
+/* Device CSR operand (int32 offsets, 0-based, FP64 values). */
+typedef struct
+{
+    int rows;
+    int cols;
+    long long nnz;
+    const int *row_ptr; /* rows + 1 */
+    const int *col_idx; /* nnz */
+    const double *values; /* nnz */
+} rtt_csr_view;
+
+/* Tuning knobs of one context.  Zero-initialise and call
+ * rtt_config_default() to get the defaults. */
+typedef struct
+{
+    /* A tile pair (A(I,K), B(K,J)) goes to the FP64 DMMA tensor-core path
+     * when nnz(A(I,K)) * nnz(B(K,J)) >= dmma_pair_cutoff; 0 disables DMMA. */
+    int dmma_pair_cutoff;
+    /* Numeric writes C's CSR directly (fused tile2csr) when nonzero;
+     * otherwise C is written as 16x16 tiles and converted by tile2csr. */
+    int fused_csr_output;
+    /* Keep C's 16x16 tile arrays on the device after numeric (needed for
+     * rtt_spgemm_tiles_view); implied when fused_csr_output == 0. */
+    int keep_tiles;
+    /* Reserved, must be zero. */
+    int reserved[8];
+} rtt_config;
+
+RTT_API void rtt_config_default(rtt_config *config);
+
+/* Per-context statistics of the last product. */
+typedef struct
+{
+    long long nnz_a;
+    long long nnz_b;
+    long long nnz_c;
+    long long nnz_cub; /* sum over (i,k) in A of nnz(B row k); flops = 2*nnz_cub */
+    long long tiles_a;
+    long long tiles_b;
+    long long tiles_c;
+    long long dmma_pairs;
+    long long sparse_pairs;
+    int kernel_launches; /* kernels launched by the last symbolic+numeric */
+    int host_syncs;      /* stream synchronisations in the last symbolic */
+} rtt_stats;
+
+/* A context owns a CUDA stream handle (borrowed), workspace and the state
+ * carried from rtt_spgemm_symbolic to rtt_spgemm_numeric.  One context must
+ * not be used by two host threads at once. */
+RTT_API int rtt_context_create(rtt_context *ctx, int device);
+RTT_API void rtt_context_destroy(rtt_context ctx);
+/* stream is a cudaStream_t (NULL = legacy default stream). */
+RTT_API int rtt_context_set_stream(rtt_context ctx, void *stream);
+RTT_API int rtt_context_set_config(rtt_context ctx, const rtt_config *config);
+RTT_API int rtt_context_get_stats(rtt_context ctx, rtt_stats *stats);
+
+/* Phase 1: csr2tile of A (and B), the three-step symbolic, exact sizes.
+ * A and B stay borrowed until rtt_spgemm_numeric returns.  Writes the exact
+ * nnz(C) and tile count of C.  Returns RTT_ERR_UNREPRESENTABLE when nnz(C)
+ * exceeds INT32_MAX. */
+RTT_API int rtt_spgemm_symbolic(rtt_context ctx, const rtt_csr_view *A,
+                        const rtt_csr_view *B, int op, long long *nnz_c,
+                        long long *tiles_c);
+
+/* Phase 2: numeric into caller-owned device buffers: c_row_ptr (rows + 1),
+ * c_col_idx and c_values (nnz_c from phase 1).  Rows come out sorted by
+ * column. */
+RTT_API int rtt_spgemm_numeric(rtt_context ctx, int *c_row_ptr, int *c_col_idx,
+                       double *c_values);
+
+/* Device pointers to C's 16x16 tiles from the last numeric (legacy SMatrix
+ * layout, plain column bytes).  Valid until the next symbolic on ctx. */
+RTT_API int rtt_spgemm_tiles_view(rtt_context ctx, SMatrix *c_tiles_device);
+
+/* Host-buffer CSR product through the device path: copies A (and B) to the
+ * device, runs both phases, copies C back into malloc'd rowpointer /
+ * columnindex / value of C (m, n, nnz set).  A and B are CSR SMatrix (only
+ * the CSR fields are read).  B == NULL means B = A for RTT_OP_AB. */
+RTT_API int rtt_spgemm_csr_host(rtt_context ctx, const SMatrix *A, const SMatrix *B,
+                        int op, SMatrix *C);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RTT_SPGEMM_H_ */

@@ -1,0 +1,332 @@
+"""ctypes front end of the CPU oracle.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, the smoke check and bench.py's
+CPU-baseline leg as the checker.  The product (rtt-spgemm_b200/) never
+imports it.
+
+Two back ends share one numpy-level interface:
+
+* ``Oracle``     liboracle.so, the C restatement (oracle.c) - always built.
+* ``Reference``  oracle/_ref/libref_*.so, the reference's own CPU code
+                 compiled unmodified from its sources (built only where the
+                 reference checkout exists; the built files travel with the
+                 repository snapshot).
+
+Tile matrices are plain dicts of numpy arrays keyed by SMatrix field name.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+TD = 16
+
+
+class SMatrix(C.Structure):
+    """Same layout as SMatrix in include/rtt_spgemm.h (reference src/common.h:50-72)."""
+
+    _fields_ = [
+        ("m", C.c_int), ("n", C.c_int), ("nnz", C.c_int), ("isSymmetric", C.c_int),
+        ("value", C.POINTER(C.c_double)), ("columnindex", C.POINTER(C.c_int)),
+        ("rowpointer", C.POINTER(C.c_int)),
+        ("tilem", C.c_int), ("tilen", C.c_int),
+        ("tile_ptr", C.POINTER(C.c_int)), ("tile_columnidx", C.POINTER(C.c_int)),
+        ("tile_rowidx", C.POINTER(C.c_int)), ("tile_nnz", C.POINTER(C.c_int)),
+        ("numtile", C.c_int),
+        ("tile_csr_Value", C.POINTER(C.c_double)), ("tile_csr_Col", C.POINTER(C.c_ubyte)),
+        ("tile_csr_Ptr", C.POINTER(C.c_ubyte)), ("mask", C.POINTER(C.c_ushort)),
+        ("csc_tile_ptr", C.POINTER(C.c_int)), ("csc_tile_rowidx", C.POINTER(C.c_int)),
+    ]
+
+
+_CT = {np.int32: C.c_int, np.float64: C.c_double, np.uint8: C.c_ubyte, np.uint16: C.c_ushort}
+
+
+def _ptr(arr: np.ndarray, ctype):
+    return arr.ctypes.data_as(C.POINTER(ctype))
+
+
+def _copy(ptr, count: int, dtype) -> np.ndarray:
+    if count <= 0 or not ptr:
+        return np.zeros(max(count, 0), dtype=dtype)
+    return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dtype, copy=True)
+
+
+def csr_smatrix(csr):
+    """SMatrix over the CSR arrays of ``csr`` (kept alive by the returned tuple)."""
+    rp = np.ascontiguousarray(csr.rowptr, dtype=np.int32)
+    ci = np.ascontiguousarray(csr.col, dtype=np.int32)
+    v = np.ascontiguousarray(csr.val, dtype=np.float64)
+    s = SMatrix()
+    s.m, s.n, s.nnz = csr.m, csr.n, int(ci.shape[0])
+    s.rowpointer, s.columnindex, s.value = _ptr(rp, C.c_int), _ptr(ci, C.c_int), _ptr(v, C.c_double)
+    return s, (rp, ci, v)
+
+
+def tiles_from_smatrix(s: SMatrix, ptr_stride: int = TD, csc: bool = False) -> dict:
+    nt = s.numtile
+    d = {
+        "m": s.m, "n": s.n, "nnz": s.nnz, "tilem": s.tilem, "tilen": s.tilen, "numtile": nt,
+        "tile_ptr": _copy(s.tile_ptr, s.tilem + 1, np.int32),
+        "tile_columnidx": _copy(s.tile_columnidx, nt, np.int32),
+        "tile_nnz": _copy(s.tile_nnz, nt + 1, np.int32),
+        "tile_csr_Ptr": _copy(s.tile_csr_Ptr, nt * ptr_stride, np.uint8),
+        "tile_csr_Col": _copy(s.tile_csr_Col, s.nnz, np.uint8),
+        "tile_csr_Value": _copy(s.tile_csr_Value, s.nnz, np.float64),
+    }
+    if s.tile_rowidx:
+        d["tile_rowidx"] = _copy(s.tile_rowidx, nt, np.int32)
+    if s.mask:
+        d["mask"] = _copy(s.mask, nt * ptr_stride, np.uint16)
+    if csc:
+        d["csc_tile_ptr"] = _copy(s.csc_tile_ptr, s.tilen + 1, np.int32)
+        d["csc_tile_rowidx"] = _copy(s.csc_tile_rowidx, nt, np.int32)
+    return d
+
+
+def smatrix_from_tiles(t: dict):
+    """SMatrix pointing at the arrays of a tile dict (plus keep-alive list)."""
+    s = SMatrix()
+    keep = []
+    s.m, s.n, s.nnz = t["m"], t["n"], t["nnz"]
+    s.tilem, s.tilen, s.numtile = t["tilem"], t["tilen"], t["numtile"]
+    for name, ct in [("tile_ptr", C.c_int), ("tile_columnidx", C.c_int), ("tile_rowidx", C.c_int),
+                     ("tile_nnz", C.c_int), ("tile_csr_Value", C.c_double),
+                     ("tile_csr_Col", C.c_ubyte), ("tile_csr_Ptr", C.c_ubyte),
+                     ("mask", C.c_ushort), ("csc_tile_ptr", C.c_int), ("csc_tile_rowidx", C.c_int)]:
+        if name in t:
+            a = np.ascontiguousarray(t[name])
+            if a.size == 0:
+                a = np.zeros(1, dtype=a.dtype)
+            keep.append(a)
+            setattr(s, name, _ptr(a, ct))
+    return s, keep
+
+
+class _Base:
+    lib: C.CDLL
+
+    def _free_tiles(self, s: SMatrix):
+        for name in ("tile_ptr", "tile_columnidx", "tile_rowidx", "tile_nnz", "tile_csr_Value",
+                     "tile_csr_Col", "tile_csr_Ptr", "mask", "csc_tile_ptr", "csc_tile_rowidx"):
+            p = getattr(s, name)
+            if p:
+                self._free(C.cast(p, C.c_void_p))
+                setattr(s, name, None)
+
+    def _free_csr(self, s: SMatrix):
+        for name in ("rowpointer", "columnindex", "value"):
+            p = getattr(s, name)
+            if p:
+                self._free(C.cast(p, C.c_void_p))
+                setattr(s, name, None)
+
+
+def build(reference: bool = True) -> None:
+    """Compile liboracle.so (and the reference libraries where the reference
+    checkout exists)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
+    if reference and Path(os.environ.get("RTT_REFERENCE_DIR", "/root/reference"), "src").is_dir():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref",
+                        "REF=" + os.environ.get("RTT_REFERENCE_DIR", "/root/reference")], check=True)
+
+
+class Oracle(_Base):
+    """The C restatement (oracle.c)."""
+
+    def __init__(self, path: Path | None = None):
+        path = path or HERE / "liboracle.so"
+        if not path.exists():
+            build(reference=False)
+        self.lib = C.CDLL(str(path))
+        L = self.lib
+        L.orc_free.argtypes = [C.c_void_p]
+        self._free = L.orc_free
+        for f in ("orc_csr2tile_row_major", "orc_csr2tile_col_major"):
+            getattr(L, f).argtypes = [C.POINTER(SMatrix)]
+            getattr(L, f).restype = C.c_int
+        L.orc_spgemm_tile.argtypes = [C.POINTER(SMatrix)] * 3 + [C.c_int]
+        L.orc_spgemm_tile.restype = C.c_int
+        L.orc_tile2csr.argtypes = [C.POINTER(SMatrix), C.c_int, C.c_int]
+        L.orc_tile2csr.restype = C.c_int
+        L.orc_tile2csr_restore_rows.argtypes = [C.POINTER(SMatrix), C.POINTER(C.c_int), C.c_int,
+                                                C.c_int, C.c_int]
+        L.orc_tile2csr_restore_rows.restype = C.c_int
+        L.orc_tile16_to_tile8.argtypes = [C.POINTER(SMatrix), C.POINTER(SMatrix)]
+        L.orc_tile16_to_tile8.restype = C.c_int
+        L.orc_spgemm_csr.argtypes = [C.c_int, C.c_int, C.c_int,
+                                     C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_spgemm_csr.restype = C.c_longlong
+        L.orc_nnzcub.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_nnzcub.restype = C.c_longlong
+        L.orc_num_threads.restype = C.c_int
+
+    def threads(self) -> int:
+        return int(self.lib.orc_num_threads())
+
+    def csr2tile_row_major(self, csr) -> dict:
+        s, keep = csr_smatrix(csr)
+        st = self.lib.orc_csr2tile_row_major(C.byref(s))
+        if st:
+            raise ValueError(f"orc_csr2tile_row_major status {st}")
+        d = tiles_from_smatrix(s)
+        self._free_tiles(s)
+        return d
+
+    def csr2tile_col_major(self, csr) -> dict:
+        s, keep = csr_smatrix(csr)
+        st = self.lib.orc_csr2tile_col_major(C.byref(s))
+        if st:
+            raise ValueError(f"orc_csr2tile_col_major status {st}")
+        d = tiles_from_smatrix(s, csc=True)
+        self._free_tiles(s)
+        return d
+
+    def spgemm_tile(self, a: dict, b: dict, quirk: bool = False) -> dict:
+        sa, ka = smatrix_from_tiles(a)
+        sb, kb = smatrix_from_tiles(b)
+        sc = SMatrix()
+        st = self.lib.orc_spgemm_tile(C.byref(sa), C.byref(sb), C.byref(sc), int(quirk))
+        if st:
+            raise ValueError(f"orc_spgemm_tile status {st}")
+        d = tiles_from_smatrix(sc)
+        self._free_tiles(sc)
+        return d
+
+    def tile2csr(self, t: dict, tile_dim: int = TD, canonical: bool = True, new_to_old=None,
+                 perm_size: int | None = None):
+        from types import SimpleNamespace
+        s, keep = smatrix_from_tiles(t)
+        if new_to_old is None:
+            st = self.lib.orc_tile2csr(C.byref(s), tile_dim, int(canonical))
+        else:
+            p = np.ascontiguousarray(new_to_old, dtype=np.int32)
+            size = p.shape[0] if perm_size is None else perm_size
+            st = self.lib.orc_tile2csr_restore_rows(C.byref(s), _ptr(p, C.c_int), size, tile_dim,
+                                                    int(canonical))
+        if st:
+            return st
+        out = SimpleNamespace(m=s.m, n=s.n, rowptr=_copy(s.rowpointer, s.m + 1, np.int32),
+                              col=_copy(s.columnindex, s.nnz, np.int32),
+                              val=_copy(s.value, s.nnz, np.float64))
+        self._free_csr(s)
+        return out
+
+    def tile16_to_tile8(self, t: dict) -> dict:
+        s, keep = smatrix_from_tiles(t)
+        o = SMatrix()
+        st = self.lib.orc_tile16_to_tile8(C.byref(s), C.byref(o))
+        if st:
+            raise ValueError(f"orc_tile16_to_tile8 status {st}")
+        d = tiles_from_smatrix(o, ptr_stride=8)
+        self._free_tiles(o)
+        return d
+
+    def spgemm_csr(self, a, b, with_abs: bool = True):
+        """FP64 row SPA: returns (rowptr int64, col int32, val f64, abs f64|None)."""
+        rp = np.zeros(a.m + 1, dtype=np.int64)
+        args = (a.m, a.n, b.n, a.rowptr.ctypes.data, a.col.ctypes.data, a.val.ctypes.data,
+                b.rowptr.ctypes.data, b.col.ctypes.data, b.val.ctypes.data)
+        nnz = self.lib.orc_spgemm_csr(*args, rp.ctypes.data, None, None, None)
+        col = np.zeros(max(nnz, 1), dtype=np.int32)
+        val = np.zeros(max(nnz, 1), dtype=np.float64)
+        ab = np.zeros(max(nnz, 1), dtype=np.float64) if with_abs else None
+        self.lib.orc_spgemm_csr(*args, rp.ctypes.data, col.ctypes.data, val.ctypes.data,
+                                ab.ctypes.data if with_abs else None)
+        return rp, col[:nnz], val[:nnz], (ab[:nnz] if with_abs else None)
+
+    def nnzcub(self, a, b) -> int:
+        return int(self.lib.orc_nnzcub(a.m, a.rowptr.ctypes.data, a.col.ctypes.data,
+                                       b.rowptr.ctypes.data))
+
+
+def reference_available() -> bool:
+    return (HERE / "_ref" / "libref_tiles.so").exists() and (HERE / "_ref" / "libref_spa.so").exists()
+
+
+class Reference(_Base):
+    """The reference's own CPU functions (compiled from its sources)."""
+
+    def __init__(self):
+        self.lib = C.CDLL(str(HERE / "_ref" / "libref_tiles.so"))
+        self.spa = C.CDLL(str(HERE / "_ref" / "libref_spa.so"))
+        L = self.lib
+        L.ref_free.argtypes = [C.c_void_p]
+        self._free = L.ref_free
+        for f in ("ref_csr2tile_row_major", "ref_csr2tile_col_major"):
+            getattr(L, f).argtypes = [C.POINTER(SMatrix)]
+        L.ref_spgemm_cpu_fixed.argtypes = [C.POINTER(SMatrix)] * 3
+        L.ref_tile2csr.argtypes = [C.POINTER(SMatrix), C.c_int]
+        L.ref_tile2csr.restype = C.c_int
+        L.ref_tile2csr_restore_rows.argtypes = [C.POINTER(SMatrix), C.POINTER(C.c_int), C.c_int,
+                                                C.c_int]
+        L.ref_tile2csr_restore_rows.restype = C.c_int
+        L.ref_output_tile_rows.restype = C.c_int
+        self.spa.ref_spgemm_serialref.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                                  C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                                  C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                  C.c_int]
+
+    def csr2tile_row_major(self, csr) -> dict:
+        s, keep = csr_smatrix(csr)
+        self.lib.ref_csr2tile_row_major(C.byref(s))
+        d = tiles_from_smatrix(s)
+        self._free_tiles(s)
+        return d
+
+    def csr2tile_col_major(self, csr) -> dict:
+        s, keep = csr_smatrix(csr)
+        self.lib.ref_csr2tile_col_major(C.byref(s))
+        d = tiles_from_smatrix(s, csc=True)
+        self._free_tiles(s)
+        return d
+
+    def spgemm_cpu(self, a: dict, b: dict) -> dict:
+        """spgemm_cpu with the in-tile column fix applied at the call site."""
+        sa, ka = smatrix_from_tiles(a)
+        sb, kb = smatrix_from_tiles(b)
+        sc = SMatrix()
+        self.lib.ref_spgemm_cpu_fixed(C.byref(sa), C.byref(sb), C.byref(sc))
+        sc.m, sc.n, sc.tilem, sc.tilen = a["m"], b["n"], a["tilem"], b["tilen"]
+        d = tiles_from_smatrix(sc)
+        self._free_tiles(sc)
+        return d
+
+    def tile2csr(self, t: dict, canonical: bool = True, new_to_old=None, perm_size=None):
+        """The reference tile2csr (8x8 tiles)."""
+        from types import SimpleNamespace
+        s, keep = smatrix_from_tiles(t)
+        if new_to_old is None:
+            ok = self.lib.ref_tile2csr(C.byref(s), int(canonical))
+        else:
+            p = np.ascontiguousarray(new_to_old, dtype=np.int32)
+            size = p.shape[0] if perm_size is None else perm_size
+            ok = self.lib.ref_tile2csr_restore_rows(C.byref(s), _ptr(p, C.c_int), size,
+                                                    int(canonical))
+        if not ok:
+            return None
+        out = SimpleNamespace(m=s.m, n=s.n, rowptr=_copy(s.rowpointer, s.m + 1, np.int32),
+                              col=_copy(s.columnindex, s.nnz, np.int32),
+                              val=_copy(s.value, s.nnz, np.float64))
+        self._free_csr(s)
+        return out
+
+    def spgemm_serialref(self, a, b):
+        rp = np.zeros(a.m + 1, dtype=np.int32)
+        nnz = C.c_int(0)
+        args = [a.rowptr.ctypes.data, a.col.ctypes.data, a.val.ctypes.data, a.m, a.n, a.nnz,
+                b.rowptr.ctypes.data, b.col.ctypes.data, b.val.ctypes.data, b.m, b.n, b.nnz]
+        self.spa.ref_spgemm_serialref(*args, rp.ctypes.data, None, None, C.addressof(nnz), 1)
+        col = np.zeros(max(nnz.value, 1), dtype=np.int32)
+        val = np.zeros(max(nnz.value, 1), dtype=np.float64)
+        self.spa.ref_spgemm_serialref(*args, rp.ctypes.data, col.ctypes.data, val.ctypes.data,
+                                      C.addressof(nnz), 0)
+        return rp, col[:nnz.value], val[:nnz.value]

@@ -1,0 +1,969 @@
+// api.cu - the extern "C" entry points declared in include/rtt_spgemm.h.
+//
+// Host-buffer drop-ins (csr2tile_row_major, csr2tile_col_major, spgemm_cpu,
+// tile2csr, tile2csr_restore_rows replacements) upload the SMatrix arrays,
+// run the sm_100a kernels and copy results into malloc'd host arrays.  They
+// share one lazily created context per device, serialised by a mutex (the
+// reference functions are not re-entrant either).  Outputs are committed to
+// the caller's SMatrix only after every copy succeeded.
+#include "rtt_internal.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <climits>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+struct rtt_context_s
+{
+    rtt::Workspace ws;
+    rtt_config cfg;
+    rtt::TileBufs A, B;
+    rtt::DevBuf bt_rowptr, bt_col, bt_val; // B = A^T for RTT_OP_AAT
+    rtt::DevBuf in_rp, in_col, in_val;     // host-buffer uploads
+    rtt::DevBuf in2_rp, in2_col, in2_val;
+    rtt::DevBuf out_rp, out_col, out_val;  // host-buffer product output
+    rtt::DevBuf counters;
+    rtt::SymbolicOut S;
+    rtt_stats stats;
+    bool have_symbolic = false;
+    bool b_alias = false;
+    bool owns_stream = false;
+};
+
+namespace
+{
+using namespace rtt;
+
+std::mutex g_mutex;
+int g_device = 0;
+rtt_context g_ctx[16] = {};
+
+int default_context(rtt_context *out)
+{
+    if (g_device < 0 || g_device >= 16)
+        return fail(RTT_ERR_INVALID_ARGUMENT, "device index out of range");
+    if (g_ctx[g_device] == nullptr)
+    {
+        rtt_context c = nullptr;
+        int st = rtt_context_create(&c, g_device);
+        if (st != RTT_OK)
+            return st;
+        g_ctx[g_device] = c;
+    }
+    RTT_CUDA(cudaSetDevice(g_device));
+    *out = g_ctx[g_device];
+    return RTT_OK;
+}
+
+template <typename T>
+int upload(DevBuf &b, const T *h, size_t n, cudaStream_t s)
+{
+    RTT_CHECK(b.ensure(sizeof(T) * n + 16, s));
+    if (n > 0)
+    {
+        if (h == nullptr)
+            return fail(RTT_ERR_INVALID_ARGUMENT, "NULL host array with nonzero length");
+        RTT_CUDA(cudaMemcpyAsync(b.p, h, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+    }
+    return RTT_OK;
+}
+
+template <typename T>
+int download(T **out, const void *d, size_t n, cudaStream_t s)
+{
+    T *h = static_cast<T *>(std::malloc(sizeof(T) * (n > 0 ? n : 1)));
+    if (h == nullptr)
+        return fail(RTT_ERR_OUT_OF_MEMORY, "host malloc failed");
+    if (n > 0)
+    {
+        cudaError_t e = cudaMemcpyAsync(h, d, sizeof(T) * n, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess)
+        {
+            std::free(h);
+            return cuda_fail(e, "device to host copy");
+        }
+    }
+    *out = h;
+    return RTT_OK;
+}
+
+// Free a set of host arrays on failure paths.
+struct HostArrays
+{
+    std::vector<void *> ptrs;
+    bool committed = false;
+    template <typename T>
+    T **slot()
+    {
+        ptrs.push_back(nullptr);
+        return reinterpret_cast<T **>(&ptrs.back());
+    }
+    ~HostArrays()
+    {
+        if (!committed)
+            for (void *p : ptrs)
+                std::free(p);
+    }
+};
+
+int map_device_error(int st)
+{
+    if (st == RTT_ERR_DEVICE_CHECK)
+    {
+        const std::string &m = last_error_ref();
+        if (m.find("code 101") != std::string::npos || m.find("code 102") != std::string::npos)
+            return fail(RTT_ERR_INVALID_CSR, "invalid CSR input: " + m);
+        if (m.find("code 109") != std::string::npos)
+            return fail(RTT_ERR_TAIL_NONEMPTY, "row past the permutation prefix is not empty");
+    }
+    return st;
+}
+
+__global__ void k_masks_from_entries(int numtile, const int *__restrict__ tnnz,
+                                     const uint8_t *__restrict__ ptr,
+                                     const uint8_t *__restrict__ col, uint16_t *__restrict__ mask)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= numtile * TD)
+        return;
+    const int t = x >> 4, r = x & 15;
+    const int b = tnnz[t], cnt = tnnz[t + 1] - b;
+    int s = ptr[(size_t)t * TD + r];
+    int e = r == TD - 1 ? cnt : ptr[(size_t)t * TD + r + 1];
+    s = min(s, cnt);
+    e = min(max(e, s), cnt);
+    uint32_t m = 0;
+    for (int i = s; i < e; ++i)
+        m |= 0x8000u >> (col[b + i] & 15);
+    mask[x] = (uint16_t)m;
+}
+
+__global__ void k_expand_ptr(int nbins, const int *__restrict__ ptr, int *__restrict__ owner)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nbins)
+        return;
+    for (int p = ptr[b]; p < ptr[b + 1]; ++p)
+        owner[p] = b;
+}
+
+__global__ void k_iota_i(int *a, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        a[i] = i;
+}
+
+__global__ void k_gather_i(const int *__restrict__ src, const int *__restrict__ idx, int n,
+                           int *__restrict__ dst)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        dst[i] = src[idx[i]];
+}
+
+__global__ void k_lower_bound(const int *__restrict__ keys, int nkeys, int nbins, int *__restrict__ ptr)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > nbins)
+        return;
+    ptr[b] = lower_bound(keys, 0, nkeys, b);
+}
+
+// Structure checks of caller-provided tiles, run before any kernel indexes
+// through them: list pointers monotone and ending at the entry count, list
+// indices in range and strictly increasing inside a list, per-tile entry
+// offsets monotone and in range, per-tile row offsets non-decreasing.
+constexpr int DERR_TILES = 110;
+
+__global__ void k_validate_lists(int nlists, const int *__restrict__ ptr, const int *__restrict__ idx,
+                                 int nidx, int max_idx, int *err)
+{
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l == 0 && (ptr[0] != 0 || ptr[nlists] != nidx))
+        set_error(err, DERR_TILES);
+    if (l >= nlists)
+        return;
+    const int b = ptr[l], e = ptr[l + 1];
+    if (b < 0 || e < b || e > nidx)
+    {
+        set_error(err, DERR_TILES);
+        return;
+    }
+    int prev = -1;
+    for (int i = b; i < e; ++i)
+    {
+        const int v = idx[i];
+        if (v < 0 || v >= max_idx || v <= prev)
+        {
+            set_error(err, DERR_TILES);
+            return;
+        }
+        prev = v;
+    }
+}
+
+__global__ void k_validate_tile_data(int nt, const int *__restrict__ tnnz, int nent, int ptr_stride,
+                                     const uint8_t *__restrict__ ptr, int *err)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt)
+        return;
+    const int b = tnnz[t], e = tnnz[t + 1];
+    if (b < 0 || e < b || e > nent)
+    {
+        set_error(err, DERR_TILES);
+        return;
+    }
+    int prev = 0;
+    for (int r = 0; r < ptr_stride; ++r)
+    {
+        const int p = ptr[(size_t)t * ptr_stride + r];
+        if (p < prev || p > e - b)
+        {
+            set_error(err, DERR_TILES);
+            return;
+        }
+        prev = p;
+    }
+}
+
+__global__ void k_validate_ptr(int n, const int *__restrict__ ptr, int maxv, int *err)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n)
+        return;
+    const int v = ptr[i];
+    if (v < 0 || v > maxv || (i < n && ptr[i + 1] < v))
+        set_error(err, DERR_TILES);
+}
+
+inline int grid_for(long long threads, int block) { return (int)((threads + block - 1) / block); }
+
+int check_tiles(Workspace &ws, const char *what)
+{
+    int st = check_device_error(ws, what);
+    if (st == RTT_ERR_DEVICE_CHECK && last_error_ref().find("code 110") != std::string::npos)
+        return fail(RTT_ERR_INVALID_ARGUMENT, std::string(what) + ": malformed tile structure");
+    return st;
+}
+
+int bits_for(int maxval)
+{
+    int b = 1;
+    while (b < 31 && (1 << b) <= maxval)
+        ++b;
+    return b;
+}
+
+bool csr_args_ok(const SMatrix *M)
+{
+    return M != nullptr && M->m >= 0 && M->n >= 0 && M->nnz >= 0 &&
+           (M->m == 0 || M->rowpointer != nullptr) &&
+           (M->nnz == 0 || (M->columnindex != nullptr && M->value != nullptr));
+}
+
+// Upload a host CSR and tile it (row-major) into T.
+int tile_host_csr(rtt_context c, const SMatrix *M, TileBufs &T, bool packed, bool sorted_rows)
+{
+    cudaStream_t s = c->ws.stream;
+    RTT_CHECK(upload(c->in_rp, M->rowpointer, (size_t)M->m + (M->m > 0 ? 1 : 0), s));
+    RTT_CHECK(upload(c->in_col, M->columnindex, (size_t)M->nnz, s));
+    RTT_CHECK(upload(c->in_val, M->value, (size_t)M->nnz, s));
+    int st = csr2tile_device(c->ws, M->m, M->n, M->nnz, c->in_rp.as<int>(), c->in_col.as<int>(),
+                             c->in_val.as<double>(), T, packed, sorted_rows);
+    st = map_device_error(st);
+    if (st != RTT_OK)
+        return st;
+    return map_device_error(check_device_error(c->ws, "csr2tile"));
+}
+
+// Upload legacy tiles (row-major A or column-major B) and build the views the
+// kernels need.  For column-major input the per-tile arrays are in tile-CSC
+// order: the CSC index is taken as given and a row index is derived from it.
+int upload_tiles(rtt_context c, const SMatrix *M, bool col_major, TileBufs &T)
+{
+    cudaStream_t s = c->ws.stream;
+    const int tilem = ceil_div(M->m, TD), tilen = ceil_div(M->n, TD);
+    if (M->numtile < 0 || M->nnz < 0 || M->tile_nnz == nullptr)
+        return fail(RTT_ERR_INVALID_ARGUMENT, "tile matrix without tile_nnz");
+    const int nt = M->numtile;
+    const int nnz = M->tile_nnz[nt];
+    if (nnz < 0 || nnz > M->nnz)
+        return fail(RTT_ERR_INVALID_ARGUMENT, "tile_nnz[numtile] exceeds nnz");
+    if (nt > 0 && (M->tile_csr_Ptr == nullptr))
+        return fail(RTT_ERR_INVALID_ARGUMENT, "tile matrix without tile_csr_Ptr");
+    if (nnz > 0 && (M->tile_csr_Col == nullptr || M->tile_csr_Value == nullptr))
+        return fail(RTT_ERR_INVALID_ARGUMENT, "tile matrix without entries");
+    T.m = M->m;
+    T.n = M->n;
+    T.tilem = tilem;
+    T.tilen = tilen;
+    T.numtile = nt;
+    T.nnz = nnz;
+    RTT_CHECK(upload(T.tile_nnz, M->tile_nnz, (size_t)nt + 1, s));
+    RTT_CHECK(upload(T.ptr, M->tile_csr_Ptr, (size_t)nt * TD, s));
+    RTT_CHECK(upload(T.col, M->tile_csr_Col, (size_t)nnz, s));
+    RTT_CHECK(upload(T.val, M->tile_csr_Value, (size_t)nnz, s));
+    RTT_CHECK(T.mask.ensure(sizeof(uint16_t) * (size_t)nt * TD + 16, s));
+    if (nt > 0)
+    {
+        k_validate_tile_data<<<grid_for(nt, 256), 256, 0, s>>>(nt, T.tile_nnz.as<int>(), nnz, TD,
+                                                               T.ptr.as<uint8_t>(), c->ws.err.as<int>());
+        c->ws.launches++;
+        RTT_CHECK(check_tiles(c->ws, "tile data"));
+        k_masks_from_entries<<<grid_for((long long)nt * TD, 256), 256, 0, s>>>(
+            nt, T.tile_nnz.as<int>(), T.ptr.as<uint8_t>(), T.col.as<uint8_t>(),
+            T.mask.as<uint16_t>());
+        c->ws.launches++;
+    }
+    if (!col_major)
+    {
+        if (M->tile_ptr == nullptr || (nt > 0 && M->tile_columnidx == nullptr))
+            return fail(RTT_ERR_INVALID_ARGUMENT, "row-major tiles without tile_ptr/tile_columnidx");
+        RTT_CHECK(upload(T.tile_ptr, M->tile_ptr, (size_t)tilem + 1, s));
+        RTT_CHECK(upload(T.tile_col, M->tile_columnidx, (size_t)nt, s));
+        T.row_data.release();
+        k_validate_lists<<<grid_for(tilem + 1, 256), 256, 0, s>>>(
+            tilem, T.tile_ptr.as<int>(), T.tile_col.as<int>(), nt, tilen, c->ws.err.as<int>());
+        c->ws.launches++;
+        return check_tiles(c->ws, "row-major tile lists");
+    }
+    if (M->csc_tile_ptr == nullptr || (nt > 0 && M->csc_tile_rowidx == nullptr))
+        return fail(RTT_ERR_INVALID_ARGUMENT, "column-major tiles without csc_tile_ptr/csc_tile_rowidx");
+    RTT_CHECK(upload(T.csc_ptr, M->csc_tile_ptr, (size_t)tilen + 1, s));
+    RTT_CHECK(upload(T.csc_row, M->csc_tile_rowidx, (size_t)nt, s));
+    T.csc_data.release();
+    k_validate_lists<<<grid_for(tilen + 1, 256), 256, 0, s>>>(
+        tilen, T.csc_ptr.as<int>(), T.csc_row.as<int>(), nt, tilem, c->ws.err.as<int>());
+    c->ws.launches++;
+    RTT_CHECK(check_tiles(c->ws, "column-major tile lists"));
+    // row view: stable sort of CSC positions by tile row
+    RTT_CHECK(T.tile_ptr.ensure(sizeof(int) * ((size_t)tilem + 1), s));
+    RTT_CHECK(T.tile_col.ensure(sizeof(int) * (size_t)nt + 16, s));
+    RTT_CHECK(T.row_data.ensure(sizeof(int) * (size_t)nt + 16, s));
+    RTT_CHECK(T.tmp0.ensure(sizeof(int) * (size_t)nt + 16, s));
+    RTT_CHECK(T.tmp1.ensure(sizeof(int) * (size_t)nt + 16, s));
+    RTT_CHECK(T.tmp2.ensure(sizeof(int) * (size_t)nt + 16, s));
+    int *owner = T.tmp0.as<int>(), *iota = T.tmp1.as<int>(), *keys = T.tmp2.as<int>();
+    if (nt > 0)
+    {
+        k_expand_ptr<<<grid_for(tilen, 256), 256, 0, s>>>(tilen, T.csc_ptr.as<int>(), owner);
+        k_iota_i<<<grid_for(nt, 256), 256, 0, s>>>(iota, nt);
+        size_t bytes = 0;
+        const int eb = bits_for(tilem);
+        RTT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, T.csc_row.as<int>(), keys, iota,
+                                                 T.row_data.as<int>(), nt, 0, eb, s));
+        RTT_CHECK(c->ws.scan_tmp.ensure(bytes, s));
+        RTT_CUDA(cub::DeviceRadixSort::SortPairs(c->ws.scan_tmp.p, bytes, T.csc_row.as<int>(), keys,
+                                                 iota, T.row_data.as<int>(), nt, 0, eb, s));
+        k_gather_i<<<grid_for(nt, 256), 256, 0, s>>>(owner, T.row_data.as<int>(), nt,
+                                                     T.tile_col.as<int>());
+        c->ws.launches += 6;
+    }
+    k_lower_bound<<<grid_for(tilem + 1, 256), 256, 0, s>>>(keys, nt, tilem, T.tile_ptr.as<int>());
+    c->ws.launches++;
+    return RTT_OK;
+}
+
+DevTiles view_with_rowdata(const TileBufs &T)
+{
+    DevTiles v = T.view();
+    v.row_data = T.row_data.p ? T.row_data.as<int>() : nullptr;
+    v.csc_data = T.csc_data.p ? T.csc_data.as<int>() : nullptr;
+    return v;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *rtt_status_string(int status)
+{
+    switch (status)
+    {
+    case RTT_OK:
+        return "ok";
+    case RTT_ERR_INVALID_ARGUMENT:
+        return "invalid argument";
+    case RTT_ERR_INVALID_CSR:
+        return "invalid CSR";
+    case RTT_ERR_SHAPE_MISMATCH:
+        return "shape mismatch";
+    case RTT_ERR_OUT_OF_MEMORY:
+        return "out of memory";
+    case RTT_ERR_CUDA:
+        return "CUDA error";
+    case RTT_ERR_UNREPRESENTABLE:
+        return "output not representable in int32";
+    case RTT_ERR_NO_DEVICE:
+        return "no usable CUDA device";
+    case RTT_ERR_DEVICE_CHECK:
+        return "device-side check failed";
+    case RTT_ERR_INVALID_PERMUTATION:
+        return "invalid permutation";
+    case RTT_ERR_TAIL_NONEMPTY:
+        return "row past the permutation prefix is not empty";
+    case RTT_ERR_STATE:
+        return "invalid call order";
+    default:
+        return "unknown status";
+    }
+}
+
+const char *rtt_last_error(void) { return rtt::last_error_ref().c_str(); }
+
+const char *rtt_version(void) { return "rtt-spgemm-b200 0.1 (sm_100a)"; }
+
+void rtt_config_default(rtt_config *config)
+{
+    if (config == nullptr)
+        return;
+    std::memset(config, 0, sizeof(*config));
+    config->dmma_pair_cutoff = 3072;
+    config->fused_csr_output = 1;
+    config->keep_tiles = 0;
+}
+
+int rtt_set_device(int device)
+{
+    std::lock_guard<std::mutex> lock(g_mutex);
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    {
+        cudaGetLastError();
+        return rtt::fail(RTT_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= count || device >= 16)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "device index out of range");
+    g_device = device;
+    return RTT_OK;
+}
+
+int rtt_context_create(rtt_context *ctx, int device)
+{
+    if (ctx == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    rtt_context c = new (std::nothrow) rtt_context_s();
+    if (c == nullptr)
+        return rtt::fail(RTT_ERR_OUT_OF_MEMORY, "context allocation failed");
+    int st = c->ws.init(device);
+    if (st != RTT_OK)
+    {
+        c->ws.destroy();
+        delete c;
+        return st;
+    }
+    rtt_config_default(&c->cfg);
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    *ctx = c;
+    return RTT_OK;
+}
+
+void rtt_context_destroy(rtt_context c)
+{
+    if (c == nullptr)
+        return;
+    cudaSetDevice(c->ws.device);
+    cudaStreamSynchronize(c->ws.stream);
+    c->A.release();
+    c->B.release();
+    c->S.release();
+    rtt::DevBuf *bufs[] = {&c->bt_rowptr, &c->bt_col, &c->bt_val, &c->in_rp, &c->in_col,
+                           &c->in_val, &c->in2_rp, &c->in2_col, &c->in2_val, &c->out_rp,
+                           &c->out_col, &c->out_val, &c->counters};
+    for (rtt::DevBuf *b : bufs)
+        b->release();
+    c->ws.destroy();
+    delete c;
+}
+
+int rtt_context_set_stream(rtt_context c, void *stream)
+{
+    if (c == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    c->ws.stream = static_cast<cudaStream_t>(stream);
+    return RTT_OK;
+}
+
+int rtt_context_set_config(rtt_context c, const rtt_config *config)
+{
+    if (c == nullptr || config == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (config->dmma_pair_cutoff < 0)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "dmma_pair_cutoff must be >= 0");
+    for (int r : config->reserved)
+        if (r != 0)
+            return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "reserved config fields must be zero");
+    c->cfg = *config;
+    return RTT_OK;
+}
+
+int rtt_context_get_stats(rtt_context c, rtt_stats *stats)
+{
+    if (c == nullptr || stats == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "NULL argument");
+    *stats = c->stats;
+    return RTT_OK;
+}
+
+// ---------------------------------------------------------------- drop-ins
+int rtt_csr2tile_row_major(SMatrix *M)
+{
+    if (!csr_args_ok(M))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "csr2tile_row_major: bad CSR arguments");
+    std::lock_guard<std::mutex> lock(g_mutex);
+    rtt_context c = nullptr;
+    RTT_CHECK(default_context(&c));
+    TileBufs &T = c->A;
+    RTT_CHECK(tile_host_csr(c, M, T, true, false));
+    cudaStream_t s = c->ws.stream;
+    const size_t nt = (size_t)T.numtile;
+    HostArrays h;
+    int **tp = h.slot<int>(), **tc = h.slot<int>(), **tr = h.slot<int>(), **tn = h.slot<int>();
+    unsigned char **P = h.slot<unsigned char>(), **Cb = h.slot<unsigned char>();
+    double **V = h.slot<double>();
+    unsigned short **Mk = h.slot<unsigned short>();
+    RTT_CHECK(download(tp, T.tile_ptr.p, (size_t)T.tilem + 1, s));
+    RTT_CHECK(download(tc, T.tile_col.p, nt, s));
+    RTT_CHECK(download(tr, T.tile_row.p, nt, s));
+    RTT_CHECK(download(tn, T.tile_nnz.p, nt + 1, s));
+    RTT_CHECK(download(P, T.ptr.p, nt * TD, s));
+    RTT_CHECK(download(Cb, T.col.p, (size_t)M->nnz, s));
+    RTT_CHECK(download(V, T.val.p, (size_t)M->nnz, s));
+    RTT_CHECK(download(Mk, T.mask.p, nt * TD, s));
+    M->tilem = T.tilem;
+    M->tilen = T.tilen;
+    M->numtile = T.numtile;
+    M->tile_ptr = *tp;
+    M->tile_columnidx = *tc;
+    M->tile_rowidx = *tr;
+    M->tile_nnz = *tn;
+    M->tile_csr_Ptr = *P;
+    M->tile_csr_Col = *Cb;
+    M->tile_csr_Value = *V;
+    M->mask = *Mk;
+    h.committed = true;
+    return RTT_OK;
+}
+
+int rtt_csr2tile_col_major(SMatrix *M)
+{
+    if (!csr_args_ok(M))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "csr2tile_col_major: bad CSR arguments");
+    std::lock_guard<std::mutex> lock(g_mutex);
+    rtt_context c = nullptr;
+    RTT_CHECK(default_context(&c));
+    TileBufs &T = c->A;
+    TileBufs &U = c->B;
+    RTT_CHECK(tile_host_csr(c, M, T, false, true));
+    RTT_CHECK(build_tile_csc(c->ws, T));
+    RTT_CHECK(tiles_to_col_major(c->ws, T, U));
+    RTT_CHECK(check_device_error(c->ws, "csr2tile_col_major"));
+    cudaStream_t s = c->ws.stream;
+    const size_t nt = (size_t)T.numtile;
+    HostArrays h;
+    int **tp = h.slot<int>(), **tc = h.slot<int>(), **tn = h.slot<int>();
+    int **cp = h.slot<int>(), **cr = h.slot<int>();
+    unsigned char **P = h.slot<unsigned char>(), **Cb = h.slot<unsigned char>();
+    double **V = h.slot<double>();
+    unsigned short **Mk = h.slot<unsigned short>();
+    int **tr = h.slot<int>();
+    RTT_CHECK(download(tp, T.tile_ptr.p, (size_t)T.tilem + 1, s));
+    RTT_CHECK(download(tc, T.tile_col.p, nt, s));
+    RTT_CHECK(download(tn, U.tile_nnz.p, nt + 1, s));
+    RTT_CHECK(download(cp, T.csc_ptr.p, (size_t)T.tilen + 1, s));
+    RTT_CHECK(download(cr, T.csc_row.p, nt, s));
+    RTT_CHECK(download(P, U.ptr.p, nt * TD, s));
+    RTT_CHECK(download(Cb, U.col.p, (size_t)M->nnz, s));
+    RTT_CHECK(download(V, U.val.p, (size_t)M->nnz, s));
+    RTT_CHECK(download(Mk, U.mask.p, nt * TD, s));
+    *tr = static_cast<int *>(std::calloc(nt > 0 ? nt : 1, sizeof(int)));
+    if (*tr == nullptr)
+        return rtt::fail(RTT_ERR_OUT_OF_MEMORY, "host calloc failed");
+    M->tilem = T.tilem;
+    M->tilen = T.tilen;
+    M->numtile = T.numtile;
+    M->tile_ptr = *tp;
+    M->tile_columnidx = *tc;
+    M->tile_rowidx = *tr;
+    M->tile_nnz = *tn;
+    M->csc_tile_ptr = *cp;
+    M->csc_tile_rowidx = *cr;
+    M->tile_csr_Ptr = *P;
+    M->tile_csr_Col = *Cb;
+    M->tile_csr_Value = *V;
+    M->mask = *Mk;
+    h.committed = true;
+    return RTT_OK;
+}
+
+int rtt_spgemm_tile(SMatrix *A, SMatrix *B, SMatrix *C)
+{
+    if (A == nullptr || B == nullptr || C == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "spgemm_tile: NULL matrix");
+    if (A->m < 0 || A->n < 0 || B->m < 0 || B->n < 0)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "spgemm_tile: negative shape");
+    if (A->n != B->m)
+        return rtt::fail(RTT_ERR_SHAPE_MISMATCH, "spgemm_tile: A->n != B->m");
+    std::lock_guard<std::mutex> lock(g_mutex);
+    rtt_context c = nullptr;
+    RTT_CHECK(default_context(&c));
+    RTT_CHECK(upload_tiles(c, A, false, c->A));
+    RTT_CHECK(upload_tiles(c, B, true, c->B));
+    const DevTiles dA = view_with_rowdata(c->A);
+    DevTiles dB = view_with_rowdata(c->B);
+    RTT_CHECK(map_device_error(symbolic_device(c->ws, dA, dB, c->S)));
+    NumericConfig nc;
+    nc.dmma_pair_cutoff = c->cfg.dmma_pair_cutoff;
+    nc.write_tiles = true;
+    RTT_CHECK(numeric_device(c->ws, dA, dB, c->S, nc));
+    RTT_CHECK(check_device_error(c->ws, "spgemm_tile numeric"));
+    cudaStream_t s = c->ws.stream;
+    SymbolicOut &S = c->S;
+    const size_t nt = (size_t)S.numtile, nnz = (size_t)S.nnz;
+    HostArrays h;
+    int **tp = h.slot<int>(), **tc = h.slot<int>(), **tr = h.slot<int>(), **tn = h.slot<int>();
+    unsigned char **P = h.slot<unsigned char>(), **Cb = h.slot<unsigned char>();
+    double **V = h.slot<double>();
+    unsigned short **Mk = h.slot<unsigned short>();
+    RTT_CHECK(download(tp, S.c_tile_ptr.p, (size_t)S.tilem + 1, s));
+    RTT_CHECK(download(tc, S.c_tile_col.p, nt, s));
+    RTT_CHECK(download(tr, S.c_tile_row.p, nt, s));
+    RTT_CHECK(download(tn, S.c_tile_nnz.p, nt + 1, s));
+    RTT_CHECK(download(P, S.c_ptr.p, nt * TD, s));
+    RTT_CHECK(download(Cb, S.c_col.p, nnz, s));
+    RTT_CHECK(download(V, S.c_val.p, nnz, s));
+    RTT_CHECK(download(Mk, S.c_mask.p, nt * TD, s));
+    C->m = A->m;
+    C->n = B->n;
+    C->tilem = S.tilem;
+    C->tilen = S.tilen;
+    C->numtile = S.numtile;
+    C->nnz = (int)S.nnz;
+    C->tile_ptr = *tp;
+    C->tile_columnidx = *tc;
+    C->tile_rowidx = *tr;
+    C->tile_nnz = *tn;
+    C->tile_csr_Ptr = *P;
+    C->tile_csr_Col = *Cb;
+    C->tile_csr_Value = *V;
+    C->mask = *Mk;
+    h.committed = true;
+    return RTT_OK;
+}
+
+int rtt_tile2csr_restore_rows(SMatrix *M, const int *new_to_old, int perm_size, int tile_dim,
+                              int canonical)
+{
+    if (M == nullptr || M->m < 0 || M->n < 0 || M->tilem < 0 || M->numtile < 0 ||
+        M->tile_ptr == nullptr || M->tile_nnz == nullptr ||
+        (M->numtile > 0 && (M->tile_columnidx == nullptr || M->tile_csr_Ptr == nullptr)) ||
+        (M->nnz > 0 && (M->tile_csr_Col == nullptr || M->tile_csr_Value == nullptr)))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "tile2csr: malformed tile matrix");
+    if (tile_dim != 8 && tile_dim != 16)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "tile2csr: tile_dim must be 8 or 16");
+    const bool identity = new_to_old == nullptr && perm_size < 0;
+    if (!identity)
+    {
+        if (perm_size < 0 || perm_size > M->m || (perm_size > 0 && new_to_old == nullptr))
+            return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "tile2csr_restore_rows: bad permutation size");
+        std::vector<unsigned char> seen((size_t)M->m, 0);
+        for (int i = 0; i < perm_size; ++i)
+        {
+            const int o = new_to_old[i];
+            if (o < 0 || o >= M->m || seen[(size_t)o])
+                return rtt::fail(RTT_ERR_INVALID_PERMUTATION,
+                                 "tile2csr_restore_rows: permutation is not one-to-one");
+            seen[(size_t)o] = 1;
+        }
+    }
+    std::lock_guard<std::mutex> lock(g_mutex);
+    rtt_context c = nullptr;
+    RTT_CHECK(default_context(&c));
+    cudaStream_t s = c->ws.stream;
+    TileBufs &T = c->A;
+    const int nt = M->numtile, tilem = M->tilem, m = M->m;
+    const int tnz = nt >= 0 ? M->tile_nnz[nt] : 0;
+    RTT_CHECK(upload(T.tile_ptr, M->tile_ptr, (size_t)tilem + 1, s));
+    RTT_CHECK(upload(T.tile_col, M->tile_columnidx, (size_t)nt, s));
+    RTT_CHECK(upload(T.tile_nnz, M->tile_nnz, (size_t)nt + 1, s));
+    RTT_CHECK(upload(T.ptr, M->tile_csr_Ptr, (size_t)nt * tile_dim, s));
+    const size_t nent = (size_t)std::max(tnz, M->nnz);
+    RTT_CHECK(upload(T.col, M->tile_csr_Col, nent, s));
+    RTT_CHECK(upload(T.val, M->tile_csr_Value, nent, s));
+    {
+        // tile lists: monotone pointers, in-range entry offsets (columns are
+        // range-checked per entry by the kernels, as the reference does)
+        k_validate_tile_data<<<grid_for(nt > 0 ? nt : 1, 256), 256, 0, s>>>(
+            nt, T.tile_nnz.as<int>(), (int)nent, tile_dim, T.ptr.as<uint8_t>(), c->ws.err.as<int>());
+        k_validate_ptr<<<grid_for(tilem + 1, 256), 256, 0, s>>>(tilem, T.tile_ptr.as<int>(), nt,
+                                                                c->ws.err.as<int>());
+        c->ws.launches += 2;
+        RTT_CHECK(check_tiles(c->ws, "tile2csr input"));
+    }
+    RTT_CHECK(upload(c->in2_rp, new_to_old, identity ? 0 : (size_t)perm_size, s));
+    const int *perm = identity ? nullptr : c->in2_rp.as<int>();
+    const int psize = identity ? -1 : perm_size;
+    RTT_CHECK(c->out_rp.ensure(sizeof(int) * ((size_t)m + 2), s));
+    RTT_CHECK(c->in_col.ensure(sizeof(int) * ((size_t)m + 2), s));
+    int *row_cnt = c->in_col.as<int>();
+    RTT_CHECK(tile2csr_count_device(c->ws, T.tile_ptr.as<int>(), T.tile_col.as<int>(),
+                                    T.tile_nnz.as<int>(), T.ptr.as<uint8_t>(), T.col.as<uint8_t>(),
+                                    m, M->n, tilem, tile_dim, perm, psize, row_cnt));
+    RTT_CHECK(map_device_error(check_device_error(c->ws, "tile2csr count")));
+    // int64 total first (overflow check), then the int32 row pointer
+    RTT_CHECK(c->in_val.ensure(sizeof(long long) * ((size_t)m + 2), s));
+    RTT_CHECK(scan_exclusive_i64(c->ws, row_cnt, c->in_val.as<long long>(), m));
+    long long total = 0;
+    RTT_CHECK(read_i64(c->ws, c->in_val.as<long long>() + m, &total));
+    if (total > (long long)INT_MAX)
+        return rtt::fail(RTT_ERR_UNREPRESENTABLE, "tile2csr: nnz exceeds int32");
+    RTT_CHECK(scan_exclusive_int(c->ws, row_cnt, c->out_rp.as<int>(), m));
+    RTT_CHECK(c->out_col.ensure(sizeof(int) * (size_t)total + 16, s));
+    RTT_CHECK(c->out_val.ensure(sizeof(double) * (size_t)total + 16, s));
+    RTT_CHECK(tile2csr_fill_device(c->ws, T.tile_ptr.as<int>(), T.tile_col.as<int>(),
+                                   T.tile_nnz.as<int>(), T.ptr.as<uint8_t>(), T.col.as<uint8_t>(),
+                                   T.val.as<double>(), m, M->n, tilem, tile_dim, perm, psize,
+                                   c->out_rp.as<int>(), c->out_col.as<int>(),
+                                   c->out_val.as<double>(), canonical == 0));
+    RTT_CHECK(map_device_error(check_device_error(c->ws, "tile2csr fill")));
+    HostArrays h;
+    int **rp = h.slot<int>(), **ci = h.slot<int>();
+    double **v = h.slot<double>();
+    RTT_CHECK(download(rp, c->out_rp.p, (size_t)m + 1, s));
+    RTT_CHECK(download(ci, c->out_col.p, (size_t)total, s));
+    RTT_CHECK(download(v, c->out_val.p, (size_t)total, s));
+    M->rowpointer = *rp;
+    M->columnindex = *ci;
+    M->value = *v;
+    M->nnz = (int)total;
+    h.committed = true;
+    return RTT_OK;
+}
+
+int rtt_tile2csr(SMatrix *M, int tile_dim, int canonical)
+{
+    return rtt_tile2csr_restore_rows(M, nullptr, -1, tile_dim, canonical);
+}
+
+void rtt_matrix_destroy(SMatrix *M, int owned_csr)
+{
+    if (M == nullptr)
+        return;
+    std::free(M->tile_ptr);
+    std::free(M->tile_columnidx);
+    std::free(M->tile_rowidx);
+    std::free(M->tile_nnz);
+    std::free(M->tile_csr_Value);
+    std::free(M->tile_csr_Col);
+    std::free(M->tile_csr_Ptr);
+    std::free(M->mask);
+    std::free(M->csc_tile_ptr);
+    std::free(M->csc_tile_rowidx);
+    M->tile_ptr = M->tile_columnidx = M->tile_rowidx = M->tile_nnz = nullptr;
+    M->csc_tile_ptr = M->csc_tile_rowidx = nullptr;
+    M->tile_csr_Value = nullptr;
+    M->tile_csr_Col = M->tile_csr_Ptr = nullptr;
+    M->mask = nullptr;
+    if (owned_csr)
+    {
+        std::free(M->rowpointer);
+        std::free(M->columnindex);
+        std::free(M->value);
+        M->rowpointer = nullptr;
+        M->columnindex = nullptr;
+        M->value = nullptr;
+    }
+}
+
+// ------------------------------------------------------------ device path
+int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view *B, int op,
+                        long long *nnz_c, long long *tiles_c)
+{
+    if (c == nullptr || A == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (op != RTT_OP_AB && op != RTT_OP_AAT)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "op must be RTT_OP_AB or RTT_OP_AAT");
+    if (op == RTT_OP_AAT && B != nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "RTT_OP_AAT takes B == NULL");
+    if (A->rows < 0 || A->cols < 0 || A->nnz < 0 || A->nnz > INT_MAX)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "bad A shape");
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    c->have_symbolic = false;
+    c->ws.launches = 0;
+    c->ws.syncs = 0;
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    Workspace &ws = c->ws;
+    RTT_CHECK(map_device_error(csr2tile_device(ws, A->rows, A->cols, (int)A->nnz, A->row_ptr,
+                                               A->col_idx, A->values, c->A, true, false)));
+    if (op == RTT_OP_AB && B == nullptr)
+    {
+        if (A->rows != A->cols)
+            return rtt::fail(RTT_ERR_SHAPE_MISMATCH, "A*A needs a square A");
+        c->b_alias = true;
+        RTT_CHECK(build_tile_csc(ws, c->A));
+    }
+    else
+    {
+        c->b_alias = false;
+        if (op == RTT_OP_AAT)
+        {
+            RTT_CHECK(csr_transpose_device(ws, A->rows, A->cols, (int)A->nnz, A->row_ptr,
+                                           A->col_idx, A->values, c->bt_rowptr, c->bt_col,
+                                           c->bt_val));
+            RTT_CHECK(map_device_error(csr2tile_device(ws, A->cols, A->rows, (int)A->nnz,
+                                                       c->bt_rowptr.as<int>(), c->bt_col.as<int>(),
+                                                       c->bt_val.as<double>(), c->B, true, false)));
+        }
+        else
+        {
+            if (B->rows != A->cols)
+                return rtt::fail(RTT_ERR_SHAPE_MISMATCH, "A->cols != B->rows");
+            if (B->nnz < 0 || B->nnz > INT_MAX)
+                return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "bad B shape");
+            RTT_CHECK(map_device_error(csr2tile_device(ws, B->rows, B->cols, (int)B->nnz,
+                                                       B->row_ptr, B->col_idx, B->values, c->B,
+                                                       true, false)));
+        }
+        RTT_CHECK(build_tile_csc(ws, c->B));
+    }
+    const TileBufs &TB = c->b_alias ? c->A : c->B;
+    RTT_CHECK(map_device_error(symbolic_device(ws, c->A.view(), TB.view(), c->S)));
+    c->stats.nnz_a = c->A.nnz;
+    c->stats.nnz_b = TB.nnz;
+    c->stats.nnz_c = c->S.nnz;
+    c->stats.tiles_a = c->A.numtile;
+    c->stats.tiles_b = TB.numtile;
+    c->stats.tiles_c = c->S.numtile;
+    c->stats.host_syncs = ws.syncs;
+    if (nnz_c)
+        *nnz_c = c->S.nnz;
+    if (tiles_c)
+        *tiles_c = c->S.numtile;
+    c->have_symbolic = true;
+    return RTT_OK;
+}
+
+int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_values)
+{
+    if (c == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (!c->have_symbolic)
+        return rtt::fail(RTT_ERR_STATE, "rtt_spgemm_numeric before rtt_spgemm_symbolic");
+    if (c_row_ptr == nullptr || (c->S.nnz > 0 && (c_col_idx == nullptr || c_values == nullptr)))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "NULL output buffer");
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    Workspace &ws = c->ws;
+    const TileBufs &TB = c->b_alias ? c->A : c->B;
+    RTT_CHECK(c->counters.ensure(sizeof(long long) * 4, ws.stream));
+    RTT_CUDA(cudaMemsetAsync(c->counters.p, 0, sizeof(long long) * 4, ws.stream));
+    NumericConfig nc;
+    nc.dmma_pair_cutoff = c->cfg.dmma_pair_cutoff;
+    nc.counters = c->counters.as<long long>();
+    const bool fused = c->cfg.fused_csr_output != 0;
+    nc.write_tiles = !fused || c->cfg.keep_tiles != 0;
+    if (fused)
+    {
+        nc.csr_rowptr = c_row_ptr;
+        nc.csr_col = c_col_idx;
+        nc.csr_val = c_values;
+    }
+    RTT_CHECK(numeric_device(ws, c->A.view(), TB.view(), c->S, nc));
+    if (!fused)
+    {
+        SymbolicOut &S = c->S;
+        RTT_CHECK(csr_rowptr_device(ws, S, c_row_ptr));
+        RTT_CHECK(tile2csr_fill_device(ws, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(),
+                                       S.c_tile_nnz.as<int>(), S.c_ptr.as<uint8_t>(),
+                                       S.c_col.as<uint8_t>(), S.c_val.as<double>(), S.m, S.n,
+                                       S.tilem, TD, nullptr, -1, c_row_ptr, c_col_idx, c_values,
+                                       false));
+    }
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars64 + 2, c->counters.p, sizeof(long long) * 2,
+                             cudaMemcpyDeviceToHost, ws.stream));
+    RTT_CHECK(check_device_error(ws, "numeric"));
+    c->stats.dmma_pairs = ws.h_scalars64[2];
+    c->stats.sparse_pairs = ws.h_scalars64[3];
+    c->stats.kernel_launches = ws.launches;
+    c->stats.host_syncs = ws.syncs;
+    return RTT_OK;
+}
+
+int rtt_spgemm_tiles_view(rtt_context c, SMatrix *out)
+{
+    if (c == nullptr || out == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!c->have_symbolic || (c->cfg.fused_csr_output && !c->cfg.keep_tiles))
+        return rtt::fail(RTT_ERR_STATE, "no C tiles kept (set keep_tiles or unfused output)");
+    SymbolicOut &S = c->S;
+    std::memset(out, 0, sizeof(*out));
+    out->m = S.m;
+    out->n = S.n;
+    out->nnz = (int)S.nnz;
+    out->tilem = S.tilem;
+    out->tilen = S.tilen;
+    out->numtile = S.numtile;
+    out->tile_ptr = S.c_tile_ptr.as<int>();
+    out->tile_columnidx = S.c_tile_col.as<int>();
+    out->tile_rowidx = S.c_tile_row.as<int>();
+    out->tile_nnz = S.c_tile_nnz.as<int>();
+    out->tile_csr_Ptr = S.c_ptr.as<unsigned char>();
+    out->tile_csr_Col = S.c_col.as<unsigned char>();
+    out->tile_csr_Value = S.c_val.as<double>();
+    out->mask = S.c_mask.as<unsigned short>();
+    return RTT_OK;
+}
+
+int rtt_spgemm_csr_host(rtt_context c, const SMatrix *A, const SMatrix *B, int op, SMatrix *C)
+{
+    if (c == nullptr || !csr_args_ok(A) || C == nullptr || (B != nullptr && !csr_args_ok(B)))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "spgemm_csr_host: bad arguments");
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    cudaStream_t s = c->ws.stream;
+    RTT_CHECK(upload(c->in_rp, A->rowpointer, (size_t)A->m + 1, s));
+    RTT_CHECK(upload(c->in_col, A->columnindex, (size_t)A->nnz, s));
+    RTT_CHECK(upload(c->in_val, A->value, (size_t)A->nnz, s));
+    rtt_csr_view va{A->m, A->n, A->nnz, c->in_rp.as<int>(), c->in_col.as<int>(),
+                    c->in_val.as<double>()};
+    rtt_csr_view vb{};
+    if (B != nullptr)
+    {
+        RTT_CHECK(upload(c->in2_rp, B->rowpointer, (size_t)B->m + 1, s));
+        RTT_CHECK(upload(c->in2_col, B->columnindex, (size_t)B->nnz, s));
+        RTT_CHECK(upload(c->in2_val, B->value, (size_t)B->nnz, s));
+        vb = rtt_csr_view{B->m, B->n, B->nnz, c->in2_rp.as<int>(), c->in2_col.as<int>(),
+                          c->in2_val.as<double>()};
+    }
+    long long nnz = 0, tiles = 0;
+    RTT_CHECK(rtt_spgemm_symbolic(c, &va, B ? &vb : nullptr, op, &nnz, &tiles));
+    const int m = A->m;
+    const int n = op == RTT_OP_AAT ? A->m : (B ? B->n : A->n);
+    RTT_CHECK(c->out_rp.ensure(sizeof(int) * ((size_t)m + 1), s));
+    RTT_CHECK(c->out_col.ensure(sizeof(int) * (size_t)nnz + 16, s));
+    RTT_CHECK(c->out_val.ensure(sizeof(double) * (size_t)nnz + 16, s));
+    RTT_CHECK(rtt_spgemm_numeric(c, c->out_rp.as<int>(), c->out_col.as<int>(),
+                                 c->out_val.as<double>()));
+    HostArrays h;
+    int **rp = h.slot<int>(), **ci = h.slot<int>();
+    double **v = h.slot<double>();
+    RTT_CHECK(download(rp, c->out_rp.p, (size_t)m + 1, s));
+    RTT_CHECK(download(ci, c->out_col.p, (size_t)nnz, s));
+    RTT_CHECK(download(v, c->out_val.p, (size_t)nnz, s));
+    std::memset(C, 0, sizeof(*C));
+    C->m = m;
+    C->n = n;
+    C->nnz = (int)nnz;
+    C->rowpointer = *rp;
+    C->columnindex = *ci;
+    C->value = *v;
+    h.committed = true;
+    return RTT_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,674 @@
+// csr2tile.cu - CSR -> 16x16 tile CSR on sm_100a.
+//
+// Semantics follow csr2tile_row_major (reference src/csr2tile.h:196-259):
+// tiles of a tile row in ascending column order, per-tile exclusive row
+// offsets (u8), entries of a (tile, row) in CSR order, packed column byte
+// (row << 4) | col, mask bit (15 - col); and csr2tile_col_major (:261-478):
+// the same tiles with per-tile data in tile-CSC order and plain column bytes.
+//
+// Fast path (every row's tile column index non-decreasing, i.e. sorted CSR):
+// a half-warp owns one tile row, one lane per scalar row.  Each lane walks
+// its row with a cursor; the half-warp takes the minimum pending tile column
+// (4 xor-shuffles), every lane consumes its entries of that tile, a
+// half-warp scan turns per-row counts into the tile's row offsets, and the
+// lanes write their entries at tile base + row offset.  Reads of col/val are
+// sequential per lane and the 16 rows of a tile row are contiguous in
+// memory, so the half-warp streams one contiguous CSR slice.
+// Generic path (unsorted rows): a warp per tile row extracts tile columns in
+// ascending order and places entries with match_any ranking, which keeps CSR
+// order inside each (tile, row).
+#include "rtt_internal.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+#include <climits>
+
+namespace rtt
+{
+namespace
+{
+
+// ------------------------------------------------------------ validation
+// flags[0]: some row's tile column decreases (needs the generic path)
+// flags[1]: some row's column decreases (entries not sorted inside rows)
+__global__ void k_validate_csr(int m, int n, int nnz, const int *__restrict__ rowptr,
+                               const int *__restrict__ col, int *err, int *flags)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r == 0 && (rowptr[0] != 0 || rowptr[m] != nnz))
+        set_error(err, DERR_CSR_ROWPTR);
+    if (r >= m)
+        return;
+    int b = rowptr[r], e = rowptr[r + 1];
+    if (b < 0 || e < b || e > nnz)
+    {
+        set_error(err, DERR_CSR_ROWPTR);
+        return;
+    }
+    int prev = -1;
+    bool tile_dec = false, col_dec = false;
+    for (int j = b; j < e; ++j)
+    {
+        int c = col[j];
+        if (c < 0 || c >= n)
+        {
+            set_error(err, DERR_CSR_COL);
+            return;
+        }
+        if (prev >= 0)
+        {
+            if ((c >> 4) < (prev >> 4))
+                tile_dec = true;
+            if (c < prev)
+                col_dec = true;
+        }
+        prev = c;
+    }
+    if (tile_dec)
+        atomicOr(&flags[0], 1);
+    if (col_dec)
+        atomicOr(&flags[1], 1);
+}
+
+// -------------------------------------------------------------- fast path
+__global__ void __launch_bounds__(256) k_c2t_count(int m, int tilem, const int *__restrict__ rowptr,
+                                                   const int *__restrict__ col, int *__restrict__ cnt)
+{
+    const int lane = threadIdx.x & 31, hl = lane & 15;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int I = gw * 2 + (lane >> 4);
+    int p = 0, e = 0;
+    if (I < tilem && I * TD + hl < m)
+    {
+        p = rowptr[I * TD + hl];
+        e = rowptr[I * TD + hl + 1];
+    }
+    int cur = p < e ? (__ldg(col + p) >> 4) : INT_MAX;
+    int count = 0;
+    for (;;)
+    {
+        const int T = half_min(cur);
+        const bool has = T != INT_MAX;
+        if (!__any_sync(FULL, has))
+            break;
+        if (has)
+        {
+            ++count;
+            while (p < e && (__ldg(col + p) >> 4) == T)
+                ++p;
+            cur = p < e ? (__ldg(col + p) >> 4) : INT_MAX;
+        }
+    }
+    if (I < tilem && hl == 0)
+        cnt[I] = count;
+}
+
+__global__ void __launch_bounds__(256) k_c2t_fill(int m, int tilem, const int *__restrict__ rowptr,
+                                                  const int *__restrict__ col,
+                                                  const double *__restrict__ val,
+                                                  const int *__restrict__ tile_ptr,
+                                                  int *__restrict__ o_tcol, int *__restrict__ o_trow,
+                                                  int *__restrict__ o_tnnz, uint8_t *__restrict__ o_ptr,
+                                                  uint8_t *__restrict__ o_col,
+                                                  double *__restrict__ o_val,
+                                                  uint16_t *__restrict__ o_mask, int packed, int *err)
+{
+    const int lane = threadIdx.x & 31, hl = lane & 15;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int I = gw * 2 + (lane >> 4);
+    const bool tr_ok = I < tilem;
+    int p = 0, e = 0, base = 0, t = 0, tend = 0;
+    if (tr_ok)
+    {
+        base = rowptr[min(I * TD, m)];
+        t = tile_ptr[I];
+        tend = tile_ptr[I + 1];
+        if (I * TD + hl < m)
+        {
+            p = rowptr[I * TD + hl];
+            e = rowptr[I * TD + hl + 1];
+        }
+    }
+    int cur = p < e ? (__ldg(col + p) >> 4) : INT_MAX;
+    for (;;)
+    {
+        const int T = half_min(cur);
+        const bool has = T != INT_MAX;
+        if (!__any_sync(FULL, has))
+            break;
+        int q = p;
+        if (has)
+            while (q < e && (__ldg(col + q) >> 4) == T)
+                ++q;
+        const int c = q - p;
+        const int incl = half_incl_scan(c);
+        const int excl = incl - c;
+        const int total = __shfl_sync(FULL, incl, (lane & 16) | 15);
+        if (has)
+        {
+            if (t >= tend)
+            {
+                set_error(err, DERR_C2T_OVERFLOW);
+            }
+            else
+            {
+                o_ptr[(size_t)t * TD + hl] = (uint8_t)excl;
+                uint16_t mk = 0;
+                int dst = base + excl;
+                for (int j = p; j < q; ++j, ++dst)
+                {
+                    const int cc = __ldg(col + j) & 15;
+                    mk |= (uint16_t)(0x8000u >> cc);
+                    o_col[dst] = (uint8_t)(packed ? ((hl << 4) | cc) : cc);
+                    o_val[dst] = __ldg(val + j);
+                }
+                o_mask[(size_t)t * TD + hl] = mk;
+                if (hl == 0)
+                {
+                    o_tcol[t] = T;
+                    o_trow[t] = I;
+                    o_tnnz[t] = base;
+                }
+            }
+            base += total;
+            ++t;
+            p = q;
+            cur = p < e ? (__ldg(col + p) >> 4) : INT_MAX;
+        }
+    }
+}
+
+// ----------------------------------------------------------- generic path
+__global__ void __launch_bounds__(256) k_c2t_count_generic(int m, int tilem,
+                                                           const int *__restrict__ rowptr,
+                                                           const int *__restrict__ col,
+                                                           int *__restrict__ cnt)
+{
+    const int lane = threadIdx.x & 31;
+    const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (I >= tilem)
+        return;
+    const int s0 = rowptr[I * TD], s1 = rowptr[min(I * TD + TD, m)];
+    int prev = -1, count = 0;
+    for (;;)
+    {
+        int mn = INT_MAX;
+        for (int j = s0 + lane; j < s1; j += 32)
+        {
+            int T = __ldg(col + j) >> 4;
+            if (T > prev && T < mn)
+                mn = T;
+        }
+        mn = warp_min(mn);
+        if (mn == INT_MAX)
+            break;
+        ++count;
+        prev = mn;
+    }
+    if (lane == 0)
+        cnt[I] = count;
+}
+
+__global__ void __launch_bounds__(128) k_c2t_fill_generic(
+    int m, int tilem, const int *__restrict__ rowptr, const int *__restrict__ col,
+    const double *__restrict__ val, const int *__restrict__ tile_ptr, int *__restrict__ o_tcol,
+    int *__restrict__ o_trow, int *__restrict__ o_tnnz, uint8_t *__restrict__ o_ptr,
+    uint8_t *__restrict__ o_col, double *__restrict__ o_val, uint16_t *__restrict__ o_mask,
+    int packed, int *err)
+{
+    __shared__ int s_rp[4][TD + 1];
+    __shared__ int s_cnt[4][TD];
+    __shared__ int s_cur[4][TD];
+    __shared__ unsigned s_mask[4][TD];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (I >= tilem)
+        return;
+    const int r0 = I * TD, nrows = min(TD, m - r0);
+    if (lane <= TD)
+        s_rp[w][lane] = rowptr[r0 + min(lane, nrows)];
+    __syncwarp();
+    const int s0 = s_rp[w][0], s1 = s_rp[w][nrows];
+    int prev = -1, t = tile_ptr[I];
+    const int tend = tile_ptr[I + 1];
+    int base = s0;
+    const unsigned lt = (1u << lane) - 1u;
+    for (;;)
+    {
+        int mn = INT_MAX;
+        for (int j = s0 + lane; j < s1; j += 32)
+        {
+            int T = __ldg(col + j) >> 4;
+            if (T > prev && T < mn)
+                mn = T;
+        }
+        const int T = warp_min(mn);
+        if (T == INT_MAX)
+            break;
+        prev = T;
+        if (lane < TD)
+        {
+            s_cnt[w][lane] = 0;
+            s_cur[w][lane] = 0;
+            s_mask[w][lane] = 0;
+        }
+        __syncwarp();
+        for (int j = s0 + lane; j < s1; j += 32)
+        {
+            if ((__ldg(col + j) >> 4) == T)
+            {
+                int r = 0;
+                while (r + 1 < nrows && s_rp[w][r + 1] <= j)
+                    ++r;
+                atomicAdd(&s_cnt[w][r], 1);
+            }
+        }
+        __syncwarp();
+        int c = lane < TD ? s_cnt[w][lane] : 0;
+        int incl = half_incl_scan(c);
+        int excl = incl - c;
+        int total = __shfl_sync(FULL, incl, 15);
+        if (t >= tend)
+        {
+            set_error(err, DERR_C2T_OVERFLOW);
+            return;
+        }
+        if (lane < TD)
+        {
+            o_ptr[(size_t)t * TD + lane] = (uint8_t)excl;
+            s_cnt[w][lane] = excl;
+        }
+        __syncwarp();
+        // place entries in CSR order, chunk by chunk
+        for (int j0 = s0; j0 < s1; j0 += 32)
+        {
+            const int j = j0 + lane;
+            bool in = false;
+            int r = 0, cc = 0;
+            if (j < s1)
+            {
+                const int cj = __ldg(col + j);
+                if ((cj >> 4) == T)
+                {
+                    in = true;
+                    cc = cj & 15;
+                    while (r + 1 < nrows && s_rp[w][r + 1] <= j)
+                        ++r;
+                }
+            }
+            const int key = in ? r : (TD + lane);
+            const unsigned peers = __match_any_sync(FULL, key);
+            if (in)
+            {
+                const int rank = __popc(peers & lt);
+                const int dst = base + s_cnt[w][r] + s_cur[w][r] + rank;
+                o_col[dst] = (uint8_t)(packed ? ((r << 4) | cc) : cc);
+                o_val[dst] = __ldg(val + j);
+                atomicOr(&s_mask[w][r], 0x8000u >> cc);
+            }
+            __syncwarp();
+            if (in && (peers & lt) == 0)
+                s_cur[w][r] += __popc(peers);
+            __syncwarp();
+        }
+        if (lane < TD)
+            o_mask[(size_t)t * TD + lane] = (uint16_t)s_mask[w][lane];
+        if (lane == 0)
+        {
+            o_tcol[t] = T;
+            o_trow[t] = I;
+            o_tnnz[t] = base;
+        }
+        base += total;
+        ++t;
+        __syncwarp();
+    }
+}
+
+// Stable insertion sort of every (tile, row) segment by column byte: the
+// in-tile order of csr2tile_col_major for rows whose columns are unsorted.
+__global__ void k_sort_tile_rows(int numtile, const int *__restrict__ tnnz,
+                                 const uint8_t *__restrict__ ptr, uint8_t *__restrict__ colb,
+                                 double *__restrict__ v)
+{
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= numtile * TD)
+        return;
+    int t = x >> 4, r = x & 15;
+    int b = tnnz[t] + ptr[(size_t)t * TD + r];
+    int e = r == TD - 1 ? tnnz[t + 1] : tnnz[t] + ptr[(size_t)t * TD + r + 1];
+    for (int i = b + 1; i < e; ++i)
+    {
+        uint8_t kc = colb[i];
+        double kv = v[i];
+        int key = kc & 15;
+        int j = i - 1;
+        while (j >= b && (colb[j] & 15) > key)
+        {
+            colb[j + 1] = colb[j];
+            v[j + 1] = v[j];
+            --j;
+        }
+        colb[j + 1] = kc;
+        v[j + 1] = kv;
+    }
+}
+
+__global__ void k_set_int(int *p, int v) { *p = v; }
+
+// ------------------------------------------------------ tile CSC / col-major
+__global__ void k_iota(int *a, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        a[i] = i;
+}
+
+__global__ void k_lower_bound_ptr(const int *__restrict__ sorted_keys, int nkeys, int nbins,
+                                  int *__restrict__ ptr)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > nbins)
+        return;
+    ptr[b] = lower_bound(sorted_keys, 0, nkeys, b);
+}
+
+__global__ void k_gather_int(const int *__restrict__ src, const int *__restrict__ idx, int n,
+                             int *__restrict__ dst)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        dst[i] = src[idx[i]];
+}
+
+__global__ void k_tile_counts(const int *__restrict__ tnnz, const int *__restrict__ order, int n,
+                              int *__restrict__ cnt)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        int t = order[i];
+        cnt[i] = tnnz[t + 1] - tnnz[t];
+    }
+}
+
+// warp per destination tile: copy row offsets, mask and entries
+__global__ void k_copy_tiles_colmajor(int n, const int *__restrict__ order,
+                                      const int *__restrict__ src_tnnz,
+                                      const uint8_t *__restrict__ src_ptr,
+                                      const uint16_t *__restrict__ src_mask,
+                                      const uint8_t *__restrict__ src_col,
+                                      const double *__restrict__ src_val,
+                                      const int *__restrict__ dst_tnnz, uint8_t *__restrict__ dst_ptr,
+                                      uint16_t *__restrict__ dst_mask, uint8_t *__restrict__ dst_col,
+                                      double *__restrict__ dst_val)
+{
+    const int lane = threadIdx.x & 31;
+    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (p >= n)
+        return;
+    const int t = order[p];
+    if (lane < TD)
+    {
+        dst_ptr[(size_t)p * TD + lane] = src_ptr[(size_t)t * TD + lane];
+        dst_mask[(size_t)p * TD + lane] = src_mask[(size_t)t * TD + lane];
+    }
+    const int sb = src_tnnz[t], cnt = src_tnnz[t + 1] - sb, db = dst_tnnz[p];
+    for (int i = lane; i < cnt; i += 32)
+    {
+        dst_col[db + i] = src_col[sb + i] & 15;
+        dst_val[db + i] = src_val[sb + i];
+    }
+}
+
+// ----------------------------------------------------------- CSR transpose
+__global__ void k_row_ids(int m, const int *__restrict__ rowptr, int *__restrict__ rows)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= m)
+        return;
+    for (int j = rowptr[r]; j < rowptr[r + 1]; ++j)
+        rows[j] = r;
+}
+
+__global__ void k_gather_transpose(int nnz, const int *__restrict__ order,
+                                   const int *__restrict__ rows, const double *__restrict__ val,
+                                   int *__restrict__ t_col, double *__restrict__ t_val)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnz)
+        return;
+    int src = order[i];
+    t_col[i] = rows[src];
+    t_val[i] = val[src];
+}
+
+int bits_for(int maxval)
+{
+    int b = 1;
+    while (b < 31 && (1 << b) <= maxval)
+        ++b;
+    return b;
+}
+
+int sort_pairs(Workspace &ws, const int *keys_in, int *keys_out, const int *vals_in, int *vals_out,
+               int n, int max_key)
+{
+    if (n <= 0)
+        return RTT_OK;
+    size_t bytes = 0;
+    const int end_bit = bits_for(max_key);
+    RTT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys_in, keys_out, vals_in, vals_out,
+                                             n, 0, end_bit, ws.stream));
+    RTT_CHECK(ws.scan_tmp.ensure(bytes, ws.stream));
+    RTT_CUDA(cub::DeviceRadixSort::SortPairs(ws.scan_tmp.p, bytes, keys_in, keys_out, vals_in,
+                                             vals_out, n, 0, end_bit, ws.stream));
+    ws.launches += 3;
+    return RTT_OK;
+}
+
+inline int grid_for(long long threads, int block) { return (int)((threads + block - 1) / block); }
+
+} // namespace
+
+int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
+                    const double *val, TileBufs &out, bool packed_col, bool sort_within_rows)
+{
+    if (m < 0 || n < 0 || nnz < 0)
+        return fail(RTT_ERR_INVALID_ARGUMENT, "csr2tile: negative size");
+    cudaStream_t s = ws.stream;
+    out.m = m;
+    out.n = n;
+    out.nnz = nnz;
+    out.tilem = ceil_div(m, TD);
+    out.tilen = ceil_div(n, TD);
+    const int tilem = out.tilem;
+
+    RTT_CHECK(out.tile_ptr.ensure(sizeof(int) * (tilem + 1), s));
+    RTT_CHECK(out.tmp0.ensure(sizeof(int) * (tilem + 1), s));
+    RTT_CHECK(out.tmp1.ensure(sizeof(int) * 4, s));
+    int *flags = out.tmp1.as<int>();
+    RTT_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * 2, s));
+    if (m == 0)
+    {
+        RTT_CUDA(cudaMemsetAsync(out.tile_ptr.p, 0, sizeof(int), s));
+        out.numtile = 0;
+        RTT_CHECK(out.tile_nnz.ensure(sizeof(int), s));
+        RTT_CUDA(cudaMemsetAsync(out.tile_nnz.p, 0, sizeof(int), s));
+        const size_t tiny = 16;
+        RTT_CHECK(out.tile_col.ensure(tiny, s));
+        RTT_CHECK(out.tile_row.ensure(tiny, s));
+        RTT_CHECK(out.ptr.ensure(tiny, s));
+        RTT_CHECK(out.mask.ensure(tiny, s));
+        RTT_CHECK(out.col.ensure(tiny, s));
+        RTT_CHECK(out.val.ensure(tiny, s));
+        return RTT_OK;
+    }
+    k_validate_csr<<<grid_for(m, 256), 256, 0, s>>>(m, n, nnz, rowptr, col, ws.err.as<int>(),
+                                                    flags);
+    ws.launches++;
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 4, flags, sizeof(int) * 2, cudaMemcpyDeviceToHost, s));
+    RTT_CHECK(check_device_error(ws, "csr2tile validate"));
+    const bool generic = ws.h_scalars[4] != 0;
+    const bool unsorted = ws.h_scalars[5] != 0;
+
+    int *cnt = out.tmp0.as<int>();
+    if (!generic)
+        k_c2t_count<<<grid_for((long long)ceil_div(tilem, 2) * 32, 256), 256, 0, s>>>(m, tilem, rowptr,
+                                                                                   col, cnt);
+    else
+        k_c2t_count_generic<<<grid_for((long long)tilem * 32, 256), 256, 0, s>>>(m, tilem, rowptr,
+                                                                               col, cnt);
+    ws.launches++;
+    RTT_CHECK(scan_exclusive_int(ws, cnt, out.tile_ptr.as<int>(), tilem));
+    int numtile = 0;
+    RTT_CHECK(read_int(ws, out.tile_ptr.as<int>() + tilem, &numtile));
+    out.numtile = numtile;
+
+    RTT_CHECK(out.tile_col.ensure(sizeof(int) * (size_t)numtile, s));
+    RTT_CHECK(out.tile_row.ensure(sizeof(int) * (size_t)numtile, s));
+    RTT_CHECK(out.tile_nnz.ensure(sizeof(int) * ((size_t)numtile + 1), s));
+    RTT_CHECK(out.ptr.ensure((size_t)numtile * TD, s));
+    RTT_CHECK(out.mask.ensure(sizeof(uint16_t) * (size_t)numtile * TD, s));
+    RTT_CHECK(out.col.ensure((size_t)nnz, s));
+    RTT_CHECK(out.val.ensure(sizeof(double) * (size_t)nnz, s));
+
+    if (!generic)
+        k_c2t_fill<<<grid_for((long long)ceil_div(tilem, 2) * 32, 256), 256, 0, s>>>(
+            m, tilem, rowptr, col, val, out.tile_ptr.as<int>(), out.tile_col.as<int>(),
+            out.tile_row.as<int>(), out.tile_nnz.as<int>(), out.ptr.as<uint8_t>(),
+            out.col.as<uint8_t>(), out.val.as<double>(), out.mask.as<uint16_t>(), packed_col ? 1 : 0,
+            ws.err.as<int>());
+    else
+        k_c2t_fill_generic<<<grid_for((long long)tilem * 32, 128), 128, 0, s>>>(
+            m, tilem, rowptr, col, val, out.tile_ptr.as<int>(), out.tile_col.as<int>(),
+            out.tile_row.as<int>(), out.tile_nnz.as<int>(), out.ptr.as<uint8_t>(),
+            out.col.as<uint8_t>(), out.val.as<double>(), out.mask.as<uint16_t>(), packed_col ? 1 : 0,
+            ws.err.as<int>());
+    ws.launches++;
+    k_set_int<<<1, 1, 0, s>>>(out.tile_nnz.as<int>() + numtile, nnz);
+    ws.launches++;
+    if (sort_within_rows && unsorted && numtile > 0)
+    {
+        k_sort_tile_rows<<<grid_for((long long)numtile * TD, 256), 256, 0, s>>>(
+            numtile, out.tile_nnz.as<int>(), out.ptr.as<uint8_t>(), out.col.as<uint8_t>(),
+            out.val.as<double>());
+        ws.launches++;
+    }
+    return RTT_OK;
+}
+
+int build_tile_csc(Workspace &ws, TileBufs &t)
+{
+    cudaStream_t s = ws.stream;
+    const int nt = t.numtile;
+    RTT_CHECK(t.csc_ptr.ensure(sizeof(int) * (t.tilen + 1), s));
+    RTT_CHECK(t.csc_row.ensure(sizeof(int) * (size_t)(nt + 1), s));
+    RTT_CHECK(t.csc_data.ensure(sizeof(int) * (size_t)(nt + 1), s));
+    RTT_CHECK(t.tmp2.ensure(sizeof(int) * (size_t)(nt + 1), s));
+    RTT_CHECK(t.tmp3.ensure(sizeof(int) * (size_t)(nt + 1), s));
+    int *iota = t.tmp2.as<int>();
+    int *sorted_keys = t.tmp3.as<int>();
+    if (nt > 0)
+    {
+        k_iota<<<grid_for(nt, 256), 256, 0, s>>>(iota, nt);
+        ws.launches++;
+        RTT_CHECK(sort_pairs(ws, t.tile_col.as<int>(), sorted_keys, iota, t.csc_data.as<int>(), nt,
+                             t.tilen));
+        k_gather_int<<<grid_for(nt, 256), 256, 0, s>>>(t.tile_row.as<int>(), t.csc_data.as<int>(),
+                                                       nt, t.csc_row.as<int>());
+        ws.launches++;
+    }
+    k_lower_bound_ptr<<<grid_for(t.tilen + 1, 256), 256, 0, s>>>(sorted_keys, nt, t.tilen,
+                                                                 t.csc_ptr.as<int>());
+    ws.launches++;
+    return RTT_OK;
+}
+
+int tiles_to_col_major(Workspace &ws, const TileBufs &rm, TileBufs &out)
+{
+    // rm must carry its CSC index (build_tile_csc)
+    cudaStream_t s = ws.stream;
+    const int nt = rm.numtile;
+    out.m = rm.m;
+    out.n = rm.n;
+    out.nnz = rm.nnz;
+    out.tilem = rm.tilem;
+    out.tilen = rm.tilen;
+    out.numtile = nt;
+    RTT_CHECK(out.tile_nnz.ensure(sizeof(int) * ((size_t)nt + 1), s));
+    RTT_CHECK(out.ptr.ensure((size_t)nt * TD + 16, s));
+    RTT_CHECK(out.mask.ensure(sizeof(uint16_t) * (size_t)nt * TD + 16, s));
+    RTT_CHECK(out.col.ensure((size_t)rm.nnz + 16, s));
+    RTT_CHECK(out.val.ensure(sizeof(double) * (size_t)rm.nnz + 16, s));
+    RTT_CHECK(out.tmp0.ensure(sizeof(int) * ((size_t)nt + 1), s));
+    int *cnt = out.tmp0.as<int>();
+    if (nt > 0)
+    {
+        k_tile_counts<<<grid_for(nt, 256), 256, 0, s>>>(rm.tile_nnz.as<int>(), rm.csc_data.as<int>(),
+                                                         nt, cnt);
+        ws.launches++;
+    }
+    RTT_CHECK(scan_exclusive_int(ws, cnt, out.tile_nnz.as<int>(), nt));
+    if (nt > 0)
+    {
+        k_copy_tiles_colmajor<<<grid_for((long long)nt * 32, 256), 256, 0, s>>>(
+            nt, rm.csc_data.as<int>(), rm.tile_nnz.as<int>(), rm.ptr.as<uint8_t>(),
+            rm.mask.as<uint16_t>(), rm.col.as<uint8_t>(), rm.val.as<double>(),
+            out.tile_nnz.as<int>(), out.ptr.as<uint8_t>(), out.mask.as<uint16_t>(),
+            out.col.as<uint8_t>(), out.val.as<double>());
+        ws.launches++;
+    }
+    return RTT_OK;
+}
+
+int csr_transpose_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
+                         const double *val, DevBuf &t_rowptr, DevBuf &t_col, DevBuf &t_val)
+{
+    cudaStream_t s = ws.stream;
+    RTT_CHECK(t_rowptr.ensure(sizeof(int) * (size_t)(n + 1), s));
+    RTT_CHECK(t_col.ensure(sizeof(int) * (size_t)nnz + 16, s));
+    RTT_CHECK(t_val.ensure(sizeof(double) * (size_t)nnz + 16, s));
+    DevBuf rows, iota, keys, order;
+    int st = RTT_OK;
+    do
+    {
+        if ((st = rows.ensure(sizeof(int) * (size_t)nnz + 16, s)) != RTT_OK)
+            break;
+        if ((st = iota.ensure(sizeof(int) * (size_t)nnz + 16, s)) != RTT_OK)
+            break;
+        if ((st = keys.ensure(sizeof(int) * (size_t)nnz + 16, s)) != RTT_OK)
+            break;
+        if ((st = order.ensure(sizeof(int) * (size_t)nnz + 16, s)) != RTT_OK)
+            break;
+        if (m > 0)
+        {
+            k_row_ids<<<grid_for(m, 256), 256, 0, s>>>(m, rowptr, rows.as<int>());
+            ws.launches++;
+        }
+        if (nnz > 0)
+        {
+            k_iota<<<grid_for(nnz, 256), 256, 0, s>>>(iota.as<int>(), nnz);
+            ws.launches++;
+            if ((st = sort_pairs(ws, col, keys.as<int>(), iota.as<int>(), order.as<int>(), nnz, n)) !=
+                RTT_OK)
+                break;
+            k_gather_transpose<<<grid_for(nnz, 256), 256, 0, s>>>(
+                nnz, order.as<int>(), rows.as<int>(), val, t_col.as<int>(), t_val.as<double>());
+            ws.launches++;
+        }
+        k_lower_bound_ptr<<<grid_for(n + 1, 256), 256, 0, s>>>(keys.as<int>(), nnz, n,
+                                                              t_rowptr.as<int>());
+        ws.launches++;
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess)
+            st = cuda_fail(e, "csr transpose");
+    } while (0);
+    cudaStreamSynchronize(s);
+    rows.release();
+    iota.release();
+    keys.release();
+    order.release();
+    return st;
+}
+
+} // namespace rtt

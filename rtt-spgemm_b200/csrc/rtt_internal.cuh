@@ -1,0 +1,281 @@
+// rtt_internal.cuh - shared device/host helpers of the sm_100a tiled SpGEMM.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <string>
+
+#include "rtt_spgemm.h"
+
+namespace rtt
+{
+
+constexpr int TD = 16;          // tile edge (reference BLOCK_SIZE)
+constexpr int WARP = 32;
+constexpr unsigned FULL = 0xffffffffu;
+
+// Device-side error words.  Kernels record the first failure with atomicCAS
+// and skip the offending access; the host reads the word after a sync.
+enum DeviceError : int
+{
+    DERR_NONE = 0,
+    DERR_CSR_ROWPTR = 101,      // row_ptr not monotone / out of range
+    DERR_CSR_COL = 102,         // column out of range
+    DERR_C2T_OVERFLOW = 103,    // csr2tile wrote past a tile row
+    DERR_SYM_OVERFLOW = 104,    // symbolic produced more tiles than counted
+    DERR_NUM_PAIRS = 105,       // numeric pair buffer overflow
+    DERR_NUM_BOUNDS = 106,      // numeric output index out of range
+    DERR_T2C_BOUNDS = 107,      // tile2csr output index out of range
+    DERR_WINDOW = 108,          // symbolic window bookkeeping failed
+};
+
+__device__ __forceinline__ void set_error(int *err, int code)
+{
+    if (err != nullptr)
+        atomicCAS(err, 0, code);
+}
+
+// Row-major 16x16 tile CSR on the device (SMatrix semantics).  col bytes may
+// be packed (row << 4) | col (A from csr2tile_row_major) or plain (B from
+// csr2tile_col_major, C): the kernels only use the low nibble.
+struct DevTiles
+{
+    int m, n, tilem, tilen, numtile, nnz;
+    const int *tile_ptr;    // tilem + 1 (row-major structure)
+    const int *tile_col;    // numtile
+    const int *tile_nnz;    // numtile + 1, offsets into col/val (data order)
+    const uint8_t *ptr;     // numtile * 16, exclusive row offsets (data order)
+    const uint8_t *col;     // nnz
+    const double *val;      // nnz
+    const uint16_t *mask;   // numtile * 16, bit (15 - c) (data order)
+    const int *row_data;    // row-major position -> data index (nullptr = identity)
+    // tile CSC (column lists of K), data index per entry
+    const int *csc_ptr;     // tilen + 1
+    const int *csc_row;     // numtile
+    const int *csc_data;    // numtile (nullptr = identity)
+};
+
+// C tile structure produced by the symbolic phase.
+struct DevCTiles
+{
+    int tilem, tilen, m, n;
+    int *tile_ptr;      // tilem + 1
+    int *tile_col;      // numtile
+    int *tile_row;      // numtile
+    int *tile_nnz;      // numtile + 1 (exclusive offsets)
+    uint16_t *mask;     // numtile * 16
+    uint8_t *ptr;       // numtile * 16
+    uint8_t *col;       // nnz
+    double *val;        // nnz
+};
+
+// ---------------------------------------------------------------- warp utils
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int warp_min(int v)
+{
+    return __reduce_min_sync(FULL, v);
+}
+
+__device__ __forceinline__ int warp_max(int v)
+{
+    return __reduce_max_sync(FULL, v);
+}
+
+// inclusive scan over the warp
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T v)
+{
+    const int l = lane_id();
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        T u = __shfl_up_sync(FULL, v, o);
+        if (l >= o)
+            v += u;
+    }
+    return v;
+}
+
+// inclusive scan inside each 16-lane half (width-16 shuffles)
+template <typename T>
+__device__ __forceinline__ T half_incl_scan(T v)
+{
+    const int l = lane_id() & 15;
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1)
+    {
+        T u = __shfl_up_sync(FULL, v, o, 16);
+        if (l >= o)
+            v += u;
+    }
+    return v;
+}
+
+__device__ __forceinline__ int half_min(int v)
+{
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1)
+        v = min(v, __shfl_xor_sync(FULL, v, o));
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T half_sum(T v)
+{
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1)
+        v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// first index in [lo, hi) with a[i] >= key
+__device__ __forceinline__ int lower_bound(const int *a, int lo, int hi, int key)
+{
+    while (lo < hi)
+    {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] < key)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__host__ __device__ __forceinline__ int ceil_div(int a, int b) { return a / b + (a % b != 0); }
+
+// --------------------------------------------------------------- host side
+std::string &last_error_ref();
+int fail(int status, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define RTT_CUDA(call)                                                        \
+    do                                                                        \
+    {                                                                         \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess)                                                \
+            return ::rtt::cuda_fail(e_, #call);                               \
+    } while (0)
+
+#define RTT_CHECK(call)                                                       \
+    do                                                                        \
+    {                                                                         \
+        int s_ = (call);                                                      \
+        if (s_ != RTT_OK)                                                     \
+            return s_;                                                        \
+    } while (0)
+
+// Grow-only device buffer owned by a workspace.
+struct DevBuf
+{
+    void *p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes, cudaStream_t s);
+    void release();
+    template <typename T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
+// Device workspace: named grow-only buffers plus pinned host scalars.
+struct Workspace
+{
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    DevBuf err;        // int device error word
+    DevBuf scan_tmp;   // CUB temp storage
+    int *h_scalars = nullptr; // pinned, 16 ints
+    long long *h_scalars64 = nullptr; // pinned, 8 long long
+    int launches = 0;
+    int syncs = 0;
+    int init(int dev);
+    void destroy();
+};
+
+// exclusive scan of n ints in place into out (n + 1 entries: out[n] = total)
+int scan_exclusive_int(Workspace &ws, const int *in, int *out, int n);
+// exclusive scan of n ints into int64 offsets (n + 1 entries)
+int scan_exclusive_i64(Workspace &ws, const int *in, long long *out, int n);
+// read the device error word (syncs the stream); returns RTT_ERR_DEVICE_CHECK on error
+int check_device_error(Workspace &ws, const char *stage);
+// copy one int / int64 from device to host (syncs)
+int read_int(Workspace &ws, const int *d, int *h);
+int read_i64(Workspace &ws, const long long *d, long long *h);
+
+// ------------------------------------------------------------- kernel hosts
+// csr2tile: row-major tiles of a device CSR.  Output arrays allocated from bufs.
+struct TileBufs
+{
+    DevBuf tile_ptr, tile_col, tile_row, tile_nnz, ptr, col, val, mask;
+    DevBuf csc_ptr, csc_row, csc_data, row_data;
+    DevBuf tmp0, tmp1, tmp2, tmp3;
+    int m = 0, n = 0, tilem = 0, tilen = 0, numtile = 0, nnz = 0;
+    void release();
+    DevTiles view() const;
+};
+
+int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
+                    const double *val, TileBufs &out, bool packed_col, bool sort_within_rows);
+// tile CSC index (column lists) over row-major tiles
+int build_tile_csc(Workspace &ws, TileBufs &t);
+// rearrange row-major tiles into the csr2tile_col_major layout (data in CSC order)
+int tiles_to_col_major(Workspace &ws, const TileBufs &rowmajor, TileBufs &out);
+// CSR transpose on the device
+int csr_transpose_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
+                         const double *val, DevBuf &t_rowptr, DevBuf &t_col, DevBuf &t_val);
+
+struct SymbolicOut
+{
+    DevBuf c_tile_ptr, c_tile_col, c_tile_row, c_tile_nnz, c_mask, c_ptr, c_col, c_val;
+    DevBuf c_row_cnt;   // m ints, per-row nnz of C
+    DevBuf c_rowptr;    // tilem + 1 int64: exclusive scan of nnz per C tile row
+    DevBuf c_tr_nnz;    // tilem ints, nnz per C tile row
+    DevBuf count_tmp;   // tilem + 1 ints
+    DevBuf tile_cnt;    // numtile ints, nnz per C tile
+    DevBuf row_prefix;  // numtile * 16 ints, CSR prefix of each (tile,row) in its tile row
+    int numtile = 0;
+    long long nnz = 0;
+    int tilem = 0, tilen = 0, m = 0, n = 0;
+    void release();
+    DevCTiles view();
+};
+
+int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S);
+
+struct NumericConfig
+{
+    int dmma_pair_cutoff = 3072;
+    bool write_tiles = true;
+    int *csr_rowptr = nullptr;  // fused CSR output when csr_col != nullptr
+    int *csr_col = nullptr;
+    double *csr_val = nullptr;
+    long long *counters = nullptr; // device [0] dmma pairs, [1] sparse pairs
+};
+
+int numeric_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
+                   const NumericConfig &cfg);
+// CSR row pointer of C (m + 1 ints) from the symbolic counts
+int csr_rowptr_device(Workspace &ws, SymbolicOut &S, int *rowptr);
+
+// tile2csr on device tiles of edge td.  Writes rowptr (m + 1) then col/val.
+int tile2csr_count_device(Workspace &ws, const int *tile_ptr, const int *tile_col,
+                          const int *tile_nnz, const uint8_t *ptr, const uint8_t *col, int m,
+                          int n, int tilem, int td, const int *new_to_old, int perm_size,
+                          int *rowptr_out);
+int tile2csr_fill_device(Workspace &ws, const int *tile_ptr, const int *tile_col,
+                         const int *tile_nnz, const uint8_t *ptr, const uint8_t *col,
+                         const double *val, int m, int n, int tilem, int td,
+                         const int *new_to_old, int perm_size, const int *rowptr, int *out_col,
+                         double *out_val, bool sort_rows);
+
+} // namespace rtt

@@ -1,0 +1,251 @@
+"""B200-native tiled FP64 SpGEMM - Python host mirror of the C ABI.
+
+Function names and argument meanings follow the reference's tiled path
+(for-the-juan/RTT-SpGEMM):
+
+==========================  ===========================================
+reference                   here (all run on the GPU through the C ABI)
+==========================  ===========================================
+csr2tile_row_major          csr2tile_row_major(csr) -> tile dict
+csr2tile_col_major          csr2tile_col_major(csr) -> tile dict
+spgemm_cpu(A, B, C)         spgemm_tile(a_tiles, b_tiles) -> tile dict
+tile2csr(C, canonical)      tile2csr(tiles, tile_dim=8, canonical=...)
+tile2csr_restore_rows       tile2csr(tiles, ..., new_to_old=perm)
+dmma_tilespgemm 8x8 export  tile16_to_tile8(c_tiles)
+device CSR -> CSR timed     Context.symbolic / Context.numeric
+==========================  ===========================================
+
+Tile matrices are dicts of numpy arrays keyed by SMatrix field name.  Errors
+raise :class:`RttError` carrying the rtt_status code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from types import SimpleNamespace
+
+import numpy as np
+
+from . import generators
+from ._abi import (EXPORTS, LIB_PATH, RTT_OP_AAT, RTT_OP_AB, Config, CsrView, RttError, SMatrix,
+                   Stats, build, check, lib)
+from .generators import CSR
+
+__all__ = ["CSR", "Context", "RttError", "build", "csr2tile_col_major", "csr2tile_row_major",
+           "generators", "lib", "spgemm_csr_host", "spgemm_tile", "tile16_to_tile8", "tile2csr",
+           "EXPORTS", "LIB_PATH", "RTT_OP_AB", "RTT_OP_AAT"]
+
+TD = 16
+
+
+def _ptr(a: np.ndarray, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def _copy(p, count: int, dtype) -> np.ndarray:
+    if count <= 0 or not p:
+        return np.zeros(max(count, 0), dtype=dtype)
+    return np.ctypeslib.as_array(p, shape=(count,)).astype(dtype, copy=True)
+
+
+def _csr_smatrix(csr):
+    rp = np.ascontiguousarray(csr.rowptr, dtype=np.int32)
+    ci = np.ascontiguousarray(csr.col, dtype=np.int32)
+    v = np.ascontiguousarray(csr.val, dtype=np.float64)
+    s = SMatrix()
+    s.m, s.n, s.nnz = csr.m, csr.n, int(ci.shape[0])
+    s.rowpointer, s.columnindex, s.value = _ptr(rp, C.c_int), _ptr(ci, C.c_int), _ptr(v, C.c_double)
+    return s, (rp, ci, v)
+
+
+def _tiles_out(s: SMatrix, ptr_stride: int = TD, csc: bool = False) -> dict:
+    nt = s.numtile
+    d = {
+        "m": s.m, "n": s.n, "nnz": s.nnz, "tilem": s.tilem, "tilen": s.tilen, "numtile": nt,
+        "tile_ptr": _copy(s.tile_ptr, s.tilem + 1, np.int32),
+        "tile_columnidx": _copy(s.tile_columnidx, nt, np.int32),
+        "tile_nnz": _copy(s.tile_nnz, nt + 1, np.int32),
+        "tile_csr_Ptr": _copy(s.tile_csr_Ptr, nt * ptr_stride, np.uint8),
+        "tile_csr_Col": _copy(s.tile_csr_Col, s.nnz, np.uint8),
+        "tile_csr_Value": _copy(s.tile_csr_Value, s.nnz, np.float64),
+    }
+    if s.tile_rowidx:
+        d["tile_rowidx"] = _copy(s.tile_rowidx, nt, np.int32)
+    if s.mask:
+        d["mask"] = _copy(s.mask, nt * ptr_stride, np.uint16)
+    if csc:
+        d["csc_tile_ptr"] = _copy(s.csc_tile_ptr, s.tilen + 1, np.int32)
+        d["csc_tile_rowidx"] = _copy(s.csc_tile_rowidx, nt, np.int32)
+    return d
+
+
+def _tiles_in(t: dict):
+    s = SMatrix()
+    keep = []
+    s.m, s.n, s.nnz = t["m"], t["n"], t["nnz"]
+    s.tilem, s.tilen, s.numtile = t["tilem"], t["tilen"], t["numtile"]
+    for name, ct in [("tile_ptr", C.c_int), ("tile_columnidx", C.c_int), ("tile_rowidx", C.c_int),
+                     ("tile_nnz", C.c_int), ("tile_csr_Value", C.c_double),
+                     ("tile_csr_Col", C.c_ubyte), ("tile_csr_Ptr", C.c_ubyte),
+                     ("mask", C.c_ushort), ("csc_tile_ptr", C.c_int), ("csc_tile_rowidx", C.c_int)]:
+        if name in t:
+            a = np.ascontiguousarray(t[name])
+            if a.size == 0:
+                a = np.zeros(1, dtype=a.dtype)
+            keep.append(a)
+            setattr(s, name, _ptr(a, ct))
+    return s, keep
+
+
+def _destroy(s: SMatrix, owned_csr: bool = False) -> None:
+    lib().rtt_matrix_destroy(C.byref(s), int(owned_csr))
+
+
+def csr2tile_row_major(csr) -> dict:
+    """GPU replacement of csr2tile_row_major (reference src/csr2tile.h:196)."""
+    s, keep = _csr_smatrix(csr)
+    check(lib().rtt_csr2tile_row_major(C.byref(s)))
+    d = _tiles_out(s)
+    _destroy(s)
+    return d
+
+
+def csr2tile_col_major(csr) -> dict:
+    """GPU replacement of csr2tile_col_major (reference src/csr2tile.h:261)."""
+    s, keep = _csr_smatrix(csr)
+    check(lib().rtt_csr2tile_col_major(C.byref(s)))
+    d = _tiles_out(s, csc=True)
+    _destroy(s)
+    return d
+
+
+def spgemm_tile(a_tiles: dict, b_tiles: dict) -> dict:
+    """GPU replacement of spgemm_cpu(A, B, C) (reference src/spgemm-cpu.h:369):
+    A from csr2tile_row_major, B from csr2tile_col_major; returns C's 16x16 tiles."""
+    sa, ka = _tiles_in(a_tiles)
+    sb, kb = _tiles_in(b_tiles)
+    sc = SMatrix()
+    check(lib().rtt_spgemm_tile(C.byref(sa), C.byref(sb), C.byref(sc)))
+    d = _tiles_out(sc)
+    _destroy(sc)
+    return d
+
+
+def tile2csr(tiles: dict, tile_dim: int = 8, canonical: bool = False, new_to_old=None,
+             perm_size: int | None = None):
+    """GPU replacement of tile2csr / tile2csr_restore_rows (reference
+    src/tile2csr.h:232, :337).  Returns a namespace with m, n, rowptr, col, val."""
+    s, keep = _tiles_in(tiles)
+    if new_to_old is None:
+        check(lib().rtt_tile2csr(C.byref(s), tile_dim, int(canonical)))
+    else:
+        p = np.ascontiguousarray(new_to_old, dtype=np.int32)
+        size = p.shape[0] if perm_size is None else perm_size
+        check(lib().rtt_tile2csr_restore_rows(C.byref(s), _ptr(p, C.c_int), size, tile_dim,
+                                              int(canonical)))
+    out = SimpleNamespace(m=s.m, n=s.n, rowptr=_copy(s.rowpointer, s.m + 1, np.int32),
+                          col=_copy(s.columnindex, s.nnz, np.int32),
+                          val=_copy(s.value, s.nnz, np.float64))
+    for name in ("rowpointer", "columnindex", "value"):
+        p = getattr(s, name)
+        if p:
+            _libc_free(C.cast(p, C.c_void_p))
+    return out
+
+
+_LIBC = C.CDLL(None)
+_LIBC.free.argtypes = [C.c_void_p]
+_LIBC.free.restype = None
+
+
+def _libc_free(p) -> None:
+    _LIBC.free(p)
+
+
+def tile16_to_tile8(c_tiles: dict) -> dict:
+    """16x16 C tiles -> the reference's native 8x8 output tiles."""
+    s, keep = _tiles_in(c_tiles)
+    o = SMatrix()
+    check(lib().rtt_tile16_to_tile8(C.byref(s), C.byref(o)))
+    d = _tiles_out(o, ptr_stride=8)
+    _destroy(o)
+    return d
+
+
+class Context:
+    """Device-resident product: device CSR in -> device CSR out, two phases.
+
+    Operands are torch CUDA tensors (int32 row_ptr / col_idx, float64 values);
+    torch only provides device memory and the stream here.
+    """
+
+    def __init__(self, device: int = 0, config: dict | None = None, stream=None):
+        h = C.c_void_p()
+        check(lib().rtt_context_create(C.byref(h), device))
+        self.handle = h
+        self.device = device
+        cfg = Config()
+        lib().rtt_config_default(C.byref(cfg))
+        for k, v in (config or {}).items():
+            setattr(cfg, k, int(v))
+        check(lib().rtt_context_set_config(self.handle, C.byref(cfg)))
+        if stream is not None:
+            check(lib().rtt_context_set_stream(self.handle, C.c_void_p(stream)))
+
+    def close(self):
+        if self.handle:
+            lib().rtt_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int):
+        check(lib().rtt_context_set_stream(self.handle, C.c_void_p(stream_ptr)))
+
+    @staticmethod
+    def _view(rows, cols, rowptr, col, val) -> CsrView:
+        return CsrView(rows, cols, int(col.numel()), rowptr.data_ptr(), col.data_ptr(),
+                       val.data_ptr())
+
+    def symbolic(self, a, b=None, op: int = RTT_OP_AB):
+        """a, b: (rows, cols, rowptr, col, val) with device tensors."""
+        va = self._view(*a)
+        vb = self._view(*b) if b is not None else None
+        nnz = C.c_longlong()
+        tiles = C.c_longlong()
+        check(lib().rtt_spgemm_symbolic(self.handle, C.byref(va), C.byref(vb) if vb else None,
+                                        op, C.byref(nnz), C.byref(tiles)))
+        return nnz.value, tiles.value
+
+    def numeric(self, rowptr, col, val):
+        check(lib().rtt_spgemm_numeric(self.handle, C.c_void_p(rowptr.data_ptr()),
+                                       C.c_void_p(col.data_ptr()), C.c_void_p(val.data_ptr())))
+
+    def stats(self) -> dict:
+        st = Stats()
+        check(lib().rtt_context_get_stats(self.handle, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in Stats._fields_}
+
+    def spgemm_csr_host(self, a, b=None, op: int = RTT_OP_AB):
+        """Host CSR in -> host CSR out through the device path (copies inside)."""
+        sa, ka = _csr_smatrix(a)
+        sb, kb = _csr_smatrix(b) if b is not None else (None, None)
+        sc = SMatrix()
+        check(lib().rtt_spgemm_csr_host(self.handle, C.byref(sa),
+                                        C.byref(sb) if sb is not None else None, op,
+                                        C.byref(sc)))
+        out = CSR(sc.m, sc.n, _copy(sc.rowpointer, sc.m + 1, np.int32),
+                  _copy(sc.columnindex, sc.nnz, np.int32), _copy(sc.value, sc.nnz, np.float64))
+        _destroy(sc, owned_csr=True)
+        return out
+
+
+def spgemm_csr_host(a, b=None, op: int = RTT_OP_AB, device: int = 0) -> CSR:
+    ctx = Context(device)
+    try:
+        return ctx.spgemm_csr_host(a, b, op)
+    finally:
+        ctx.close()

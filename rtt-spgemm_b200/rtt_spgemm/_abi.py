@@ -1,0 +1,133 @@
+"""ctypes binding of librtt_spgemm.so (include/rtt_spgemm.h).
+
+The library is the product: every function here calls one extern "C" entry
+point that runs sm_100a kernels.  If the shared library is missing, loading
+fails loudly - there is no Python or CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+PKG_ROOT = Path(__file__).resolve().parent.parent  # rtt-spgemm_b200/
+LIB_PATH = PKG_ROOT / "librtt_spgemm.so"
+
+RTT_OK = 0
+RTT_OP_AB = 0
+RTT_OP_AAT = 1
+STATUS = {
+    0: "RTT_OK", 1: "RTT_ERR_INVALID_ARGUMENT", 2: "RTT_ERR_INVALID_CSR",
+    3: "RTT_ERR_SHAPE_MISMATCH", 4: "RTT_ERR_OUT_OF_MEMORY", 5: "RTT_ERR_CUDA",
+    6: "RTT_ERR_UNREPRESENTABLE", 7: "RTT_ERR_NO_DEVICE", 8: "RTT_ERR_DEVICE_CHECK",
+    9: "RTT_ERR_INVALID_PERMUTATION", 10: "RTT_ERR_TAIL_NONEMPTY", 11: "RTT_ERR_STATE",
+}
+
+# Every symbol include/rtt_spgemm.h declares.
+EXPORTS = [
+    "rtt_status_string", "rtt_last_error", "rtt_version", "rtt_set_device",
+    "rtt_csr2tile_row_major", "rtt_csr2tile_col_major", "rtt_spgemm_tile", "rtt_tile2csr",
+    "rtt_tile2csr_restore_rows", "rtt_tile16_to_tile8", "rtt_matrix_destroy",
+    "rtt_config_default", "rtt_context_create", "rtt_context_destroy", "rtt_context_set_stream",
+    "rtt_context_set_config", "rtt_context_get_stats", "rtt_spgemm_symbolic",
+    "rtt_spgemm_numeric", "rtt_spgemm_tiles_view", "rtt_spgemm_csr_host",
+]
+
+
+class RttError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class SMatrix(C.Structure):
+    """The reference SMatrix (src/common.h:50-72), byte for byte."""
+
+    _fields_ = [
+        ("m", C.c_int), ("n", C.c_int), ("nnz", C.c_int), ("isSymmetric", C.c_int),
+        ("value", C.POINTER(C.c_double)), ("columnindex", C.POINTER(C.c_int)),
+        ("rowpointer", C.POINTER(C.c_int)),
+        ("tilem", C.c_int), ("tilen", C.c_int),
+        ("tile_ptr", C.POINTER(C.c_int)), ("tile_columnidx", C.POINTER(C.c_int)),
+        ("tile_rowidx", C.POINTER(C.c_int)), ("tile_nnz", C.POINTER(C.c_int)),
+        ("numtile", C.c_int),
+        ("tile_csr_Value", C.POINTER(C.c_double)), ("tile_csr_Col", C.POINTER(C.c_ubyte)),
+        ("tile_csr_Ptr", C.POINTER(C.c_ubyte)), ("mask", C.POINTER(C.c_ushort)),
+        ("csc_tile_ptr", C.POINTER(C.c_int)), ("csc_tile_rowidx", C.POINTER(C.c_int)),
+    ]
+
+
+class CsrView(C.Structure):
+    _fields_ = [("rows", C.c_int), ("cols", C.c_int), ("nnz", C.c_longlong),
+                ("row_ptr", C.c_void_p), ("col_idx", C.c_void_p), ("values", C.c_void_p)]
+
+
+class Config(C.Structure):
+    _fields_ = [("dmma_pair_cutoff", C.c_int), ("fused_csr_output", C.c_int),
+                ("keep_tiles", C.c_int), ("reserved", C.c_int * 8)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("nnz_a", C.c_longlong), ("nnz_b", C.c_longlong), ("nnz_c", C.c_longlong),
+                ("nnz_cub", C.c_longlong), ("tiles_a", C.c_longlong),
+                ("tiles_b", C.c_longlong), ("tiles_c", C.c_longlong),
+                ("dmma_pairs", C.c_longlong), ("sparse_pairs", C.c_longlong),
+                ("kernel_launches", C.c_int), ("host_syncs", C.c_int)]
+
+
+def build(verbose: bool = False) -> Path:
+    """Compile librtt_spgemm.so for sm_100a (nvcc cross-compiles without a GPU)."""
+    out = subprocess.run(["make", "-s", "-j8", "-C", str(PKG_ROOT / "csrc")],
+                         capture_output=not verbose, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("building librtt_spgemm.so failed:\n" + (out.stderr or "")[-4000:])
+    return LIB_PATH
+
+
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    """Load the C-ABI library (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing; build it with rtt_spgemm.build()")
+    L = C.CDLL(str(LIB_PATH))
+    P = C.POINTER
+    L.rtt_status_string.restype = C.c_char_p
+    L.rtt_status_string.argtypes = [C.c_int]
+    L.rtt_last_error.restype = C.c_char_p
+    L.rtt_version.restype = C.c_char_p
+    L.rtt_set_device.argtypes = [C.c_int]
+    for f in ("rtt_csr2tile_row_major", "rtt_csr2tile_col_major"):
+        getattr(L, f).argtypes = [P(SMatrix)]
+    L.rtt_spgemm_tile.argtypes = [P(SMatrix)] * 3
+    L.rtt_tile2csr.argtypes = [P(SMatrix), C.c_int, C.c_int]
+    L.rtt_tile2csr_restore_rows.argtypes = [P(SMatrix), P(C.c_int), C.c_int, C.c_int, C.c_int]
+    L.rtt_tile16_to_tile8.argtypes = [P(SMatrix), P(SMatrix)]
+    L.rtt_matrix_destroy.argtypes = [P(SMatrix), C.c_int]
+    L.rtt_matrix_destroy.restype = None
+    L.rtt_config_default.argtypes = [P(Config)]
+    L.rtt_config_default.restype = None
+    L.rtt_context_create.argtypes = [P(C.c_void_p), C.c_int]
+    L.rtt_context_destroy.argtypes = [C.c_void_p]
+    L.rtt_context_destroy.restype = None
+    L.rtt_context_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.rtt_context_set_config.argtypes = [C.c_void_p, P(Config)]
+    L.rtt_context_get_stats.argtypes = [C.c_void_p, P(Stats)]
+    L.rtt_spgemm_symbolic.argtypes = [C.c_void_p, P(CsrView), P(CsrView), C.c_int,
+                                      P(C.c_longlong), P(C.c_longlong)]
+    L.rtt_spgemm_numeric.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.rtt_spgemm_tiles_view.argtypes = [C.c_void_p, P(SMatrix)]
+    L.rtt_spgemm_csr_host.argtypes = [C.c_void_p, P(SMatrix), P(SMatrix), C.c_int, P(SMatrix)]
+    _LIB = L
+    return L
+
+
+def check(status: int) -> None:
+    if status != RTT_OK:
+        msg = lib().rtt_last_error().decode(errors="replace")
+        raise RttError(status, msg)

@@ -1,0 +1,140 @@
+"""GPU parity of the device-resident CSR -> CSR product (the timed path):
+csr2tile(A, B) -> symbolic -> numeric (fused tile2csr or separate) against the
+FP64 row-SPA oracle.  Structure bit-exact, values within 1e-12 * (|A||B|)_ij.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import rtt_spgemm as R
+from rtt_spgemm import generators as G
+from conftest import assert_csr_close
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _dev(A):
+    d = torch.device("cuda:0")
+    return (A.m, A.n, torch.from_numpy(A.rowptr).to(d), torch.from_numpy(A.col).to(d),
+            torch.from_numpy(A.val).to(d))
+
+
+def _run(ctx, A, B=None, op=R.RTT_OP_AB):
+    nnz, tiles = ctx.symbolic(_dev(A), _dev(B) if B is not None else None, op)
+    d = torch.device("cuda:0")
+    rp = torch.full((A.m + 1,), -7, dtype=torch.int32, device=d)
+    ci = torch.full((max(nnz, 1),), -7, dtype=torch.int32, device=d)
+    va = torch.full((max(nnz, 1),), float("nan"), dtype=torch.float64, device=d)
+    ctx.numeric(rp, ci, va)
+    torch.cuda.synchronize()
+    return rp.cpu().numpy(), ci[:nnz].cpu().numpy(), va[:nnz].cpu().numpy(), nnz, tiles
+
+
+CASES = {
+    "lap2d_256": lambda: G.laplacian_2d(256),
+    "lap2d_ragged": lambda: G.laplacian_2d(37, 11),
+    "stencil27_12": lambda: G.stencil_27(12, 3),
+    "rmat_12": lambda: G.rmat(12, 16, seed=1),
+    "banded": lambda: G.banded_scatter(3000, 40, seed=9),
+    "unsorted": lambda: G.random_csr(300, 300, 0.02, seed=3, sort=False),
+    "duplicates": lambda: G.random_csr(200, 200, 0.03, seed=4, duplicates=0.3),
+    "dense": lambda: G.random_csr(96, 96, 0.85, seed=6),
+}
+
+CONFIGS = {
+    "fused_dmma": dict(fused_csr_output=1, dmma_pair_cutoff=3072),
+    "fused_nodmma": dict(fused_csr_output=1, dmma_pair_cutoff=0),
+    "unfused": dict(fused_csr_output=0, dmma_pair_cutoff=3072),
+    "all_dmma": dict(fused_csr_output=1, dmma_pair_cutoff=1),
+}
+
+
+@pytest.mark.parametrize("cfg", list(CONFIGS))
+@pytest.mark.parametrize("case", list(CASES))
+def test_a_squared(case, cfg, orc):
+    A = CASES[case]()
+    ctx = R.Context(0, CONFIGS[cfg])
+    rp, ci, va, nnz, tiles = _run(ctx, A)
+    erp, ecol, evals, eabs = orc.spgemm_csr(A, A)
+    assert_csr_close(rp, ci, va, erp, ecol, evals, eabs, f"{case}/{cfg}: ")
+    st = ctx.stats()
+    assert st["nnz_c"] == nnz
+    if cfg == "all_dmma" and nnz > 0:
+        assert st["dmma_pairs"] > 0 and st["sparse_pairs"] == 0
+    if cfg == "fused_nodmma":
+        assert st["dmma_pairs"] == 0
+    ctx.close()
+
+
+@pytest.mark.parametrize("case", ["rmat_12", "lap2d_ragged", "banded", "unsorted"])
+def test_a_at(case, orc):
+    A = CASES[case]()
+    ctx = R.Context(0)
+    rp, ci, va, nnz, _ = _run(ctx, A, None, R.RTT_OP_AAT)
+    At = A.transpose()
+    erp, ecol, evals, eabs = orc.spgemm_csr(A, At)
+    assert_csr_close(rp, ci, va, erp, ecol, evals, eabs, f"{case} AAT: ")
+    ctx.close()
+
+
+def test_general_ab(orc):
+    A = G.random_csr(500, 300, 0.02, seed=31)
+    B = G.random_csr(300, 700, 0.015, seed=32)
+    ctx = R.Context(0)
+    rp, ci, va, nnz, _ = _run(ctx, A, B)
+    erp, ecol, evals, eabs = orc.spgemm_csr(A, B)
+    assert_csr_close(rp, ci, va, erp, ecol, evals, eabs, "A*B: ")
+    ctx.close()
+
+
+def test_deterministic_and_reusable(orc):
+    """Two runs on one context give bitwise-identical values (no atomics in
+    the value accumulation), and the context can switch problems."""
+    A = G.stencil_27(10, 5)
+    ctx = R.Context(0)
+    r1 = _run(ctx, A)
+    B = G.laplacian_2d(40)
+    _run(ctx, B)
+    r2 = _run(ctx, A)
+    assert np.array_equal(r1[0], r2[0]) and np.array_equal(r1[1], r2[1])
+    assert np.array_equal(r1[2].view(np.int64), r2[2].view(np.int64))
+    ctx.close()
+
+
+def test_empty_and_tiny(orc):
+    ctx = R.Context(0)
+    for A in (G.CSR(5, 5, np.zeros(6, np.int32), np.zeros(0, np.int32), np.zeros(0)),
+              G.CSR(1, 1, np.array([0, 1], np.int32), np.array([0], np.int32), np.array([3.0]))):
+        rp, ci, va, nnz, _ = _run(ctx, A)
+        erp, ecol, evals, eabs = orc.spgemm_csr(A, A)
+        assert_csr_close(rp, ci, va, erp, ecol, evals, eabs, "tiny: ")
+    ctx.close()
+
+
+def test_host_buffer_entry(orc):
+    A = G.laplacian_2d(100)
+    C = R.spgemm_csr_host(A)
+    erp, ecol, evals, eabs = orc.spgemm_csr(A, A)
+    assert_csr_close(C.rowptr, C.col, C.val, erp, ecol, evals, eabs, "host entry: ")
+
+
+def test_kat_2d_laplacian_closed_form():
+    """C = A^2 of the 5-point Laplacian (diag 4, off -1) on a 256^2 grid:
+    nnz(C) = 846,852; C_ii = 16 + deg(i); distance-1 entries -8; distance-2
+    entries 1 (straight) or 2 (diagonal, two paths)."""
+    nx = 256
+    A = G.laplacian_2d(nx)
+    C = R.spgemm_csr_host(A)
+    assert C.nnz == 846852
+    rows = np.repeat(np.arange(C.m), np.diff(C.rowptr))
+    deg = np.diff(A.rowptr) - 1
+    xi, yi = rows % nx, rows // nx
+    xj, yj = C.col % nx, C.col // nx
+    dx, dy = np.abs(xi - xj), np.abs(yi - yj)
+    expect = np.where((dx == 0) & (dy == 0), 16.0 + deg[rows],
+             np.where(dx + dy == 1, -8.0,
+             np.where((dx == 1) & (dy == 1), 2.0, 1.0)))
+    assert np.array_equal(C.val, expect)

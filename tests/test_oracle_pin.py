@@ -1,0 +1,139 @@
+"""CPU: pin the oracle restatement (oracle/oracle.c) against the reference's
+own CPU code (compiled from its sources into oracle/_ref) and against the
+committed golden fixtures generated from it (tests/golden/make_golden.py).
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from rtt_spgemm import generators as G
+from conftest import assert_tiles_equal
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+CASES = {
+    "lap2d_16": lambda: G.laplacian_2d(16),
+    "lap2d_ragged": lambda: G.laplacian_2d(13, 7),
+    "rand_sorted": lambda: G.random_csr(100, 100, 0.05, seed=1),
+    "rand_rect": lambda: G.random_csr(37, 53, 0.1, seed=2),
+    "unsorted": lambda: G.random_csr(50, 50, 0.1, seed=3, sort=False),
+    "duplicates": lambda: G.random_csr(50, 50, 0.1, seed=4, duplicates=0.3),
+    "stencil27_6": lambda: G.stencil_27(6, 1),
+    "rmat_8": lambda: G.rmat(8, 8, seed=2),
+    "empty_7x9": lambda: G.CSR(7, 9, np.zeros(8, np.int32), np.zeros(0, np.int32), np.zeros(0)),
+}
+ROW_KEYS = ["tilem", "tilen", "numtile", "tile_ptr", "tile_columnidx", "tile_rowidx", "tile_nnz",
+            "tile_csr_Ptr", "tile_csr_Col", "tile_csr_Value", "mask"]
+COL_KEYS = ["tilem", "tilen", "numtile", "tile_ptr", "tile_columnidx", "tile_rowidx", "tile_nnz",
+            "tile_csr_Ptr", "tile_csr_Col", "tile_csr_Value", "mask", "csc_tile_ptr",
+            "csc_tile_rowidx"]
+C_KEYS = ["tile_ptr", "tile_columnidx", "tile_nnz", "tile_csr_Ptr", "tile_csr_Col",
+          "tile_csr_Value", "numtile", "nnz"]
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_csr2tile_restatement_matches_reference(case, orc, ref):
+    A = CASES[case]()
+    assert_tiles_equal(orc.csr2tile_row_major(A), ref.csr2tile_row_major(A), ROW_KEYS, case)
+    assert_tiles_equal(orc.csr2tile_col_major(A), ref.csr2tile_col_major(A), COL_KEYS, case)
+
+
+@pytest.mark.parametrize("case", [k for k in CASES if k not in ("rand_rect", "empty_7x9")])
+def test_spgemm_restatement_matches_reference(case, orc, ref):
+    """With the step-3 quirk reproduced the restatement equals spgemm_cpu bit
+    for bit (values included: both sum in the same order without FMA)."""
+    A = CASES[case]()
+    ra, rb = ref.csr2tile_row_major(A), ref.csr2tile_col_major(A)
+    want = ref.spgemm_cpu(ra, rb)
+    got = orc.spgemm_tile(orc.csr2tile_row_major(A), orc.csr2tile_col_major(A), quirk=True)
+    assert_tiles_equal(got, want, C_KEYS, case)
+
+
+def test_step3_quirk_only_changes_ragged_tile_counts(orc, ref):
+    """On a ragged shape the quirk inflates step-3 counts (tile_nnz) only; the
+    entries step 4 writes are the fixed semantics' entries."""
+    A = G.random_csr(100, 100, 0.05, seed=1)  # n % 16 == 4
+    oa, ob = orc.csr2tile_row_major(A), orc.csr2tile_col_major(A)
+    fixed = orc.spgemm_tile(oa, ob, quirk=False)
+    quirk = orc.spgemm_tile(oa, ob, quirk=True)
+    assert np.array_equal(fixed["tile_ptr"], quirk["tile_ptr"])
+    assert np.array_equal(fixed["tile_columnidx"], quirk["tile_columnidx"])
+    assert not np.array_equal(fixed["tile_nnz"], quirk["tile_nnz"])
+    # every quirk tile holds the fixed tile's entries first, then zero padding
+    for s in range(fixed["numtile"]):
+        fb, fe = fixed["tile_nnz"][s], fixed["tile_nnz"][s + 1]
+        qb = quirk["tile_nnz"][s]
+        assert np.array_equal(fixed["tile_csr_Value"][fb:fe], quirk["tile_csr_Value"][qb:qb + fe - fb])
+
+
+@pytest.mark.parametrize("case", ["lap2d_16", "rmat_8", "duplicates", "lap2d_ragged"])
+def test_tile2csr_restatement_matches_reference(case, orc, ref):
+    A = CASES[case]()
+    c16 = orc.spgemm_tile(orc.csr2tile_row_major(A), orc.csr2tile_col_major(A))
+    c8 = orc.tile16_to_tile8(c16)
+    for canonical in (True, False):
+        got = orc.tile2csr(c8, 8, canonical)
+        want = ref.tile2csr(c8, canonical)
+        assert np.array_equal(got.rowptr, want.rowptr) and np.array_equal(got.col, want.col)
+        assert np.array_equal(got.val, want.val)
+    perm = np.random.default_rng(1).permutation(A.m).astype(np.int32)
+    got = orc.tile2csr(c8, 8, True, new_to_old=perm)
+    want = ref.tile2csr(c8, True, new_to_old=perm)
+    assert np.array_equal(got.rowptr, want.rowptr) and np.array_equal(got.col, want.col)
+
+
+@pytest.mark.parametrize("case", ["lap2d_16", "rmat_8", "duplicates", "stencil27_6"])
+def test_row_spa_matches_reference_serialref(case, orc, ref):
+    """FP64 row SPA vs the reference's spgemm_serialref (dense-row SPA)."""
+    A = CASES[case]()
+    rp, col, val, _ = orc.spgemm_csr(A, A, with_abs=False)
+    wrp, wcol, wval = ref.spgemm_serialref(A, A)
+    assert np.array_equal(rp, wrp.astype(np.int64)) and np.array_equal(col, wcol)
+    assert np.array_equal(val, wval)
+
+
+def test_tile_product_equals_row_spa(orc):
+    """The tile path and the row SPA agree on structure (tile2csr of C)."""
+    A = G.stencil_27(6, 2)
+    c16 = orc.spgemm_tile(orc.csr2tile_row_major(A), orc.csr2tile_col_major(A))
+    csr = orc.tile2csr(c16, 16, True)
+    rp, col, val, ab = orc.spgemm_csr(A, A)
+    assert np.array_equal(csr.rowptr.astype(np.int64), rp) and np.array_equal(csr.col, col)
+    assert np.all(np.abs(csr.val - val) <= 1e-12 * ab)
+
+
+def _golden_files():
+    return sorted(GOLDEN.glob("*.npz"))
+
+
+@pytest.mark.parametrize("path", _golden_files(), ids=lambda p: p.stem)
+def test_oracle_matches_golden_fixture(path, orc):
+    """Fixtures hold the reference's own outputs; the oracle must reproduce them."""
+    z = np.load(path)
+    A = G.CSR(int(z["m"]), int(z["n"]), z["rowptr"], z["col"], z["val"])
+    rm = orc.csr2tile_row_major(A)
+    cm = orc.csr2tile_col_major(A)
+    for k in ROW_KEYS[3:]:
+        assert np.array_equal(rm[k], z["row_" + k]), k
+    for k in COL_KEYS[3:]:
+        assert np.array_equal(cm[k], z["col_" + k]), k
+    if "c_tile_ptr" in z:
+        c = orc.spgemm_tile(rm, cm, quirk=bool(z["quirk"]))
+        for k in ("tile_ptr", "tile_columnidx", "tile_nnz", "tile_csr_Ptr", "tile_csr_Col",
+                  "tile_csr_Value"):
+            assert np.array_equal(c[k], z["c_" + k]), k
+
+
+def test_golden_fixtures_present():
+    assert len(_golden_files()) >= 4
+
+
+def test_kat_2d_closed_form_nnz(orc):
+    A = G.laplacian_2d(256)
+    assert A.nnz == 326656
+    rp, _, _, _ = orc.spgemm_csr(A, A, with_abs=False)
+    assert rp[-1] == 846852
+    assert orc.nnzcub(A, A) == 1629192
