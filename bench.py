@@ -1,0 +1,360 @@
+"""Benchmark of the tiled FP64 SpGEMM path on B200.
+
+One step = one full device-resident product C = A*A of the workload:
+csr2tile(A) (B = A shares A's tiles) -> tile CSC index -> symbolic steps 1-2
+-> allocation of C -> numeric (tile2csr fused) -> device CSR(C).  Inputs are
+resident in HBM when the timed region starts; A's CSR (284 MB for the 3-D
+workload) is larger than L2, so no explicit flush is needed.
+
+Metric: SpGEMM GFLOP/s = 2 * nnzCub / t (nnzCub = sum over (i,k) in A of
+nnz(B row k)), the reference's definition.  Algorithmic bytes follow the
+reference's model 4(m_A+1)+12 nnz_A + 4(m_B+1)+12 nnz_B + 4(m_C+1)+12 nnz_C.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+  python bench.py --impl reference ...   # the reference's CPU code, host cores
+
+Multi-GPU (torchrun): the workload is replicated per rank (independent
+products, no collective on the data path); value = all ranks' flops / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "rtt-spgemm_b200"))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+WORKLOADS = {
+    "stencil27_96": "3-D 27-point stencil, 96^3 grid (n=884,736), C = A^2, natural ordering",
+    "stencil27_96_brick": "3-D 27-point stencil, 96^3 grid, 2x2x4 brick ordering, C = A^2",
+    "laplacian2d_256": "2-D 5-point Laplacian, 256^2 grid (n=65,536), C = A^2",
+}
+
+
+def make_workload(name: str, seed: int):
+    from rtt_spgemm import generators as G
+    if name == "stencil27_96":
+        return G.stencil_27(96, seed)
+    if name == "stencil27_96_brick":
+        return G.stencil_27(96, seed).permute_symmetric(G.brick_permutation(96))
+    if name == "laplacian2d_256":
+        return G.laplacian_2d(256)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def nnz_cub(A) -> int:
+    return int(np.diff(A.rowptr).astype(np.int64)[A.col].sum())
+
+
+def alg_bytes(m, nnz_a, nnz_b, nnz_c) -> int:
+    return 3 * 4 * (m + 1) + 12 * (nnz_a + nnz_b + nnz_c)
+
+
+def load_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def load_traffic(workload: str):
+    p = ROOT / "profiles" / "numeric_traffic.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        e = d.get(workload)
+        if e:
+            return e.get("dram_bytes_per_launch")
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                   "-lms", "100"]
+            if self.uuid:
+                cmd += ["-i", self.uuid]
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(cmd, stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline_port(A, flops: float) -> dict:
+    import oracle
+    orc = oracle.Oracle()
+    t0 = time.perf_counter()
+    orc.spgemm_csr(A, A, with_abs=False)
+    dt = time.perf_counter() - t0
+    return {"value": flops / dt / 1e9, "unit": "GFLOP/s", "cores": orc.threads(), "kind": "port",
+            "sample": "full product, FP64 OpenMP row SPA restating spgemm_serialref "
+                      "(src/external/cusparse/spgemm_serialref_spa.h)", "seconds": dt}
+
+
+def run_reference(args) -> None:
+    """The reference's own CPU SpGEMM (csr2tile_row_major + spgemm_cpu, compiled
+    from its sources), on a bounded sample of the workload's tile rows."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    A = make_workload(args.workload, args.seed)
+    from rtt_spgemm import generators as G
+    if oracle.reference_available():
+        ref = oracle.Reference()
+        b_tiles = ref.csr2tile_col_major(A)  # B prepared once, outside the timed steps
+        rows = min(A.m, args.ref_tile_rows * 16)
+        rp = A.rowptr[: rows + 1].copy()
+        As = G.CSR(rows, A.n, rp, A.col[: rp[-1]].copy(), A.val[: rp[-1]].copy())
+        flops = 2.0 * int(np.diff(A.rowptr).astype(np.int64)[As.col].sum())
+        times = []
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            a_tiles = ref.csr2tile_row_major(As)
+            ref.spgemm_cpu(a_tiles, b_tiles)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                times.append(dt)
+        t = statistics.median(times)
+        kind, cores = "reference", 1
+        sample = (f"first {rows} rows of A ({rows // 16} tile rows) times all of B per step: "
+                  f"csr2tile_row_major(A rows) + spgemm_cpu (src/spgemm-cpu.h:369, serial, with "
+                  f"the in-tile column fix at the call site); B's csr2tile_col_major done once "
+                  f"before timing")
+    else:
+        flops = 2.0 * nnz_cub(A)
+        cb = cpu_baseline_port(A, flops)
+        t, kind, cores, sample = cb["seconds"], "port", cb["cores"], cb["sample"]
+    value = flops / t / 1e9
+    line = {"impl": "reference", "metric": "SpGEMM GFLOP/s", "value": value, "unit": "GFLOP/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": args.workload, "description": WORKLOADS[args.workload]},
+            "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+    import rtt_spgemm as R
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    A = make_workload(args.workload, args.seed)
+    cub = nnz_cub(A)
+    flops = 2.0 * cub
+    stream = torch.cuda.current_stream(dev)
+    ctx = R.Context(local, {"stage_timing": 1, "dmma_pair_cutoff": args.dmma_cutoff,
+                            "fused_csr_output": 0 if args.unfused else 1})
+    ctx.set_stream(stream.cuda_stream)
+    rp = torch.from_numpy(A.rowptr).to(dev)
+    ci = torch.from_numpy(A.col).to(dev)
+    va = torch.from_numpy(A.val).to(dev)
+    a_view = (A.m, A.n, rp, ci, va)
+
+    def step():
+        nnz, _ = ctx.symbolic(a_view)
+        crp = torch.empty(A.m + 1, dtype=torch.int32, device=dev)
+        cci = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+        cva = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
+        ctx.numeric(crp, cci, cva)
+        return nnz
+
+    nnz_c = 0
+    for _ in range(args.warmup):
+        nnz_c = step()
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(dev).uuid)
+        uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    torch.cuda.synchronize(dev)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    stage = {"csr2tile_ms": [], "symbolic_ms": [], "numeric_kernel_ms": []}
+    launches = 0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        nnz_c = step()
+        st = ctx.stats()
+        for k in stage:
+            stage[k].append(st[k])
+        launches += st["kernel_launches"]
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * flops / (ms * 1e-3) / 1e9
+
+    st = ctx.stats()
+    peaks = load_peaks()
+    abytes = alg_bytes(A.m, A.nnz, A.nnz, nnz_c)
+    num_ms = statistics.mean(stage["numeric_kernel_ms"])
+    achieved = abytes / (num_ms * 1e-3) / 1e9
+    traffic = load_traffic(args.workload)
+
+    # end to end through the host-buffer C-ABI call (rtt_spgemm_csr_host):
+    # H2D of A from pinned memory, the product, D2H of C into malloc'd arrays
+    e2e = None
+    if rank == 0 or world > 1:
+        pin_rp = torch.from_numpy(A.rowptr).pin_memory()
+        pin_ci = torch.from_numpy(A.col).pin_memory()
+        pin_va = torch.from_numpy(A.val).pin_memory()
+        Ah = R.CSR(A.m, A.n, pin_rp.numpy(), pin_ci.numpy(), pin_va.numpy())
+        ctx.spgemm_csr_host(Ah)  # warm
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        n_e2e = max(1, min(3, args.steps))
+        e0.record(stream)
+        for _ in range(n_e2e):
+            Ch = ctx.spgemm_csr_host(Ah)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e_ms = e0.elapsed_time(e1) / n_e2e
+        if dist:
+            t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e = {"value": world * flops / (e2e_ms * 1e-3) / 1e9, "unit": "GFLOP/s",
+               "h2d_bytes_per_step": 4 * (A.m + 1) + 12 * A.nnz,
+               "d2h_bytes_per_step": 4 * (A.m + 1) + 12 * int(Ch.nnz), "ms_per_step": e2e_ms}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(A, flops)
+        cpu.pop("seconds", None)
+
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    step_frac = abytes / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"]
+    line = {
+        "metric": "SpGEMM GFLOP/s", "value": value, "unit": "GFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator; no public matrix collection available)",
+        "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
+                   "n": A.m, "nnz_a": A.nnz, "nnz_c": nnz_c, "nnz_cub": cub, "flops": flops,
+                   "tiles_a": st["tiles_a"], "tiles_c": st["tiles_c"],
+                   "alg_bytes": abytes, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (A CSR %.0f MB > 126 MB), no flush" %
+                         ((4 * (A.m + 1) + 12 * A.nnz) / 1e6),
+                   "dmma_pair_cutoff": args.dmma_cutoff, "fused_tile2csr": not args.unfused},
+        "roofline": {"bound": "hbm", "kernel": "k_numeric (numeric + fused tile2csr)",
+                     "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "peak_source": peaks["source"], "kernel_ms": num_ms,
+                     "step_frac": step_frac},
+        "stages_ms": {k: statistics.mean(v) for k, v in stage.items()},
+        "dmma_pairs": st["dmma_pairs"], "sparse_pairs": st["sparse_pairs"],
+        "host_syncs_per_step": st["host_syncs"],
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="stencil27_96", choices=list(WORKLOADS))
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--dmma-cutoff", type=int, default=3072)
+    ap.add_argument("--unfused", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-tile-rows", type=int, default=256)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

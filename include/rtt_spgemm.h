@@ -210,8 +210,11 @@ typedef struct
     /* Keep C's 16x16 tile arrays on the device after numeric (needed for
      * rtt_spgemm_tiles_view); implied when fused_csr_output == 0. */
     int keep_tiles;
+    /* Record CUDA events around the stages (csr2tile, symbolic, numeric
+     * kernel) on the context's stream; results land in rtt_stats. */
+    int stage_timing;
     /* Reserved, must be zero. */
-    int reserved[8];
+    int reserved[7];
 } rtt_config;
 
 RTT_API void rtt_config_default(rtt_config *config);
@@ -230,6 +233,12 @@ typedef struct
     long long sparse_pairs;
     int kernel_launches; /* kernels launched by the last symbolic+numeric */
     int host_syncs;      /* stream synchronisations in the last symbolic */
+    /* Stage times of the last product in ms (stage_timing != 0, else 0):
+     * csr2tile of A and B + tile CSC index, symbolic steps 1-2 with their
+     * scans, and the numeric kernel alone. */
+    double csr2tile_ms;
+    double symbolic_ms;
+    double numeric_kernel_ms;
 } rtt_stats;
 
 /* A context owns a CUDA stream handle (borrowed), workspace and the state

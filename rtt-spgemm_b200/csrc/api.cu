@@ -92,22 +92,26 @@ int download(T **out, const void *d, size_t n, cudaStream_t s)
     return RTT_OK;
 }
 
-// Free a set of host arrays on failure paths.
+// Free a set of host arrays on failure paths.  Slots live in a fixed array so
+// the pointers handed out stay valid while more slots are taken.
 struct HostArrays
 {
-    std::vector<void *> ptrs;
+    static constexpr int kMax = 16;
+    void *ptrs[kMax] = {};
+    int used = 0;
     bool committed = false;
     template <typename T>
     T **slot()
     {
-        ptrs.push_back(nullptr);
-        return reinterpret_cast<T **>(&ptrs.back());
+        if (used >= kMax)
+            std::abort(); // programming error: raise kMax
+        return reinterpret_cast<T **>(&ptrs[used++]);
     }
     ~HostArrays()
     {
         if (!committed)
-            for (void *p : ptrs)
-                std::free(p);
+            for (int i = 0; i < used; ++i)
+                std::free(ptrs[i]);
     }
 };
 
@@ -700,8 +704,10 @@ int rtt_tile2csr_restore_rows(SMatrix *M, const int *new_to_old, int perm_size, 
     {
         // tile lists: monotone pointers, in-range entry offsets (columns are
         // range-checked per entry by the kernels, as the reference does)
+        // row offsets are clamped per row by the kernels (as the reference
+        // does), so only the per-tile entry ranges are checked here
         k_validate_tile_data<<<grid_for(nt > 0 ? nt : 1, 256), 256, 0, s>>>(
-            nt, T.tile_nnz.as<int>(), (int)nent, tile_dim, T.ptr.as<uint8_t>(), c->ws.err.as<int>());
+            nt, T.tile_nnz.as<int>(), (int)nent, 0, T.ptr.as<uint8_t>(), c->ws.err.as<int>());
         k_validate_ptr<<<grid_for(tilem + 1, 256), 256, 0, s>>>(tilem, T.tile_ptr.as<int>(), nt,
                                                                 c->ws.err.as<int>());
         c->ws.launches += 2;
@@ -800,6 +806,9 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
     c->ws.syncs = 0;
     std::memset(&c->stats, 0, sizeof(c->stats));
     Workspace &ws = c->ws;
+    const bool timing = c->cfg.stage_timing != 0;
+    if (timing)
+        RTT_CUDA(cudaEventRecord(ws.ev[0], ws.stream));
     RTT_CHECK(map_device_error(csr2tile_device(ws, A->rows, A->cols, (int)A->nnz, A->row_ptr,
                                                A->col_idx, A->values, c->A, true, false)));
     if (op == RTT_OP_AB && B == nullptr)
@@ -834,7 +843,19 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
         RTT_CHECK(build_tile_csc(ws, c->B));
     }
     const TileBufs &TB = c->b_alias ? c->A : c->B;
+    if (timing)
+        RTT_CUDA(cudaEventRecord(ws.ev[1], ws.stream));
     RTT_CHECK(map_device_error(symbolic_device(ws, c->A.view(), TB.view(), c->S)));
+    if (timing)
+    {
+        float t01 = 0.f, t12 = 0.f;
+        RTT_CUDA(cudaEventRecord(ws.ev[2], ws.stream));
+        RTT_CUDA(cudaEventSynchronize(ws.ev[2]));
+        RTT_CUDA(cudaEventElapsedTime(&t01, ws.ev[0], ws.ev[1]));
+        RTT_CUDA(cudaEventElapsedTime(&t12, ws.ev[1], ws.ev[2]));
+        c->stats.csr2tile_ms = t01;
+        c->stats.symbolic_ms = t12;
+    }
     c->stats.nnz_a = c->A.nnz;
     c->stats.nnz_b = TB.nnz;
     c->stats.nnz_c = c->S.nnz;
@@ -866,6 +887,11 @@ int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_
     NumericConfig nc;
     nc.dmma_pair_cutoff = c->cfg.dmma_pair_cutoff;
     nc.counters = c->counters.as<long long>();
+    if (c->cfg.stage_timing)
+    {
+        nc.ev_begin = ws.ev[3];
+        nc.ev_end = ws.ev[4];
+    }
     const bool fused = c->cfg.fused_csr_output != 0;
     nc.write_tiles = !fused || c->cfg.keep_tiles != 0;
     if (fused)
@@ -888,6 +914,12 @@ int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_
     RTT_CUDA(cudaMemcpyAsync(ws.h_scalars64 + 2, c->counters.p, sizeof(long long) * 2,
                              cudaMemcpyDeviceToHost, ws.stream));
     RTT_CHECK(check_device_error(ws, "numeric"));
+    if (c->cfg.stage_timing && c->S.numtile > 0)
+    {
+        float tn = 0.f;
+        RTT_CUDA(cudaEventElapsedTime(&tn, ws.ev[3], ws.ev[4]));
+        c->stats.numeric_kernel_ms = tn;
+    }
     c->stats.dmma_pairs = ws.h_scalars64[2];
     c->stats.sparse_pairs = ws.h_scalars64[3];
     c->stats.kernel_launches = ws.launches;

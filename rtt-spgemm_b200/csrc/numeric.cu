@@ -321,6 +321,8 @@ int numeric_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symbolic
     if (nt == 0)
         return RTT_OK;
     const int grid = (int)((nt + NUM_WARPS - 1) / NUM_WARPS);
+    if (cfg.ev_begin != nullptr)
+        RTT_CUDA(cudaEventRecord(cfg.ev_begin, s));
     if (cfg.dmma_pair_cutoff > 0)
     {
         const size_t smem = sizeof(NumSmemDense) * NUM_WARPS;
@@ -346,6 +348,8 @@ int numeric_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symbolic
             cfg.csr_col, cfg.csr_val, 0, cfg.counters, ws.err.as<int>());
     }
     ws.launches++;
+    if (cfg.ev_end != nullptr)
+        RTT_CUDA(cudaEventRecord(cfg.ev_end, s));
     return RTT_OK;
 }
 

@@ -28,6 +28,7 @@ enum DeviceError : int
     DERR_NUM_BOUNDS = 106,      // numeric output index out of range
     DERR_T2C_BOUNDS = 107,      // tile2csr output index out of range
     DERR_WINDOW = 108,          // symbolic window bookkeeping failed
+    DERR_T2C_TAIL = 109,        // tile2csr: row past the permutation prefix not empty
 };
 
 __device__ __forceinline__ void set_error(int *err, int code)
@@ -198,6 +199,7 @@ struct Workspace
     long long *h_scalars64 = nullptr; // pinned, 8 long long
     int launches = 0;
     int syncs = 0;
+    cudaEvent_t ev[6] = {};  // stage timing events (recorded on stream)
     int init(int dev);
     void destroy();
 };
@@ -260,6 +262,8 @@ struct NumericConfig
     int *csr_col = nullptr;
     double *csr_val = nullptr;
     long long *counters = nullptr; // device [0] dmma pairs, [1] sparse pairs
+    cudaEvent_t ev_begin = nullptr; // recorded around the numeric kernel when set
+    cudaEvent_t ev_end = nullptr;
 };
 
 int numeric_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,

@@ -97,6 +97,9 @@ int Workspace::init(int dev)
         RTT_CUDA(cudaMallocHost(&h_scalars, sizeof(int) * 16));
         RTT_CUDA(cudaMallocHost(&h_scalars64, sizeof(long long) * 8));
     }
+    for (cudaEvent_t &e : ev)
+        if (e == nullptr)
+            RTT_CUDA(cudaEventCreate(&e));
     return RTT_OK;
 }
 
@@ -110,6 +113,12 @@ void Workspace::destroy()
         cudaFreeHost(h_scalars64);
     h_scalars = nullptr;
     h_scalars64 = nullptr;
+    for (cudaEvent_t &e : ev)
+        if (e != nullptr)
+        {
+            cudaEventDestroy(e);
+            e = nullptr;
+        }
 }
 
 namespace

@@ -64,7 +64,7 @@ __global__ void k_t2c_count(const int *__restrict__ tile_ptr, const int *__restr
     else if (row >= perm_size)
     {
         if (cnt != 0)
-            set_error(err, DERR_T2C_BOUNDS);
+            set_error(err, DERR_T2C_TAIL);
     }
     else
         row_cnt[new_to_old[row]] = cnt;

@@ -65,7 +65,7 @@ class CsrView(C.Structure):
 
 class Config(C.Structure):
     _fields_ = [("dmma_pair_cutoff", C.c_int), ("fused_csr_output", C.c_int),
-                ("keep_tiles", C.c_int), ("reserved", C.c_int * 8)]
+                ("keep_tiles", C.c_int), ("stage_timing", C.c_int), ("reserved", C.c_int * 7)]
 
 
 class Stats(C.Structure):
@@ -73,7 +73,9 @@ class Stats(C.Structure):
                 ("nnz_cub", C.c_longlong), ("tiles_a", C.c_longlong),
                 ("tiles_b", C.c_longlong), ("tiles_c", C.c_longlong),
                 ("dmma_pairs", C.c_longlong), ("sparse_pairs", C.c_longlong),
-                ("kernel_launches", C.c_int), ("host_syncs", C.c_int)]
+                ("kernel_launches", C.c_int), ("host_syncs", C.c_int),
+                ("csr2tile_ms", C.c_double), ("symbolic_ms", C.c_double),
+                ("numeric_kernel_ms", C.c_double)]
 
 
 def build(verbose: bool = False) -> Path:
