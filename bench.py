@@ -37,6 +37,7 @@ WORKLOADS = {
     "stencil27_96": "3-D 27-point stencil, 96^3 grid (n=884,736), C = A^2, natural ordering",
     "stencil27_96_brick": "3-D 27-point stencil, 96^3 grid, 2x2x4 brick ordering, C = A^2",
     "laplacian2d_256": "2-D 5-point Laplacian, 256^2 grid (n=65,536), C = A^2",
+    "stencil27_80": "3-D 27-point stencil, 80^3 grid (n=512,000), C = A^2 (profiling size)",
 }
 
 
@@ -48,6 +49,8 @@ def make_workload(name: str, seed: int):
         return G.stencil_27(96, seed).permute_symmetric(G.brick_permutation(96))
     if name == "laplacian2d_256":
         return G.laplacian_2d(256)
+    if name == "stencil27_80":
+        return G.stencil_27(80, seed)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -210,7 +213,8 @@ def run_ours(args) -> None:
     flops = 2.0 * cub
     stream = torch.cuda.current_stream(dev)
     ctx = R.Context(local, {"stage_timing": 1, "dmma_pair_cutoff": args.dmma_cutoff,
-                            "fused_csr_output": 0 if args.unfused else 1})
+                            "fused_csr_output": 0 if args.unfused else 1,
+                            "b_staging": 0 if args.no_staging else 1})
     ctx.set_stream(stream.cuda_stream)
     rp = torch.from_numpy(A.rowptr).to(dev)
     ci = torch.from_numpy(A.col).to(dev)
@@ -273,7 +277,7 @@ def run_ours(args) -> None:
     # end to end through the host-buffer C-ABI call (rtt_spgemm_csr_host):
     # H2D of A from pinned memory, the product, D2H of C into malloc'd arrays
     e2e = None
-    if rank == 0 or world > 1:
+    if not args.no_e2e:
         pin_rp = torch.from_numpy(A.rowptr).pin_memory()
         pin_ci = torch.from_numpy(A.col).pin_memory()
         pin_va = torch.from_numpy(A.val).pin_memory()
@@ -318,7 +322,8 @@ def run_ours(args) -> None:
                    "alg_bytes": abytes, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (A CSR %.0f MB > 126 MB), no flush" %
                          ((4 * (A.m + 1) + 12 * A.nnz) / 1e6),
-                   "dmma_pair_cutoff": args.dmma_cutoff, "fused_tile2csr": not args.unfused},
+                   "dmma_pair_cutoff": args.dmma_cutoff, "fused_tile2csr": not args.unfused,
+                   "b_staging": not args.no_staging},
         "roofline": {"bound": "hbm", "kernel": "k_numeric (numeric + fused tile2csr)",
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
@@ -346,6 +351,8 @@ def main() -> None:
     ap.add_argument("--dmma-cutoff", type=int, default=3072)
     ap.add_argument("--unfused", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-staging", action="store_true")
     ap.add_argument("--ref-tile-rows", type=int, default=256)
     args = ap.parse_args()
     if args.warmup < 3:

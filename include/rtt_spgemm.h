@@ -213,8 +213,11 @@ typedef struct
     /* Record CUDA events around the stages (csr2tile, symbolic, numeric
      * kernel) on the context's stream; results land in rtt_stats. */
     int stage_timing;
+    /* How the numeric step reads B tile rows: 1 = TMA bulk copies into a
+     * shared-memory ring (default), 0 = direct loads through L1/L2. */
+    int b_staging;
     /* Reserved, must be zero. */
-    int reserved[7];
+    int reserved[6];
 } rtt_config;
 
 RTT_API void rtt_config_default(rtt_config *config);

@@ -26,11 +26,18 @@ struct rtt_context_s
     rtt::DevBuf in2_rp, in2_col, in2_val;
     rtt::DevBuf out_rp, out_col, out_val;  // host-buffer product output
     rtt::DevBuf counters;
+    rtt::DevBuf maxnnz;
     rtt::SymbolicOut S;
     rtt_stats stats;
     bool have_symbolic = false;
     bool b_alias = false;
     bool owns_stream = false;
+    // B as scalar CSR rows for the numeric step (borrowed or owned above)
+    const int *b_rp = nullptr;
+    const int *b_ci = nullptr;
+    const double *b_va = nullptr;
+    long long b_nnz = 0;
+    bool b_dups = false;
 };
 
 namespace
@@ -375,6 +382,26 @@ int upload_tiles(rtt_context c, const SMatrix *M, bool col_major, TileBufs &T)
     return RTT_OK;
 }
 
+// The DMMA variant of the numeric kernel reserves extra shared memory; use it
+// only when some tile pair can reach the configured cutoff.
+int effective_cutoff(rtt_context c, const DevTiles &A, const DevTiles &B, int *cutoff)
+{
+    *cutoff = c->cfg.dmma_pair_cutoff;
+    if (*cutoff <= 0)
+        return RTT_OK;
+    RTT_CHECK(c->counters.ensure(sizeof(long long) * 4, c->ws.stream));
+    RTT_CHECK(c->maxnnz.ensure(sizeof(int) * 2, c->ws.stream));
+    RTT_CHECK(max_tile_nnz_device(c->ws, A.tile_nnz, A.numtile, c->maxnnz.as<int>()));
+    RTT_CHECK(max_tile_nnz_device(c->ws, B.tile_nnz, B.numtile, c->maxnnz.as<int>() + 1));
+    RTT_CUDA(cudaMemcpyAsync(c->ws.h_scalars + 10, c->maxnnz.p, sizeof(int) * 2,
+                             cudaMemcpyDeviceToHost, c->ws.stream));
+    RTT_CUDA(cudaStreamSynchronize(c->ws.stream));
+    c->ws.syncs++;
+    if ((long long)c->ws.h_scalars[10] * c->ws.h_scalars[11] < (long long)*cutoff)
+        *cutoff = 0;
+    return RTT_OK;
+}
+
 DevTiles view_with_rowdata(const TileBufs &T)
 {
     DevTiles v = T.view();
@@ -432,6 +459,7 @@ void rtt_config_default(rtt_config *config)
     config->dmma_pair_cutoff = 3072;
     config->fused_csr_output = 1;
     config->keep_tiles = 0;
+    config->b_staging = 1;
 }
 
 int rtt_set_device(int device)
@@ -480,7 +508,7 @@ void rtt_context_destroy(rtt_context c)
     c->S.release();
     rtt::DevBuf *bufs[] = {&c->bt_rowptr, &c->bt_col, &c->bt_val, &c->in_rp, &c->in_col,
                            &c->in_val, &c->in2_rp, &c->in2_col, &c->in2_val, &c->out_rp,
-                           &c->out_col, &c->out_val, &c->counters};
+                           &c->out_col, &c->out_val, &c->counters, &c->maxnnz};
     for (rtt::DevBuf *b : bufs)
         b->release();
     c->ws.destroy();
@@ -623,10 +651,36 @@ int rtt_spgemm_tile(SMatrix *A, SMatrix *B, SMatrix *C)
     const DevTiles dA = view_with_rowdata(c->A);
     DevTiles dB = view_with_rowdata(c->B);
     RTT_CHECK(map_device_error(symbolic_device(c->ws, dA, dB, c->S)));
+    // B's scalar CSR rows for the numeric step, assembled on the device from
+    // the column-major tiles (tile2csr through the row->data index)
+    {
+        cudaStream_t s = c->ws.stream;
+        const int mb = B->m;
+        RTT_CHECK(c->in2_rp.ensure(sizeof(int) * ((size_t)mb + 2), s));
+        RTT_CHECK(c->in_col.ensure(sizeof(int) * ((size_t)mb + 2), s));
+        int *cnt = c->in_col.as<int>();
+        RTT_CHECK(tile2csr_count_device(c->ws, dB.tile_ptr, dB.tile_col, dB.tile_nnz, dB.ptr,
+                                        dB.col, mb, B->n, dB.tilem, TD, nullptr, -1, cnt,
+                                        dB.row_data));
+        RTT_CHECK(scan_exclusive_int(c->ws, cnt, c->in2_rp.as<int>(), mb));
+        int bnnz = 0;
+        RTT_CHECK(read_int(c->ws, c->in2_rp.as<int>() + mb, &bnnz));
+        RTT_CHECK(c->in2_col.ensure(sizeof(int) * (size_t)bnnz + 16, s));
+        RTT_CHECK(c->in2_val.ensure(sizeof(double) * (size_t)bnnz + 16, s));
+        RTT_CHECK(tile2csr_fill_device(c->ws, dB.tile_ptr, dB.tile_col, dB.tile_nnz, dB.ptr, dB.col,
+                                       dB.val, mb, B->n, dB.tilem, TD, nullptr, -1,
+                                       c->in2_rp.as<int>(), c->in2_col.as<int>(),
+                                       c->in2_val.as<double>(), false, dB.row_data));
+        dB.csr_rowptr = c->in2_rp.as<int>();
+        dB.csr_col = c->in2_col.as<int>();
+        dB.csr_val = c->in2_val.as<double>();
+        dB.nnz = bnnz;
+    }
     NumericConfig nc;
-    nc.dmma_pair_cutoff = c->cfg.dmma_pair_cutoff;
+    RTT_CHECK(effective_cutoff(c, dA, dB, &nc.dmma_pair_cutoff));
     nc.write_tiles = true;
-    RTT_CHECK(numeric_device(c->ws, dA, dB, c->S, nc));
+    nc.conflict_safe = true; // caller tiles may repeat a coordinate
+    RTT_CHECK(numeric_rows_device(c->ws, dA, dB, c->S, nc));
     RTT_CHECK(check_device_error(c->ws, "spgemm_tile numeric"));
     cudaStream_t s = c->ws.stream;
     SymbolicOut &S = c->S;
@@ -817,6 +871,11 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
             return rtt::fail(RTT_ERR_SHAPE_MISMATCH, "A*A needs a square A");
         c->b_alias = true;
         RTT_CHECK(build_tile_csc(ws, c->A));
+        c->b_rp = A->row_ptr;
+        c->b_ci = A->col_idx;
+        c->b_va = A->values;
+        c->b_nnz = A->nnz;
+        c->b_dups = c->A.dup_cols;
     }
     else
     {
@@ -829,6 +888,10 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
             RTT_CHECK(map_device_error(csr2tile_device(ws, A->cols, A->rows, (int)A->nnz,
                                                        c->bt_rowptr.as<int>(), c->bt_col.as<int>(),
                                                        c->bt_val.as<double>(), c->B, true, false)));
+            c->b_rp = c->bt_rowptr.as<int>();
+            c->b_ci = c->bt_col.as<int>();
+            c->b_va = c->bt_val.as<double>();
+            c->b_nnz = A->nnz;
         }
         else
         {
@@ -839,7 +902,12 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
             RTT_CHECK(map_device_error(csr2tile_device(ws, B->rows, B->cols, (int)B->nnz,
                                                        B->row_ptr, B->col_idx, B->values, c->B,
                                                        true, false)));
+            c->b_rp = B->row_ptr;
+            c->b_ci = B->col_idx;
+            c->b_va = B->values;
+            c->b_nnz = B->nnz;
         }
+        c->b_dups = c->B.dup_cols;
         RTT_CHECK(build_tile_csc(ws, c->B));
     }
     const TileBufs &TB = c->b_alias ? c->A : c->B;
@@ -885,8 +953,9 @@ int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_
     RTT_CHECK(c->counters.ensure(sizeof(long long) * 4, ws.stream));
     RTT_CUDA(cudaMemsetAsync(c->counters.p, 0, sizeof(long long) * 4, ws.stream));
     NumericConfig nc;
-    nc.dmma_pair_cutoff = c->cfg.dmma_pair_cutoff;
+    RTT_CHECK(effective_cutoff(c, c->A.view(), TB.view(), &nc.dmma_pair_cutoff));
     nc.counters = c->counters.as<long long>();
+    nc.b_staging = c->cfg.b_staging != 0;
     if (c->cfg.stage_timing)
     {
         nc.ev_begin = ws.ev[3];
@@ -900,7 +969,13 @@ int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_
         nc.csr_col = c_col_idx;
         nc.csr_val = c_values;
     }
-    RTT_CHECK(numeric_device(ws, c->A.view(), TB.view(), c->S, nc));
+    DevTiles dB = TB.view();
+    dB.csr_rowptr = c->b_rp;
+    dB.csr_col = c->b_ci;
+    dB.csr_val = c->b_va;
+    dB.nnz = (int)c->b_nnz;
+    nc.conflict_safe = c->b_dups;
+    RTT_CHECK(numeric_rows_device(ws, c->A.view(), dB, c->S, nc));
     if (!fused)
     {
         SymbolicOut &S = c->S;

@@ -45,7 +45,7 @@ __global__ void k_validate_csr(int m, int n, int nnz, const int *__restrict__ ro
         return;
     }
     int prev = -1;
-    bool tile_dec = false, col_dec = false;
+    bool tile_dec = false, col_dec = false, col_dup = false;
     for (int j = b; j < e; ++j)
     {
         int c = col[j];
@@ -60,6 +60,8 @@ __global__ void k_validate_csr(int m, int n, int nnz, const int *__restrict__ ro
                 tile_dec = true;
             if (c < prev)
                 col_dec = true;
+            if (c == prev)
+                col_dup = true;
         }
         prev = c;
     }
@@ -67,6 +69,8 @@ __global__ void k_validate_csr(int m, int n, int nnz, const int *__restrict__ ro
         atomicOr(&flags[0], 1);
     if (col_dec)
         atomicOr(&flags[1], 1);
+    if (col_dup)
+        atomicOr(&flags[2], 1);
 }
 
 // -------------------------------------------------------------- fast path
@@ -487,7 +491,7 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
     RTT_CHECK(out.tmp0.ensure(sizeof(int) * (tilem + 1), s));
     RTT_CHECK(out.tmp1.ensure(sizeof(int) * 4, s));
     int *flags = out.tmp1.as<int>();
-    RTT_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * 2, s));
+    RTT_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * 3, s));
     if (m == 0)
     {
         RTT_CUDA(cudaMemsetAsync(out.tile_ptr.p, 0, sizeof(int), s));
@@ -506,10 +510,12 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
     k_validate_csr<<<grid_for(m, 256), 256, 0, s>>>(m, n, nnz, rowptr, col, ws.err.as<int>(),
                                                     flags);
     ws.launches++;
-    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 4, flags, sizeof(int) * 2, cudaMemcpyDeviceToHost, s));
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 4, flags, sizeof(int) * 3, cudaMemcpyDeviceToHost, s));
     RTT_CHECK(check_device_error(ws, "csr2tile validate"));
     const bool generic = ws.h_scalars[4] != 0;
     const bool unsorted = ws.h_scalars[5] != 0;
+    // rows that are unsorted may hide repeated columns too
+    out.dup_cols = ws.h_scalars[6] != 0 || unsorted;
 
     int *cnt = out.tmp0.as<int>();
     if (!generic)

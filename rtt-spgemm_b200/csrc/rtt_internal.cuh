@@ -55,6 +55,11 @@ struct DevTiles
     const int *csc_ptr;     // tilen + 1
     const int *csc_row;     // numtile
     const int *csc_data;    // numtile (nullptr = identity)
+    // the same matrix as scalar CSR rows (B side of the numeric step; the
+    // row-k segments of B tile row K concatenated in column order)
+    const int *csr_rowptr;  // m + 1
+    const int *csr_col;     // nnz
+    const double *csr_val;  // nnz
 };
 
 // C tile structure produced by the symbolic phase.
@@ -222,6 +227,7 @@ struct TileBufs
     DevBuf csc_ptr, csc_row, csc_data, row_data;
     DevBuf tmp0, tmp1, tmp2, tmp3;
     int m = 0, n = 0, tilem = 0, tilen = 0, numtile = 0, nnz = 0;
+    bool dup_cols = false; // some row may repeat a column (set by csr2tile_device)
     void release();
     DevTiles view() const;
 };
@@ -257,6 +263,7 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
 struct NumericConfig
 {
     int dmma_pair_cutoff = 3072;
+    bool b_staging = true;          // TMA staging of B tile rows in the numeric step
     bool write_tiles = true;
     int *csr_rowptr = nullptr;  // fused CSR output when csr_col != nullptr
     int *csr_col = nullptr;
@@ -264,22 +271,28 @@ struct NumericConfig
     long long *counters = nullptr; // device [0] dmma pairs, [1] sparse pairs
     cudaEvent_t ev_begin = nullptr; // recorded around the numeric kernel when set
     cudaEvent_t ev_end = nullptr;
+    bool conflict_safe = false;     // B rows may repeat a column: accumulate with shared atomics
 };
 
 int numeric_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
                    const NumericConfig &cfg);
 // CSR row pointer of C (m + 1 ints) from the symbolic counts
 int csr_rowptr_device(Workspace &ws, SymbolicOut &S, int *rowptr);
+// numeric step, one CTA per C tile row (TMA-staged B tile rows)
+int numeric_rows_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
+                        const NumericConfig &cfg);
+// largest per-tile entry count of a tile matrix (device scalar *out)
+int max_tile_nnz_device(Workspace &ws, const int *tile_nnz, int numtile, int *out);
 
 // tile2csr on device tiles of edge td.  Writes rowptr (m + 1) then col/val.
 int tile2csr_count_device(Workspace &ws, const int *tile_ptr, const int *tile_col,
                           const int *tile_nnz, const uint8_t *ptr, const uint8_t *col, int m,
                           int n, int tilem, int td, const int *new_to_old, int perm_size,
-                          int *rowptr_out);
+                          int *rowptr_out, const int *row_data = nullptr);
 int tile2csr_fill_device(Workspace &ws, const int *tile_ptr, const int *tile_col,
                          const int *tile_nnz, const uint8_t *ptr, const uint8_t *col,
                          const double *val, int m, int n, int tilem, int td,
                          const int *new_to_old, int perm_size, const int *rowptr, int *out_col,
-                         double *out_val, bool sort_rows);
+                         double *out_val, bool sort_rows, const int *row_data = nullptr);
 
 } // namespace rtt

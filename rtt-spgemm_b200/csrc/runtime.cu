@@ -225,6 +225,9 @@ DevTiles TileBufs::view() const
     t.csc_ptr = csc_ptr.as<int>();
     t.csc_row = csc_row.as<int>();
     t.csc_data = csc_data.as<int>();
+    t.csr_rowptr = nullptr;
+    t.csr_col = nullptr;
+    t.csr_val = nullptr;
     return t;
 }
 

@@ -35,7 +35,7 @@ __global__ void k_t2c_count(const int *__restrict__ tile_ptr, const int *__restr
                             const int *__restrict__ tile_nnz, const uint8_t *__restrict__ ptr,
                             const uint8_t *__restrict__ col, int m, int n, int tilem, int td,
                             const int *__restrict__ new_to_old, int perm_size,
-                            int *__restrict__ row_cnt, int *err)
+                            const int *__restrict__ row_data, int *__restrict__ row_cnt, int *err)
 {
     const long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int tr = (int)(x / td), lr = (int)(x % td);
@@ -48,10 +48,11 @@ __global__ void k_t2c_count(const int *__restrict__ tile_ptr, const int *__restr
     int cnt = 0;
     for (int t = tile_ptr[tr]; t < tile_ptr[tr + 1]; ++t)
     {
-        const int tnz = tile_nnz[t + 1] - tile_nnz[t], off = tile_nnz[t];
+        const int d = row_data ? row_data[t] : t; // data index of row-major tile t
+        const int tnz = tile_nnz[d + 1] - tile_nnz[d], off = tile_nnz[d];
         const int tc = tile_col[t];
         int s, e;
-        t2c_bounds(ptr, (size_t)t * td, lr, rc, tnz, s, e);
+        t2c_bounds(ptr, (size_t)d * td, lr, rc, tnz, s, e);
         for (int i = s; i < e; ++i)
         {
             const int lc = col[off + i];
@@ -74,7 +75,8 @@ __global__ void k_t2c_fill(const int *__restrict__ tile_ptr, const int *__restri
                            const int *__restrict__ tile_nnz, const uint8_t *__restrict__ ptr,
                            const uint8_t *__restrict__ col, const double *__restrict__ val, int m,
                            int n, int tilem, int td, const int *__restrict__ new_to_old,
-                           int perm_size, const int *__restrict__ rowptr, long long nnz,
+                           int perm_size, const int *__restrict__ row_data,
+                           const int *__restrict__ rowptr, long long nnz,
                            int *__restrict__ out_col, double *__restrict__ out_val, int *err)
 {
     const long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -96,10 +98,11 @@ __global__ void k_t2c_fill(const int *__restrict__ tile_ptr, const int *__restri
     const long long oend = rowptr[dst_row + 1];
     for (int t = tile_ptr[tr]; t < tile_ptr[tr + 1]; ++t)
     {
-        const int tnz = tile_nnz[t + 1] - tile_nnz[t], off = tile_nnz[t];
+        const int d = row_data ? row_data[t] : t; // data index of row-major tile t
+        const int tnz = tile_nnz[d + 1] - tile_nnz[d], off = tile_nnz[d];
         const int tc = tile_col[t];
         int s, e;
-        t2c_bounds(ptr, (size_t)t * td, lr, rc, tnz, s, e);
+        t2c_bounds(ptr, (size_t)d * td, lr, rc, tnz, s, e);
         for (int i = s; i < e; ++i)
         {
             const int lc = col[off + i];
@@ -168,14 +171,14 @@ inline int grid_for(long long threads, int block) { return (int)((threads + bloc
 int tile2csr_count_device(Workspace &ws, const int *tile_ptr, const int *tile_col,
                           const int *tile_nnz, const uint8_t *ptr, const uint8_t *col, int m,
                           int n, int tilem, int td, const int *new_to_old, int perm_size,
-                          int *row_cnt)
+                          int *row_cnt, const int *row_data)
 {
     RTT_CUDA(cudaMemsetAsync(row_cnt, 0, sizeof(int) * (size_t)(m + 1), ws.stream));
     if (tilem > 0)
     {
         k_t2c_count<<<grid_for((long long)tilem * td, 256), 256, 0, ws.stream>>>(
-            tile_ptr, tile_col, tile_nnz, ptr, col, m, n, tilem, td, new_to_old, perm_size, row_cnt,
-            ws.err.as<int>());
+            tile_ptr, tile_col, tile_nnz, ptr, col, m, n, tilem, td, new_to_old, perm_size,
+            row_data, row_cnt, ws.err.as<int>());
         ws.launches++;
     }
     return RTT_OK;
@@ -185,7 +188,7 @@ int tile2csr_fill_device(Workspace &ws, const int *tile_ptr, const int *tile_col
                          const int *tile_nnz, const uint8_t *ptr, const uint8_t *col,
                          const double *val, int m, int n, int tilem, int td,
                          const int *new_to_old, int perm_size, const int *rowptr, int *out_col,
-                         double *out_val, bool sort_rows)
+                         double *out_val, bool sort_rows, const int *row_data)
 {
     int total = 0;
     RTT_CHECK(read_int(ws, rowptr + m, &total));
@@ -194,7 +197,7 @@ int tile2csr_fill_device(Workspace &ws, const int *tile_ptr, const int *tile_col
     {
         k_t2c_fill<<<grid_for((long long)tilem * td, 256), 256, 0, ws.stream>>>(
             tile_ptr, tile_col, tile_nnz, ptr, col, val, m, n, tilem, td, new_to_old, perm_size,
-            rowptr, nnz, out_col, out_val, ws.err.as<int>());
+            row_data, rowptr, nnz, out_col, out_val, ws.err.as<int>());
         ws.launches++;
     }
     if (sort_rows && m > 0)

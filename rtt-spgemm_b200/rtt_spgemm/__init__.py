@@ -211,18 +211,25 @@ class Context:
                        val.data_ptr())
 
     def symbolic(self, a, b=None, op: int = RTT_OP_AB):
-        """a, b: (rows, cols, rowptr, col, val) with device tensors."""
+        """a, b: (rows, cols, rowptr, col, val) with device tensors.  The
+        operands stay borrowed by the library until numeric() returns; the
+        context keeps references to them until then."""
         va = self._view(*a)
         vb = self._view(*b) if b is not None else None
         nnz = C.c_longlong()
         tiles = C.c_longlong()
+        self._borrowed = (a, b)
         check(lib().rtt_spgemm_symbolic(self.handle, C.byref(va), C.byref(vb) if vb else None,
                                         op, C.byref(nnz), C.byref(tiles)))
         return nnz.value, tiles.value
 
     def numeric(self, rowptr, col, val):
-        check(lib().rtt_spgemm_numeric(self.handle, C.c_void_p(rowptr.data_ptr()),
-                                       C.c_void_p(col.data_ptr()), C.c_void_p(val.data_ptr())))
+        try:
+            check(lib().rtt_spgemm_numeric(self.handle, C.c_void_p(rowptr.data_ptr()),
+                                           C.c_void_p(col.data_ptr()),
+                                           C.c_void_p(val.data_ptr())))
+        finally:
+            self._borrowed = None
 
     def stats(self) -> dict:
         st = Stats()

@@ -65,7 +65,8 @@ class CsrView(C.Structure):
 
 class Config(C.Structure):
     _fields_ = [("dmma_pair_cutoff", C.c_int), ("fused_csr_output", C.c_int),
-                ("keep_tiles", C.c_int), ("stage_timing", C.c_int), ("reserved", C.c_int * 7)]
+                ("keep_tiles", C.c_int), ("stage_timing", C.c_int), ("b_staging", C.c_int),
+                ("reserved", C.c_int * 6)]
 
 
 class Stats(C.Structure):
