@@ -157,6 +157,31 @@ RTT_API int rtt_tile2csr_restore_rows(SMatrix *matrix, const int *row_new_to_old
                               int permutation_size, int tile_dim,
                               int canonical);
 
+/* tile2csr on DEVICE tiles into caller-owned DEVICE CSR buffers, allocating
+ * nothing (no cudaMalloc/cudaFree, no pinned host memory).  No counterpart in
+ * the reference: its tile2csr (src/tile2csr.h:232) mallocs its output.  For
+ * callers that may not allocate while they run: code whose device memory is
+ * owned by an outer framework's pool or arena, and serving loops that must not
+ * take cudaMalloc's device-wide synchronisation.
+ * matrix: m, n, tilem, numtile, nnz (entries in tile_csr_Col/Value) and the
+ * device arrays tile_ptr, tile_columnidx, tile_nnz, tile_csr_Ptr, tile_csr_Col,
+ * tile_csr_Value on the CURRENT device, tiles of edge tile_dim (8 or 16) as
+ * rtt_tile2csr takes them; rowpointer: caller's device array of m + 1 ints,
+ * always written; columnindex, value: caller's device arrays with room for
+ * out_capacity entries, or both NULL to ask only for the size.  *out_nnz
+ * receives the entry count of the result.  Results equal rtt_tile2csr's.
+ * Runs on stream (a cudaStream_t; NULL = legacy default stream) and returns
+ * after its work there has finished.
+ * Limits: m <= 33,554,432 rows (larger m returns RTT_ERR_INVALID_ARGUMENT
+ * with a message naming the limit); its working memory is a 1 MiB static
+ * device array per device.  The first call on a device looks that array up
+ * (cudaGetSymbolAddress) and may load the module: make it before any stream
+ * capture.  Calls that overlapped on one device would share the array and
+ * race, so calls through this process are serialised by a lock. */
+RTT_API int rtt_tile2csr_device_noalloc(const SMatrix *matrix, int tile_dim, int canonical,
+                                        long long out_capacity, long long *out_nnz,
+                                        void *stream);
+
 /* Split a legacy 16x16 tile C (as produced by rtt_spgemm_tile) into the
  * reference's native 8x8 output layout: the SMatrix that dmma_tilespgemm
  * exports (src/dmma_spgemm.h:6399-6488) - tile_ptr over 8-row tile rows,

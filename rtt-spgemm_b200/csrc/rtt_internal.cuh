@@ -294,5 +294,14 @@ int tile2csr_fill_device(Workspace &ws, const int *tile_ptr, const int *tile_col
                          const double *val, int m, int n, int tilem, int td,
                          const int *new_to_old, int perm_size, const int *rowptr, int *out_col,
                          double *out_val, bool sort_rows, const int *row_data = nullptr);
+// launch-only forms (no workspace, identity row order): the caller owns the
+// stream and the error word; row_cnt needs m entries cleared to zero
+int tile2csr_count_launch(cudaStream_t s, const int *tile_ptr, const int *tile_col,
+                          const int *tile_nnz, const uint8_t *ptr, const uint8_t *col, int m,
+                          int n, int tilem, int td, int *row_cnt, int *err);
+int tile2csr_fill_launch(cudaStream_t s, const int *tile_ptr, const int *tile_col,
+                         const int *tile_nnz, const uint8_t *ptr, const uint8_t *col,
+                         const double *val, int m, int n, int tilem, int td, const int *rowptr,
+                         long long nnz, int *out_col, double *out_val, bool sort_rows, int *err);
 
 } // namespace rtt

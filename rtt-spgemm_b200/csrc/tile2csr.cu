@@ -208,4 +208,38 @@ int tile2csr_fill_device(Workspace &ws, const int *tile_ptr, const int *tile_col
     return RTT_OK;
 }
 
+int tile2csr_count_launch(cudaStream_t s, const int *tile_ptr, const int *tile_col,
+                          const int *tile_nnz, const uint8_t *ptr, const uint8_t *col, int m,
+                          int n, int tilem, int td, int *row_cnt, int *err)
+{
+    if (tilem > 0)
+    {
+        k_t2c_count<<<grid_for((long long)tilem * td, 256), 256, 0, s>>>(
+            tile_ptr, tile_col, tile_nnz, ptr, col, m, n, tilem, td, nullptr, -1, nullptr,
+            row_cnt, err);
+        RTT_CUDA(cudaGetLastError());
+    }
+    return RTT_OK;
+}
+
+int tile2csr_fill_launch(cudaStream_t s, const int *tile_ptr, const int *tile_col,
+                         const int *tile_nnz, const uint8_t *ptr, const uint8_t *col,
+                         const double *val, int m, int n, int tilem, int td, const int *rowptr,
+                         long long nnz, int *out_col, double *out_val, bool sort_rows, int *err)
+{
+    if (tilem > 0)
+    {
+        k_t2c_fill<<<grid_for((long long)tilem * td, 256), 256, 0, s>>>(
+            tile_ptr, tile_col, tile_nnz, ptr, col, val, m, n, tilem, td, nullptr, -1, nullptr,
+            rowptr, nnz, out_col, out_val, err);
+        RTT_CUDA(cudaGetLastError());
+    }
+    if (sort_rows && m > 0)
+    {
+        k_sort_rows<<<grid_for(m, 128), 128, 0, s>>>(m, rowptr, out_col, out_val);
+        RTT_CUDA(cudaGetLastError());
+    }
+    return RTT_OK;
+}
+
 } // namespace rtt

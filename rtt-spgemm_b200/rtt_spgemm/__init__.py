@@ -32,6 +32,7 @@ from .generators import CSR
 
 __all__ = ["CSR", "Context", "RttError", "build", "csr2tile_col_major", "csr2tile_row_major",
            "generators", "lib", "spgemm_csr_host", "spgemm_tile", "tile16_to_tile8", "tile2csr",
+           "tile2csr_device_noalloc",
            "EXPORTS", "LIB_PATH", "RTT_OP_AB", "RTT_OP_AAT"]
 
 TD = 16
@@ -169,6 +170,32 @@ def tile16_to_tile8(c_tiles: dict) -> dict:
     d = _tiles_out(o, ptr_stride=8)
     _destroy(o)
     return d
+
+
+def tile2csr_device_noalloc(tiles: dict, rowptr, col=None, val=None, tile_dim: int = 16,
+                            canonical: bool = False, stream: int = 0) -> int:
+    """tile2csr on device tiles into caller-owned device buffers, allocating
+    nothing (rtt_tile2csr_device_noalloc).  ``tiles`` holds m, n, tilem,
+    numtile, nnz and torch CUDA tensors tile_ptr, tile_columnidx, tile_nnz,
+    tile_csr_Ptr, tile_csr_Col, tile_csr_Value; rowptr (m + 1 int32) is always
+    written; col/val None asks for the size only.  Returns nnz of the CSR."""
+    s = SMatrix()
+    s.m, s.n, s.nnz = tiles["m"], tiles["n"], tiles["nnz"]
+    s.tilem, s.numtile = tiles["tilem"], tiles["numtile"]
+    for name, ct in [("tile_ptr", C.c_int), ("tile_columnidx", C.c_int), ("tile_nnz", C.c_int),
+                     ("tile_csr_Ptr", C.c_ubyte), ("tile_csr_Col", C.c_ubyte),
+                     ("tile_csr_Value", C.c_double)]:
+        setattr(s, name, C.cast(C.c_void_p(tiles[name].data_ptr()), C.POINTER(ct)))
+    s.rowpointer = C.cast(C.c_void_p(rowptr.data_ptr()), C.POINTER(C.c_int))
+    cap = 0
+    if col is not None:
+        s.columnindex = C.cast(C.c_void_p(col.data_ptr()), C.POINTER(C.c_int))
+        s.value = C.cast(C.c_void_p(val.data_ptr()), C.POINTER(C.c_double))
+        cap = min(int(col.numel()), int(val.numel()))
+    nnz = C.c_longlong()
+    check(lib().rtt_tile2csr_device_noalloc(C.byref(s), tile_dim, int(canonical), cap,
+                                            C.byref(nnz), C.c_void_p(stream)))
+    return nnz.value
 
 
 class Context:

@@ -32,6 +32,7 @@ EXPORTS = [
     "rtt_config_default", "rtt_context_create", "rtt_context_destroy", "rtt_context_set_stream",
     "rtt_context_set_config", "rtt_context_get_stats", "rtt_spgemm_symbolic",
     "rtt_spgemm_numeric", "rtt_spgemm_tiles_view", "rtt_spgemm_csr_host",
+    "rtt_tile2csr_device_noalloc",
 ]
 
 
@@ -111,6 +112,8 @@ def lib() -> C.CDLL:
     L.rtt_tile2csr.argtypes = [P(SMatrix), C.c_int, C.c_int]
     L.rtt_tile2csr_restore_rows.argtypes = [P(SMatrix), P(C.c_int), C.c_int, C.c_int, C.c_int]
     L.rtt_tile16_to_tile8.argtypes = [P(SMatrix), P(SMatrix)]
+    L.rtt_tile2csr_device_noalloc.argtypes = [P(SMatrix), C.c_int, C.c_int, C.c_longlong,
+                                              P(C.c_longlong), C.c_void_p]
     L.rtt_matrix_destroy.argtypes = [P(SMatrix), C.c_int]
     L.rtt_matrix_destroy.restype = None
     L.rtt_config_default.argtypes = [P(Config)]
