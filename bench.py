@@ -214,7 +214,7 @@ def run_ours(args) -> None:
     stream = torch.cuda.current_stream(dev)
     ctx = R.Context(local, {"stage_timing": 1, "dmma_pair_cutoff": args.dmma_cutoff,
                             "fused_csr_output": 0 if args.unfused else 1,
-                            "b_staging": 0 if args.no_staging else 1})
+                            "b_staging": 1 if args.staging else 0})
     ctx.set_stream(stream.cuda_stream)
     rp = torch.from_numpy(A.rowptr).to(dev)
     ci = torch.from_numpy(A.col).to(dev)
@@ -323,7 +323,7 @@ def run_ours(args) -> None:
                    "l2": "inputs larger than L2 (A CSR %.0f MB > 126 MB), no flush" %
                          ((4 * (A.m + 1) + 12 * A.nnz) / 1e6),
                    "dmma_pair_cutoff": args.dmma_cutoff, "fused_tile2csr": not args.unfused,
-                   "b_staging": not args.no_staging},
+                   "b_staging": bool(args.staging)},
         "roofline": {"bound": "hbm", "kernel": "k_numeric (numeric + fused tile2csr)",
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
@@ -352,7 +352,8 @@ def main() -> None:
     ap.add_argument("--unfused", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-staging", action="store_true")
+    ap.add_argument("--staging", action="store_true",
+                    help="TMA-staged numeric kernel instead of the default flat one")
     ap.add_argument("--ref-tile-rows", type=int, default=256)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -238,8 +238,10 @@ typedef struct
     /* Record CUDA events around the stages (csr2tile, symbolic, numeric
      * kernel) on the context's stream; results land in rtt_stats. */
     int stage_timing;
-    /* How the numeric step reads B tile rows: 1 = TMA bulk copies into a
-     * shared-memory ring (default), 0 = direct loads through L1/L2. */
+    /* Numeric kernel without DMMA pairs: 0 = warp-private Gustavson with
+     * direct loads of B's rows (default, fastest on B200), 1 = B tile rows
+     * streamed by TMA bulk copies through a shared-memory stage ring (the
+     * kernel that also runs the DMMA pairs). */
     int b_staging;
     /* Reserved, must be zero. */
     int reserved[6];

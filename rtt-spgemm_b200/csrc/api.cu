@@ -459,7 +459,7 @@ void rtt_config_default(rtt_config *config)
     config->dmma_pair_cutoff = 3072;
     config->fused_csr_output = 1;
     config->keep_tiles = 0;
-    config->b_staging = 1;
+    config->b_staging = 0;
 }
 
 int rtt_set_device(int device)
@@ -680,7 +680,8 @@ int rtt_spgemm_tile(SMatrix *A, SMatrix *B, SMatrix *C)
     RTT_CHECK(effective_cutoff(c, dA, dB, &nc.dmma_pair_cutoff));
     nc.write_tiles = true;
     nc.conflict_safe = true; // caller tiles may repeat a coordinate
-    RTT_CHECK(numeric_rows_device(c->ws, dA, dB, c->S, nc));
+    nc.b_staging = c->cfg.b_staging != 0;
+    RTT_CHECK(numeric_select_device(c->ws, dA, dB, c->S, nc));
     RTT_CHECK(check_device_error(c->ws, "spgemm_tile numeric"));
     cudaStream_t s = c->ws.stream;
     SymbolicOut &S = c->S;
@@ -975,7 +976,7 @@ int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_
     dB.csr_val = c->b_va;
     dB.nnz = (int)c->b_nnz;
     nc.conflict_safe = c->b_dups;
-    RTT_CHECK(numeric_rows_device(ws, c->A.view(), dB, c->S, nc));
+    RTT_CHECK(numeric_select_device(ws, c->A.view(), dB, c->S, nc));
     if (!fused)
     {
         SymbolicOut &S = c->S;
@@ -997,6 +998,9 @@ int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_
     }
     c->stats.dmma_pairs = ws.h_scalars64[2];
     c->stats.sparse_pairs = ws.h_scalars64[3];
+    // the numeric kernels count every (a_ik, b_kj) pair once: sum over A
+    // entries of nnz(B(k, :)), the reference's nnzCub
+    c->stats.nnz_cub = ws.h_scalars64[3];
     c->stats.kernel_launches = ws.launches;
     c->stats.host_syncs = ws.syncs;
     return RTT_OK;

@@ -1,0 +1,448 @@
+// numeric_flat.cu - step 3 (values) of the tiled SpGEMM without a copy
+// pipeline: one CTA per C tile row, each warp owns RPW scalar rows and runs
+// Gustavson over its own A entries with no CTA-wide synchronisation inside
+// the product phase.
+//
+//   C(i, :) = sum over k in A(i, :) of a_ik * B(k, :)        (rows i of tile row I)
+//
+// (Reference: spgemm_cpu step 4, src/spgemm-cpu.h:284-367, row-organised as in
+// the Super16 path, src/super16_symbolic.cuh:973-1073.)
+//
+// Every B row is used about once per tile row (a tile row's A entries hit
+// distinct k almost always), so staging B in shared memory buys no reuse; what
+// matters is the instruction count per product and the number of warps with
+// loads in flight.  Per warp:
+//   1. lanes take 32 A tiles of the tile row at a time and read the row ranges
+//      of the warp's rows; a warp scan numbers the entries;
+//   2. lanes take 32 of those entries at a time: each lane finds its tile with
+//      a 5-step shuffle search, reads a_ik and B's row range [fs, fe) for
+//      k - all 32 lanes' loads in flight together - and writes the entry to
+//      the warp's list in shared memory;
+//   3. the warp walks the list GROUP entries at a time: it loads the GROUP B
+//      rows' heads (lane l: entry fs + l), then adds a_ik * b_kj into the
+//      row's accumulator slot, entry by entry in list order.
+// The accumulator is the C tile row in CSR order in shared memory, one FP64
+// per structural entry; (tile s, row r, col c) sits at
+// base[r][s] + popc(mask[r][s] >> (16 - c)).  The [row][slot] table has an odd
+// row stride, so the lanes of one B row (same C row, different slots) read
+// distinct banks.  A warp's rows are its own and lanes of one B row hit
+// distinct columns, so the adds need no atomics and every output is summed in
+// the fixed order (K, k) ascending - bitwise reproducible.  (With repeated
+// columns in a B row the SAFE instantiation adds with shared atomics.)
+//
+// Windows of C tiles (<= F_SLOT_CAP tiles, <= F_ACC_CAP entries) bound shared
+// memory; products whose C tile is outside the window are skipped and the A
+// list is walked again for the next window.  Shared memory (~38 KB) and
+// registers (<= 48) are sized so that five CTAs share an SM: the kernel is
+// latency-bound and lives on the number of warps in flight.
+#include "rtt_internal.cuh"
+
+namespace rtt
+{
+namespace
+{
+
+constexpr int FW = 8;                       // warps per CTA
+constexpr int RPW = TD / FW;                // rows per warp
+constexpr int F_THREADS = FW * 32;
+constexpr int F_MIN_CTAS = 5;               // CTAs per SM the launch bounds aim at
+constexpr int F_ACC_CAP = 2304;             // FP64 accumulator slots per window
+constexpr int F_SLOT_CAP = 128;             // C tiles per window
+constexpr int F_CM_STRIDE = F_SLOT_CAP + 1; // row stride of cm: rows land in distinct banks
+constexpr int F_SPAN_CAP = 4096;            // tile-column span of the slot table
+constexpr int GROUP = 2;                    // B rows loaded together
+static_assert(RPW == 1 || RPW == 2, "one or two rows per warp");
+
+struct FlatSmem
+{
+    double acc[F_ACC_CAP];
+    uint32_t cm[TD * F_CM_STRIDE];    // [row][slot]: (acc base << 16) | row mask
+    int cJ[F_SLOT_CAP];
+    uint8_t slot8[F_SPAN_CAP];        // tile column - Jlo -> slot (255 = none)
+    int4 ent[FW][32];                 // per warp: B row start, length, cm row offset, -
+    double enta[FW][32];              // per warp: a_ik
+    int rowtot[TD];
+    int rowacc0[TD + 1];
+    int rowcsr0[TD];
+    int rowrun[TD];
+    int win_nnz;
+};
+
+struct Window
+{
+    int Jlo, Jspan, nW;
+    bool table;
+};
+
+__device__ __forceinline__ int flat_slot(const FlatSmem &S, const Window &W, int J)
+{
+    const int d = J - W.Jlo;
+    if ((unsigned)d > (unsigned)W.Jspan)
+        return -1;
+    if (W.table)
+    {
+        const int s = S.slot8[d];
+        return s == 255 ? -1 : s;
+    }
+    const int s = lower_bound(S.cJ, 0, W.nW, J);
+    return (s < W.nW && S.cJ[s] == J) ? s : -1;
+}
+
+template <bool SAFE>
+__device__ __forceinline__ void flat_add(FlatSmem &S, const Window &W, const uint32_t *cmr,
+                                         int col, double a, double b)
+{
+    const int slot = flat_slot(S, W, col >> 4);
+    if (slot < 0)
+        return;
+    const uint32_t w = cmr[slot];
+    const int pos = (int)(w >> 16) + __popc((w & 0xFFFFu) >> (16 - (col & 15)));
+    if (SAFE)
+        atomicAdd(&S.acc[pos], a * b);
+    else
+        S.acc[pos] = fma(a, b, S.acc[pos]);
+}
+
+// Column indices of one (row, window) into the CSR output: lanes over slots.
+__device__ __forceinline__ void write_row_cols(const FlatSmem &S, int r, int nW, long long rowpos,
+                                               int acc0, long long nnzC, int *csr_col, int *err)
+{
+    const uint32_t *cmr = S.cm + r * F_CM_STRIDE;
+    for (int s = lane_id(); s < nW; s += 32)
+    {
+        const uint32_t w = cmr[s];
+        uint32_t mm = w & 0xFFFFu;
+        const long long pos = rowpos + ((int)(w >> 16) - acc0);
+        const int cb = S.cJ[s] * TD;
+        int k = 0;
+        while (mm)
+        {
+            const int c = __clz(mm) - 16;
+            mm &= ~(0x8000u >> c);
+            if (pos + k >= nnzC)
+            {
+                set_error(err, DERR_NUM_BOUNDS);
+                break;
+            }
+            csr_col[pos + k] = cb + c;
+            ++k;
+        }
+    }
+}
+
+template <bool SAFE>
+__global__ void __launch_bounds__(F_THREADS, F_MIN_CTAS)
+    k_numeric_flat(DevTiles A, DevTiles B, int tilem, long long nnzC,
+                   const int *__restrict__ c_tile_ptr, const int *__restrict__ c_tile_col,
+                   const uint16_t *__restrict__ c_mask, const int *__restrict__ c_tile_nnz,
+                   uint8_t *__restrict__ c_ptr, uint8_t *__restrict__ c_colb,
+                   double *__restrict__ c_val, const int *__restrict__ csr_rowptr,
+                   int *__restrict__ csr_col, double *__restrict__ csr_val, long long *counters,
+                   int *err)
+{
+    extern __shared__ __align__(128) unsigned char dyn[];
+    FlatSmem &S = *reinterpret_cast<FlatSmem *>(dyn);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int I = blockIdx.x;
+    if (I >= tilem)
+        return;
+    const int a0 = __ldg(A.tile_ptr + I), a1 = __ldg(A.tile_ptr + I + 1);
+    const int cs0 = __ldg(c_tile_ptr + I), cs1 = __ldg(c_tile_ptr + I + 1);
+    if (cs0 == cs1 || a0 == a1)
+        return; // no C tiles in this tile row (uniform)
+    if (tid < TD)
+        S.rowrun[tid] = 0;
+    const int nrows = min(TD, A.m - I * TD);
+    const int r0 = warp * RPW, r1 = r0 + RPW - 1;
+    long long n_fma = 0;
+    int4 *ent = S.ent[warp];
+    double *enta = S.enta[warp];
+
+    for (int w0 = cs0; w0 < cs1;)
+    {
+        // ---- window [w0, w1): longest run of <= F_SLOT_CAP tiles, <= F_ACC_CAP entries
+        const int base_nnz = __ldg(c_tile_nnz + w0);
+        bool ok = false;
+        if (tid < F_SLOT_CAP && w0 + tid < cs1)
+            ok = __ldg(c_tile_nnz + w0 + tid + 1) - base_nnz <= F_ACC_CAP;
+        const int nW = __syncthreads_count(ok);
+        if (nW == 0)
+        {
+            if (tid == 0)
+                set_error(err, DERR_NUM_BOUNDS); // a C tile holds at most 256 entries
+            return;
+        }
+        const int w1 = w0 + nW;
+        if (tid == 0)
+            S.win_nnz = __ldg(c_tile_nnz + w1) - base_nnz;
+        for (int i = tid; i < nW * TD; i += F_THREADS)
+            S.cm[(i & 15) * F_CM_STRIDE + (i >> 4)] = __ldg(c_mask + (size_t)w0 * TD + i);
+        for (int i = tid; i < nW; i += F_THREADS)
+            S.cJ[i] = __ldg(c_tile_col + w0 + i);
+        for (int i = tid; i < F_SPAN_CAP / 4; i += F_THREADS)
+            reinterpret_cast<uint32_t *>(S.slot8)[i] = 0xFFFFFFFFu;
+        __syncthreads();
+        Window W;
+        W.Jlo = S.cJ[0];
+        W.Jspan = S.cJ[nW - 1] - W.Jlo;
+        W.nW = nW;
+        W.table = W.Jspan < F_SPAN_CAP;
+        if (W.table)
+            for (int i = tid; i < nW; i += F_THREADS)
+                S.slot8[S.cJ[i] - W.Jlo] = (uint8_t)i;
+        // per-row prefix over the window's tiles (each warp its own rows)
+#pragma unroll
+        for (int rr = 0; rr < RPW; ++rr)
+        {
+            uint32_t *cmr = S.cm + (r0 + rr) * F_CM_STRIDE;
+            int run = 0;
+            for (int s0 = 0; s0 < nW; s0 += 32)
+            {
+                const int s = s0 + lane;
+                const uint32_t m = s < nW ? cmr[s] : 0u;
+                const int v = __popc(m);
+                const int incl = warp_incl_scan(v);
+                if (s < nW)
+                    cmr[s] = ((uint32_t)(run + incl - v) << 16) | m;
+                run += __shfl_sync(FULL, incl, 31);
+            }
+            if (lane == 0)
+                S.rowtot[r0 + rr] = run;
+        }
+        __syncthreads();
+        // row starts in the window accumulator (every warp scans the 16 totals)
+        {
+            const int v = lane < TD ? S.rowtot[lane] : 0;
+            const int incl = warp_incl_scan(v);
+            if (warp == 0 && lane <= TD)
+                S.rowacc0[lane] = incl - v; // lane 16: v = 0, so this is the window total
+            const int acc_r0 = __shfl_sync(FULL, incl - v, r0);
+            const int acc_r1 = __shfl_sync(FULL, incl - v, r1);
+#pragma unroll
+            for (int rr = 0; rr < RPW; ++rr)
+            {
+                uint32_t *cmr = S.cm + (r0 + rr) * F_CM_STRIDE;
+                const uint32_t add = (uint32_t)(rr ? acc_r1 : acc_r0) << 16;
+                for (int s = lane; s < nW; s += 32)
+                    cmr[s] += add;
+            }
+        }
+        if (tid < nrows && csr_rowptr != nullptr)
+            S.rowcsr0[tid] = __ldg(csr_rowptr + I * TD + tid) + S.rowrun[tid];
+        for (int i = tid; i < S.win_nnz; i += F_THREADS)
+            S.acc[i] = 0.0;
+        __syncthreads();
+
+        // ---- products: warp-private, no CTA barrier
+        if (r0 < nrows)
+        {
+            for (int t0 = a0; t0 < a1; t0 += 32)
+            {
+                const int t = t0 + lane;
+                int eb = 0, em = 0, n = 0, tn0 = 0, K = 0;
+                if (t < a1)
+                {
+                    tn0 = __ldg(A.tile_nnz + t);
+                    const int tcnt = __ldg(A.tile_nnz + t + 1) - tn0;
+                    const uint8_t *pp = A.ptr + (size_t)t * TD;
+                    eb = pp[r0];
+                    const int ee = r1 + 1 < TD ? (int)pp[r1 + 1] : tcnt;
+                    em = RPW == 2 ? (int)pp[r1] : ee; // first entry of row r1
+                    n = max(ee - eb, 0);
+                    K = __ldg(A.tile_col + t);
+                }
+                const int incl = warp_incl_scan(n);
+                const int total = __shfl_sync(FULL, incl, 31);
+                for (int q0 = 0; q0 < total; q0 += 32)
+                {
+                    // lane's entry q of the batch: owner tile by shuffle search
+                    const int q = q0 + lane;
+                    int own = 0;
+#pragma unroll
+                    for (int b = 16; b > 0; b >>= 1)
+                        if (__shfl_sync(FULL, incl, own + b - 1) <= q)
+                            own += b;
+                    own = min(own, 31);
+                    const int o_incl = __shfl_sync(FULL, incl, own);
+                    const int o_n = __shfl_sync(FULL, n, own);
+                    const int o_eb = __shfl_sync(FULL, eb, own);
+                    const int o_em = __shfl_sync(FULL, em, own);
+                    const int o_tn0 = __shfl_sync(FULL, tn0, own);
+                    const int o_K = __shfl_sync(FULL, K, own);
+                    int fs = 0, len = 0, rq = r0;
+                    double a = 0.0;
+                    if (q < total)
+                    {
+                        const int e = o_eb + (q - (o_incl - o_n));
+                        rq = e < o_em ? r0 : r1;
+                        const int k = o_K * TD + (A.col[o_tn0 + e] & 15);
+                        a = __ldg(A.val + o_tn0 + e);
+                        if (k < B.m)
+                        {
+                            fs = min(max(__ldg(B.csr_rowptr + k), 0), B.nnz);
+                            len = min(max(__ldg(B.csr_rowptr + k + 1), fs), B.nnz) - fs;
+                        }
+                        if (w0 == cs0) // count each pair once, in the first window
+                            n_fma += len;
+                    }
+                    ent[lane] = make_int4(fs, len, rq * F_CM_STRIDE, 0);
+                    enta[lane] = a;
+                    __syncwarp();
+                    const int nb = min(32, total - q0);
+                    for (int j = 0; j < nb; j += GROUP)
+                    {
+                        int4 ge[GROUP];
+                        int gcol[GROUP];
+                        double gb[GROUP];
+#pragma unroll
+                        for (int u = 0; u < GROUP; ++u)
+                        {
+                            ge[u] = ent[(j + u) & 31];
+                            if (j + u >= nb)
+                                ge[u].y = 0;
+                        }
+#pragma unroll
+                        for (int u = 0; u < GROUP; ++u)
+                        {
+                            gcol[u] = 0;
+                            gb[u] = 0.0;
+                            if (lane < ge[u].y)
+                            {
+                                gcol[u] = __ldg(B.csr_col + ge[u].x + lane);
+                                gb[u] = __ldg(B.csr_val + ge[u].x + lane);
+                            }
+                        }
+#pragma unroll
+                        for (int u = 0; u < GROUP; ++u)
+                        {
+                            const double au = enta[(j + u) & 31];
+                            const uint32_t *cmr = S.cm + ge[u].z;
+                            if (lane < ge[u].y)
+                                flat_add<SAFE>(S, W, cmr, gcol[u], au, gb[u]);
+                            for (int f = 32 + lane; f < ge[u].y; f += 32)
+                                flat_add<SAFE>(S, W, cmr, __ldg(B.csr_col + ge[u].x + f), au,
+                                               __ldg(B.csr_val + ge[u].x + f));
+                        }
+                    }
+                    __syncwarp(); // the next batch overwrites this warp's list
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- write-out of the window: each warp its own rows
+        if (csr_col != nullptr)
+        {
+#pragma unroll
+            for (int rr = 0; rr < RPW; ++rr)
+            {
+                const int r = r0 + rr;
+                if (r >= nrows)
+                    break;
+                const int b0 = S.rowacc0[r], b1 = S.rowacc0[r + 1];
+                const long long dst = (long long)S.rowcsr0[r] - b0;
+                if (dst + b1 > nnzC)
+                {
+                    if (lane == 0)
+                        set_error(err, DERR_NUM_BOUNDS);
+                    continue;
+                }
+                for (int p = b0 + lane; p < b1; p += 32)
+                    csr_val[dst + p] = S.acc[p];
+                write_row_cols(S, r, nW, S.rowcsr0[r], b0, nnzC, csr_col, err);
+            }
+        }
+        if (c_val != nullptr)
+        {
+            for (int it = tid; it < nW * TD; it += F_THREADS)
+            {
+                const int s = it >> 4, r = it & 15;
+                const uint32_t w = S.cm[r * F_CM_STRIDE + s];
+                const uint32_t m = w & 0xFFFFu;
+                const int abase = (int)(w >> 16);
+                const int t = w0 + s;
+                int pre = 0;
+                for (int rr = 0; rr < r; ++rr)
+                    pre += __popc(S.cm[rr * F_CM_STRIDE + s] & 0xFFFFu);
+                c_ptr[(size_t)t * TD + r] = (uint8_t)pre;
+                const long long tpos = (long long)__ldg(c_tile_nnz + t) + pre;
+                uint32_t mm = m;
+                int k = 0;
+                while (mm)
+                {
+                    const int c = __clz(mm) - 16;
+                    mm &= ~(0x8000u >> c);
+                    if (tpos + k >= nnzC)
+                    {
+                        set_error(err, DERR_NUM_BOUNDS);
+                        break;
+                    }
+                    c_colb[tpos + k] = (uint8_t)c;
+                    c_val[tpos + k] = S.acc[abase + k];
+                    ++k;
+                }
+            }
+        }
+        __syncthreads();
+        if (tid < TD)
+            S.rowrun[tid] += S.rowtot[tid];
+        __syncthreads();
+        w0 = w1;
+    }
+    if (counters != nullptr)
+    {
+        // n_fma: each lane counted the B row lengths of its own entries
+        const long long nf = warp_sum(n_fma);
+        if (lane == 0 && nf)
+            atomicAdd((unsigned long long *)&counters[1], (unsigned long long)nf);
+    }
+}
+
+} // namespace
+
+int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
+                        const NumericConfig &cfg)
+{
+    cudaStream_t s = ws.stream;
+    const size_t nnz = (size_t)S.nnz;
+    if (cfg.write_tiles)
+    {
+        RTT_CHECK(S.c_col.ensure(nnz + 16, s));
+        RTT_CHECK(S.c_val.ensure(sizeof(double) * nnz + 16, s));
+    }
+    if (cfg.csr_col != nullptr)
+        RTT_CHECK(csr_rowptr_device(ws, S, cfg.csr_rowptr));
+    if (S.numtile == 0 || S.tilem == 0)
+        return RTT_OK;
+    if (cfg.ev_begin != nullptr)
+        RTT_CUDA(cudaEventRecord(cfg.ev_begin, s));
+    const size_t smem = sizeof(FlatSmem);
+    auto launch = [&](auto kern) -> int {
+        RTT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<S.tilem, F_THREADS, smem, s>>>(
+            A, B, S.tilem, S.nnz, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(),
+            S.c_mask.as<uint16_t>(), S.c_tile_nnz.as<int>(), S.c_ptr.as<uint8_t>(),
+            cfg.write_tiles ? S.c_col.as<uint8_t>() : nullptr,
+            cfg.write_tiles ? S.c_val.as<double>() : nullptr, cfg.csr_col ? cfg.csr_rowptr : nullptr,
+            cfg.csr_col, cfg.csr_val, cfg.counters, ws.err.as<int>());
+        return RTT_OK;
+    };
+    if (cfg.conflict_safe)
+        RTT_CHECK(launch(k_numeric_flat<true>));
+    else
+        RTT_CHECK(launch(k_numeric_flat<false>));
+    ws.launches++;
+    if (cfg.ev_end != nullptr)
+        RTT_CUDA(cudaEventRecord(cfg.ev_end, s));
+    return RTT_OK;
+}
+
+int numeric_select_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
+                          const NumericConfig &cfg)
+{
+    if (cfg.dmma_pair_cutoff > 0 || cfg.b_staging)
+        return numeric_rows_device(ws, A, B, S, cfg);
+    return numeric_flat_device(ws, A, B, S, cfg);
+}
+
+} // namespace rtt

@@ -433,7 +433,8 @@ __global__ void __launch_bounds__(NR_THREADS, DMMA ? 2 : 3)
                             const int lo_e = staged ? 0 : ebase, hi_e = S.p_e1[ai] - (staged ? ebase : 0);
                             const int fs = max(brp[k] - eoff, lo_e);
                             const int fe = min(max(brp[k + 1] - eoff, fs), hi_e);
-                            n_fma += fe - fs;
+                            if (w0 == cs0) // count each pair once, in the first window
+                                n_fma += fe - fs;
                             for (int f = fs + lane; f < fe; f += 32)
                             {
                                 const int col = bcol[f];

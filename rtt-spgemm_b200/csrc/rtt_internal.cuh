@@ -281,6 +281,12 @@ int csr_rowptr_device(Workspace &ws, SymbolicOut &S, int *rowptr);
 // numeric step, one CTA per C tile row (TMA-staged B tile rows)
 int numeric_rows_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
                         const NumericConfig &cfg);
+// numeric step without a copy pipeline: warp-private Gustavson per row pair
+int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
+                        const NumericConfig &cfg);
+// the flat kernel unless DMMA pairs exist or TMA staging of B is asked for
+int numeric_select_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
+                          const NumericConfig &cfg);
 // largest per-tile entry count of a tile matrix (device scalar *out)
 int max_tile_nnz_device(Workspace &ws, const int *tile_nnz, int numtile, int *out);
 

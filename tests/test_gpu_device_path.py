@@ -52,6 +52,9 @@ CONFIGS = {
     "fused_nodmma": dict(fused_csr_output=1, dmma_pair_cutoff=0),
     "unfused": dict(fused_csr_output=0, dmma_pair_cutoff=3072),
     "all_dmma": dict(fused_csr_output=1, dmma_pair_cutoff=1),
+    "flat": dict(fused_csr_output=1, dmma_pair_cutoff=0, b_staging=0),
+    "flat_unfused": dict(fused_csr_output=0, dmma_pair_cutoff=0, b_staging=0),
+    "staged": dict(fused_csr_output=1, dmma_pair_cutoff=0, b_staging=1),
 }
 
 
@@ -65,11 +68,12 @@ def test_a_squared(case, cfg, orc):
     assert_csr_close(rp, ci, va, erp, ecol, evals, eabs, f"{case}/{cfg}: ")
     st = ctx.stats()
     assert st["nnz_c"] == nnz
+    assert st["nnz_cub"] == orc.nnzcub(A, A)
     if cfg == "all_dmma" and nnz > 0:
         # every pair qualifies; B tile rows wider than the per-step table
         # (64 tiles) still take the sparse path
         assert st["dmma_pairs"] > 0
-    if cfg == "fused_nodmma":
+    if cfg in ("fused_nodmma", "flat", "flat_unfused", "staged"):
         assert st["dmma_pairs"] == 0
     ctx.close()
 
