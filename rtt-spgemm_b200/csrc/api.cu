@@ -650,9 +650,8 @@ int rtt_spgemm_tile(SMatrix *A, SMatrix *B, SMatrix *C)
     RTT_CHECK(upload_tiles(c, B, true, c->B));
     const DevTiles dA = view_with_rowdata(c->A);
     DevTiles dB = view_with_rowdata(c->B);
-    RTT_CHECK(map_device_error(symbolic_device(c->ws, dA, dB, c->S)));
-    // B's scalar CSR rows for the numeric step, assembled on the device from
-    // the column-major tiles (tile2csr through the row->data index)
+    // B's scalar CSR rows for the symbolic and numeric steps, assembled on the
+    // device from the column-major tiles (tile2csr through the row->data index)
     {
         cudaStream_t s = c->ws.stream;
         const int mb = B->m;
@@ -676,6 +675,7 @@ int rtt_spgemm_tile(SMatrix *A, SMatrix *B, SMatrix *C)
         dB.csr_val = c->in2_val.as<double>();
         dB.nnz = bnnz;
     }
+    RTT_CHECK(map_device_error(symbolic_device(c->ws, dA, dB, c->S)));
     NumericConfig nc;
     RTT_CHECK(effective_cutoff(c, dA, dB, &nc.dmma_pair_cutoff));
     nc.write_tiles = true;
@@ -871,7 +871,6 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
         if (A->rows != A->cols)
             return rtt::fail(RTT_ERR_SHAPE_MISMATCH, "A*A needs a square A");
         c->b_alias = true;
-        RTT_CHECK(build_tile_csc(ws, c->A));
         c->b_rp = A->row_ptr;
         c->b_ci = A->col_idx;
         c->b_va = A->values;
@@ -909,12 +908,16 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
             c->b_nnz = B->nnz;
         }
         c->b_dups = c->B.dup_cols;
-        RTT_CHECK(build_tile_csc(ws, c->B));
     }
     const TileBufs &TB = c->b_alias ? c->A : c->B;
     if (timing)
         RTT_CUDA(cudaEventRecord(ws.ev[1], ws.stream));
-    RTT_CHECK(map_device_error(symbolic_device(ws, c->A.view(), TB.view(), c->S)));
+    DevTiles dB = TB.view();
+    dB.csr_rowptr = c->b_rp;
+    dB.csr_col = c->b_ci;
+    dB.csr_val = c->b_va;
+    dB.nnz = (int)c->b_nnz;
+    RTT_CHECK(map_device_error(symbolic_device(ws, c->A.view(), dB, c->S)));
     if (timing)
     {
         float t01 = 0.f, t12 = 0.f;

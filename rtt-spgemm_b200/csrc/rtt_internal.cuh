@@ -250,7 +250,6 @@ struct SymbolicOut
     DevBuf c_tr_nnz;    // tilem ints, nnz per C tile row
     DevBuf count_tmp;   // tilem + 1 ints
     DevBuf tile_cnt;    // numtile ints, nnz per C tile
-    DevBuf row_prefix;  // numtile * 16 ints, CSR prefix of each (tile,row) in its tile row
     int numtile = 0;
     long long nnz = 0;
     int tilem = 0, tilen = 0, m = 0, n = 0;
@@ -274,8 +273,6 @@ struct NumericConfig
     bool conflict_safe = false;     // B rows may repeat a column: accumulate with shared atomics
 };
 
-int numeric_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
-                   const NumericConfig &cfg);
 // CSR row pointer of C (m + 1 ints) from the symbolic counts
 int csr_rowptr_device(Workspace &ws, SymbolicOut &S, int *rowptr);
 // numeric step, one CTA per C tile row (TMA-staged B tile rows)

@@ -9,13 +9,15 @@
 // Windows wider than the bitmap are processed in passes.
 //
 // Step 2 (reference step3, src/spgemm-cpu.h:185-281, and the exact-mask step,
-// src/super16_symbolic.cuh:1399-1662): exact structure of every C tile as 16
-// row masks, C(I,J)[r] = OR over K, over k in A(I,K)[r] of B(K,J)[k].  For each
-// K of the tile row, the lanes take the B tiles of B.row(K) (one per lane),
-// stage their 16 row masks in shared memory and OR them over A(I,K)'s entries
-// row by row; results are OR-ed into the window's slot masks with shared
-// atomics.  Per-tile counts, per-(tile,row) CSR prefixes, per-row counts and
-// the tile row total come straight out of the masks with popc.
+// src/super16_symbolic.cuh:1399-1662): the exact structure of every C tile as
+// 16 row masks.  One CTA per tile row I: the CTA rebuilds the tile row's C
+// tile list (the step-1 union, as a bitmap, compacted into a column -> slot
+// table), then each warp ORs, for its two rows r and every A entry (r, k), the
+// columns of B's CSR row k into the row masks of their C tiles - the same
+// warp-private walk as the numeric step, with shared atomics on 32-bit words
+// that hold the warp's two rows.  Tile rows with more C tiles than the slot
+// table holds are processed in column windows.  Per-tile counts, per-row
+// counts and the tile row total come out of the masks with popc.
 #include "rtt_internal.cuh"
 
 #include <climits>
@@ -27,7 +29,6 @@ namespace
 
 constexpr int WWORDS = 256;             // bitmap words per warp -> 8192 tile columns
 constexpr int WBITS = WWORDS * 32;
-constexpr int SCAP = 256;               // C tiles per window in step 2
 constexpr int SYM_WARPS = 4;            // warps per CTA
 
 struct WarpSmem1
@@ -37,15 +38,19 @@ struct WarpSmem1
     int pre[32];
 };
 
-struct WarpSmem2
+constexpr int S2_WARPS = 8;              // warps per CTA, two rows each
+constexpr int S2_THREADS = S2_WARPS * 32;
+constexpr int S2_SLOTS = 254;            // C tiles per window (slot 255 = none)
+constexpr int S2_STRIDE = 257;           // odd stride: the warps' mask rows in distinct banks
+
+struct CtaSmem2
 {
     uint32_t bitmap[WWORDS];
     int wordpre[WWORDS];
-    int start[32];
-    int pre[32];
-    uint32_t smask[SCAP * 8];           // 16 u16 rows per slot
-    uint32_t bmask[32 * 17];            // per-lane staged B masks, stride 17
-    int rowcnt[TD];
+    uint8_t slot8[WBITS];                // window column -> slot
+    uint32_t mw[S2_WARPS * S2_STRIDE];   // per warp and slot: row 2w (low 16), 2w+1 (high 16)
+    int4 ent[S2_WARPS][32];              // per warp: B row start, length, mask shift, -
+    int lo, hi, nb, wend;
 };
 
 // Window bounds [lo, hi] of the tile columns reachable from tile row I.
@@ -145,197 +150,281 @@ __global__ void __launch_bounds__(SYM_WARPS * 32) k_sym_count(DevTiles A, DevTil
         cnt[I] = count;
 }
 
-// Step 2.  Outputs per C tile: column, tile row, 16 row masks, entry count and
-// the per-row CSR prefix within the tile row; per scalar row: entry count;
-// per tile row: entry total.
-__global__ void __launch_bounds__(SYM_WARPS * 32)
-    k_sym_struct(DevTiles A, DevTiles B, const int *__restrict__ c_tile_ptr,
-                 int *__restrict__ c_tile_col, int *__restrict__ c_tile_row,
-                 uint32_t *__restrict__ c_mask32, int *__restrict__ c_tile_cnt,
-                 int *__restrict__ c_row_prefix, int *__restrict__ c_row_cnt,
-                 int *__restrict__ c_tr_nnz, int *err)
+// Step 2.  Outputs per C tile: column, tile row, 16 row masks and entry
+// count; per scalar row: entry count; per tile row: entry total.
+__global__ void __launch_bounds__(S2_THREADS, 4)
+    k_sym_rows(DevTiles A, DevTiles B, const int *__restrict__ c_tile_ptr,
+               int *__restrict__ c_tile_col, int *__restrict__ c_tile_row,
+               uint16_t *__restrict__ c_mask, int *__restrict__ c_tile_cnt,
+               int *__restrict__ c_row_cnt, int *__restrict__ c_tr_nnz, int *err)
 {
-    extern __shared__ __align__(16) unsigned char dyn[];
-    WarpSmem2 &S = reinterpret_cast<WarpSmem2 *>(dyn)[threadIdx.x >> 5];
-    const int lane = lane_id();
-    const int I = blockIdx.x * SYM_WARPS + (threadIdx.x >> 5);
+    __shared__ CtaSmem2 S;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int I = blockIdx.x;
     if (I >= A.tilem)
         return;
     const int a0 = __ldg(A.tile_ptr + I), a1 = __ldg(A.tile_ptr + I + 1);
-    const int cbeg = c_tile_ptr[I], cend = c_tile_ptr[I + 1];
-    if (lane < TD)
-        S.rowcnt[lane] = 0;
-    int lo, hi;
-    row_window(A, B, a0, a1, lo, hi);
-    int cbase = cbeg;
-    int rowrun = 0; // lane r (< 16): running CSR prefix of row r over the row's tiles
-    const bool multi = hi >= 0 && ((long long)hi - lo + 1 > SCAP);
-    long long w = lo;
-    while (hi >= 0 && w <= hi)
+    const int cbeg = __ldg(c_tile_ptr + I), cend = __ldg(c_tile_ptr + I + 1);
+    const int nrows = min(TD, A.m - I * TD);
+    const int r0 = warp * 2, r1 = r0 + 1;
+    uint32_t *mw = S.mw + warp * S2_STRIDE;
+    int4 *ent = S.ent[warp];
+    int run0 = 0, run1 = 0; // entries of rows r0, r1 so far
+
+    // tile-column range reachable from the tile row
+    if (tid == 0)
     {
-        // choose a window [w, wend) with at most SCAP C tiles
-        int width = WBITS;
-        int nW = 0;
-        int wend = 0;
-        for (;;)
+        S.lo = INT_MAX;
+        S.hi = -1;
+    }
+    __syncthreads();
+    {
+        int lo = INT_MAX, hi = -1;
+        for (int a = a0 + tid; a < a1; a += S2_THREADS)
         {
-            wend = (int)min((long long)hi + 1, w + width);
-            for (int i = lane; i < WWORDS; i += 32)
-                S.bitmap[i] = 0;
-            __syncwarp();
-            fill_bitmap(A, B, a0, a1, (int)w, wend, multi, S.bitmap, S.start, S.pre);
-            int c = 0;
-            for (int i = lane; i < WWORDS; i += 32)
-                c += __popc(S.bitmap[i]);
-            nW = warp_sum(c);
-            if (nW <= SCAP || width <= SCAP)
-                break;
-            width >>= 1;
-            __syncwarp();
-        }
-        // word prefix of the bitmap (slot rank lookup)
-        {
-            int run = 0;
-            for (int base = 0; base < WWORDS; base += 32)
+            const int K = __ldg(A.tile_col + a);
+            const int b0 = __ldg(B.tile_ptr + K), b1 = __ldg(B.tile_ptr + K + 1);
+            if (b0 < b1)
             {
-                const int v = __popc(S.bitmap[base + lane]);
-                const int incl = warp_incl_scan(v);
-                S.wordpre[base + lane] = run + incl - v;
-                run += __shfl_sync(FULL, incl, 31);
+                lo = min(lo, __ldg(B.tile_col + b0));
+                hi = max(hi, __ldg(B.tile_col + b1 - 1));
             }
         }
-        for (int i = lane; i < nW * 8; i += 32)
-            S.smask[i] = 0;
-        __syncwarp();
-        if (cbase + nW > cend)
+        lo = warp_min(lo);
+        hi = warp_max(hi);
+        if (lane == 0)
         {
-            set_error(err, DERR_SYM_OVERFLOW);
+            atomicMin(&S.lo, lo);
+            atomicMax(&S.hi, hi);
+        }
+    }
+    __syncthreads();
+    const int lo = S.lo, hi = S.hi;
+    const bool clip = hi >= 0 && (long long)hi - lo + 1 > WBITS;
+    int cbase = cbeg;
+    for (long long wl = lo; hi >= 0 && wl <= hi;)
+    {
+        const int w = (int)wl;
+        int wend = (int)min((long long)hi + 1, wl + WBITS);
+        // ---- C tiles of the window: bitmap of the B tile columns in [w, wend)
+        for (int i = tid; i < WWORDS; i += S2_THREADS)
+            S.bitmap[i] = 0u;
+        __syncthreads();
+        for (int a = a0 + warp; a < a1; a += S2_WARPS)
+        {
+            const int K = __ldg(A.tile_col + a);
+            int b0 = __ldg(B.tile_ptr + K), b1 = __ldg(B.tile_ptr + K + 1);
+            if (clip)
+            {
+                b0 = lower_bound(B.tile_col, b0, b1, w);
+                b1 = lower_bound(B.tile_col, b0, b1, wend);
+            }
+            for (int j = b0 + lane; j < b1; j += 32)
+            {
+                const int off = __ldg(B.tile_col + j) - w;
+                atomicOr(&S.bitmap[off >> 5], 1u << (off & 31));
+            }
+        }
+        __syncthreads();
+        if (warp == 0)
+        {
+            int run = 0;
+            for (int q0 = 0; q0 < WWORDS; q0 += 32)
+            {
+                const int v = __popc(S.bitmap[q0 + lane]);
+                const int incl = warp_incl_scan(v);
+                S.wordpre[q0 + lane] = run + incl - v;
+                run += __shfl_sync(FULL, incl, 31);
+            }
+            if (lane == 0)
+            {
+                int nb = run, we = wend;
+                if (nb > S2_SLOTS)
+                {
+                    // cut the window after its S2_SLOTS-th tile column
+                    int q = 0;
+                    while (S.wordpre[q] + __popc(S.bitmap[q]) < S2_SLOTS)
+                        ++q;
+                    uint32_t bits = S.bitmap[q];
+                    for (int k = S.wordpre[q]; k < S2_SLOTS - 1; ++k)
+                        bits &= bits - 1;
+                    we = w + q * 32 + __ffs(bits); // one past the last kept column
+                    nb = S2_SLOTS;
+                }
+                S.nb = nb;
+                S.wend = we;
+            }
+        }
+        __syncthreads();
+        const int nb = S.nb;
+        wend = S.wend;
+        const int wlen = wend - w;
+        if (cbase + nb > cend)
+        {
+            if (tid == 0)
+                set_error(err, DERR_SYM_OVERFLOW);
             return;
         }
-        // C tile columns of this window
-        for (int wi = lane; wi < WWORDS; wi += 32)
+        for (int i = tid; i < WBITS / 4; i += S2_THREADS)
+            reinterpret_cast<uint32_t *>(S.slot8)[i] = 0xFFFFFFFFu;
+        __syncthreads();
+        for (int q = tid; q < WWORDS; q += S2_THREADS)
         {
-            uint32_t bits = S.bitmap[wi];
-            int slot = S.wordpre[wi];
+            uint32_t bits = S.bitmap[q];
+            int slot = S.wordpre[q];
             while (bits)
             {
                 const int b = __ffs(bits) - 1;
                 bits &= bits - 1;
-                c_tile_col[cbase + slot] = (int)w + wi * 32 + b;
-                c_tile_row[cbase + slot] = I;
+                const int d = q * 32 + b;
+                if (d < wlen)
+                {
+                    S.slot8[d] = (uint8_t)slot;
+                    c_tile_col[cbase + slot] = w + d;
+                    c_tile_row[cbase + slot] = I;
+                }
                 ++slot;
             }
         }
-        // mask products, one B tile per lane, K by K
-        for (int a = a0; a < a1; ++a)
+        for (int i = lane; i < nb; i += 32)
+            mw[i] = 0u;
+        __syncthreads();
+
+        // ---- masks: warp-private walk over the warp's A entries
+        if (r0 < nrows)
         {
-            const int K = __ldg(A.tile_col + a);
-            const int b0 = __ldg(B.tile_ptr + K), b1 = __ldg(B.tile_ptr + K + 1);
-            int s = b0, e = b1;
-            if (multi)
+            for (int t0 = a0; t0 < a1; t0 += 32)
             {
-                s = lower_bound(B.tile_col, b0, b1, (int)w);
-                e = lower_bound(B.tile_col, s, b1, wend);
-            }
-            if (s >= e)
-                continue;
-            const int an = __ldg(A.tile_nnz + a);
-            const uint4 ap = *reinterpret_cast<const uint4 *>(A.ptr + (size_t)a * TD);
-            const int aend = __ldg(A.tile_nnz + a + 1) - an;
-            for (int jb0 = s; jb0 < e; jb0 += 32)
-            {
-                const int jb = jb0 + lane;
-                const bool act = jb < e;
-                int slot = 0;
-                if (act)
+                const int t = t0 + lane;
+                int eb = 0, em = 0, n = 0, tn0 = 0, K = 0;
+                if (t < a1)
                 {
-                    const int J = __ldg(B.tile_col + jb);
-                    const int tb = B.row_data ? __ldg(B.row_data + jb) : jb;
-                    const int off = J - (int)w;
-                    const uint32_t word = S.bitmap[off >> 5];
-                    slot = S.wordpre[off >> 5] + __popc(word & ((1u << (off & 31)) - 1u));
-                    const uint4 *bm = reinterpret_cast<const uint4 *>(B.mask + (size_t)tb * TD);
-                    const uint4 m0 = __ldg(bm), m1 = __ldg(bm + 1);
-                    uint32_t *dst = &S.bmask[lane * 17];
-                    const uint32_t wv[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
-#pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                    {
-                        dst[2 * q] = wv[q] & 0xFFFFu;
-                        dst[2 * q + 1] = wv[q] >> 16;
-                    }
+                    tn0 = __ldg(A.tile_nnz + t);
+                    const int tcnt = __ldg(A.tile_nnz + t + 1) - tn0;
+                    const uint8_t *pp = A.ptr + (size_t)t * TD;
+                    eb = pp[r0];
+                    em = pp[r1];
+                    const int ee = r1 + 1 < TD ? (int)pp[r1 + 1] : tcnt;
+                    n = max(ee - eb, 0);
+                    K = __ldg(A.tile_col + t);
                 }
-                __syncwarp();
-                if (act)
+                const int incl = warp_incl_scan(n);
+                const int total = __shfl_sync(FULL, incl, 31);
+                for (int q0 = 0; q0 < total; q0 += 32)
                 {
-                    const uint32_t *bml = &S.bmask[lane * 17];
-                    const uint32_t pw[4] = {ap.x, ap.y, ap.z, ap.w};
-                    uint32_t prod[8];
+                    const int q = q0 + lane;
+                    int own = 0;
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        prod[q] = 0;
-#pragma unroll
-                    for (int r = 0; r < TD; ++r)
+                    for (int b = 16; b > 0; b >>= 1)
+                        if (__shfl_sync(FULL, incl, own + b - 1) <= q)
+                            own += b;
+                    own = min(own, 31);
+                    const int o_incl = __shfl_sync(FULL, incl, own);
+                    const int o_n = __shfl_sync(FULL, n, own);
+                    const int o_eb = __shfl_sync(FULL, eb, own);
+                    const int o_em = __shfl_sync(FULL, em, own);
+                    const int o_tn0 = __shfl_sync(FULL, tn0, own);
+                    const int o_K = __shfl_sync(FULL, K, own);
+                    int fs = 0, len = 0, sh = 0;
+                    if (q < total)
                     {
-                        const int i0 = (pw[r >> 2] >> ((r & 3) * 8)) & 0xFF;
-                        const int i1 = r == TD - 1 ? aend : ((pw[(r + 1) >> 2] >> (((r + 1) & 3) * 8)) & 0xFF);
-                        uint32_t pr = 0;
-                        for (int i = i0; i < i1; ++i)
-                            pr |= bml[__ldg(A.col + an + i) & 15];
-                        prod[r >> 1] |= pr << ((r & 1) * 16);
+                        const int e = o_eb + (q - (o_incl - o_n));
+                        sh = e < o_em ? 0 : 16;
+                        const int k = o_K * TD + (A.col[o_tn0 + e] & 15);
+                        if (k < B.m)
+                        {
+                            fs = min(max(__ldg(B.csr_rowptr + k), 0), B.nnz);
+                            len = min(max(__ldg(B.csr_rowptr + k + 1), fs), B.nnz) - fs;
+                        }
                     }
+                    ent[lane] = make_int4(fs, len, sh, 0);
+                    __syncwarp();
+                    const int nbat = min(32, total - q0);
+                    for (int j = 0; j < nbat; j += 2)
+                    {
+                        int4 e0 = ent[j], e1 = ent[(j + 1) & 31];
+                        if (j + 1 >= nbat)
+                            e1.y = 0;
+                        const int c0 = lane < e0.y ? __ldg(B.csr_col + e0.x + lane) : -1;
+                        const int c1 = lane < e1.y ? __ldg(B.csr_col + e1.x + lane) : -1;
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        if (prod[q])
-                            atomicOr(&S.smask[slot * 8 + q], prod[q]);
+                        for (int u = 0; u < 2; ++u)
+                        {
+                            const int4 eu = u ? e1 : e0;
+                            const int cu = u ? c1 : c0;
+                            for (int f = lane; f < eu.y; f += 32)
+                            {
+                                const int col = f == lane ? cu : __ldg(B.csr_col + eu.x + f);
+                                const int d = (col >> 4) - w;
+                                if ((unsigned)d < (unsigned)wlen)
+                                {
+                                    const int sl = S.slot8[d];
+                                    if (sl != 255)
+                                        atomicOr(&mw[sl], (0x8000u >> (col & 15)) << eu.z);
+                                }
+                            }
+                        }
+                    }
+                    __syncwarp(); // the next batch overwrites this warp's list
                 }
-                __syncwarp();
             }
         }
-        __syncwarp();
-        // write masks, tile counts and per-row prefixes; accumulate row counts
-        for (int q = lane; q < nW * 8; q += 32)
-            c_mask32[(size_t)(cbase + q / 8) * 8 + (q & 7)] = S.smask[q];
-        for (int sl = lane; sl < nW; sl += 32)
+        // per-row counts of the window (each warp its own rows)
+        {
+            int c0 = 0, c1 = 0;
+            for (int i = lane; i < nb; i += 32)
+            {
+                const uint32_t v = mw[i];
+                c0 += __popc(v & 0xFFFFu);
+                c1 += __popc(v >> 16);
+            }
+            run0 += warp_sum(c0);
+            run1 += warp_sum(c1);
+        }
+        __syncthreads();
+        // ---- outputs of the window: masks (coalesced u16), tile counts
+        for (int i = tid; i < nb * TD; i += S2_THREADS)
+        {
+            const int sl = i >> 4, r = i & 15;
+            const uint32_t v = S.mw[(r >> 1) * S2_STRIDE + sl];
+            c_mask[(size_t)(cbase + sl) * TD + r] = (uint16_t)((v >> ((r & 1) * 16)) & 0xFFFFu);
+        }
+        for (int sl = tid; sl < nb; sl += S2_THREADS)
         {
             int c = 0;
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
-                c += __popc(S.smask[sl * 8 + q]);
+            for (int wv = 0; wv < S2_WARPS; ++wv)
+                c += __popc(S.mw[wv * S2_STRIDE + sl]);
             c_tile_cnt[cbase + sl] = c;
         }
-        // per-row running prefix across the window's tiles (lanes = rows)
-        if (lane < TD)
-        {
-            const int r = lane;
-            for (int sl = 0; sl < nW; ++sl)
-            {
-                c_row_prefix[(size_t)(cbase + sl) * TD + r] = rowrun;
-                rowrun += __popc((S.smask[sl * 8 + (r >> 1)] >> ((r & 1) * 16)) & 0xFFFFu);
-            }
-        }
-        __syncwarp();
-        cbase += nW;
-        w = wend;
+        __syncthreads();
+        cbase += nb;
+        wl = wend;
     }
     if (cbase != cend)
-        set_error(err, DERR_SYM_OVERFLOW);
-    const int nrows = min(TD, A.m - I * TD);
-    int total = 0;
-    if (lane < TD)
     {
-        if (lane < nrows)
-            c_row_cnt[I * TD + lane] = rowrun;
-        total = rowrun;
+        if (tid == 0)
+            set_error(err, DERR_SYM_OVERFLOW);
+        return;
     }
-    total = warp_sum(total);
     if (lane == 0)
-        c_tr_nnz[I] = total;
+    {
+        if (r0 < nrows)
+            c_row_cnt[I * TD + r0] = run0;
+        if (r1 < nrows)
+            c_row_cnt[I * TD + r1] = run1;
+    }
+    // tile row total
+    __shared__ int tot;
+    if (tid == 0)
+        tot = 0;
+    __syncthreads();
+    if (lane == 0)
+        atomicAdd(&tot, run0 + run1);
+    __syncthreads();
+    if (tid == 0)
+        c_tr_nnz[I] = tot;
 }
-
-__global__ void k_set_i64(long long *p, long long v) { *p = v; }
-
-inline int grid_for(long long threads, int block) { return (int)((threads + block - 1) / block); }
 
 } // namespace
 
@@ -372,16 +461,12 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
     RTT_CHECK(S.c_rowptr.ensure(sizeof(long long) * (size_t)(tilem + 1), s));
     RTT_CHECK(S.c_tr_nnz.ensure(sizeof(int) * (size_t)(tilem + 1), s));
     RTT_CHECK(S.tile_cnt.ensure(sizeof(int) * (nt + 1), s));
-    RTT_CHECK(S.row_prefix.ensure(sizeof(int) * nt * TD, s));
     if (tilem > 0)
     {
-        const size_t smem = sizeof(WarpSmem2) * SYM_WARPS;
-        RTT_CUDA(cudaFuncSetAttribute(k_sym_struct, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-        k_sym_struct<<<ceil_div(tilem, SYM_WARPS), SYM_WARPS * 32, smem, s>>>(
+        k_sym_rows<<<tilem, S2_THREADS, 0, s>>>(
             A, B, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(), S.c_tile_row.as<int>(),
-            S.c_mask.as<uint32_t>(), S.tile_cnt.as<int>(), S.row_prefix.as<int>(),
-            S.c_row_cnt.as<int>(), S.c_tr_nnz.as<int>(), ws.err.as<int>());
+            S.c_mask.as<uint16_t>(), S.tile_cnt.as<int>(), S.c_row_cnt.as<int>(),
+            S.c_tr_nnz.as<int>(), ws.err.as<int>());
         ws.launches++;
     }
     // exact sizes: nnz(C) as int64 over tile rows first (int32 overflow check)

@@ -99,6 +99,20 @@ def test_general_ab(orc):
     ctx.close()
 
 
+def test_wide_and_crowded_tile_rows(orc):
+    """C tile rows whose tile columns span more than the 8192-column bitmap of
+    the symbolic step, and rows with more C tiles than one slot window: both
+    are processed in column windows."""
+    A = G.random_csr(40, 500, 0.05, seed=41)
+    B = G.random_csr(500, 300000, 0.0004, seed=42)
+    ctx = R.Context(0)
+    rp, ci, va, nnz, tiles = _run(ctx, A, B)
+    erp, ecol, evals, eabs = orc.spgemm_csr(A, B)
+    assert_csr_close(rp, ci, va, erp, ecol, evals, eabs, "wide A*B: ")
+    assert tiles > 2 * 254  # several slot windows per C tile row
+    ctx.close()
+
+
 def test_deterministic_and_reusable(orc):
     """Two runs on one context give bitwise-identical values (no atomics in
     the value accumulation), and the context can switch problems."""
