@@ -88,15 +88,30 @@ __device__ __forceinline__ int flat_slot(const FlatSmem &S, const Window &W, int
     return (s < W.nW && S.cJ[s] == J) ? s : -1;
 }
 
-template <bool SAFE>
+// One product into the accumulator.  CHECK = false is the single-window case
+// with a slot table: every product's C tile is in the window by construction
+// (the symbolic step saw the same A tiles and B rows), so the lookup runs
+// without branches; the two clamps only keep inconsistent operands inside
+// this CTA's shared memory.
+template <bool SAFE, bool CHECK>
 __device__ __forceinline__ void flat_add(FlatSmem &S, const Window &W, const uint32_t *cmr,
                                          int col, double a, double b)
 {
-    const int slot = flat_slot(S, W, col >> 4);
-    if (slot < 0)
-        return;
+    int slot;
+    if (CHECK)
+    {
+        slot = flat_slot(S, W, col >> 4);
+        if (slot < 0)
+            return;
+    }
+    else
+    {
+        slot = S.slot8[min((unsigned)((col >> 4) - W.Jlo), (unsigned)(F_SPAN_CAP - 1))];
+    }
     const uint32_t w = cmr[slot];
-    const int pos = (int)(w >> 16) + __popc((w & 0xFFFFu) >> (16 - (col & 15)));
+    int pos = (int)(w >> 16) + __popc((w & 0xFFFFu) >> (16 - (col & 15)));
+    if (!CHECK)
+        pos = min(pos, F_ACC_CAP - 1);
     if (SAFE)
         atomicAdd(&S.acc[pos], a * b);
     else
@@ -128,6 +143,109 @@ __device__ __forceinline__ void write_row_cols(const FlatSmem &S, int r, int nW,
             ++k;
         }
     }
+}
+
+// The warp's products for one window: every A entry (r, k) of its rows r0, r1
+// times B's row k.  Returns the number of products when count is set.
+template <bool SAFE, bool CHECK>
+__device__ __forceinline__ long long warp_products(FlatSmem &S, const Window &W, const DevTiles &A,
+                                                   const DevTiles &B, int a0, int a1, int r0,
+                                                   int r1, bool count, int4 *ent, double *enta)
+{
+    const int lane = lane_id();
+    long long n_fma = 0;
+    for (int t0 = a0; t0 < a1; t0 += 32)
+    {
+        const int t = t0 + lane;
+        int eb = 0, em = 0, n = 0, tn0 = 0, K = 0;
+        if (t < a1)
+        {
+            tn0 = __ldg(A.tile_nnz + t);
+            const int tcnt = __ldg(A.tile_nnz + t + 1) - tn0;
+            const uint8_t *pp = A.ptr + (size_t)t * TD;
+            eb = pp[r0];
+            const int ee = r1 + 1 < TD ? (int)pp[r1 + 1] : tcnt;
+            em = RPW == 2 ? (int)pp[r1] : ee; // first entry of row r1
+            n = max(ee - eb, 0);
+            K = __ldg(A.tile_col + t);
+        }
+        const int incl = warp_incl_scan(n);
+        const int total = __shfl_sync(FULL, incl, 31);
+        for (int q0 = 0; q0 < total; q0 += 32)
+        {
+            // lane's entry q of the batch: owner tile by shuffle search
+            const int q = q0 + lane;
+            int own = 0;
+#pragma unroll
+            for (int b = 16; b > 0; b >>= 1)
+                if (__shfl_sync(FULL, incl, own + b - 1) <= q)
+                    own += b;
+            own = min(own, 31);
+            const int o_incl = __shfl_sync(FULL, incl, own);
+            const int o_n = __shfl_sync(FULL, n, own);
+            const int o_eb = __shfl_sync(FULL, eb, own);
+            const int o_em = __shfl_sync(FULL, em, own);
+            const int o_tn0 = __shfl_sync(FULL, tn0, own);
+            const int o_K = __shfl_sync(FULL, K, own);
+            int fs = 0, len = 0, rq = r0;
+            double a = 0.0;
+            if (q < total)
+            {
+                const int e = o_eb + (q - (o_incl - o_n));
+                rq = e < o_em ? r0 : r1;
+                const int k = o_K * TD + (A.col[o_tn0 + e] & 15);
+                a = __ldg(A.val + o_tn0 + e);
+                if (k < B.m)
+                {
+                    fs = min(max(__ldg(B.csr_rowptr + k), 0), B.nnz);
+                    len = min(max(__ldg(B.csr_rowptr + k + 1), fs), B.nnz) - fs;
+                }
+                if (count) // each pair once, in the first window
+                    n_fma += len;
+            }
+            ent[lane] = make_int4(fs, len, rq * F_CM_STRIDE, 0);
+            enta[lane] = a;
+            __syncwarp();
+            const int nb = min(32, total - q0);
+            for (int j = 0; j < nb; j += GROUP)
+            {
+                int4 ge[GROUP];
+                int gcol[GROUP];
+                double gb[GROUP];
+#pragma unroll
+                for (int u = 0; u < GROUP; ++u)
+                {
+                    ge[u] = ent[(j + u) & 31];
+                    if (j + u >= nb)
+                        ge[u].y = 0;
+                }
+#pragma unroll
+                for (int u = 0; u < GROUP; ++u)
+                {
+                    gcol[u] = 0;
+                    gb[u] = 0.0;
+                    if (lane < ge[u].y)
+                    {
+                        gcol[u] = __ldg(B.csr_col + ge[u].x + lane);
+                        gb[u] = __ldg(B.csr_val + ge[u].x + lane);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < GROUP; ++u)
+                {
+                    const double au = enta[(j + u) & 31];
+                    const uint32_t *cmr = S.cm + ge[u].z;
+                    if (lane < ge[u].y)
+                        flat_add<SAFE, CHECK>(S, W, cmr, gcol[u], au, gb[u]);
+                    for (int f = 32 + lane; f < ge[u].y; f += 32)
+                        flat_add<SAFE, CHECK>(S, W, cmr, __ldg(B.csr_col + ge[u].x + f), au,
+                                       __ldg(B.csr_val + ge[u].x + f));
+                }
+            }
+            __syncwarp(); // the next batch overwrites this warp's list
+        }
+    }
+    return n_fma;
 }
 
 template <bool SAFE>
@@ -175,8 +293,17 @@ __global__ void __launch_bounds__(F_THREADS, F_MIN_CTAS)
         const int w1 = w0 + nW;
         if (tid == 0)
             S.win_nnz = __ldg(c_tile_nnz + w1) - base_nnz;
-        for (int i = tid; i < nW * TD; i += F_THREADS)
-            S.cm[(i & 15) * F_CM_STRIDE + (i >> 4)] = __ldg(c_mask + (size_t)w0 * TD + i);
+        {
+            // two rows' masks per 32-bit word (c_mask rows are 32-byte aligned per tile)
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(c_mask + (size_t)w0 * TD);
+            for (int i = tid; i < nW * (TD / 2); i += F_THREADS)
+            {
+                const uint32_t v = __ldg(src + i);
+                const int s = i >> 3, r = (i & 7) * 2;
+                S.cm[r * F_CM_STRIDE + s] = v & 0xFFFFu;
+                S.cm[(r + 1) * F_CM_STRIDE + s] = v >> 16;
+            }
+        }
         for (int i = tid; i < nW; i += F_THREADS)
             S.cJ[i] = __ldg(c_tile_col + w0 + i);
         for (int i = tid; i < F_SPAN_CAP / 4; i += F_THREADS)
@@ -190,41 +317,41 @@ __global__ void __launch_bounds__(F_THREADS, F_MIN_CTAS)
         if (W.table)
             for (int i = tid; i < nW; i += F_THREADS)
                 S.slot8[S.cJ[i] - W.Jlo] = (uint8_t)i;
-        // per-row prefix over the window's tiles (each warp its own rows)
-#pragma unroll
-        for (int rr = 0; rr < RPW; ++rr)
+        // accumulator bases: (row r, slot s) starts at the entries of rows < r
+        // plus those of row r in slots < s.  Thread (r = tid / 16, part =
+        // tid % 16) owns a run of slots: sum, half-warp scan, write.
         {
-            uint32_t *cmr = S.cm + (r0 + rr) * F_CM_STRIDE;
-            int run = 0;
-            for (int s0 = 0; s0 < nW; s0 += 32)
+            static_assert(F_THREADS == TD * 16, "one half-warp per row");
+            const int r = tid >> 4, part = tid & 15;
+            const int per = (nW + 15) >> 4;
+            const int s0 = min(part * per, nW), s1 = min(s0 + per, nW);
+            uint32_t *cmr = S.cm + r * F_CM_STRIDE;
+            int sum = 0;
+            for (int s = s0; s < s1; ++s)
+                sum += __popc(cmr[s]);
+            const int incl = half_incl_scan(sum);
+            if (part == 15)
+                S.rowtot[r] = incl;
+            __syncthreads();
+            int racc = 0; // entries of rows < r
+            for (int q = 0; q < r; ++q)
+                racc += S.rowtot[q];
+            if (tid == 0)
             {
-                const int s = s0 + lane;
-                const uint32_t m = s < nW ? cmr[s] : 0u;
-                const int v = __popc(m);
-                const int incl = warp_incl_scan(v);
-                if (s < nW)
-                    cmr[s] = ((uint32_t)(run + incl - v) << 16) | m;
-                run += __shfl_sync(FULL, incl, 31);
+                int t = 0;
+                for (int q = 0; q < TD; ++q)
+                {
+                    S.rowacc0[q] = t;
+                    t += S.rowtot[q];
+                }
+                S.rowacc0[TD] = t;
             }
-            if (lane == 0)
-                S.rowtot[r0 + rr] = run;
-        }
-        __syncthreads();
-        // row starts in the window accumulator (every warp scans the 16 totals)
-        {
-            const int v = lane < TD ? S.rowtot[lane] : 0;
-            const int incl = warp_incl_scan(v);
-            if (warp == 0 && lane <= TD)
-                S.rowacc0[lane] = incl - v; // lane 16: v = 0, so this is the window total
-            const int acc_r0 = __shfl_sync(FULL, incl - v, r0);
-            const int acc_r1 = __shfl_sync(FULL, incl - v, r1);
-#pragma unroll
-            for (int rr = 0; rr < RPW; ++rr)
+            int run = racc + incl - sum;
+            for (int s = s0; s < s1; ++s)
             {
-                uint32_t *cmr = S.cm + (r0 + rr) * F_CM_STRIDE;
-                const uint32_t add = (uint32_t)(rr ? acc_r1 : acc_r0) << 16;
-                for (int s = lane; s < nW; s += 32)
-                    cmr[s] += add;
+                const uint32_t m = cmr[s];
+                cmr[s] = ((uint32_t)run << 16) | m;
+                run += __popc(m);
             }
         }
         if (tid < nrows && csr_rowptr != nullptr)
@@ -236,97 +363,11 @@ __global__ void __launch_bounds__(F_THREADS, F_MIN_CTAS)
         // ---- products: warp-private, no CTA barrier
         if (r0 < nrows)
         {
-            for (int t0 = a0; t0 < a1; t0 += 32)
-            {
-                const int t = t0 + lane;
-                int eb = 0, em = 0, n = 0, tn0 = 0, K = 0;
-                if (t < a1)
-                {
-                    tn0 = __ldg(A.tile_nnz + t);
-                    const int tcnt = __ldg(A.tile_nnz + t + 1) - tn0;
-                    const uint8_t *pp = A.ptr + (size_t)t * TD;
-                    eb = pp[r0];
-                    const int ee = r1 + 1 < TD ? (int)pp[r1 + 1] : tcnt;
-                    em = RPW == 2 ? (int)pp[r1] : ee; // first entry of row r1
-                    n = max(ee - eb, 0);
-                    K = __ldg(A.tile_col + t);
-                }
-                const int incl = warp_incl_scan(n);
-                const int total = __shfl_sync(FULL, incl, 31);
-                for (int q0 = 0; q0 < total; q0 += 32)
-                {
-                    // lane's entry q of the batch: owner tile by shuffle search
-                    const int q = q0 + lane;
-                    int own = 0;
-#pragma unroll
-                    for (int b = 16; b > 0; b >>= 1)
-                        if (__shfl_sync(FULL, incl, own + b - 1) <= q)
-                            own += b;
-                    own = min(own, 31);
-                    const int o_incl = __shfl_sync(FULL, incl, own);
-                    const int o_n = __shfl_sync(FULL, n, own);
-                    const int o_eb = __shfl_sync(FULL, eb, own);
-                    const int o_em = __shfl_sync(FULL, em, own);
-                    const int o_tn0 = __shfl_sync(FULL, tn0, own);
-                    const int o_K = __shfl_sync(FULL, K, own);
-                    int fs = 0, len = 0, rq = r0;
-                    double a = 0.0;
-                    if (q < total)
-                    {
-                        const int e = o_eb + (q - (o_incl - o_n));
-                        rq = e < o_em ? r0 : r1;
-                        const int k = o_K * TD + (A.col[o_tn0 + e] & 15);
-                        a = __ldg(A.val + o_tn0 + e);
-                        if (k < B.m)
-                        {
-                            fs = min(max(__ldg(B.csr_rowptr + k), 0), B.nnz);
-                            len = min(max(__ldg(B.csr_rowptr + k + 1), fs), B.nnz) - fs;
-                        }
-                        if (w0 == cs0) // count each pair once, in the first window
-                            n_fma += len;
-                    }
-                    ent[lane] = make_int4(fs, len, rq * F_CM_STRIDE, 0);
-                    enta[lane] = a;
-                    __syncwarp();
-                    const int nb = min(32, total - q0);
-                    for (int j = 0; j < nb; j += GROUP)
-                    {
-                        int4 ge[GROUP];
-                        int gcol[GROUP];
-                        double gb[GROUP];
-#pragma unroll
-                        for (int u = 0; u < GROUP; ++u)
-                        {
-                            ge[u] = ent[(j + u) & 31];
-                            if (j + u >= nb)
-                                ge[u].y = 0;
-                        }
-#pragma unroll
-                        for (int u = 0; u < GROUP; ++u)
-                        {
-                            gcol[u] = 0;
-                            gb[u] = 0.0;
-                            if (lane < ge[u].y)
-                            {
-                                gcol[u] = __ldg(B.csr_col + ge[u].x + lane);
-                                gb[u] = __ldg(B.csr_val + ge[u].x + lane);
-                            }
-                        }
-#pragma unroll
-                        for (int u = 0; u < GROUP; ++u)
-                        {
-                            const double au = enta[(j + u) & 31];
-                            const uint32_t *cmr = S.cm + ge[u].z;
-                            if (lane < ge[u].y)
-                                flat_add<SAFE>(S, W, cmr, gcol[u], au, gb[u]);
-                            for (int f = 32 + lane; f < ge[u].y; f += 32)
-                                flat_add<SAFE>(S, W, cmr, __ldg(B.csr_col + ge[u].x + f), au,
-                                               __ldg(B.csr_val + ge[u].x + f));
-                        }
-                    }
-                    __syncwarp(); // the next batch overwrites this warp's list
-                }
-            }
+            // count each pair once, in the first window
+            if (W.table && nW == cs1 - cs0)
+                n_fma += warp_products<SAFE, false>(S, W, A, B, a0, a1, r0, r1, w0 == cs0, ent, enta);
+            else
+                n_fma += warp_products<SAFE, true>(S, W, A, B, a0, a1, r0, r1, w0 == cs0, ent, enta);
         }
         __syncthreads();
 

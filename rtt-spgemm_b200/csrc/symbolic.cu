@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(SYM_WARPS * 32) k_sym_count(DevTiles A, DevTil
 
 // Step 2.  Outputs per C tile: column, tile row, 16 row masks and entry
 // count; per scalar row: entry count; per tile row: entry total.
-__global__ void __launch_bounds__(S2_THREADS, 4)
+__global__ void __launch_bounds__(S2_THREADS, 5)
     k_sym_rows(DevTiles A, DevTiles B, const int *__restrict__ c_tile_ptr,
                int *__restrict__ c_tile_col, int *__restrict__ c_tile_row,
                uint16_t *__restrict__ c_mask, int *__restrict__ c_tile_cnt,
