@@ -32,7 +32,9 @@
 //
 // Windows of C tiles (<= F_SLOT_CAP tiles, <= F_ACC_CAP entries) bound shared
 // memory; products whose C tile is outside the window are skipped and the A
-// list is walked again for the next window.  Shared memory (~38 KB) and
+// list is walked again for the next window.  Each product also stores its
+// column beside its accumulator slot, so the CSR write-out of a row is two
+// contiguous copies.  Shared memory (~43 KB) and
 // registers (<= 48) are sized so that five CTAs share an SM: the kernel is
 // latency-bound and lives on the number of warps in flight.
 #include "rtt_internal.cuh"
@@ -46,7 +48,7 @@ constexpr int FW = 8;                       // warps per CTA
 constexpr int RPW = TD / FW;                // rows per warp
 constexpr int F_THREADS = FW * 32;
 constexpr int F_MIN_CTAS = 5;               // CTAs per SM the launch bounds aim at
-constexpr int F_ACC_CAP = 2304;             // FP64 accumulator slots per window
+constexpr int F_ACC_CAP = 2048;             // accumulator slots per window
 constexpr int F_SLOT_CAP = 128;             // C tiles per window
 constexpr int F_CM_STRIDE = F_SLOT_CAP + 1; // row stride of cm: rows land in distinct banks
 constexpr int F_SPAN_CAP = 4096;            // tile-column span of the slot table
@@ -56,6 +58,7 @@ static_assert(RPW == 1 || RPW == 2, "one or two rows per warp");
 struct FlatSmem
 {
     double acc[F_ACC_CAP];
+    int ccol[F_ACC_CAP];              // column of each accumulator slot (written by the products)
     uint32_t cm[TD * F_CM_STRIDE];    // [row][slot]: (acc base << 16) | row mask
     int cJ[F_SLOT_CAP];
     uint8_t slot8[F_SPAN_CAP];        // tile column - Jlo -> slot (255 = none)
@@ -116,33 +119,7 @@ __device__ __forceinline__ void flat_add(FlatSmem &S, const Window &W, const uin
         atomicAdd(&S.acc[pos], a * b);
     else
         S.acc[pos] = fma(a, b, S.acc[pos]);
-}
-
-// Column indices of one (row, window) into the CSR output: lanes over slots.
-__device__ __forceinline__ void write_row_cols(const FlatSmem &S, int r, int nW, long long rowpos,
-                                               int acc0, long long nnzC, int *csr_col, int *err)
-{
-    const uint32_t *cmr = S.cm + r * F_CM_STRIDE;
-    for (int s = lane_id(); s < nW; s += 32)
-    {
-        const uint32_t w = cmr[s];
-        uint32_t mm = w & 0xFFFFu;
-        const long long pos = rowpos + ((int)(w >> 16) - acc0);
-        const int cb = S.cJ[s] * TD;
-        int k = 0;
-        while (mm)
-        {
-            const int c = __clz(mm) - 16;
-            mm &= ~(0x8000u >> c);
-            if (pos + k >= nnzC)
-            {
-                set_error(err, DERR_NUM_BOUNDS);
-                break;
-            }
-            csr_col[pos + k] = cb + c;
-            ++k;
-        }
-    }
+    S.ccol[pos] = col; // every structural entry receives at least one product
 }
 
 // The warp's products for one window: every A entry (r, k) of its rows r0, r1
@@ -389,8 +366,10 @@ __global__ void __launch_bounds__(F_THREADS, F_MIN_CTAS)
                     continue;
                 }
                 for (int p = b0 + lane; p < b1; p += 32)
+                {
                     csr_val[dst + p] = S.acc[p];
-                write_row_cols(S, r, nW, S.rowcsr0[r], b0, nnzC, csr_col, err);
+                    csr_col[dst + p] = S.ccol[p];
+                }
             }
         }
         if (c_val != nullptr)
