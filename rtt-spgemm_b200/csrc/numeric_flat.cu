@@ -214,9 +214,10 @@ __device__ __forceinline__ long long warp_products(FlatSmem &S, const Window &W,
                     const uint32_t *cmr = S.cm + ge[u].z;
                     if (lane < ge[u].y)
                         flat_add<SAFE, CHECK>(S, W, cmr, gcol[u], au, gb[u]);
-                    for (int f = 32 + lane; f < ge[u].y; f += 32)
-                        flat_add<SAFE, CHECK>(S, W, cmr, __ldg(B.csr_col + ge[u].x + f), au,
-                                       __ldg(B.csr_val + ge[u].x + f));
+                    if (ge[u].y > 32) // rows longer than a warp (uniform branch)
+                        for (int f = 32 + lane; f < ge[u].y; f += 32)
+                            flat_add<SAFE, CHECK>(S, W, cmr, __ldg(B.csr_col + ge[u].x + f), au,
+                                                  __ldg(B.csr_val + ge[u].x + f));
                 }
             }
             __syncwarp(); // the next batch overwrites this warp's list

@@ -340,6 +340,16 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
                     ent[lane] = make_int4(fs, len, sh, 0);
                     __syncwarp();
                     const int nbat = min(32, total - q0);
+                    // one column of B row k into the mask of row r's C tile
+                    auto mark = [&](int col, int sh) {
+                        const int d = (col >> 4) - w;
+                        if ((unsigned)d < (unsigned)wlen)
+                        {
+                            const int sl = S.slot8[d];
+                            if (sl != 255)
+                                atomicOr(&mw[sl], (0x8000u >> (col & 15)) << sh);
+                        }
+                    };
                     for (int j = 0; j < nbat; j += 2)
                     {
                         int4 e0 = ent[j], e1 = ent[(j + 1) & 31];
@@ -347,23 +357,16 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
                             e1.y = 0;
                         const int c0 = lane < e0.y ? __ldg(B.csr_col + e0.x + lane) : -1;
                         const int c1 = lane < e1.y ? __ldg(B.csr_col + e1.x + lane) : -1;
-#pragma unroll
-                        for (int u = 0; u < 2; ++u)
-                        {
-                            const int4 eu = u ? e1 : e0;
-                            const int cu = u ? c1 : c0;
-                            for (int f = lane; f < eu.y; f += 32)
-                            {
-                                const int col = f == lane ? cu : __ldg(B.csr_col + eu.x + f);
-                                const int d = (col >> 4) - w;
-                                if ((unsigned)d < (unsigned)wlen)
-                                {
-                                    const int sl = S.slot8[d];
-                                    if (sl != 255)
-                                        atomicOr(&mw[sl], (0x8000u >> (col & 15)) << eu.z);
-                                }
-                            }
-                        }
+                        if (c0 >= 0)
+                            mark(c0, e0.z);
+                        if (e0.y > 32) // rows longer than a warp (uniform branch)
+                            for (int f = 32 + lane; f < e0.y; f += 32)
+                                mark(__ldg(B.csr_col + e0.x + f), e0.z);
+                        if (c1 >= 0)
+                            mark(c1, e1.z);
+                        if (e1.y > 32)
+                            for (int f = 32 + lane; f < e1.y; f += 32)
+                                mark(__ldg(B.csr_col + e1.x + f), e1.z);
                     }
                     __syncwarp(); // the next batch overwrites this warp's list
                 }
