@@ -284,8 +284,12 @@ __global__ void __launch_bounds__(F_THREADS, F_MIN_CTAS)
         }
         for (int i = tid; i < nW; i += F_THREADS)
             S.cJ[i] = __ldg(c_tile_col + w0 + i);
-        for (int i = tid; i < F_SPAN_CAP / 4; i += F_THREADS)
-            reinterpret_cast<uint32_t *>(S.slot8)[i] = 0xFFFFFFFFu;
+        {
+            // the slot table covers the window's tile-column span only
+            const int span = __ldg(c_tile_col + w1 - 1) - __ldg(c_tile_col + w0) + 1;
+            for (int i = tid; i < min((span + 3) / 4, F_SPAN_CAP / 4); i += F_THREADS)
+                reinterpret_cast<uint32_t *>(S.slot8)[i] = 0xFFFFFFFFu;
+        }
         __syncthreads();
         Window W;
         W.Jlo = S.cJ[0];

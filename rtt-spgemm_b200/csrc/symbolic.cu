@@ -134,13 +134,14 @@ __global__ void __launch_bounds__(SYM_WARPS * 32) k_sym_count(DevTiles A, DevTil
         const bool multi = (long long)hi - lo + 1 > WBITS;
         for (long long w = lo; w <= hi; w += WBITS)
         {
-            for (int i = lane; i < WWORDS; i += 32)
+            const int wend = (int)min((long long)hi + 1, w + WBITS);
+            const int nwords = (int)((wend - w + 31) >> 5);
+            for (int i = lane; i < nwords; i += 32)
                 S.bitmap[i] = 0;
             __syncwarp();
-            const int wend = (int)min((long long)hi + 1, w + WBITS);
             fill_bitmap(A, B, a0, a1, (int)w, wend, multi, S.bitmap, S.start, S.pre);
             int c = 0;
-            for (int i = lane; i < WWORDS; i += 32)
+            for (int i = lane; i < nwords; i += 32)
                 c += __popc(S.bitmap[i]);
             count += warp_sum(c);
             __syncwarp();
@@ -206,8 +207,9 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
     {
         const int w = (int)wl;
         int wend = (int)min((long long)hi + 1, wl + WBITS);
+        const int nwords = (wend - w + 31) >> 5; // bitmap words the window can touch
         // ---- C tiles of the window: bitmap of the B tile columns in [w, wend)
-        for (int i = tid; i < WWORDS; i += S2_THREADS)
+        for (int i = tid; i < nwords; i += S2_THREADS)
             S.bitmap[i] = 0u;
         __syncthreads();
         for (int a = a0 + warp; a < a1; a += S2_WARPS)
@@ -229,11 +231,12 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
         if (warp == 0)
         {
             int run = 0;
-            for (int q0 = 0; q0 < WWORDS; q0 += 32)
+            for (int q0 = 0; q0 < nwords; q0 += 32)
             {
-                const int v = __popc(S.bitmap[q0 + lane]);
+                const int v = q0 + lane < nwords ? __popc(S.bitmap[q0 + lane]) : 0;
                 const int incl = warp_incl_scan(v);
-                S.wordpre[q0 + lane] = run + incl - v;
+                if (q0 + lane < nwords)
+                    S.wordpre[q0 + lane] = run + incl - v;
                 run += __shfl_sync(FULL, incl, 31);
             }
             if (lane == 0)
@@ -265,10 +268,10 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
                 set_error(err, DERR_SYM_OVERFLOW);
             return;
         }
-        for (int i = tid; i < WBITS / 4; i += S2_THREADS)
+        for (int i = tid; i < (wlen + 3) / 4; i += S2_THREADS)
             reinterpret_cast<uint32_t *>(S.slot8)[i] = 0xFFFFFFFFu;
         __syncthreads();
-        for (int q = tid; q < WWORDS; q += S2_THREADS)
+        for (int q = tid; q < nwords; q += S2_THREADS)
         {
             uint32_t bits = S.bitmap[q];
             int slot = S.wordpre[q];
