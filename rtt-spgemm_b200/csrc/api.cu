@@ -10,6 +10,7 @@
 
 #include <cub/device/device_radix_sort.cuh>
 
+#include <algorithm>
 #include <climits>
 #include <cstdlib>
 #include <cstring>
@@ -38,6 +39,9 @@ struct rtt_context_s
     const double *b_va = nullptr;
     long long b_nnz = 0;
     bool b_dups = false;
+    // page-locked staging of the host-buffer entry points (created on first use)
+    void *hstage[2] = {};
+    cudaEvent_t hstage_ev[2] = {};
 };
 
 namespace
@@ -65,34 +69,129 @@ int default_context(rtt_context *out)
     return RTT_OK;
 }
 
+// Host <-> device copies of the host-buffer entry points.  Page-locked host
+// memory is copied directly.  Pageable memory goes through two page-locked
+// staging buffers of the context: the DMA of one chunk overlaps the
+// multi-threaded host copy of the other (which also takes the first-touch page
+// faults of freshly malloc'd outputs on all cores instead of one).
+constexpr size_t kStageBytes = size_t(32) << 20;
+constexpr size_t kDirectBytes = size_t(4) << 20; // below this a plain copy is as fast
+
+void par_memcpy(void *dst, const void *src, size_t bytes)
+{
+    const size_t piece = size_t(1) << 20;
+    const long long n = (long long)((bytes + piece - 1) / piece);
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < n; ++i)
+    {
+        const size_t off = (size_t)i * piece;
+        std::memcpy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off,
+                    std::min(piece, bytes - off));
+    }
+}
+
+bool is_pageable(const void *p)
+{
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess)
+    {
+        cudaGetLastError(); // clear the sticky-free error of an unknown pointer
+        return true;
+    }
+    return at.type == cudaMemoryTypeUnregistered;
+}
+
+int ensure_stage(rtt_context c)
+{
+    for (int b = 0; b < 2; ++b)
+    {
+        if (c->hstage[b] == nullptr)
+            RTT_CUDA(cudaMallocHost(&c->hstage[b], kStageBytes));
+        if (c->hstage_ev[b] == nullptr)
+            RTT_CUDA(cudaEventCreateWithFlags(&c->hstage_ev[b], cudaEventDisableTiming));
+    }
+    return RTT_OK;
+}
+
+int h2d(rtt_context c, void *dst, const void *src, size_t bytes, cudaStream_t s)
+{
+    if (bytes < kDirectBytes || !is_pageable(src))
+    {
+        RTT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+        return RTT_OK;
+    }
+    RTT_CHECK(ensure_stage(c));
+    for (size_t off = 0, i = 0; off < bytes; off += kStageBytes, ++i)
+    {
+        const int b = (int)(i & 1);
+        const size_t n = std::min(kStageBytes, bytes - off);
+        RTT_CUDA(cudaEventSynchronize(c->hstage_ev[b])); // previous copy out of this buffer
+        par_memcpy(c->hstage[b], static_cast<const char *>(src) + off, n);
+        RTT_CUDA(cudaMemcpyAsync(static_cast<char *>(dst) + off, c->hstage[b], n,
+                                 cudaMemcpyHostToDevice, s));
+        RTT_CUDA(cudaEventRecord(c->hstage_ev[b], s));
+    }
+    return RTT_OK;
+}
+
+int d2h(rtt_context c, void *dst, const void *src, size_t bytes, cudaStream_t s)
+{
+    if (bytes < kDirectBytes || !is_pageable(dst))
+    {
+        RTT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+        RTT_CUDA(cudaStreamSynchronize(s));
+        return RTT_OK;
+    }
+    RTT_CHECK(ensure_stage(c));
+    const size_t nch = (bytes + kStageBytes - 1) / kStageBytes;
+    auto issue = [&](size_t i) -> int {
+        const int b = (int)(i & 1);
+        const size_t off = i * kStageBytes, n = std::min(kStageBytes, bytes - off);
+        RTT_CUDA(cudaMemcpyAsync(c->hstage[b], static_cast<const char *>(src) + off, n,
+                                 cudaMemcpyDeviceToHost, s));
+        RTT_CUDA(cudaEventRecord(c->hstage_ev[b], s));
+        return RTT_OK;
+    };
+    RTT_CUDA(cudaStreamSynchronize(s)); // staging buffers free of earlier uploads
+    RTT_CHECK(issue(0));
+    for (size_t i = 0; i < nch; ++i)
+    {
+        if (i + 1 < nch)
+            RTT_CHECK(issue(i + 1)); // its buffer's previous chunk was copied out below
+        const int b = (int)(i & 1);
+        RTT_CUDA(cudaEventSynchronize(c->hstage_ev[b]));
+        const size_t off = i * kStageBytes;
+        par_memcpy(static_cast<char *>(dst) + off, c->hstage[b], std::min(kStageBytes, bytes - off));
+    }
+    return RTT_OK;
+}
+
 template <typename T>
-int upload(DevBuf &b, const T *h, size_t n, cudaStream_t s)
+int upload(rtt_context c, DevBuf &b, const T *h, size_t n, cudaStream_t s)
 {
     RTT_CHECK(b.ensure(sizeof(T) * n + 16, s));
     if (n > 0)
     {
         if (h == nullptr)
             return fail(RTT_ERR_INVALID_ARGUMENT, "NULL host array with nonzero length");
-        RTT_CUDA(cudaMemcpyAsync(b.p, h, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+        RTT_CHECK(h2d(c, b.p, h, sizeof(T) * n, s));
     }
     return RTT_OK;
 }
 
 template <typename T>
-int download(T **out, const void *d, size_t n, cudaStream_t s)
+int download(rtt_context c, T **out, const void *d, size_t n, cudaStream_t s)
 {
     T *h = static_cast<T *>(std::malloc(sizeof(T) * (n > 0 ? n : 1)));
     if (h == nullptr)
         return fail(RTT_ERR_OUT_OF_MEMORY, "host malloc failed");
     if (n > 0)
     {
-        cudaError_t e = cudaMemcpyAsync(h, d, sizeof(T) * n, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess)
-            e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess)
+        const int st = d2h(c, h, d, sizeof(T) * n, s);
+        if (st != RTT_OK)
         {
             std::free(h);
-            return cuda_fail(e, "device to host copy");
+            return st;
         }
     }
     *out = h;
@@ -283,9 +382,9 @@ bool csr_args_ok(const SMatrix *M)
 int tile_host_csr(rtt_context c, const SMatrix *M, TileBufs &T, bool packed, bool sorted_rows)
 {
     cudaStream_t s = c->ws.stream;
-    RTT_CHECK(upload(c->in_rp, M->rowpointer, (size_t)M->m + (M->m > 0 ? 1 : 0), s));
-    RTT_CHECK(upload(c->in_col, M->columnindex, (size_t)M->nnz, s));
-    RTT_CHECK(upload(c->in_val, M->value, (size_t)M->nnz, s));
+    RTT_CHECK(upload(c, c->in_rp, M->rowpointer, (size_t)M->m + (M->m > 0 ? 1 : 0), s));
+    RTT_CHECK(upload(c, c->in_col, M->columnindex, (size_t)M->nnz, s));
+    RTT_CHECK(upload(c, c->in_val, M->value, (size_t)M->nnz, s));
     int st = csr2tile_device(c->ws, M->m, M->n, M->nnz, c->in_rp.as<int>(), c->in_col.as<int>(),
                              c->in_val.as<double>(), T, packed, sorted_rows);
     st = map_device_error(st);
@@ -317,10 +416,10 @@ int upload_tiles(rtt_context c, const SMatrix *M, bool col_major, TileBufs &T)
     T.tilen = tilen;
     T.numtile = nt;
     T.nnz = nnz;
-    RTT_CHECK(upload(T.tile_nnz, M->tile_nnz, (size_t)nt + 1, s));
-    RTT_CHECK(upload(T.ptr, M->tile_csr_Ptr, (size_t)nt * TD, s));
-    RTT_CHECK(upload(T.col, M->tile_csr_Col, (size_t)nnz, s));
-    RTT_CHECK(upload(T.val, M->tile_csr_Value, (size_t)nnz, s));
+    RTT_CHECK(upload(c, T.tile_nnz, M->tile_nnz, (size_t)nt + 1, s));
+    RTT_CHECK(upload(c, T.ptr, M->tile_csr_Ptr, (size_t)nt * TD, s));
+    RTT_CHECK(upload(c, T.col, M->tile_csr_Col, (size_t)nnz, s));
+    RTT_CHECK(upload(c, T.val, M->tile_csr_Value, (size_t)nnz, s));
     RTT_CHECK(T.mask.ensure(sizeof(uint16_t) * (size_t)nt * TD + 16, s));
     if (nt > 0)
     {
@@ -337,8 +436,8 @@ int upload_tiles(rtt_context c, const SMatrix *M, bool col_major, TileBufs &T)
     {
         if (M->tile_ptr == nullptr || (nt > 0 && M->tile_columnidx == nullptr))
             return fail(RTT_ERR_INVALID_ARGUMENT, "row-major tiles without tile_ptr/tile_columnidx");
-        RTT_CHECK(upload(T.tile_ptr, M->tile_ptr, (size_t)tilem + 1, s));
-        RTT_CHECK(upload(T.tile_col, M->tile_columnidx, (size_t)nt, s));
+        RTT_CHECK(upload(c, T.tile_ptr, M->tile_ptr, (size_t)tilem + 1, s));
+        RTT_CHECK(upload(c, T.tile_col, M->tile_columnidx, (size_t)nt, s));
         T.row_data.release();
         k_validate_lists<<<grid_for(tilem + 1, 256), 256, 0, s>>>(
             tilem, T.tile_ptr.as<int>(), T.tile_col.as<int>(), nt, tilen, c->ws.err.as<int>());
@@ -347,8 +446,8 @@ int upload_tiles(rtt_context c, const SMatrix *M, bool col_major, TileBufs &T)
     }
     if (M->csc_tile_ptr == nullptr || (nt > 0 && M->csc_tile_rowidx == nullptr))
         return fail(RTT_ERR_INVALID_ARGUMENT, "column-major tiles without csc_tile_ptr/csc_tile_rowidx");
-    RTT_CHECK(upload(T.csc_ptr, M->csc_tile_ptr, (size_t)tilen + 1, s));
-    RTT_CHECK(upload(T.csc_row, M->csc_tile_rowidx, (size_t)nt, s));
+    RTT_CHECK(upload(c, T.csc_ptr, M->csc_tile_ptr, (size_t)tilen + 1, s));
+    RTT_CHECK(upload(c, T.csc_row, M->csc_tile_rowidx, (size_t)nt, s));
     T.csc_data.release();
     k_validate_lists<<<grid_for(tilen + 1, 256), 256, 0, s>>>(
         tilen, T.csc_ptr.as<int>(), T.csc_row.as<int>(), nt, tilem, c->ws.err.as<int>());
@@ -511,6 +610,13 @@ void rtt_context_destroy(rtt_context c)
                            &c->out_col, &c->out_val, &c->counters, &c->maxnnz};
     for (rtt::DevBuf *b : bufs)
         b->release();
+    for (int b = 0; b < 2; ++b)
+    {
+        if (c->hstage[b] != nullptr)
+            cudaFreeHost(c->hstage[b]);
+        if (c->hstage_ev[b] != nullptr)
+            cudaEventDestroy(c->hstage_ev[b]);
+    }
     c->ws.destroy();
     delete c;
 }
@@ -561,14 +667,14 @@ int rtt_csr2tile_row_major(SMatrix *M)
     unsigned char **P = h.slot<unsigned char>(), **Cb = h.slot<unsigned char>();
     double **V = h.slot<double>();
     unsigned short **Mk = h.slot<unsigned short>();
-    RTT_CHECK(download(tp, T.tile_ptr.p, (size_t)T.tilem + 1, s));
-    RTT_CHECK(download(tc, T.tile_col.p, nt, s));
-    RTT_CHECK(download(tr, T.tile_row.p, nt, s));
-    RTT_CHECK(download(tn, T.tile_nnz.p, nt + 1, s));
-    RTT_CHECK(download(P, T.ptr.p, nt * TD, s));
-    RTT_CHECK(download(Cb, T.col.p, (size_t)M->nnz, s));
-    RTT_CHECK(download(V, T.val.p, (size_t)M->nnz, s));
-    RTT_CHECK(download(Mk, T.mask.p, nt * TD, s));
+    RTT_CHECK(download(c, tp, T.tile_ptr.p, (size_t)T.tilem + 1, s));
+    RTT_CHECK(download(c, tc, T.tile_col.p, nt, s));
+    RTT_CHECK(download(c, tr, T.tile_row.p, nt, s));
+    RTT_CHECK(download(c, tn, T.tile_nnz.p, nt + 1, s));
+    RTT_CHECK(download(c, P, T.ptr.p, nt * TD, s));
+    RTT_CHECK(download(c, Cb, T.col.p, (size_t)M->nnz, s));
+    RTT_CHECK(download(c, V, T.val.p, (size_t)M->nnz, s));
+    RTT_CHECK(download(c, Mk, T.mask.p, nt * TD, s));
     M->tilem = T.tilem;
     M->tilen = T.tilen;
     M->numtile = T.numtile;
@@ -606,15 +712,15 @@ int rtt_csr2tile_col_major(SMatrix *M)
     double **V = h.slot<double>();
     unsigned short **Mk = h.slot<unsigned short>();
     int **tr = h.slot<int>();
-    RTT_CHECK(download(tp, T.tile_ptr.p, (size_t)T.tilem + 1, s));
-    RTT_CHECK(download(tc, T.tile_col.p, nt, s));
-    RTT_CHECK(download(tn, U.tile_nnz.p, nt + 1, s));
-    RTT_CHECK(download(cp, T.csc_ptr.p, (size_t)T.tilen + 1, s));
-    RTT_CHECK(download(cr, T.csc_row.p, nt, s));
-    RTT_CHECK(download(P, U.ptr.p, nt * TD, s));
-    RTT_CHECK(download(Cb, U.col.p, (size_t)M->nnz, s));
-    RTT_CHECK(download(V, U.val.p, (size_t)M->nnz, s));
-    RTT_CHECK(download(Mk, U.mask.p, nt * TD, s));
+    RTT_CHECK(download(c, tp, T.tile_ptr.p, (size_t)T.tilem + 1, s));
+    RTT_CHECK(download(c, tc, T.tile_col.p, nt, s));
+    RTT_CHECK(download(c, tn, U.tile_nnz.p, nt + 1, s));
+    RTT_CHECK(download(c, cp, T.csc_ptr.p, (size_t)T.tilen + 1, s));
+    RTT_CHECK(download(c, cr, T.csc_row.p, nt, s));
+    RTT_CHECK(download(c, P, U.ptr.p, nt * TD, s));
+    RTT_CHECK(download(c, Cb, U.col.p, (size_t)M->nnz, s));
+    RTT_CHECK(download(c, V, U.val.p, (size_t)M->nnz, s));
+    RTT_CHECK(download(c, Mk, U.mask.p, nt * TD, s));
     *tr = static_cast<int *>(std::calloc(nt > 0 ? nt : 1, sizeof(int)));
     if (*tr == nullptr)
         return rtt::fail(RTT_ERR_OUT_OF_MEMORY, "host calloc failed");
@@ -691,14 +797,14 @@ int rtt_spgemm_tile(SMatrix *A, SMatrix *B, SMatrix *C)
     unsigned char **P = h.slot<unsigned char>(), **Cb = h.slot<unsigned char>();
     double **V = h.slot<double>();
     unsigned short **Mk = h.slot<unsigned short>();
-    RTT_CHECK(download(tp, S.c_tile_ptr.p, (size_t)S.tilem + 1, s));
-    RTT_CHECK(download(tc, S.c_tile_col.p, nt, s));
-    RTT_CHECK(download(tr, S.c_tile_row.p, nt, s));
-    RTT_CHECK(download(tn, S.c_tile_nnz.p, nt + 1, s));
-    RTT_CHECK(download(P, S.c_ptr.p, nt * TD, s));
-    RTT_CHECK(download(Cb, S.c_col.p, nnz, s));
-    RTT_CHECK(download(V, S.c_val.p, nnz, s));
-    RTT_CHECK(download(Mk, S.c_mask.p, nt * TD, s));
+    RTT_CHECK(download(c, tp, S.c_tile_ptr.p, (size_t)S.tilem + 1, s));
+    RTT_CHECK(download(c, tc, S.c_tile_col.p, nt, s));
+    RTT_CHECK(download(c, tr, S.c_tile_row.p, nt, s));
+    RTT_CHECK(download(c, tn, S.c_tile_nnz.p, nt + 1, s));
+    RTT_CHECK(download(c, P, S.c_ptr.p, nt * TD, s));
+    RTT_CHECK(download(c, Cb, S.c_col.p, nnz, s));
+    RTT_CHECK(download(c, V, S.c_val.p, nnz, s));
+    RTT_CHECK(download(c, Mk, S.c_mask.p, nt * TD, s));
     C->m = A->m;
     C->n = B->n;
     C->tilem = S.tilem;
@@ -749,13 +855,13 @@ int rtt_tile2csr_restore_rows(SMatrix *M, const int *new_to_old, int perm_size, 
     TileBufs &T = c->A;
     const int nt = M->numtile, tilem = M->tilem, m = M->m;
     const int tnz = nt >= 0 ? M->tile_nnz[nt] : 0;
-    RTT_CHECK(upload(T.tile_ptr, M->tile_ptr, (size_t)tilem + 1, s));
-    RTT_CHECK(upload(T.tile_col, M->tile_columnidx, (size_t)nt, s));
-    RTT_CHECK(upload(T.tile_nnz, M->tile_nnz, (size_t)nt + 1, s));
-    RTT_CHECK(upload(T.ptr, M->tile_csr_Ptr, (size_t)nt * tile_dim, s));
+    RTT_CHECK(upload(c, T.tile_ptr, M->tile_ptr, (size_t)tilem + 1, s));
+    RTT_CHECK(upload(c, T.tile_col, M->tile_columnidx, (size_t)nt, s));
+    RTT_CHECK(upload(c, T.tile_nnz, M->tile_nnz, (size_t)nt + 1, s));
+    RTT_CHECK(upload(c, T.ptr, M->tile_csr_Ptr, (size_t)nt * tile_dim, s));
     const size_t nent = (size_t)std::max(tnz, M->nnz);
-    RTT_CHECK(upload(T.col, M->tile_csr_Col, nent, s));
-    RTT_CHECK(upload(T.val, M->tile_csr_Value, nent, s));
+    RTT_CHECK(upload(c, T.col, M->tile_csr_Col, nent, s));
+    RTT_CHECK(upload(c, T.val, M->tile_csr_Value, nent, s));
     {
         // tile lists: monotone pointers, in-range entry offsets (columns are
         // range-checked per entry by the kernels, as the reference does)
@@ -768,7 +874,7 @@ int rtt_tile2csr_restore_rows(SMatrix *M, const int *new_to_old, int perm_size, 
         c->ws.launches += 2;
         RTT_CHECK(check_tiles(c->ws, "tile2csr input"));
     }
-    RTT_CHECK(upload(c->in2_rp, new_to_old, identity ? 0 : (size_t)perm_size, s));
+    RTT_CHECK(upload(c, c->in2_rp, new_to_old, identity ? 0 : (size_t)perm_size, s));
     const int *perm = identity ? nullptr : c->in2_rp.as<int>();
     const int psize = identity ? -1 : perm_size;
     RTT_CHECK(c->out_rp.ensure(sizeof(int) * ((size_t)m + 2), s));
@@ -797,9 +903,9 @@ int rtt_tile2csr_restore_rows(SMatrix *M, const int *new_to_old, int perm_size, 
     HostArrays h;
     int **rp = h.slot<int>(), **ci = h.slot<int>();
     double **v = h.slot<double>();
-    RTT_CHECK(download(rp, c->out_rp.p, (size_t)m + 1, s));
-    RTT_CHECK(download(ci, c->out_col.p, (size_t)total, s));
-    RTT_CHECK(download(v, c->out_val.p, (size_t)total, s));
+    RTT_CHECK(download(c, rp, c->out_rp.p, (size_t)m + 1, s));
+    RTT_CHECK(download(c, ci, c->out_col.p, (size_t)total, s));
+    RTT_CHECK(download(c, v, c->out_val.p, (size_t)total, s));
     M->rowpointer = *rp;
     M->columnindex = *ci;
     M->value = *v;
@@ -1040,17 +1146,17 @@ int rtt_spgemm_csr_host(rtt_context c, const SMatrix *A, const SMatrix *B, int o
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "spgemm_csr_host: bad arguments");
     RTT_CUDA(cudaSetDevice(c->ws.device));
     cudaStream_t s = c->ws.stream;
-    RTT_CHECK(upload(c->in_rp, A->rowpointer, (size_t)A->m + 1, s));
-    RTT_CHECK(upload(c->in_col, A->columnindex, (size_t)A->nnz, s));
-    RTT_CHECK(upload(c->in_val, A->value, (size_t)A->nnz, s));
+    RTT_CHECK(upload(c, c->in_rp, A->rowpointer, (size_t)A->m + 1, s));
+    RTT_CHECK(upload(c, c->in_col, A->columnindex, (size_t)A->nnz, s));
+    RTT_CHECK(upload(c, c->in_val, A->value, (size_t)A->nnz, s));
     rtt_csr_view va{A->m, A->n, A->nnz, c->in_rp.as<int>(), c->in_col.as<int>(),
                     c->in_val.as<double>()};
     rtt_csr_view vb{};
     if (B != nullptr)
     {
-        RTT_CHECK(upload(c->in2_rp, B->rowpointer, (size_t)B->m + 1, s));
-        RTT_CHECK(upload(c->in2_col, B->columnindex, (size_t)B->nnz, s));
-        RTT_CHECK(upload(c->in2_val, B->value, (size_t)B->nnz, s));
+        RTT_CHECK(upload(c, c->in2_rp, B->rowpointer, (size_t)B->m + 1, s));
+        RTT_CHECK(upload(c, c->in2_col, B->columnindex, (size_t)B->nnz, s));
+        RTT_CHECK(upload(c, c->in2_val, B->value, (size_t)B->nnz, s));
         vb = rtt_csr_view{B->m, B->n, B->nnz, c->in2_rp.as<int>(), c->in2_col.as<int>(),
                           c->in2_val.as<double>()};
     }
@@ -1066,9 +1172,9 @@ int rtt_spgemm_csr_host(rtt_context c, const SMatrix *A, const SMatrix *B, int o
     HostArrays h;
     int **rp = h.slot<int>(), **ci = h.slot<int>();
     double **v = h.slot<double>();
-    RTT_CHECK(download(rp, c->out_rp.p, (size_t)m + 1, s));
-    RTT_CHECK(download(ci, c->out_col.p, (size_t)nnz, s));
-    RTT_CHECK(download(v, c->out_val.p, (size_t)nnz, s));
+    RTT_CHECK(download(c, rp, c->out_rp.p, (size_t)m + 1, s));
+    RTT_CHECK(download(c, ci, c->out_col.p, (size_t)nnz, s));
+    RTT_CHECK(download(c, v, c->out_val.p, (size_t)nnz, s));
     std::memset(C, 0, sizeof(*C));
     C->m = m;
     C->n = n;

@@ -21,6 +21,7 @@ raise :class:`RttError` carrying the rtt_status code.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from types import SimpleNamespace
 
 import numpy as np
@@ -40,6 +41,19 @@ TD = 16
 
 def _ptr(a: np.ndarray, ct):
     return a.ctypes.data_as(C.POINTER(ct))
+
+
+def _adopt(p, count: int, dtype) -> np.ndarray:
+    """numpy view of an array the library malloc'd; the memory is freed when
+    the last view of it goes away (no copy of large outputs)."""
+    addr = C.cast(p, C.c_void_p).value if p else None
+    if count <= 0 or not addr:
+        if addr:
+            _libc_free(addr)
+        return np.zeros(max(count, 0), dtype=dtype)
+    buf = (C.c_char * (count * np.dtype(dtype).itemsize)).from_address(addr)
+    weakref.finalize(buf, _libc_free, addr)
+    return np.frombuffer(buf, dtype=dtype, count=count)
 
 
 def _copy(p, count: int, dtype) -> np.ndarray:
@@ -143,14 +157,9 @@ def tile2csr(tiles: dict, tile_dim: int = 8, canonical: bool = False, new_to_old
         size = p.shape[0] if perm_size is None else perm_size
         check(lib().rtt_tile2csr_restore_rows(C.byref(s), _ptr(p, C.c_int), size, tile_dim,
                                               int(canonical)))
-    out = SimpleNamespace(m=s.m, n=s.n, rowptr=_copy(s.rowpointer, s.m + 1, np.int32),
-                          col=_copy(s.columnindex, s.nnz, np.int32),
-                          val=_copy(s.value, s.nnz, np.float64))
-    for name in ("rowpointer", "columnindex", "value"):
-        p = getattr(s, name)
-        if p:
-            _libc_free(C.cast(p, C.c_void_p))
-    return out
+    return SimpleNamespace(m=s.m, n=s.n, rowptr=_adopt(s.rowpointer, s.m + 1, np.int32),
+                           col=_adopt(s.columnindex, s.nnz, np.int32),
+                           val=_adopt(s.value, s.nnz, np.float64))
 
 
 _LIBC = C.CDLL(None)
@@ -271,10 +280,9 @@ class Context:
         check(lib().rtt_spgemm_csr_host(self.handle, C.byref(sa),
                                         C.byref(sb) if sb is not None else None, op,
                                         C.byref(sc)))
-        out = CSR(sc.m, sc.n, _copy(sc.rowpointer, sc.m + 1, np.int32),
-                  _copy(sc.columnindex, sc.nnz, np.int32), _copy(sc.value, sc.nnz, np.float64))
-        _destroy(sc, owned_csr=True)
-        return out
+        # C's arrays were malloc'd by the library: hand them to numpy as they are
+        return CSR(sc.m, sc.n, _adopt(sc.rowpointer, sc.m + 1, np.int32),
+                   _adopt(sc.columnindex, sc.nnz, np.int32), _adopt(sc.value, sc.nnz, np.float64))
 
 
 def spgemm_csr_host(a, b=None, op: int = RTT_OP_AB, device: int = 0) -> CSR:
