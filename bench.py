@@ -195,6 +195,7 @@ def run_reference(args) -> None:
 def run_ours(args) -> None:
     import torch
     import rtt_spgemm as R
+    from rtt_spgemm import shards
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -260,19 +261,15 @@ def run_ours(args) -> None:
     if dist:
         dist.barrier()
     clocks = sampler.stop()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * flops / (ms * 1e-3) / 1e9
+    ms = shards.max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
+    value = shards.replica_throughput(world, flops, ms)
 
     st = ctx.stats()
     peaks = load_peaks()
     abytes = alg_bytes(A.m, A.nnz, A.nnz, nnz_c)
     num_ms = statistics.mean(stage["numeric_kernel_ms"])
     achieved = abytes / (num_ms * 1e-3) / 1e9
-    traffic = load_traffic(args.workload)
+    traffic = None if args.staging or args.unfused else load_traffic(args.workload)
 
     # end to end through the host-buffer C-ABI call (rtt_spgemm_csr_host):
     # H2D of A from pinned memory, the product, D2H of C into malloc'd arrays
@@ -292,12 +289,8 @@ def run_ours(args) -> None:
             Ch = ctx.spgemm_csr_host(Ah)
         e1.record(stream)
         torch.cuda.synchronize(dev)
-        e2e_ms = e0.elapsed_time(e1) / n_e2e
-        if dist:
-            t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
-        e2e = {"value": world * flops / (e2e_ms * 1e-3) / 1e9, "unit": "GFLOP/s",
+        e2e_ms = shards.max_over_ranks(e0.elapsed_time(e1) / n_e2e)
+        e2e = {"value": shards.replica_throughput(world, flops, e2e_ms), "unit": "GFLOP/s",
                "h2d_bytes_per_step": 4 * (A.m + 1) + 12 * A.nnz,
                "d2h_bytes_per_step": 4 * (A.m + 1) + 12 * int(Ch.nnz), "ms_per_step": e2e_ms}
 
@@ -324,7 +317,9 @@ def run_ours(args) -> None:
                          ((4 * (A.m + 1) + 12 * A.nnz) / 1e6),
                    "dmma_pair_cutoff": args.dmma_cutoff, "fused_tile2csr": not args.unfused,
                    "b_staging": bool(args.staging)},
-        "roofline": {"bound": "hbm", "kernel": "k_numeric (numeric + fused tile2csr)",
+        "roofline": {"bound": "hbm",
+                     "kernel": ("k_numeric_rows (TMA-staged numeric + fused tile2csr)" if args.staging
+                                else "k_numeric_flat (numeric + fused tile2csr)"),
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "peak_source": peaks["source"], "kernel_ms": num_ms,
