@@ -189,6 +189,37 @@ RTT_API int rtt_tile2csr_device_noalloc(const SMatrix *matrix, int tile_dim, int
  * bytes per tile, column byte = col % 8.  Empty 8x8 quadrants are dropped. */
 RTT_API int rtt_tile16_to_tile8(const SMatrix *c16, SMatrix *c8);
 
+/* The reference's HybridTileMatrix (src/dmma_tiles.h:29-62), field for field
+ * (MAT_PTR_TYPE = int): 32-element leaf tiles, 8x4 for A and 4x8 for B. */
+typedef struct
+{
+    int rows, cols, tile_rows, tile_cols, tile_row_count, tile_col_count;
+    int num_tiles, payload_size, dense_tiles, sparse_tiles;
+    int *tile_row_ptr;      /* tile_row_count + 1 */
+    int *tile_col_idx;      /* num_tiles */
+    int *value_offsets;     /* num_tiles + 1; span 32 <=> dense tile */
+    unsigned int *masks;    /* num_tiles, bit = physical index */
+    double *values;         /* payload_size */
+    int *tile_col_ptr;      /* optional tile CSC: tile_col_count + 1 */
+    int *tile_row_idx;      /* num_tiles */
+    int *csc_tile_ids;      /* num_tiles, ids in the tile CSR */
+} rtt_hybrid_tiles;
+
+/* Replaces csr_to_hybrid_tiles (src/dmma_tiles.h:243-438): host CSR in, hybrid
+ * leaf tiles out (malloc'd arrays; free with rtt_hybrid_tiles_destroy).  A
+ * uses (8, 4, col_major = 0), B uses (4, 8, col_major = 1); tile_rows *
+ * tile_cols must be 32 and 1 <= dense_threshold <= 32.  Repeated coordinates
+ * are summed.  Invalid CSR returns RTT_ERR_INVALID_CSR, other bad arguments
+ * RTT_ERR_INVALID_ARGUMENT; out is untouched on failure (the reference's
+ * transactional contract). */
+RTT_API int rtt_csr_to_hybrid_tiles(const SMatrix *csr, int tile_rows, int tile_cols,
+                                    int col_major, int dense_threshold, int build_csc,
+                                    rtt_hybrid_tiles *out);
+
+/* Frees the arrays of a hybrid tile matrix and zeroes it (the reference's
+ * destroy_hybrid_tile_matrix, src/dmma_tiles.h:64-79). */
+RTT_API void rtt_hybrid_tiles_destroy(rtt_hybrid_tiles *tiles);
+
 /* Frees every array the library allocated into matrix (tile fields, the csc
  * fields and, when owned_csr != 0, rowpointer/columnindex/value) and sets the
  * pointers to NULL.  The reference matrix_destroy (src/csr2tile.h:481-492)

@@ -127,6 +127,100 @@ class _Base:
                 setattr(s, name, None)
 
 
+class HybridTiles(C.Structure):
+    """HybridTileMatrix flattened (oracle/ref_tiles.cpp ref_hybrid; the
+    reference's src/dmma_tiles.h:29-62 with MAT_PTR_TYPE = int)."""
+
+    _fields_ = [(k, C.c_int) for k in ("rows", "cols", "tile_rows", "tile_cols",
+                                       "tile_row_count", "tile_col_count", "num_tiles",
+                                       "payload_size", "dense_tiles", "sparse_tiles")] + [
+        ("tile_row_ptr", C.POINTER(C.c_int)), ("tile_col_idx", C.POINTER(C.c_int)),
+        ("value_offsets", C.POINTER(C.c_int)), ("masks", C.POINTER(C.c_uint)),
+        ("values", C.POINTER(C.c_double)), ("tile_col_ptr", C.POINTER(C.c_int)),
+        ("tile_row_idx", C.POINTER(C.c_int)), ("csc_tile_ids", C.POINTER(C.c_int))]
+
+
+HYBRID_FIELDS = ("tile_row_ptr", "tile_col_idx", "value_offsets", "masks", "values",
+                 "tile_col_ptr", "tile_row_idx", "csc_tile_ids")
+
+
+def hybrid_to_dict(h) -> dict:
+    d = {k: getattr(h, k) for k in ("rows", "cols", "tile_rows", "tile_cols", "tile_row_count",
+                                    "tile_col_count", "num_tiles", "payload_size", "dense_tiles",
+                                    "sparse_tiles")}
+    nt = h.num_tiles
+    sizes = {"tile_row_ptr": h.tile_row_count + 1, "tile_col_idx": nt, "value_offsets": nt + 1,
+             "masks": nt, "values": h.payload_size, "tile_col_ptr": h.tile_col_count + 1,
+             "tile_row_idx": nt, "csc_tile_ids": nt}
+    types = {"masks": np.uint32, "values": np.float64}
+    for k in HYBRID_FIELDS:
+        p = getattr(h, k)
+        d[k] = _copy(p, sizes[k], types.get(k, np.int32)) if p else None
+    return d
+
+
+def csr_to_hybrid_tiles(csr, tile_rows: int, tile_cols: int, col_major: bool,
+                        dense_threshold: int, build_csc: bool) -> dict:
+    """Restatement of csr_to_hybrid_tiles (src/dmma_tiles.h:243-438) in numpy:
+    per tile row, entries keyed by (tile column, physical index) where the
+    physical index is r * tile_cols + c (row-major payload) or c * tile_rows + r
+    (column-major payload) (:163-224); repeated coordinates summed in CSR
+    order; a tile with >= dense_threshold distinct entries stores 32 values in
+    physical order, otherwise its values packed in mask-bit order (:334-351);
+    optional tile CSC in tile-row order (:372-409)."""
+    m, n = csr.m, csr.n
+    trc = -(-m // tile_rows) if m else 0
+    tcc = -(-n // tile_cols) if n else 0
+    rows = np.repeat(np.arange(m, dtype=np.int64), np.diff(csr.rowptr))
+    cols = csr.col.astype(np.int64)
+    lr, lc = rows % tile_rows, cols % tile_cols
+    phys = lc * tile_rows + lr if col_major else lr * tile_cols + lc
+    trow, tcol = rows // tile_rows, cols // tile_cols
+    key = (trow << 40) | (tcol << 5) | phys
+    order = np.argsort(key, kind="stable")
+    ks, vs = key[order], csr.val[order]
+    head = np.ones(ks.size, bool)
+    head[1:] = ks[1:] != ks[:-1]
+    starts = np.flatnonzero(head)
+    ukey = ks[starts]
+    uval = np.add.reduceat(vs, starts) if ks.size else np.zeros(0)
+    tkey = ukey >> 5
+    thead = np.ones(ukey.size, bool)
+    thead[1:] = tkey[1:] != tkey[:-1]
+    tstart = np.flatnonzero(thead)
+    ntiles = tstart.size
+    tend = np.append(tstart[1:], ukey.size)
+    counts = tend - tstart
+    uph = (ukey & 31).astype(np.int64)
+    masks = np.array([np.bitwise_or.reduce(np.left_shift(np.uint32(1), uph[a:b].astype(np.uint32)))
+                      for a, b in zip(tstart, tend)], dtype=np.uint32) if ntiles else np.zeros(0, np.uint32)
+    dense = counts >= dense_threshold
+    sizes = np.where(dense, 32, counts)
+    offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    values = np.zeros(int(offs[-1]))
+    for t in range(ntiles):
+        a, b = tstart[t], tend[t]
+        if dense[t]:
+            values[offs[t] + uph[a:b]] = uval[a:b]
+        else:
+            values[offs[t]:offs[t] + (b - a)] = uval[a:b]
+    t_row = (ukey[tstart] >> 40).astype(np.int64)
+    t_col = ((ukey[tstart] >> 5) & ((1 << 35) - 1)).astype(np.int32)
+    tile_row_ptr = np.concatenate([[0], np.cumsum(np.bincount(t_row, minlength=trc))]).astype(np.int32)
+    d = {"rows": m, "cols": n, "tile_rows": tile_rows, "tile_cols": tile_cols,
+         "tile_row_count": trc, "tile_col_count": tcc, "num_tiles": ntiles,
+         "payload_size": int(offs[-1]), "dense_tiles": int(dense.sum()),
+         "sparse_tiles": int(ntiles - dense.sum()), "tile_row_ptr": tile_row_ptr,
+         "tile_col_idx": t_col, "value_offsets": offs, "masks": masks, "values": values,
+         "tile_col_ptr": None, "tile_row_idx": None, "csc_tile_ids": None}
+    if build_csc:
+        corder = np.argsort(t_col, kind="stable")
+        d["tile_col_ptr"] = np.concatenate([[0], np.cumsum(np.bincount(t_col, minlength=tcc))]).astype(np.int32)
+        d["csc_tile_ids"] = corder.astype(np.int32)
+        d["tile_row_idx"] = t_row[corder].astype(np.int32)
+    return d
+
+
 def build(reference: bool = True) -> None:
     """Compile liboracle.so (and the reference libraries where the reference
     checkout exists)."""
@@ -242,6 +336,11 @@ class Oracle(_Base):
                                 ab.ctypes.data if with_abs else None)
         return rp, col[:nnz], val[:nnz], (ab[:nnz] if with_abs else None)
 
+    def csr_to_hybrid_tiles(self, csr, tile_rows=8, tile_cols=4, col_major=False,
+                            dense_threshold=24, build_csc=False) -> dict:
+        return csr_to_hybrid_tiles(csr, tile_rows, tile_cols, col_major, dense_threshold,
+                                   build_csc)
+
     def nnzcub(self, a, b) -> int:
         return int(self.lib.orc_nnzcub(a.m, a.rowptr.ctypes.data, a.col.ctypes.data,
                                        b.rowptr.ctypes.data))
@@ -318,6 +417,24 @@ class Reference(_Base):
                               val=_copy(s.value, s.nnz, np.float64))
         self._free_csr(s)
         return out
+
+    def csr_to_hybrid_tiles(self, csr, tile_rows=8, tile_cols=4, col_major=False,
+                            dense_threshold=24, build_csc=False):
+        """The reference's csr_to_hybrid_tiles; None when it returns false."""
+        s, keep = csr_smatrix(csr)
+        h = HybridTiles()
+        L = self.lib
+        L.ref_csr_to_hybrid_tiles.argtypes = [C.POINTER(SMatrix), C.c_int, C.c_int, C.c_int,
+                                              C.c_int, C.c_int, C.POINTER(HybridTiles)]
+        if not L.ref_csr_to_hybrid_tiles(C.byref(s), tile_rows, tile_cols, int(col_major),
+                                         dense_threshold, int(build_csc), C.byref(h)):
+            return None
+        d = hybrid_to_dict(h)
+        for k in HYBRID_FIELDS:
+            p = getattr(h, k)
+            if p:
+                self._free(C.cast(p, C.c_void_p))
+        return d
 
     def spgemm_serialref(self, a, b):
         rp = np.zeros(a.m + 1, dtype=np.int32)

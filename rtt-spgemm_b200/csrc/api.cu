@@ -914,6 +914,43 @@ int rtt_tile2csr_restore_rows(SMatrix *M, const int *new_to_old, int perm_size, 
     return RTT_OK;
 }
 
+int rtt_csr_to_hybrid_tiles(const SMatrix *M, int tile_rows, int tile_cols, int col_major,
+                            int dense_threshold, int build_csc, rtt_hybrid_tiles *out)
+{
+    if (M == nullptr || out == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "hybrid tiles: NULL argument");
+    if (tile_rows <= 0 || tile_cols <= 0 || tile_rows * tile_cols != 32 || dense_threshold < 1 ||
+        dense_threshold > 32)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT,
+                         "hybrid tiles: tile_rows * tile_cols must be 32, 1 <= threshold <= 32");
+    if (M->m < 0 || M->n < 0 || M->nnz < 0 || (M->m == 0 && M->nnz != 0) ||
+        (M->m > 0 && M->rowpointer == nullptr) ||
+        (M->nnz > 0 && (M->columnindex == nullptr || M->value == nullptr)))
+        return rtt::fail(RTT_ERR_INVALID_CSR, "hybrid tiles: malformed CSR");
+    if ((long long)M->n / tile_cols >= (1ll << 30) || (long long)M->m / tile_rows >= (1ll << 29))
+        return rtt::fail(RTT_ERR_UNREPRESENTABLE, "hybrid tiles: tile grid too large");
+    std::lock_guard<std::mutex> lock(g_mutex);
+    rtt_context c = nullptr;
+    RTT_CHECK(default_context(&c));
+    return map_device_error(csr_to_hybrid_host(c->ws, M, tile_rows, tile_cols, col_major,
+                                               dense_threshold, build_csc, out));
+}
+
+void rtt_hybrid_tiles_destroy(rtt_hybrid_tiles *h)
+{
+    if (h == nullptr)
+        return;
+    std::free(h->tile_row_ptr);
+    std::free(h->tile_col_idx);
+    std::free(h->value_offsets);
+    std::free(h->masks);
+    std::free(h->values);
+    std::free(h->tile_col_ptr);
+    std::free(h->tile_row_idx);
+    std::free(h->csc_tile_ids);
+    std::memset(h, 0, sizeof(*h));
+}
+
 int rtt_tile2csr(SMatrix *M, int tile_dim, int canonical)
 {
     return rtt_tile2csr_restore_rows(M, nullptr, -1, tile_dim, canonical);

@@ -1,0 +1,401 @@
+// hybrid.cu - CSR -> 32-element hybrid leaf tiles (8x4 A / 4x8 B) on sm_100a.
+//
+// Semantics of csr_to_hybrid_tiles (reference src/dmma_tiles.h:243-438, the
+// container at :29-62): tiles of tile_rows x tile_cols (= 32) elements; the
+// physical index of a local (r, c) is r * tile_cols + c (row-major payload,
+// A) or c * tile_rows + r (column-major payload, B); repeated coordinates are
+// summed; a tile whose distinct count reaches dense_threshold stores all 32
+// values in physical order (zeros included), any other tile stores its values
+// packed in increasing mask-bit order; value_offsets is the running payload
+// size, so a tile is dense exactly when its span is 32.  The optional tile
+// CSC lists, per tile column, the tile rows and tile-CSR ids in tile-row order.
+//
+// The reference walks tile rows on the host, sorting each row's entries.  Here
+// every entry gets one 64-bit key (tile row, tile column, physical index),
+// one device radix sort orders the whole matrix, and the tiles fall out of
+// segment heads, scans and one scatter - all on the device.
+#include "rtt_internal.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <climits>
+#include <cstdlib>
+#include <cstring>
+
+namespace rtt
+{
+namespace
+{
+
+constexpr int ELEMS = 32;
+constexpr int TC_BITS = 30; // tile column field width in the key
+constexpr int PH_BITS = 5;  // physical index field width
+
+__global__ void k_hyb_validate(int m, int n, int nnz, const int *__restrict__ rowptr,
+                               const int *__restrict__ col, int *err)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0 && (rowptr[0] != 0 || rowptr[m] != nnz))
+        set_error(err, DERR_CSR_ROWPTR);
+    if (i < m && rowptr[i + 1] < rowptr[i])
+        set_error(err, DERR_CSR_ROWPTR);
+    if (i < nnz && (col[i] < 0 || col[i] >= n))
+        set_error(err, DERR_CSR_COL);
+}
+
+// One warp per row: key of every entry (tile row | tile column | physical).
+__global__ void k_hyb_keys(int m, const int *__restrict__ rowptr, const int *__restrict__ col,
+                           int tr, int tc, int col_major, unsigned long long *__restrict__ keys)
+{
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= m)
+        return;
+    const int row = (int)w;
+    const unsigned long long trow = (unsigned long long)(row / tr);
+    const int lr = row % tr;
+    for (int e = rowptr[row] + lane; e < rowptr[row + 1]; e += 32)
+    {
+        const int c = col[e];
+        const int lc = c % tc;
+        const int ph = col_major ? lc * tr + lr : lr * tc + lc;
+        keys[e] = (trow << (TC_BITS + PH_BITS)) | ((unsigned long long)(c / tc) << PH_BITS) |
+                  (unsigned long long)ph;
+    }
+}
+
+// Heads of distinct coordinates (entry level) and of tiles (coordinate level).
+__global__ void k_hyb_heads(int nnz, const unsigned long long *__restrict__ keys,
+                            int *__restrict__ coord_head, int *__restrict__ tile_head)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnz)
+        return;
+    const unsigned long long k = keys[i];
+    const bool newc = i == 0 || keys[i - 1] != k;
+    coord_head[i] = newc ? 1 : 0;
+    tile_head[i] = (newc && (i == 0 || (keys[i - 1] >> PH_BITS) != (k >> PH_BITS))) ? 1 : 0;
+}
+
+// Per distinct coordinate: its value (sum of its run, in sorted = CSR order),
+// its tile's mask bit and count; per tile head: column, tile row, first
+// coordinate.  coord_id / tile_id are inclusive scans of the heads.
+__global__ void k_hyb_tiles(int nnz, const unsigned long long *__restrict__ keys,
+                            const double *__restrict__ vals, const int *__restrict__ coord_head,
+                            const int *__restrict__ coord_id, const int *__restrict__ tile_id,
+                            double *__restrict__ cval, unsigned char *__restrict__ cphys,
+                            int *__restrict__ ctile, unsigned int *__restrict__ mask,
+                            int *__restrict__ tcount, int *__restrict__ tcol,
+                            int *__restrict__ trow, int *__restrict__ tfirst)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnz || !coord_head[i])
+        return;
+    const unsigned long long k = keys[i];
+    double s = vals[i];
+    for (long long j = i + 1; j < nnz && keys[j] == k; ++j)
+        s += vals[j];
+    const int cid = coord_id[i] - 1, t = tile_id[i] - 1;
+    const int ph = (int)(k & ((1ull << PH_BITS) - 1));
+    cval[cid] = s;
+    cphys[cid] = (unsigned char)ph;
+    ctile[cid] = t;
+    atomicOr(&mask[t], 1u << ph);
+    atomicAdd(&tcount[t], 1);
+    if (i == 0 || (keys[i - 1] >> PH_BITS) != (k >> PH_BITS))
+    {
+        tcol[t] = (int)((k >> PH_BITS) & ((1ull << TC_BITS) - 1));
+        trow[t] = (int)(k >> (TC_BITS + PH_BITS));
+        tfirst[t] = cid;
+    }
+}
+
+__global__ void k_hyb_sizes(int ntiles, const int *__restrict__ tcount, int thr,
+                            int *__restrict__ tsize, int *__restrict__ row_hist,
+                            const int *__restrict__ trow, int *__restrict__ ndense)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles)
+        return;
+    const bool dense = tcount[t] >= thr;
+    tsize[t] = dense ? ELEMS : tcount[t];
+    atomicAdd(&row_hist[trow[t]], 1);
+    if (dense)
+        atomicAdd(ndense, 1);
+}
+
+__global__ void k_hyb_values(int ncoord, const double *__restrict__ cval,
+                             const unsigned char *__restrict__ cphys,
+                             const int *__restrict__ ctile, const int *__restrict__ tfirst,
+                             const int *__restrict__ toff, const int *__restrict__ tcount, int thr,
+                             double *__restrict__ values)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncoord)
+        return;
+    const int t = ctile[c];
+    const int slot = tcount[t] >= thr ? (int)cphys[c] : c - tfirst[t];
+    values[toff[t] + slot] = cval[c];
+}
+
+__global__ void k_hyb_hist(int n, const int *__restrict__ key, int *__restrict__ hist)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        atomicAdd(&hist[key[i]], 1);
+}
+
+__global__ void k_hyb_iota(int n, int *__restrict__ a)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        a[i] = i;
+}
+
+__global__ void k_hyb_gather(int n, const int *__restrict__ idx, const int *__restrict__ src,
+                             int *__restrict__ dst)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        dst[i] = src[idx[i]];
+}
+
+inline int blocks(long long n, int b) { return (int)((n + b - 1) / b); }
+
+template <typename T>
+int alloc_dev(T **p, size_t n)
+{
+    RTT_CUDA(cudaMalloc((void **)p, sizeof(T) * (n > 0 ? n : 1)));
+    return RTT_OK;
+}
+
+// Exclusive scan of n ints into out (n + 1 entries).
+int scan_into(Workspace &ws, const int *in, int *out, int n)
+{
+    return scan_exclusive_int(ws, in, out, n);
+}
+
+struct DevArrays
+{
+    static constexpr int kMax = 40;
+    void *p[kMax] = {};
+    int used = 0;
+    template <typename T>
+    int get(T **out, size_t n)
+    {
+        if (used >= kMax)
+            return fail(RTT_ERR_STATE, "hybrid tiles: too many device arrays");
+        RTT_CHECK(alloc_dev(out, n));
+        p[used++] = *out;
+        return RTT_OK;
+    }
+    ~DevArrays()
+    {
+        for (int i = 0; i < used; ++i)
+            cudaFree(p[i]);
+    }
+};
+
+template <typename T>
+int to_host(T **out, const T *d, size_t n, cudaStream_t s)
+{
+    *out = nullptr;
+    if (n == 0)
+        return RTT_OK;
+    T *h = static_cast<T *>(std::malloc(sizeof(T) * n));
+    if (h == nullptr)
+        return fail(RTT_ERR_OUT_OF_MEMORY, "host malloc failed");
+    cudaError_t e = cudaMemcpyAsync(h, d, sizeof(T) * n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+    {
+        std::free(h);
+        return cuda_fail(e, "hybrid tiles: device to host copy");
+    }
+    *out = h;
+    return RTT_OK;
+}
+
+} // namespace
+
+int csr_to_hybrid_host(Workspace &ws, const SMatrix *M, int tr, int tc, int col_major, int thr,
+                       int build_csc, rtt_hybrid_tiles *out)
+{
+    cudaStream_t s = ws.stream;
+    const int m = M->m, n = M->n, nnz = M->nnz;
+    DevArrays D;
+    int *rp = nullptr, *ci = nullptr;
+    double *va = nullptr;
+    RTT_CHECK(D.get(&rp, (size_t)m + 1));
+    RTT_CHECK(D.get(&ci, (size_t)nnz));
+    RTT_CHECK(D.get(&va, (size_t)nnz));
+    RTT_CUDA(cudaMemcpyAsync(rp, M->rowpointer, sizeof(int) * ((size_t)m + 1), cudaMemcpyHostToDevice, s));
+    if (nnz > 0)
+    {
+        RTT_CUDA(cudaMemcpyAsync(ci, M->columnindex, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, s));
+        RTT_CUDA(cudaMemcpyAsync(va, M->value, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice, s));
+    }
+    RTT_CUDA(cudaMemsetAsync(ws.err.p, 0, sizeof(int), s));
+    k_hyb_validate<<<blocks(std::max(m + 1, nnz), 256), 256, 0, s>>>(m, n, nnz, rp, ci, ws.err.as<int>());
+    RTT_CHECK(check_device_error(ws, "hybrid tiles: CSR"));
+
+    const int trc = m / tr + (m % tr != 0), tcc = n / tc + (n % tc != 0);
+    rtt_hybrid_tiles r{};
+    r.rows = m;
+    r.cols = n;
+    r.tile_rows = tr;
+    r.tile_cols = tc;
+    r.tile_row_count = trc;
+    r.tile_col_count = tcc;
+
+    unsigned long long *keys = nullptr, *skeys = nullptr;
+    double *svals = nullptr;
+    int *chead = nullptr, *thead = nullptr, *cid = nullptr, *tid = nullptr;
+    RTT_CHECK(D.get(&keys, (size_t)nnz));
+    RTT_CHECK(D.get(&skeys, (size_t)nnz));
+    RTT_CHECK(D.get(&svals, (size_t)nnz));
+    RTT_CHECK(D.get(&chead, (size_t)nnz + 1));
+    RTT_CHECK(D.get(&thead, (size_t)nnz + 1));
+    RTT_CHECK(D.get(&cid, (size_t)nnz + 1));
+    RTT_CHECK(D.get(&tid, (size_t)nnz + 1));
+    int ncoord = 0, ntiles = 0;
+    if (nnz > 0)
+    {
+        k_hyb_keys<<<blocks((long long)m * 32, 256), 256, 0, s>>>(m, rp, ci, tr, tc, col_major, keys);
+        int hibit = 0; // key bits in use
+        {
+            unsigned long long top = ((unsigned long long)trc << (TC_BITS + PH_BITS));
+            while (hibit < 64 && (top >> hibit) != 0)
+                ++hibit;
+            hibit = std::max(hibit, TC_BITS + PH_BITS);
+        }
+        size_t bytes = 0;
+        RTT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys, skeys, va, svals, nnz, 0,
+                                                 hibit, s));
+        RTT_CHECK(ws.scan_tmp.ensure(bytes, s));
+        RTT_CUDA(cub::DeviceRadixSort::SortPairs(ws.scan_tmp.p, bytes, keys, skeys, va, svals, nnz,
+                                                 0, hibit, s));
+        k_hyb_heads<<<blocks(nnz, 256), 256, 0, s>>>(nnz, skeys, chead, thead);
+        // inclusive scans: coordinate / tile id of every entry
+        RTT_CHECK(scan_into(ws, chead, cid, nnz)); // cid[i + 1] = inclusive count
+        RTT_CHECK(scan_into(ws, thead, tid, nnz));
+        RTT_CHECK(read_int(ws, cid + nnz, &ncoord));
+        RTT_CHECK(read_int(ws, tid + nnz, &ntiles));
+    }
+    // per coordinate / per tile arrays
+    double *cval = nullptr;
+    unsigned char *cphys = nullptr;
+    int *ctile = nullptr, *tcount = nullptr, *tcol = nullptr, *trow = nullptr, *tfirst = nullptr,
+        *tsize = nullptr, *toff = nullptr, *row_hist = nullptr, *rowptr = nullptr, *ndense = nullptr;
+    unsigned int *mask = nullptr;
+    double *values = nullptr;
+    RTT_CHECK(D.get(&cval, (size_t)ncoord));
+    RTT_CHECK(D.get(&cphys, (size_t)ncoord));
+    RTT_CHECK(D.get(&ctile, (size_t)ncoord));
+    RTT_CHECK(D.get(&tcount, (size_t)ntiles));
+    RTT_CHECK(D.get(&tcol, (size_t)ntiles));
+    RTT_CHECK(D.get(&trow, (size_t)ntiles));
+    RTT_CHECK(D.get(&tfirst, (size_t)ntiles));
+    RTT_CHECK(D.get(&tsize, (size_t)ntiles));
+    RTT_CHECK(D.get(&toff, (size_t)ntiles + 1));
+    RTT_CHECK(D.get(&row_hist, (size_t)trc + 1));
+    RTT_CHECK(D.get(&rowptr, (size_t)trc + 1));
+    RTT_CHECK(D.get(&ndense, 1));
+    RTT_CHECK(D.get(&mask, (size_t)ntiles));
+    RTT_CUDA(cudaMemsetAsync(mask, 0, sizeof(unsigned) * (size_t)std::max(ntiles, 1), s));
+    RTT_CUDA(cudaMemsetAsync(tcount, 0, sizeof(int) * (size_t)std::max(ntiles, 1), s));
+    RTT_CUDA(cudaMemsetAsync(row_hist, 0, sizeof(int) * ((size_t)trc + 1), s));
+    RTT_CUDA(cudaMemsetAsync(ndense, 0, sizeof(int), s));
+    int payload = 0, ndense_h = 0;
+    if (nnz > 0)
+    {
+        k_hyb_tiles<<<blocks(nnz, 256), 256, 0, s>>>(nnz, skeys, svals, chead, cid + 1, tid + 1,
+                                                     cval, cphys, ctile, mask, tcount, tcol, trow,
+                                                     tfirst);
+        k_hyb_sizes<<<blocks(ntiles, 256), 256, 0, s>>>(ntiles, tcount, thr, tsize, row_hist, trow,
+                                                       ndense);
+        RTT_CHECK(scan_into(ws, tsize, toff, ntiles));
+        RTT_CHECK(read_int(ws, toff + ntiles, &payload));
+        RTT_CHECK(read_int(ws, ndense, &ndense_h));
+    }
+    else
+    {
+        RTT_CUDA(cudaMemsetAsync(toff, 0, sizeof(int), s));
+    }
+    RTT_CHECK(scan_into(ws, row_hist, rowptr, trc));
+    RTT_CHECK(D.get(&values, (size_t)payload));
+    RTT_CUDA(cudaMemsetAsync(values, 0, sizeof(double) * (size_t)std::max(payload, 1), s));
+    if (ncoord > 0)
+        k_hyb_values<<<blocks(ncoord, 256), 256, 0, s>>>(ncoord, cval, cphys, ctile, tfirst, toff,
+                                                         tcount, thr, values);
+    r.num_tiles = ntiles;
+    r.payload_size = payload;
+    r.dense_tiles = ndense_h;
+    r.sparse_tiles = ntiles - ndense_h;
+
+    int *csc_ptr = nullptr, *csc_row = nullptr, *csc_ids = nullptr;
+    if (build_csc)
+    {
+        int *col_hist = nullptr, *iota = nullptr, *skey = nullptr;
+        RTT_CHECK(D.get(&col_hist, (size_t)tcc + 1));
+        RTT_CHECK(D.get(&csc_ptr, (size_t)tcc + 1));
+        RTT_CHECK(D.get(&iota, (size_t)ntiles));
+        RTT_CHECK(D.get(&skey, (size_t)ntiles));
+        RTT_CHECK(D.get(&csc_ids, (size_t)ntiles));
+        RTT_CHECK(D.get(&csc_row, (size_t)ntiles));
+        if (ntiles > 0)
+        {
+            // stable sort of tile ids by tile column keeps tile-row order per column
+            k_hyb_iota<<<blocks(ntiles, 256), 256, 0, s>>>(ntiles, iota);
+            int cbits = 1;
+            while (cbits < 31 && (tcc >> cbits) != 0)
+                ++cbits;
+            size_t bytes = 0;
+            RTT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, tcol, skey, iota, csc_ids,
+                                                     ntiles, 0, cbits, s));
+            RTT_CHECK(ws.scan_tmp.ensure(bytes, s));
+            RTT_CUDA(cub::DeviceRadixSort::SortPairs(ws.scan_tmp.p, bytes, tcol, skey, iota,
+                                                     csc_ids, ntiles, 0, cbits, s));
+            k_hyb_gather<<<blocks(ntiles, 256), 256, 0, s>>>(ntiles, csc_ids, trow, csc_row);
+        }
+        // column pointer: scan of the tiles per tile column
+        RTT_CUDA(cudaMemsetAsync(col_hist, 0, sizeof(int) * ((size_t)tcc + 1), s));
+        if (ntiles > 0)
+            k_hyb_hist<<<blocks(ntiles, 256), 256, 0, s>>>(ntiles, tcol, col_hist);
+        RTT_CHECK(scan_into(ws, col_hist, csc_ptr, tcc));
+    }
+    RTT_CHECK(check_device_error(ws, "hybrid tiles"));
+
+    // host copies (malloc'd, caller frees with rtt_hybrid_tiles_destroy)
+    rtt_hybrid_tiles h = r;
+    int st = RTT_OK;
+    if (st == RTT_OK)
+        st = to_host(&h.tile_row_ptr, rowptr, (size_t)trc + 1, s);
+    if (st == RTT_OK)
+        st = to_host(&h.tile_col_idx, tcol, (size_t)ntiles, s);
+    if (st == RTT_OK)
+        st = to_host(&h.value_offsets, toff, (size_t)ntiles + 1, s);
+    if (st == RTT_OK)
+        st = to_host(&h.masks, mask, (size_t)ntiles, s);
+    if (st == RTT_OK)
+        st = to_host(&h.values, values, (size_t)payload, s);
+    if (st == RTT_OK && build_csc)
+    {
+        st = to_host(&h.tile_col_ptr, csc_ptr, (size_t)tcc + 1, s);
+        if (st == RTT_OK)
+            st = to_host(&h.tile_row_idx, csc_row, (size_t)ntiles, s);
+        if (st == RTT_OK)
+            st = to_host(&h.csc_tile_ids, csc_ids, (size_t)ntiles, s);
+    }
+    if (st != RTT_OK)
+    {
+        rtt_hybrid_tiles_destroy(&h);
+        return st;
+    }
+    *out = h;
+    return RTT_OK;
+}
+
+} // namespace rtt

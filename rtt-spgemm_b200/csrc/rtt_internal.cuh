@@ -297,6 +297,9 @@ int tile2csr_fill_device(Workspace &ws, const int *tile_ptr, const int *tile_col
                          const double *val, int m, int n, int tilem, int td,
                          const int *new_to_old, int perm_size, const int *rowptr, int *out_col,
                          double *out_val, bool sort_rows, const int *row_data = nullptr);
+// CSR (host arrays) -> hybrid leaf tiles on the device, results malloc'd into out
+int csr_to_hybrid_host(Workspace &ws, const SMatrix *M, int tile_rows, int tile_cols,
+                       int col_major, int dense_threshold, int build_csc, rtt_hybrid_tiles *out);
 // launch-only forms (no workspace, identity row order): the caller owns the
 // stream and the error word; row_cnt needs m entries cleared to zero
 int tile2csr_count_launch(cudaStream_t s, const int *tile_ptr, const int *tile_col,

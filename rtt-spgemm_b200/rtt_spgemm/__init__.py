@@ -27,13 +27,13 @@ from types import SimpleNamespace
 import numpy as np
 
 from . import generators
-from ._abi import (EXPORTS, LIB_PATH, RTT_OP_AAT, RTT_OP_AB, Config, CsrView, RttError, SMatrix,
-                   Stats, build, check, lib)
+from ._abi import (EXPORTS, LIB_PATH, RTT_OP_AAT, RTT_OP_AB, Config, CsrView, HybridTiles,
+                   RttError, SMatrix, Stats, build, check, lib)
 from .generators import CSR
 
 __all__ = ["CSR", "Context", "RttError", "build", "csr2tile_col_major", "csr2tile_row_major",
            "generators", "lib", "spgemm_csr_host", "spgemm_tile", "tile16_to_tile8", "tile2csr",
-           "tile2csr_device_noalloc",
+           "tile2csr_device_noalloc", "csr_to_hybrid_tiles",
            "EXPORTS", "LIB_PATH", "RTT_OP_AB", "RTT_OP_AAT"]
 
 TD = 16
@@ -178,6 +178,39 @@ def tile16_to_tile8(c_tiles: dict) -> dict:
     check(lib().rtt_tile16_to_tile8(C.byref(s), C.byref(o)))
     d = _tiles_out(o, ptr_stride=8)
     _destroy(o)
+    return d
+
+
+HYBRID_FIELDS = ("tile_row_ptr", "tile_col_idx", "value_offsets", "masks", "values",
+                 "tile_col_ptr", "tile_row_idx", "csc_tile_ids")
+
+
+def hybrid_dict(h) -> dict:
+    """A HybridTiles structure (either library's) as a dict of numpy arrays."""
+    d = {k: getattr(h, k) for k in ("rows", "cols", "tile_rows", "tile_cols", "tile_row_count",
+                                    "tile_col_count", "num_tiles", "payload_size", "dense_tiles",
+                                    "sparse_tiles")}
+    nt = h.num_tiles
+    sizes = {"tile_row_ptr": h.tile_row_count + 1, "tile_col_idx": nt, "value_offsets": nt + 1,
+             "masks": nt, "values": h.payload_size, "tile_col_ptr": h.tile_col_count + 1,
+             "tile_row_idx": nt, "csc_tile_ids": nt}
+    types = {"masks": np.uint32, "values": np.float64}
+    for k in HYBRID_FIELDS:
+        p = getattr(h, k)
+        d[k] = _copy(p, sizes[k], types.get(k, np.int32)) if p else None
+    return d
+
+
+def csr_to_hybrid_tiles(csr, tile_rows: int = 8, tile_cols: int = 4, col_major: bool = False,
+                        dense_threshold: int = 24, build_csc: bool = False) -> dict:
+    """GPU replacement of csr_to_hybrid_tiles (reference src/dmma_tiles.h:243):
+    A uses (8, 4, row-major payload), B (4, 8, column-major payload)."""
+    s, keep = _csr_smatrix(csr)
+    h = HybridTiles()
+    check(lib().rtt_csr_to_hybrid_tiles(C.byref(s), tile_rows, tile_cols, int(col_major),
+                                        dense_threshold, int(build_csc), C.byref(h)))
+    d = hybrid_dict(h)
+    lib().rtt_hybrid_tiles_destroy(C.byref(h))
     return d
 
 

@@ -32,7 +32,7 @@ EXPORTS = [
     "rtt_config_default", "rtt_context_create", "rtt_context_destroy", "rtt_context_set_stream",
     "rtt_context_set_config", "rtt_context_get_stats", "rtt_spgemm_symbolic",
     "rtt_spgemm_numeric", "rtt_spgemm_tiles_view", "rtt_spgemm_csr_host",
-    "rtt_tile2csr_device_noalloc",
+    "rtt_tile2csr_device_noalloc", "rtt_csr_to_hybrid_tiles", "rtt_hybrid_tiles_destroy",
 ]
 
 
@@ -68,6 +68,19 @@ class Config(C.Structure):
     _fields_ = [("dmma_pair_cutoff", C.c_int), ("fused_csr_output", C.c_int),
                 ("keep_tiles", C.c_int), ("stage_timing", C.c_int), ("b_staging", C.c_int),
                 ("reserved", C.c_int * 6)]
+
+
+class HybridTiles(C.Structure):
+    """rtt_hybrid_tiles = the reference's HybridTileMatrix (src/dmma_tiles.h:29-62)."""
+
+    _fields_ = [("rows", C.c_int), ("cols", C.c_int), ("tile_rows", C.c_int),
+                ("tile_cols", C.c_int), ("tile_row_count", C.c_int), ("tile_col_count", C.c_int),
+                ("num_tiles", C.c_int), ("payload_size", C.c_int), ("dense_tiles", C.c_int),
+                ("sparse_tiles", C.c_int),
+                ("tile_row_ptr", C.POINTER(C.c_int)), ("tile_col_idx", C.POINTER(C.c_int)),
+                ("value_offsets", C.POINTER(C.c_int)), ("masks", C.POINTER(C.c_uint)),
+                ("values", C.POINTER(C.c_double)), ("tile_col_ptr", C.POINTER(C.c_int)),
+                ("tile_row_idx", C.POINTER(C.c_int)), ("csc_tile_ids", C.POINTER(C.c_int))]
 
 
 class Stats(C.Structure):
@@ -112,6 +125,10 @@ def lib() -> C.CDLL:
     L.rtt_tile2csr.argtypes = [P(SMatrix), C.c_int, C.c_int]
     L.rtt_tile2csr_restore_rows.argtypes = [P(SMatrix), P(C.c_int), C.c_int, C.c_int, C.c_int]
     L.rtt_tile16_to_tile8.argtypes = [P(SMatrix), P(SMatrix)]
+    L.rtt_csr_to_hybrid_tiles.argtypes = [P(SMatrix), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                          P(HybridTiles)]
+    L.rtt_hybrid_tiles_destroy.argtypes = [P(HybridTiles)]
+    L.rtt_hybrid_tiles_destroy.restype = None
     L.rtt_tile2csr_device_noalloc.argtypes = [P(SMatrix), C.c_int, C.c_int, C.c_longlong,
                                               P(C.c_longlong), C.c_void_p]
     L.rtt_matrix_destroy.argtypes = [P(SMatrix), C.c_int]

@@ -137,3 +137,70 @@ def test_kat_2d_closed_form_nnz(orc):
     rp, _, _, _ = orc.spgemm_csr(A, A, with_abs=False)
     assert rp[-1] == 846852
     assert orc.nnzcub(A, A) == 1629192
+
+
+# ---------------------------------------------------------------- hybrid leaf tiles
+def _kat_a():
+    """The worked example of the reference's design document (section 10):
+    A's reordered entries (0,0)=a, (1,1)=c, (2,4)=b, (3,5)=d in 8x4 tiles."""
+    return G.CSR(4, 8, np.array([0, 1, 2, 3, 4], np.int32), np.array([0, 1, 4, 5], np.int32),
+                 np.array([1.0, 3.0, 2.0, 4.0]))
+
+
+def _assert_hybrid_equal(got, want, tag="", exact=True):
+    for k in ("rows", "cols", "tile_rows", "tile_cols", "tile_row_count", "tile_col_count",
+              "num_tiles", "payload_size", "dense_tiles", "sparse_tiles"):
+        assert got[k] == want[k], f"{tag}{k}: {got[k]} != {want[k]}"
+    for k in ("tile_row_ptr", "tile_col_idx", "value_offsets", "masks", "tile_col_ptr",
+              "tile_row_idx", "csc_tile_ids"):
+        g, w = got[k], want[k]
+        if w is None or len(w) == 0:
+            assert g is None or len(g) == 0, f"{tag}{k}"
+            continue
+        assert np.array_equal(g, w), f"{tag}{k} differs"
+    gv = got["values"] if got["values"] is not None else np.zeros(0)
+    wv = want["values"] if want["values"] is not None else np.zeros(0)
+    if exact:
+        assert np.array_equal(gv.view(np.int64), wv.view(np.int64)), f"{tag}values"
+    else:
+        assert np.allclose(gv, wv, rtol=1e-12, atol=1e-12), f"{tag}values"
+
+
+def test_hybrid_kat_oracle(orc):
+    h = orc.csr_to_hybrid_tiles(_kat_a(), 8, 4, False, 24)
+    assert list(h["tile_row_ptr"]) == [0, 2] and list(h["tile_col_idx"]) == [0, 1]
+    assert list(h["value_offsets"]) == [0, 2, 4]
+    assert list(h["masks"]) == [0x00000021, 0x00002100]
+    assert list(h["values"]) == [1.0, 3.0, 2.0, 4.0]  # [a, c, b, d]
+
+
+HYB_CASES = [
+    ("a_8x4", 8, 4, False, 24, True),
+    ("b_4x8", 4, 8, True, 24, True),
+    ("dense_all", 8, 4, False, 1, False),
+    ("dense_none", 4, 8, True, 32, True),
+    ("thin_2x16", 2, 16, False, 12, True),
+]
+
+
+@pytest.mark.parametrize("cfg", HYB_CASES, ids=[c[0] for c in HYB_CASES])
+@pytest.mark.parametrize("mat", ["stencil", "ragged", "dense", "empty_rows"])
+def test_hybrid_oracle_matches_reference(ref, orc, cfg, mat):
+    A = {"stencil": lambda: G.stencil_27(5, 2), "ragged": lambda: G.laplacian_2d(13, 7),
+         "dense": lambda: G.random_csr(37, 29, 0.6, seed=8),
+         "empty_rows": lambda: G.random_csr(50, 70, 0.01, seed=9)}[mat]()
+    _, tr, tc, cm, thr, csc = cfg
+    _assert_hybrid_equal(orc.csr_to_hybrid_tiles(A, tr, tc, cm, thr, csc),
+                         ref.csr_to_hybrid_tiles(A, tr, tc, cm, thr, csc), f"{mat}/{cfg[0]}: ")
+
+
+def test_hybrid_kat_reference(ref):
+    h = ref.csr_to_hybrid_tiles(_kat_a(), 8, 4, False, 24)
+    assert list(h["masks"]) == [0x00000021, 0x00002100]
+    assert list(h["values"]) == [1.0, 3.0, 2.0, 4.0]
+
+
+def test_hybrid_duplicates_summed(ref, orc):
+    A = G.random_csr(40, 40, 0.1, seed=12, duplicates=0.3)
+    _assert_hybrid_equal(orc.csr_to_hybrid_tiles(A, 8, 4, False, 4, True),
+                         ref.csr_to_hybrid_tiles(A, 8, 4, False, 4, True), "dups: ", exact=False)
