@@ -216,6 +216,45 @@ RTT_API int rtt_csr_to_hybrid_tiles(const SMatrix *csr, int tile_rows, int tile_
                                     int col_major, int dense_threshold, int build_csc,
                                     rtt_hybrid_tiles *out);
 
+/* Tail-queue admission (the reference's DmmaTileTailQueuePolicy / CostModel /
+ * Plan, src/dmma_tile_tail_queue.h:20-121; enabled is the policy switch). */
+typedef struct
+{
+    int enabled;
+    double admission_threshold; /* FP32 work above this admits a task (256) */
+    double chunk_target;        /* work per chunk (256) */
+    int max_chunks;             /* 2..32 (8) */
+    double max_heavy_fraction;  /* (0.01) */
+    int record_capacity;        /* (1 << 20) */
+    long long workspace_limit_bytes; /* (1 GiB) */
+    int workspace_reduction;    /* (1) */
+} rtt_tail_policy;
+
+typedef struct
+{
+    double intercept, scan, match, output; /* (0, 1, 8, 0.25) */
+} rtt_tail_cost_model;
+
+typedef struct
+{
+    int reason; /* DmmaTileTailQueueGateReason: 0 off, 1 enabled, 2 invalid policy,
+                   3 invalid task, 4 zero heavy, 5 record capacity, 6 heavy fraction,
+                   7 workspace capacity */
+    long long output_tasks, ordinary_tasks, heavy_tasks, chunks;
+    long long descriptor_bytes, heavy_flag_bytes, partial_workspace_bytes;
+    double heavy_fraction, average_chunks;
+} rtt_tail_plan;
+
+/* Replaces dmma_plan_tile_tail_queue (src/dmma_tile_tail_queue.h:190-291),
+ * planned on the GPU: task i is described by scans[i], matches[i] and
+ * output_nnz[i] (host arrays of ntasks); chunks_out[i] receives the task's
+ * chunk count (0 = ordinary task), and plan the summary and gate reason,
+ * exactly as the reference computes them (FP32 admission arithmetic). */
+RTT_API int rtt_plan_tail_queue(int ntasks, const int *scans, const int *matches,
+                                const int *output_nnz, const rtt_tail_policy *policy,
+                                const rtt_tail_cost_model *model, int *chunks_out,
+                                rtt_tail_plan *plan);
+
 /* Frees the arrays of a hybrid tile matrix and zeroes it (the reference's
  * destroy_hybrid_tile_matrix, src/dmma_tiles.h:64-79). */
 RTT_API void rtt_hybrid_tiles_destroy(rtt_hybrid_tiles *tiles);

@@ -221,6 +221,62 @@ def csr_to_hybrid_tiles(csr, tile_rows: int, tile_cols: int, col_major: bool,
     return d
 
 
+def plan_tail_queue(scans, matches, output_nnz, policy: dict, model: dict):
+    """Restatement of dmma_plan_tile_tail_queue (src/dmma_tile_tail_queue.h:190-291)
+    with the chunk rule of :148-176 in numpy float32 (round-to-nearest, no
+    contraction).  Returns (chunks per task, summary dict)."""
+    sc = np.asarray(scans, np.int64)
+    mt = np.asarray(matches, np.int64)
+    on = np.asarray(output_nnz, np.int64)
+    n = sc.size
+    plan = dict(reason=0, output_tasks=n, ordinary_tasks=n, heavy_tasks=0, chunks=0,
+                descriptor_bytes=0, heavy_flag_bytes=0, partial_workspace_bytes=0,
+                heavy_fraction=0.0, average_chunks=0.0)
+    zero = np.zeros(n, np.int32)
+    if not policy["enabled"]:
+        return zero, plan
+    fin = np.isfinite
+    ok = (fin(policy["admission_threshold"]) and policy["admission_threshold"] > 0 and
+          fin(policy["chunk_target"]) and policy["chunk_target"] > 0 and
+          2 <= policy["max_chunks"] <= 32 and fin(policy["max_heavy_fraction"]) and
+          0 <= policy["max_heavy_fraction"] <= 1 and policy["record_capacity"] > 0 and
+          all(fin(model[k]) and model[k] >= 0 for k in ("intercept", "scan", "match", "output")))
+    if not ok:
+        plan["reason"] = 2
+        return zero, plan
+    f32 = np.float32
+    work = f32(model["scan"]) * sc.astype(f32) + f32(model["match"]) * mt.astype(f32)
+    admit = (work > f32(policy["admission_threshold"])) & (sc > 1)
+    req = np.ceil(work / f32(policy["chunk_target"]))
+    ch = np.where(req >= f32(policy["max_chunks"]), policy["max_chunks"],
+                  np.clip(req, -2**31, 2**31 - 1).astype(np.int64))
+    ch = np.minimum(np.maximum(ch, 2), sc)
+    ch = np.where(admit & (ch >= 2), ch, 0).astype(np.int64)
+    invalid = (sc < 0) | (mt < 0) | (mt > sc) | (on < 0) | (on > 64)
+    ch[invalid] = 0
+    heavy = ch > 0
+    first_invalid = int(np.argmax(invalid)) if invalid.any() else n
+    over = np.cumsum(heavy) > policy["record_capacity"]
+    first_over = int(np.argmax(over)) if over.any() else n
+    if first_invalid < n or first_over < n:
+        plan["reason"] = 3 if first_invalid <= first_over else 5
+        return zero, plan
+    h, c = int(heavy.sum()), int(ch.sum())
+    plan.update(heavy_tasks=h, ordinary_tasks=n - h, chunks=c,
+                heavy_fraction=0.0 if n == 0 else h / n, average_chunks=0.0 if h == 0 else c / h,
+                heavy_flag_bytes=((n + 31) // 32) * 4, descriptor_bytes=c * 16,
+                partial_workspace_bytes=c * 512)
+    if h == 0:
+        plan["reason"] = 4
+    elif plan["heavy_fraction"] > policy["max_heavy_fraction"]:
+        plan["reason"] = 6
+    elif policy["workspace_reduction"] and plan["partial_workspace_bytes"] > policy["workspace_limit_bytes"]:
+        plan["reason"] = 7
+    else:
+        plan["reason"] = 1
+    return ch.astype(np.int32), plan
+
+
 def build(reference: bool = True) -> None:
     """Compile liboracle.so (and the reference libraries where the reference
     checkout exists)."""
@@ -435,6 +491,30 @@ class Reference(_Base):
             if p:
                 self._free(C.cast(p, C.c_void_p))
         return d
+
+    def plan_tail_queue(self, scans, matches, output_nnz, policy: dict, model: dict):
+        """The reference's dmma_plan_tile_tail_queue (via ref_plan_tile_tail_queue)."""
+        L = self.lib
+        L.ref_plan_tile_tail_queue.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                               C.c_double, C.c_double, C.c_int, C.c_double,
+                                               C.c_int, C.c_longlong, C.c_int, C.c_double,
+                                               C.c_double, C.c_double, C.c_double, C.c_void_p,
+                                               C.c_void_p]
+        sc = np.ascontiguousarray(scans, np.int32)
+        mt = np.ascontiguousarray(matches, np.int32)
+        on = np.ascontiguousarray(output_nnz, np.int32)
+        n = sc.size
+        ch = np.zeros(max(n, 1), np.int32)
+        summ = np.zeros(5, np.int64)
+        if not policy["enabled"]:
+            return ch[:n], 0
+        reason = L.ref_plan_tile_tail_queue(
+            n, sc.ctypes.data, mt.ctypes.data, on.ctypes.data, policy["admission_threshold"],
+            policy["chunk_target"], policy["max_chunks"], policy["max_heavy_fraction"],
+            policy["record_capacity"], policy["workspace_limit_bytes"],
+            policy["workspace_reduction"], model["intercept"], model["scan"], model["match"],
+            model["output"], ch.ctypes.data, summ.ctypes.data)
+        return ch[:n], (reason, summ)
 
     def spgemm_serialref(self, a, b):
         rp = np.zeros(a.m + 1, dtype=np.int32)

@@ -936,6 +936,34 @@ int rtt_csr_to_hybrid_tiles(const SMatrix *M, int tile_rows, int tile_cols, int 
                                                dense_threshold, build_csc, out));
 }
 
+int rtt_plan_tail_queue(int ntasks, const int *scans, const int *matches, const int *output_nnz,
+                        const rtt_tail_policy *policy, const rtt_tail_cost_model *model,
+                        int *chunks_out, rtt_tail_plan *plan)
+{
+    if (ntasks < 0 || policy == nullptr || model == nullptr || plan == nullptr ||
+        (ntasks > 0 && (scans == nullptr || matches == nullptr || output_nnz == nullptr ||
+                        chunks_out == nullptr)))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "plan_tail_queue: bad arguments");
+    std::lock_guard<std::mutex> lock(g_mutex);
+    rtt_context c = nullptr;
+    RTT_CHECK(default_context(&c));
+    cudaStream_t s = c->ws.stream;
+    const size_t n = (size_t)ntasks;
+    RTT_CHECK(upload(c, c->in_rp, scans, n, s));
+    RTT_CHECK(upload(c, c->in_col, matches, n, s));
+    RTT_CHECK(upload(c, c->in2_rp, output_nnz, n, s));
+    RTT_CHECK(c->out_rp.ensure(sizeof(int) * (n + 1), s));
+    RTT_CHECK(plan_tail_queue_device(c->ws, ntasks, c->in_rp.as<int>(), c->in_col.as<int>(),
+                                     c->in2_rp.as<int>(), *policy, *model, c->out_rp.as<int>(),
+                                     plan));
+    if (ntasks > 0)
+    {
+        RTT_CUDA(cudaMemcpyAsync(chunks_out, c->out_rp.p, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+        RTT_CUDA(cudaStreamSynchronize(s));
+    }
+    return RTT_OK;
+}
+
 void rtt_hybrid_tiles_destroy(rtt_hybrid_tiles *h)
 {
     if (h == nullptr)

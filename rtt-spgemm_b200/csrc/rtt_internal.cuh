@@ -297,6 +297,10 @@ int tile2csr_fill_device(Workspace &ws, const int *tile_ptr, const int *tile_col
                          const double *val, int m, int n, int tilem, int td,
                          const int *new_to_old, int perm_size, const int *rowptr, int *out_col,
                          double *out_val, bool sort_rows, const int *row_data = nullptr);
+// tail-queue admission plan of n tasks (device arrays); chunks per task into d_chunks
+int plan_tail_queue_device(Workspace &ws, int n, const int *d_scans, const int *d_matches,
+                           const int *d_out, const rtt_tail_policy &policy,
+                           const rtt_tail_cost_model &model, int *d_chunks, rtt_tail_plan *plan);
 // CSR (host arrays) -> hybrid leaf tiles on the device, results malloc'd into out
 int csr_to_hybrid_host(Workspace &ws, const SMatrix *M, int tile_rows, int tile_cols,
                        int col_major, int dense_threshold, int build_csc, rtt_hybrid_tiles *out);

@@ -28,12 +28,14 @@ import numpy as np
 
 from . import generators
 from ._abi import (EXPORTS, LIB_PATH, RTT_OP_AAT, RTT_OP_AB, Config, CsrView, HybridTiles,
-                   RttError, SMatrix, Stats, build, check, lib)
+                   RttError, SMatrix, Stats, TailCostModel, TailPlan, TailPolicy, build, check,
+                   lib)
 from .generators import CSR
 
 __all__ = ["CSR", "Context", "RttError", "build", "csr2tile_col_major", "csr2tile_row_major",
            "generators", "lib", "spgemm_csr_host", "spgemm_tile", "tile16_to_tile8", "tile2csr",
-           "tile2csr_device_noalloc", "csr_to_hybrid_tiles",
+           "tile2csr_device_noalloc", "csr_to_hybrid_tiles", "plan_tail_queue",
+           "TAIL_POLICY_DEFAULT", "TAIL_MODEL_DEFAULT",
            "EXPORTS", "LIB_PATH", "RTT_OP_AB", "RTT_OP_AAT"]
 
 TD = 16
@@ -212,6 +214,31 @@ def csr_to_hybrid_tiles(csr, tile_rows: int = 8, tile_cols: int = 4, col_major: 
     d = hybrid_dict(h)
     lib().rtt_hybrid_tiles_destroy(C.byref(h))
     return d
+
+
+# the reference's defaults (src/dmma_tile_tail_queue.h:20-40), enabled
+TAIL_POLICY_DEFAULT = dict(enabled=1, admission_threshold=256.0, chunk_target=256.0, max_chunks=8,
+                           max_heavy_fraction=0.01, record_capacity=1 << 20,
+                           workspace_limit_bytes=1 << 30, workspace_reduction=1)
+TAIL_MODEL_DEFAULT = dict(intercept=0.0, scan=1.0, match=8.0, output=0.25)
+
+
+def plan_tail_queue(scans, matches, output_nnz, policy: dict | None = None,
+                    model: dict | None = None):
+    """GPU replacement of dmma_plan_tile_tail_queue (reference
+    src/dmma_tile_tail_queue.h:190).  Returns (chunks per task, plan dict)."""
+    sc = np.ascontiguousarray(scans, dtype=np.int32)
+    mt = np.ascontiguousarray(matches, dtype=np.int32)
+    on = np.ascontiguousarray(output_nnz, dtype=np.int32)
+    n = int(sc.shape[0])
+    pol = TailPolicy(**{**TAIL_POLICY_DEFAULT, **(policy or {})})
+    mod = TailCostModel(**{**TAIL_MODEL_DEFAULT, **(model or {})})
+    chunks = np.zeros(max(n, 1), np.int32)
+    plan = TailPlan()
+    check(lib().rtt_plan_tail_queue(n, _ptr(sc, C.c_int), _ptr(mt, C.c_int), _ptr(on, C.c_int),
+                                    C.byref(pol), C.byref(mod), _ptr(chunks, C.c_int),
+                                    C.byref(plan)))
+    return chunks[:n], {k: getattr(plan, k) for k, _ in TailPlan._fields_}
 
 
 def tile2csr_device_noalloc(tiles: dict, rowptr, col=None, val=None, tile_dim: int = 16,

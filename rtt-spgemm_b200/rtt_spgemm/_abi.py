@@ -33,6 +33,7 @@ EXPORTS = [
     "rtt_context_set_config", "rtt_context_get_stats", "rtt_spgemm_symbolic",
     "rtt_spgemm_numeric", "rtt_spgemm_tiles_view", "rtt_spgemm_csr_host",
     "rtt_tile2csr_device_noalloc", "rtt_csr_to_hybrid_tiles", "rtt_hybrid_tiles_destroy",
+    "rtt_plan_tail_queue",
 ]
 
 
@@ -83,6 +84,25 @@ class HybridTiles(C.Structure):
                 ("tile_row_idx", C.POINTER(C.c_int)), ("csc_tile_ids", C.POINTER(C.c_int))]
 
 
+class TailPolicy(C.Structure):
+    _fields_ = [("enabled", C.c_int), ("admission_threshold", C.c_double),
+                ("chunk_target", C.c_double), ("max_chunks", C.c_int),
+                ("max_heavy_fraction", C.c_double), ("record_capacity", C.c_int),
+                ("workspace_limit_bytes", C.c_longlong), ("workspace_reduction", C.c_int)]
+
+
+class TailCostModel(C.Structure):
+    _fields_ = [("intercept", C.c_double), ("scan", C.c_double), ("match", C.c_double),
+                ("output", C.c_double)]
+
+
+class TailPlan(C.Structure):
+    _fields_ = [("reason", C.c_int)] + [(k, C.c_longlong) for k in (
+        "output_tasks", "ordinary_tasks", "heavy_tasks", "chunks", "descriptor_bytes",
+        "heavy_flag_bytes", "partial_workspace_bytes")] + [
+        ("heavy_fraction", C.c_double), ("average_chunks", C.c_double)]
+
+
 class Stats(C.Structure):
     _fields_ = [("nnz_a", C.c_longlong), ("nnz_b", C.c_longlong), ("nnz_c", C.c_longlong),
                 ("nnz_cub", C.c_longlong), ("tiles_a", C.c_longlong),
@@ -127,6 +147,8 @@ def lib() -> C.CDLL:
     L.rtt_tile16_to_tile8.argtypes = [P(SMatrix), P(SMatrix)]
     L.rtt_csr_to_hybrid_tiles.argtypes = [P(SMatrix), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                           P(HybridTiles)]
+    L.rtt_plan_tail_queue.argtypes = [C.c_int, P(C.c_int), P(C.c_int), P(C.c_int),
+                                      P(TailPolicy), P(TailCostModel), P(C.c_int), P(TailPlan)]
     L.rtt_hybrid_tiles_destroy.argtypes = [P(HybridTiles)]
     L.rtt_hybrid_tiles_destroy.restype = None
     L.rtt_tile2csr_device_noalloc.argtypes = [P(SMatrix), C.c_int, C.c_int, C.c_longlong,

@@ -1,0 +1,35 @@
+"""GPU parity of rtt_plan_tail_queue (the reference's dmma_plan_tile_tail_queue,
+src/dmma_tile_tail_queue.h:190) against the oracle restatement, which
+test_oracle_pin.py pins to the reference: chunk counts and gate reasons exact."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as O
+import rtt_spgemm as R
+from test_oracle_pin import TAIL_CASES, TAIL_MODEL, TAIL_POLICY, tail_tasks
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case", list(TAIL_CASES))
+def test_tail_planner_matches_oracle(case):
+    pol, mod, tk = TAIL_CASES[case]
+    pol, mod = {**TAIL_POLICY, **pol}, {**TAIL_MODEL, **mod}
+    s, m, o = tail_tasks(**tk)
+    ch, plan = R.plan_tail_queue(s, m, o, pol, mod)
+    want_ch, want = O.plan_tail_queue(s, m, o, pol, mod)
+    assert plan["reason"] == want["reason"], case
+    assert np.array_equal(ch, want_ch)
+    for k in ("output_tasks", "ordinary_tasks", "heavy_tasks", "chunks", "descriptor_bytes",
+              "heavy_flag_bytes", "partial_workspace_bytes"):
+        assert plan[k] == want[k], k
+    assert plan["heavy_fraction"] == pytest.approx(want["heavy_fraction"])
+
+
+def test_tail_planner_disabled_and_empty():
+    ch, plan = R.plan_tail_queue([5, 900], [1, 800], [3, 4], dict(enabled=0))
+    assert plan["reason"] == 0 and list(ch) == [0, 0]
+    ch, plan = R.plan_tail_queue([], [], [])
+    assert plan["reason"] == 4 and plan["output_tasks"] == 0

@@ -204,3 +204,50 @@ def test_hybrid_duplicates_summed(ref, orc):
     A = G.random_csr(40, 40, 0.1, seed=12, duplicates=0.3)
     _assert_hybrid_equal(orc.csr_to_hybrid_tiles(A, 8, 4, False, 4, True),
                          ref.csr_to_hybrid_tiles(A, 8, 4, False, 4, True), "dups: ", exact=False)
+
+
+# ---------------------------------------------------------------- tail-queue planner
+TAIL_POLICY = dict(enabled=1, admission_threshold=256.0, chunk_target=256.0, max_chunks=8,
+                   max_heavy_fraction=0.01, record_capacity=1 << 20,
+                   workspace_limit_bytes=1 << 30, workspace_reduction=1)
+TAIL_MODEL = dict(intercept=0.0, scan=1.0, match=8.0, output=0.25)
+
+
+def tail_tasks(n, seed, heavy_rate=0.01, invalid_at=None):
+    rng = np.random.default_rng(seed)
+    scans = rng.integers(0, 40, n)
+    heavy = rng.random(n) < heavy_rate
+    scans[heavy] = rng.integers(40, 5000, heavy.sum())
+    matches = (scans * rng.random(n)).astype(np.int64)
+    out = rng.integers(0, 65, n)
+    if invalid_at is not None:
+        matches[invalid_at] = scans[invalid_at] + 1
+    return scans, matches, out
+
+
+TAIL_CASES = {
+    "default": (dict(), dict(), dict(n=5000, seed=1)),
+    "enabled": (dict(max_heavy_fraction=0.5), dict(), dict(n=5000, seed=2, heavy_rate=0.02)),
+    "fraction_gate": (dict(), dict(), dict(n=3000, seed=3, heavy_rate=0.2)),
+    "zero_heavy": (dict(admission_threshold=1e9), dict(), dict(n=1000, seed=4)),
+    "workspace_gate": (dict(max_heavy_fraction=1.0, workspace_limit_bytes=4096), dict(), dict(n=2000, seed=5)),
+    "record_capacity": (dict(max_heavy_fraction=1.0, record_capacity=3), dict(), dict(n=2000, seed=6, heavy_rate=0.05)),
+    "invalid_task": (dict(max_heavy_fraction=1.0), dict(), dict(n=2000, seed=7, invalid_at=900)),
+    "odd_model": (dict(chunk_target=33.3, max_chunks=32, max_heavy_fraction=1.0),
+                  dict(scan=0.37, match=3.1), dict(n=4000, seed=8, heavy_rate=0.3)),
+    "invalid_policy": (dict(max_chunks=1), dict(), dict(n=100, seed=9)),
+}
+
+
+@pytest.mark.parametrize("case", list(TAIL_CASES))
+def test_tail_planner_oracle_matches_reference(ref, case):
+    import oracle as O
+    pol, mod, tk = TAIL_CASES[case]
+    pol, mod = {**TAIL_POLICY, **pol}, {**TAIL_MODEL, **mod}
+    s, m, o = tail_tasks(**tk)
+    ch, plan = O.plan_tail_queue(s, m, o, pol, mod)
+    rch, (reason, summ) = ref.plan_tail_queue(s, m, o, pol, mod)
+    assert plan["reason"] == reason
+    assert np.array_equal(ch, rch)
+    assert [plan["heavy_tasks"], plan["chunks"], plan["descriptor_bytes"],
+            plan["partial_workspace_bytes"], plan["heavy_flag_bytes"]] == list(summ)
