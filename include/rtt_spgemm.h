@@ -376,6 +376,27 @@ RTT_API int rtt_spgemm_tiles_view(rtt_context ctx, SMatrix *c_tiles_device);
 RTT_API int rtt_spgemm_csr_host(rtt_context ctx, const SMatrix *A, const SMatrix *B,
                         int op, SMatrix *C);
 
+/* Batched form (no single reference function: it batches the device path
+ * above over independent products, the north star's "many SpGEMMs of uneven
+ * sizes in one launch").  count products C_i = A_i * B_i (B == NULL: C_i =
+ * A_i^2, A_i square), device CSR views in; all instances run through ONE
+ * csr2tile, ONE symbolic and ONE numeric pass over their block diagonal
+ * (every instance padded to a multiple of 16 rows and columns).
+ * nnz_c[i] receives nnz(C_i); *nnz_total their sum.  A and B stay borrowed
+ * until rtt_spgemm_batched_numeric returns.  Limits: the padded totals and
+ * the total nnz must fit int32 (else RTT_ERR_UNREPRESENTABLE). */
+RTT_API int rtt_spgemm_batched_symbolic(rtt_context ctx, int count, const rtt_csr_view *A,
+                                        const rtt_csr_view *B, long long *nnz_c,
+                                        long long *nnz_total);
+
+/* Writes the products of the last batched symbolic.  c_row_ptr: the
+ * instances' row pointers one after another (instance i's A_i.rows + 1
+ * entries, starting at 0, at offset sum_{j<i} (A_j.rows + 1)); c_col_idx /
+ * c_values: nnz_total entries, instance i's at offset sum_{j<i} nnz_c[j], with
+ * columns local to the instance.  Work is queued on the context's stream. */
+RTT_API int rtt_spgemm_batched_numeric(rtt_context ctx, int *c_row_ptr, int *c_col_idx,
+                                       double *c_values);
+
 #ifdef __cplusplus
 }
 #endif

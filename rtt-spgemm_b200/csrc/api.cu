@@ -42,6 +42,13 @@ struct rtt_context_s
     // page-locked staging of the host-buffer entry points (created on first use)
     void *hstage[2] = {};
     cudaEvent_t hstage_ev[2] = {};
+    // batched products: block-diagonal operands and per-instance bookkeeping
+    rtt::DevBuf bat_a_rp, bat_a_col, bat_a_val, bat_b_rp, bat_b_col, bat_b_val;
+    rtt::DevBuf bat_meta, bat_big_rp, bat_nnz;
+    bool bat_active = false;
+    int bat_count = 0, bat_rows = 0;
+    // offsets (in ints) of the device meta arrays inside bat_meta
+    size_t bat_rows_off = 0, bat_rowoff_off = 0, bat_sec_off = 0, bat_colsub_off = 0;
 };
 
 namespace
@@ -607,7 +614,10 @@ void rtt_context_destroy(rtt_context c)
     c->S.release();
     rtt::DevBuf *bufs[] = {&c->bt_rowptr, &c->bt_col, &c->bt_val, &c->in_rp, &c->in_col,
                            &c->in_val, &c->in2_rp, &c->in2_col, &c->in2_val, &c->out_rp,
-                           &c->out_col, &c->out_val, &c->counters, &c->maxnnz};
+                           &c->out_col, &c->out_val, &c->counters, &c->maxnnz,
+                           &c->bat_a_rp, &c->bat_a_col, &c->bat_a_val, &c->bat_b_rp,
+                           &c->bat_b_col, &c->bat_b_val, &c->bat_meta, &c->bat_big_rp,
+                           &c->bat_nnz};
     for (rtt::DevBuf *b : bufs)
         b->release();
     for (int b = 0; b < 2; ++b)
@@ -1028,6 +1038,7 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "bad A shape");
     RTT_CUDA(cudaSetDevice(c->ws.device));
     c->have_symbolic = false;
+    c->bat_active = false;
     c->ws.launches = 0;
     c->ws.syncs = 0;
     std::memset(&c->stats, 0, sizeof(c->stats));
@@ -1177,6 +1188,165 @@ int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_
     c->stats.nnz_cub = ws.h_scalars64[3];
     c->stats.kernel_launches = ws.launches;
     c->stats.host_syncs = ws.syncs;
+    return RTT_OK;
+}
+
+// ------------------------------------------------------------ batched products
+namespace
+{
+inline long long pad16(long long v) { return (v + 15) / 16 * 16; }
+
+bool view_ok(const rtt_csr_view &v)
+{
+    return v.rows >= 0 && v.cols >= 0 && v.nnz >= 0 && v.nnz <= INT_MAX &&
+           v.row_ptr != nullptr && (v.nnz == 0 || (v.col_idx != nullptr && v.values != nullptr));
+}
+
+// Block-diagonal assembly of count instances into (rp, col, val): instance i's
+// rows start at row_off[i] (multiples of 16), its columns are shifted by
+// col_add[i].  meta_base points at count * 3 pointer slots + int arrays.
+int assemble(rtt_context c, int count, const rtt_csr_view *V, const std::vector<int> &row_off,
+             const std::vector<int> &col_add, DevBuf &rp, DevBuf &col, DevBuf &val)
+{
+    Workspace &ws = c->ws;
+    cudaStream_t s = ws.stream;
+    const int total_rows = row_off[(size_t)count];
+    std::vector<int> rows((size_t)count), nnz_off((size_t)count + 1, 0);
+    std::vector<const void *> tab((size_t)count * 3);
+    for (int i = 0; i < count; ++i)
+    {
+        rows[(size_t)i] = V[i].rows;
+        nnz_off[(size_t)i + 1] = nnz_off[(size_t)i] + (int)V[i].nnz;
+        tab[(size_t)i] = V[i].row_ptr;
+        tab[(size_t)count + i] = V[i].col_idx;
+        tab[(size_t)2 * count + i] = V[i].values;
+    }
+    const int nnz = nnz_off[(size_t)count];
+    // device copy of the tables: pointers first (8-byte aligned), then ints
+    DevBuf tabd;
+    const size_t ints = (size_t)count * 3 + 2;
+    RTT_CHECK(tabd.ensure(sizeof(void *) * tab.size() + sizeof(int) * ints, s));
+    char *base = tabd.as<char>();
+    int *d_rows = reinterpret_cast<int *>(base + sizeof(void *) * tab.size());
+    int *d_rowoff = d_rows + count, *d_coladd = d_rowoff + count + 1, *d_nnzoff = d_coladd + count;
+    std::vector<int> packed;
+    packed.insert(packed.end(), rows.begin(), rows.end());
+    packed.insert(packed.end(), row_off.begin(), row_off.end());
+    packed.insert(packed.end(), col_add.begin(), col_add.begin() + count);
+    packed.insert(packed.end(), nnz_off.begin(), nnz_off.end());
+    RTT_CUDA(cudaMemcpyAsync(base, tab.data(), sizeof(void *) * tab.size(), cudaMemcpyHostToDevice, s));
+    RTT_CUDA(cudaMemcpyAsync(d_rows, packed.data(), sizeof(int) * packed.size(), cudaMemcpyHostToDevice, s));
+    RTT_CHECK(rp.ensure(sizeof(int) * ((size_t)total_rows + 1), s));
+    RTT_CHECK(col.ensure(sizeof(int) * (size_t)nnz + 16, s));
+    RTT_CHECK(val.ensure(sizeof(double) * (size_t)nnz + 16, s));
+    const void *const *tp = reinterpret_cast<const void *const *>(base);
+    RTT_CHECK(batch_assemble_device(ws, count, total_rows, reinterpret_cast<const int *const *>(tp),
+                                    reinterpret_cast<const int *const *>(tp + count),
+                                    reinterpret_cast<const double *const *>(tp + 2 * count),
+                                    d_rows, d_rowoff, d_coladd, d_nnzoff, rp.as<int>(),
+                                    col.as<int>(), val.as<double>()));
+    RTT_CUDA(cudaStreamSynchronize(s)); // the tables are released on return
+    tabd.release();
+    return RTT_OK;
+}
+} // namespace
+
+int rtt_spgemm_batched_symbolic(rtt_context c, int count, const rtt_csr_view *A,
+                                const rtt_csr_view *B, long long *nnz_c, long long *nnz_total)
+{
+    if (c == nullptr || count < 1 || A == nullptr || nnz_c == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "batched: bad arguments");
+    long long R = 0, K = 0, P = 0, annz = 0, bnnz = 0, sec = 0;
+    std::vector<int> row_off((size_t)count + 1), col_off((size_t)count + 1),
+        pcol_off((size_t)count + 1), sec_off((size_t)count), rows((size_t)count);
+    for (int i = 0; i < count; ++i)
+    {
+        if (!view_ok(A[i]) || (B != nullptr && !view_ok(B[i])))
+            return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "batched: bad instance " + std::to_string(i));
+        if (B == nullptr ? A[i].rows != A[i].cols : B[i].rows != A[i].cols)
+            return rtt::fail(RTT_ERR_SHAPE_MISMATCH, "batched: instance " + std::to_string(i) +
+                                                         " has mismatched shapes");
+        row_off[(size_t)i] = (int)R;
+        col_off[(size_t)i] = (int)K;
+        pcol_off[(size_t)i] = (int)P;
+        sec_off[(size_t)i] = (int)sec;
+        rows[(size_t)i] = A[i].rows;
+        R += pad16(A[i].rows);
+        K += pad16(A[i].cols);
+        P += pad16(B ? B[i].cols : A[i].cols);
+        annz += A[i].nnz;
+        bnnz += B ? B[i].nnz : 0;
+        sec += A[i].rows + 1;
+        if (R > INT_MAX / 2 || K > INT_MAX / 2 || P > INT_MAX / 2 || annz > INT_MAX ||
+            bnnz > INT_MAX || sec > INT_MAX)
+            return rtt::fail(RTT_ERR_UNREPRESENTABLE, "batched: batch exceeds int32 sizes");
+    }
+    row_off[(size_t)count] = (int)R;
+    col_off[(size_t)count] = (int)K;
+    pcol_off[(size_t)count] = (int)P;
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    Workspace &ws = c->ws;
+    cudaStream_t s = ws.stream;
+    // A's block diagonal (rows at row_off, columns shifted to col_off)
+    RTT_CHECK(assemble(c, count, A, row_off, col_off, c->bat_a_rp, c->bat_a_col, c->bat_a_val));
+    rtt_csr_view va{(int)R, (int)K, annz, c->bat_a_rp.as<int>(), c->bat_a_col.as<int>(),
+                    c->bat_a_val.as<double>()};
+    rtt_csr_view vb{};
+    if (B != nullptr)
+    {
+        RTT_CHECK(assemble(c, count, B, col_off, pcol_off, c->bat_b_rp, c->bat_b_col,
+                           c->bat_b_val));
+        vb = rtt_csr_view{(int)K, (int)P, bnnz, c->bat_b_rp.as<int>(), c->bat_b_col.as<int>(),
+                          c->bat_b_val.as<double>()};
+    }
+    long long nnz = 0, tiles = 0;
+    RTT_CHECK(rtt_spgemm_symbolic(c, &va, B ? &vb : nullptr, RTT_OP_AB, &nnz, &tiles));
+    // per-instance bookkeeping on the device: rows, row offsets, sections, column shifts
+    const size_t meta = (size_t)count * 4 + 1;
+    RTT_CHECK(c->bat_meta.ensure(sizeof(int) * meta, s));
+    std::vector<int> packed;
+    packed.insert(packed.end(), rows.begin(), rows.end());
+    packed.insert(packed.end(), row_off.begin(), row_off.end());
+    packed.insert(packed.end(), sec_off.begin(), sec_off.end());
+    packed.insert(packed.end(), pcol_off.begin(), pcol_off.begin() + count);
+    RTT_CUDA(cudaMemcpyAsync(c->bat_meta.p, packed.data(), sizeof(int) * packed.size(),
+                             cudaMemcpyHostToDevice, s));
+    c->bat_rows_off = 0;
+    c->bat_rowoff_off = (size_t)count;
+    c->bat_sec_off = (size_t)count * 2 + 1;
+    c->bat_colsub_off = (size_t)count * 3 + 1;
+    RTT_CHECK(c->bat_nnz.ensure(sizeof(long long) * (size_t)count, s));
+    const int *meta_d = c->bat_meta.as<int>();
+    RTT_CHECK(batch_count_device(ws, count, meta_d + c->bat_rowoff_off, meta_d + c->bat_rows_off,
+                                 c->S.c_row_cnt.as<int>(), c->bat_nnz.as<long long>()));
+    RTT_CUDA(cudaMemcpyAsync(nnz_c, c->bat_nnz.p, sizeof(long long) * (size_t)count,
+                             cudaMemcpyDeviceToHost, s));
+    RTT_CUDA(cudaStreamSynchronize(s));
+    if (nnz_total)
+        *nnz_total = nnz;
+    c->bat_active = true;
+    c->bat_count = count;
+    c->bat_rows = (int)R;
+    return RTT_OK;
+}
+
+int rtt_spgemm_batched_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_values)
+{
+    if (c == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (!c->bat_active || !c->have_symbolic)
+        return rtt::fail(RTT_ERR_STATE, "rtt_spgemm_batched_numeric before rtt_spgemm_batched_symbolic");
+    if (c_row_ptr == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "NULL output buffer");
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    cudaStream_t s = c->ws.stream;
+    RTT_CHECK(c->bat_big_rp.ensure(sizeof(int) * ((size_t)c->bat_rows + 1), s));
+    RTT_CHECK(rtt_spgemm_numeric(c, c->bat_big_rp.as<int>(), c_col_idx, c_values));
+    const int *meta_d = c->bat_meta.as<int>();
+    RTT_CHECK(batch_split_device(c->ws, c->bat_count, c->bat_rows, meta_d + c->bat_rowoff_off,
+                                 meta_d + c->bat_rows_off, meta_d + c->bat_sec_off,
+                                 meta_d + c->bat_colsub_off, c->bat_big_rp.as<int>(), c_row_ptr,
+                                 c_col_idx));
     return RTT_OK;
 }
 

@@ -297,6 +297,16 @@ int tile2csr_fill_device(Workspace &ws, const int *tile_ptr, const int *tile_col
                          const double *val, int m, int n, int tilem, int td,
                          const int *new_to_old, int perm_size, const int *rowptr, int *out_col,
                          double *out_val, bool sort_rows, const int *row_data = nullptr);
+// batched products (block-diagonal operands)
+int batch_assemble_device(Workspace &ws, int count, int total_rows, const int *const *rp_tab,
+                          const int *const *ci_tab, const double *const *va_tab, const int *rows,
+                          const int *row_off, const int *col_add, const int *nnz_off, int *out_rp,
+                          int *out_col, double *out_val);
+int batch_count_device(Workspace &ws, int count, const int *row_off, const int *rows,
+                       const int *row_cnt, long long *nnz);
+int batch_split_device(Workspace &ws, int count, int total_rows, const int *row_off,
+                       const int *rows, const int *sec_off, const int *col_sub, const int *big_rp,
+                       int *out_rp, int *col);
 // tail-queue admission plan of n tasks (device arrays); chunks per task into d_chunks
 int plan_tail_queue_device(Workspace &ws, int n, const int *d_scans, const int *d_matches,
                            const int *d_out, const rtt_tail_policy &policy,

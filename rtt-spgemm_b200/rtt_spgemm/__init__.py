@@ -35,7 +35,7 @@ from .generators import CSR
 __all__ = ["CSR", "Context", "RttError", "build", "csr2tile_col_major", "csr2tile_row_major",
            "generators", "lib", "spgemm_csr_host", "spgemm_tile", "tile16_to_tile8", "tile2csr",
            "tile2csr_device_noalloc", "csr_to_hybrid_tiles", "plan_tail_queue",
-           "TAIL_POLICY_DEFAULT", "TAIL_MODEL_DEFAULT",
+           "TAIL_POLICY_DEFAULT", "TAIL_MODEL_DEFAULT", "spgemm_batched",
            "EXPORTS", "LIB_PATH", "RTT_OP_AB", "RTT_OP_AAT"]
 
 TD = 16
@@ -327,6 +327,27 @@ class Context:
         finally:
             self._borrowed = None
 
+    def batched_symbolic(self, As, Bs=None):
+        """Batched form: As (and Bs) are lists of (rows, cols, rowptr, col, val)
+        device tuples.  Returns (nnz per instance, total nnz).  The operands
+        stay borrowed until batched_numeric() returns."""
+        count = len(As)
+        va = (CsrView * count)(*[self._view(*a) for a in As])
+        vb = (CsrView * count)(*[self._view(*b) for b in Bs]) if Bs is not None else None
+        nnz = (C.c_longlong * count)()
+        tot = C.c_longlong()
+        self._borrowed = (As, Bs)
+        check(lib().rtt_spgemm_batched_symbolic(self.handle, count, va, vb, nnz, C.byref(tot)))
+        return list(nnz), tot.value
+
+    def batched_numeric(self, rowptr, col, val):
+        try:
+            check(lib().rtt_spgemm_batched_numeric(self.handle, C.c_void_p(rowptr.data_ptr()),
+                                                   C.c_void_p(col.data_ptr()),
+                                                   C.c_void_p(val.data_ptr())))
+        finally:
+            self._borrowed = None
+
     def stats(self) -> dict:
         st = Stats()
         check(lib().rtt_context_get_stats(self.handle, C.byref(st)))
@@ -343,6 +364,27 @@ class Context:
         # C's arrays were malloc'd by the library: hand them to numpy as they are
         return CSR(sc.m, sc.n, _adopt(sc.rowpointer, sc.m + 1, np.int32),
                    _adopt(sc.columnindex, sc.nnz, np.int32), _adopt(sc.value, sc.nnz, np.float64))
+
+
+def spgemm_batched(ctx: "Context", As, Bs=None):
+    """C_i = A_i * B_i (or A_i^2) for a list of device CSR tuples, through one
+    pipeline run.  Returns per-instance (rowptr, col, val) device tensor views
+    of three concatenated output buffers."""
+    import torch
+
+    nnz, total = ctx.batched_symbolic(As, Bs)
+    dev = As[0][2].device
+    rows = [int(a[0]) for a in As]
+    rp = torch.empty(sum(r + 1 for r in rows), dtype=torch.int32, device=dev)
+    col = torch.empty(max(total, 1), dtype=torch.int32, device=dev)
+    val = torch.empty(max(total, 1), dtype=torch.float64, device=dev)
+    ctx.batched_numeric(rp, col, val)
+    out, r0, e0 = [], 0, 0
+    for r, z in zip(rows, nnz):
+        out.append((rp[r0:r0 + r + 1], col[e0:e0 + z], val[e0:e0 + z]))
+        r0 += r + 1
+        e0 += z
+    return out
 
 
 def spgemm_csr_host(a, b=None, op: int = RTT_OP_AB, device: int = 0) -> CSR:

@@ -189,6 +189,18 @@ def banded_scatter(n: int, half_bw: int, p: float = 0.5, scatter_max: int = 4,
     return CSR(n, n, rp.astype(np.int32), (key % n).astype(np.int32), val)
 
 
+def batched_instances(count: int, n_lo: int = 2000, n_hi: int = 200000, seed: int = 0) -> list:
+    """The batched configuration's instances: n_i log-uniform in [n_lo, n_hi],
+    each banded (half-bandwidth uniform in 8..64, band entries kept with
+    probability 0.5) plus 0..4 random off-band entries per row, values
+    uniform in [-1, 1)."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), size=count)).astype(np.int64)
+    hb = rng.integers(8, 65, size=count)
+    return [banded_scatter(int(n), int(h), 0.5, 4, seed=int(seed * 100003 + i))
+            for i, (n, h) in enumerate(zip(ns, hb))]
+
+
 def random_csr(m: int, n: int, density: float, seed: int = 0, sort: bool = True,
                duplicates: float = 0.0, explicit_zeros: float = 0.0) -> CSR:
     """Uniform random CSR for edge-case tests: optionally unsorted rows,
