@@ -38,6 +38,9 @@ WORKLOADS = {
     "stencil27_96_brick": "3-D 27-point stencil, 96^3 grid, 2x2x4 brick ordering, C = A^2",
     "laplacian2d_256": "2-D 5-point Laplacian, 256^2 grid (n=65,536), C = A^2",
     "stencil27_80": "3-D 27-point stencil, 80^3 grid (n=512,000), C = A^2 (profiling size)",
+    "batched": "independent A_i^2: n_i log-uniform in [2,000, 200,000], banded (half-bandwidth "
+               "8..64, band kept w.p. 0.5) + 0..4 random entries per row; batched form vs one "
+               "call per product",
 }
 
 
@@ -192,6 +195,78 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args) -> None:
+    """Batched form against the plain one-call-per-product path on the same
+    instances: SpGEMMs/s of each, instances processed in memory-bounded waves."""
+    import torch
+    import rtt_spgemm as R
+    from rtt_spgemm import generators as G
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    As = G.batched_instances(args.batch_count, 2000, 200000, seed=args.seed)
+    flops = sum(2.0 * nnz_cub(A) for A in As)
+    views = [(A.m, A.n, torch.from_numpy(A.rowptr).to(dev), torch.from_numpy(A.col).to(dev),
+              torch.from_numpy(A.val).to(dev)) for A in As]
+    waves, cur, rows = [], [], 0
+    for i, A in enumerate(As):
+        if cur and rows + A.m > args.wave_rows:
+            waves.append(cur)
+            cur, rows = [], 0
+        cur.append(i)
+        rows += A.m
+    if cur:
+        waves.append(cur)
+    ctx = R.Context(0, {"stage_timing": 0, "dmma_pair_cutoff": args.dmma_cutoff,
+                        "b_staging": 1 if args.staging else 0})
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+
+    def batched():
+        for w in waves:
+            R.spgemm_batched(ctx, [views[i] for i in w])
+
+    def plain():
+        for v in views:
+            nnz, _ = ctx.symbolic(v)
+            rp = torch.empty(v[0] + 1, dtype=torch.int32, device=dev)
+            ci = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+            va = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
+            ctx.numeric(rp, ci, va)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / args.steps
+
+    ms_b = timed(batched)
+    ms_p = timed(plain)
+    n = len(As)
+    line = {
+        "metric": "SpGEMMs/s (batched)", "value": n / (ms_b * 1e-3), "unit": "SpGEMMs/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_b,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": "batched", "description": WORKLOADS["batched"], "instances": n,
+                   "rows_total": int(sum(A.m for A in As)), "nnz_a_total": int(sum(A.nnz for A in As)),
+                   "flops": flops, "waves": len(waves), "wave_rows": args.wave_rows,
+                   "dmma_pair_cutoff": args.dmma_cutoff},
+        "gflops_batched": flops / (ms_b * 1e-3) / 1e9,
+        "plain": {"spgemms_per_s": n / (ms_p * 1e-3), "ms_per_step": ms_p,
+                  "gflops": flops / (ms_p * 1e-3) / 1e9},
+        "batched_over_plain": ms_p / ms_b,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def run_ours(args) -> None:
     import torch
     import rtt_spgemm as R
@@ -343,10 +418,12 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="stencil27_96", choices=list(WORKLOADS))
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--dmma-cutoff", type=int, default=3072)
+    ap.add_argument("--dmma-cutoff", type=int, default=0)
     ap.add_argument("--unfused", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--batch-count", type=int, default=128)
+    ap.add_argument("--wave-rows", type=int, default=4_000_000)
     ap.add_argument("--staging", action="store_true",
                     help="TMA-staged numeric kernel instead of the default flat one")
     ap.add_argument("--ref-tile-rows", type=int, default=256)
@@ -355,6 +432,8 @@ def main() -> None:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batched":
+        run_batched(args)
     else:
         run_ours(args)
 

@@ -297,7 +297,10 @@ typedef struct
 typedef struct
 {
     /* A tile pair (A(I,K), B(K,J)) goes to the FP64 DMMA tensor-core path
-     * when nnz(A(I,K)) * nnz(B(K,J)) >= dmma_pair_cutoff; 0 disables DMMA. */
+     * when nnz(A(I,K)) * nnz(B(K,J)) >= dmma_pair_cutoff; 0 disables DMMA
+     * (the default: the flat scalar kernel measured faster on every workload
+     * tried, banded batches with dense tiles included; 3072 is a typical
+     * value for brick-ordered stencils). */
     int dmma_pair_cutoff;
     /* Numeric writes C's CSR directly (fused tile2csr) when nonzero;
      * otherwise C is written as 16x16 tiles and converted by tile2csr. */

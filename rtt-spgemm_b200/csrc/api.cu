@@ -562,7 +562,7 @@ void rtt_config_default(rtt_config *config)
     if (config == nullptr)
         return;
     std::memset(config, 0, sizeof(*config));
-    config->dmma_pair_cutoff = 3072;
+    config->dmma_pair_cutoff = 0;
     config->fused_csr_output = 1;
     config->keep_tiles = 0;
     config->b_staging = 0;

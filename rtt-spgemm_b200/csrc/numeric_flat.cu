@@ -30,7 +30,7 @@
 // the fixed order (K, k) ascending - bitwise reproducible.  (With repeated
 // columns in a B row the SAFE instantiation adds with shared atomics.)
 //
-// Windows of C tiles (<= F_SLOT_CAP tiles, <= F_ACC_CAP entries) bound shared
+// Windows of C tiles (<= F_SLOT_CAP tiles, <= ACC entries) bound shared
 // memory; products whose C tile is outside the window are skipped and the A
 // list is walked again for the next window.  Each product also stores its
 // column beside its accumulator slot, so the CSR write-out of a row is two
@@ -47,18 +47,22 @@ namespace
 constexpr int FW = 8;                       // warps per CTA
 constexpr int RPW = TD / FW;                // rows per warp
 constexpr int F_THREADS = FW * 32;
-constexpr int F_MIN_CTAS = 5;               // CTAs per SM the launch bounds aim at
-constexpr int F_ACC_CAP = 2048;             // accumulator slots per window
+// Two shapes of the kernel: 2048 accumulator slots at five CTAs per SM for
+// tile rows up to 2048 entries, 4608 slots at three CTAs per SM for wider
+// ones (a window of more entries than slots walks the tile row again).
+constexpr int ACC_SMALL = 2048, CTAS_SMALL = 5;
+constexpr int ACC_LARGE = 4608, CTAS_LARGE = 3;
 constexpr int F_SLOT_CAP = 128;             // C tiles per window
 constexpr int F_CM_STRIDE = F_SLOT_CAP + 1; // row stride of cm: rows land in distinct banks
 constexpr int F_SPAN_CAP = 4096;            // tile-column span of the slot table
 constexpr int GROUP = 2;                    // B rows loaded together
 static_assert(RPW == 1 || RPW == 2, "one or two rows per warp");
 
+template <int ACC>
 struct FlatSmem
 {
-    double acc[F_ACC_CAP];
-    int ccol[F_ACC_CAP];              // column of each accumulator slot (written by the products)
+    double acc[ACC];
+    int ccol[ACC];                    // column of each accumulator slot (written by the products)
     uint32_t cm[TD * F_CM_STRIDE];    // [row][slot]: (acc base << 16) | row mask
     int cJ[F_SLOT_CAP];
     uint8_t slot8[F_SPAN_CAP];        // tile column - Jlo -> slot (255 = none)
@@ -77,7 +81,8 @@ struct Window
     bool table;
 };
 
-__device__ __forceinline__ int flat_slot(const FlatSmem &S, const Window &W, int J)
+template <class Smem>
+__device__ __forceinline__ int flat_slot(const Smem &S, const Window &W, int J)
 {
     const int d = J - W.Jlo;
     if ((unsigned)d > (unsigned)W.Jspan)
@@ -96,8 +101,8 @@ __device__ __forceinline__ int flat_slot(const FlatSmem &S, const Window &W, int
 // (the symbolic step saw the same A tiles and B rows), so the lookup runs
 // without branches; the two clamps only keep inconsistent operands inside
 // this CTA's shared memory.
-template <bool SAFE, bool CHECK>
-__device__ __forceinline__ void flat_add(FlatSmem &S, const Window &W, const uint32_t *cmr,
+template <bool SAFE, bool CHECK, int ACC>
+__device__ __forceinline__ void flat_add(FlatSmem<ACC> &S, const Window &W, const uint32_t *cmr,
                                          int col, double a, double b)
 {
     int slot;
@@ -114,7 +119,7 @@ __device__ __forceinline__ void flat_add(FlatSmem &S, const Window &W, const uin
     const uint32_t w = cmr[slot];
     int pos = (int)(w >> 16) + __popc((w & 0xFFFFu) >> (16 - (col & 15)));
     if (!CHECK)
-        pos = min(pos, F_ACC_CAP - 1);
+        pos = min(pos, ACC - 1);
     if (SAFE)
         atomicAdd(&S.acc[pos], a * b);
     else
@@ -124,8 +129,8 @@ __device__ __forceinline__ void flat_add(FlatSmem &S, const Window &W, const uin
 
 // The warp's products for one window: every A entry (r, k) of its rows r0, r1
 // times B's row k.  Returns the number of products when count is set.
-template <bool SAFE, bool CHECK>
-__device__ __forceinline__ long long warp_products(FlatSmem &S, const Window &W, const DevTiles &A,
+template <bool SAFE, bool CHECK, int ACC>
+__device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Window &W, const DevTiles &A,
                                                    const DevTiles &B, int a0, int a1, int r0,
                                                    int r1, bool count, int4 *ent, double *enta)
 {
@@ -213,10 +218,10 @@ __device__ __forceinline__ long long warp_products(FlatSmem &S, const Window &W,
                     const double au = enta[(j + u) & 31];
                     const uint32_t *cmr = S.cm + ge[u].z;
                     if (lane < ge[u].y)
-                        flat_add<SAFE, CHECK>(S, W, cmr, gcol[u], au, gb[u]);
+                        flat_add<SAFE, CHECK, ACC>(S, W, cmr, gcol[u], au, gb[u]);
                     if (ge[u].y > 32) // rows longer than a warp (uniform branch)
                         for (int f = 32 + lane; f < ge[u].y; f += 32)
-                            flat_add<SAFE, CHECK>(S, W, cmr, __ldg(B.csr_col + ge[u].x + f), au,
+                            flat_add<SAFE, CHECK, ACC>(S, W, cmr, __ldg(B.csr_col + ge[u].x + f), au,
                                                   __ldg(B.csr_val + ge[u].x + f));
                 }
             }
@@ -226,8 +231,8 @@ __device__ __forceinline__ long long warp_products(FlatSmem &S, const Window &W,
     return n_fma;
 }
 
-template <bool SAFE>
-__global__ void __launch_bounds__(F_THREADS, F_MIN_CTAS)
+template <bool SAFE, int ACC, int MIN_CTAS>
+__global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
     k_numeric_flat(DevTiles A, DevTiles B, int tilem, long long nnzC,
                    const int *__restrict__ c_tile_ptr, const int *__restrict__ c_tile_col,
                    const uint16_t *__restrict__ c_mask, const int *__restrict__ c_tile_nnz,
@@ -237,7 +242,7 @@ __global__ void __launch_bounds__(F_THREADS, F_MIN_CTAS)
                    int *err)
 {
     extern __shared__ __align__(128) unsigned char dyn[];
-    FlatSmem &S = *reinterpret_cast<FlatSmem *>(dyn);
+    FlatSmem<ACC> &S = *reinterpret_cast<FlatSmem<ACC> *>(dyn);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int I = blockIdx.x;
     if (I >= tilem)
@@ -260,7 +265,7 @@ __global__ void __launch_bounds__(F_THREADS, F_MIN_CTAS)
         const int base_nnz = __ldg(c_tile_nnz + w0);
         bool ok = false;
         if (tid < F_SLOT_CAP && w0 + tid < cs1)
-            ok = __ldg(c_tile_nnz + w0 + tid + 1) - base_nnz <= F_ACC_CAP;
+            ok = __ldg(c_tile_nnz + w0 + tid + 1) - base_nnz <= ACC;
         const int nW = __syncthreads_count(ok);
         if (nW == 0)
         {
@@ -347,9 +352,9 @@ __global__ void __launch_bounds__(F_THREADS, F_MIN_CTAS)
         {
             // count each pair once, in the first window
             if (W.table && nW == cs1 - cs0)
-                n_fma += warp_products<SAFE, false>(S, W, A, B, a0, a1, r0, r1, w0 == cs0, ent, enta);
+                n_fma += warp_products<SAFE, false, ACC>(S, W, A, B, a0, a1, r0, r1, w0 == cs0, ent, enta);
             else
-                n_fma += warp_products<SAFE, true>(S, W, A, B, a0, a1, r0, r1, w0 == cs0, ent, enta);
+                n_fma += warp_products<SAFE, true, ACC>(S, W, A, B, a0, a1, r0, r1, w0 == cs0, ent, enta);
         }
         __syncthreads();
 
@@ -441,8 +446,7 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
         return RTT_OK;
     if (cfg.ev_begin != nullptr)
         RTT_CUDA(cudaEventRecord(cfg.ev_begin, s));
-    const size_t smem = sizeof(FlatSmem);
-    auto launch = [&](auto kern) -> int {
+    auto launch = [&](auto kern, size_t smem) -> int {
         RTT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<S.tilem, F_THREADS, smem, s>>>(
             A, B, S.tilem, S.nnz, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(),
@@ -452,10 +456,14 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
             cfg.csr_col, cfg.csr_val, cfg.counters, ws.err.as<int>());
         return RTT_OK;
     };
+    const bool large = S.max_tr_nnz > ACC_SMALL;
+    const size_t sm_small = sizeof(FlatSmem<ACC_SMALL>), sm_large = sizeof(FlatSmem<ACC_LARGE>);
     if (cfg.conflict_safe)
-        RTT_CHECK(launch(k_numeric_flat<true>));
+        RTT_CHECK(large ? launch(k_numeric_flat<true, ACC_LARGE, CTAS_LARGE>, sm_large)
+                        : launch(k_numeric_flat<true, ACC_SMALL, CTAS_SMALL>, sm_small));
     else
-        RTT_CHECK(launch(k_numeric_flat<false>));
+        RTT_CHECK(large ? launch(k_numeric_flat<false, ACC_LARGE, CTAS_LARGE>, sm_large)
+                        : launch(k_numeric_flat<false, ACC_SMALL, CTAS_SMALL>, sm_small));
     ws.launches++;
     if (cfg.ev_end != nullptr)
         RTT_CUDA(cudaEventRecord(cfg.ev_end, s));

@@ -178,9 +178,13 @@ def banded_scatter(n: int, half_bw: int, p: float = 0.5, scatter_max: int = 4,
     ns = rng.integers(0, scatter_max + 1, size=n)
     srow = np.repeat(np.arange(n, dtype=np.int64), ns)
     scol = rng.integers(0, n, size=srow.shape[0])
-    rows = np.concatenate([rows, srow])
-    cols = np.concatenate([cols, scol])
-    key = np.unique(rows * n + cols)
+    # band keys are already sorted (row-major, offsets ascending): merge in the
+    # few sorted scattered keys and drop repeats instead of sorting everything
+    bkey = rows * n + cols
+    skey = np.sort(srow * n + scol)
+    key = np.insert(bkey, np.searchsorted(bkey, skey), skey)
+    if key.size:
+        key = key[np.concatenate([[True], key[1:] != key[:-1]])]
     r = key // n
     cnt = np.bincount(r, minlength=n)
     rp = np.zeros(n + 1, dtype=np.int64)

@@ -42,6 +42,7 @@ CASES = {
     "stencil27_12": lambda: G.stencil_27(12, 3),
     "rmat_12": lambda: G.rmat(12, 16, seed=1),
     "banded": lambda: G.banded_scatter(3000, 40, seed=9),
+    "banded_wide": lambda: G.banded_scatter(2000, 64, seed=5),  # tile rows > 2048 entries
     "unsorted": lambda: G.random_csr(300, 300, 0.02, seed=3, sort=False),
     "duplicates": lambda: G.random_csr(200, 200, 0.03, seed=4, duplicates=0.3),
     "dense": lambda: G.random_csr(96, 96, 0.85, seed=6),
