@@ -47,11 +47,11 @@ namespace
 constexpr int FW = 8;                       // warps per CTA
 constexpr int RPW = TD / FW;                // rows per warp
 constexpr int F_THREADS = FW * 32;
-// Two shapes of the kernel: 2048 accumulator slots at five CTAs per SM for
-// tile rows up to 2048 entries, 4608 slots at three CTAs per SM for wider
-// ones (a window of more entries than slots walks the tile row again).
+// 2048 accumulator slots at five CTAs per SM.  (A second shape with 4608
+// slots at three CTAs per SM, one window for tile rows up to 4608 entries,
+// measured slower on banded batches than this one with row windows: the
+// kernel lives on warps in flight.)
 constexpr int ACC_SMALL = 2048, CTAS_SMALL = 5;
-constexpr int ACC_LARGE = 4608, CTAS_LARGE = 3;
 constexpr int F_SLOT_CAP = 128;             // C tiles per window
 constexpr int F_CM_STRIDE = F_SLOT_CAP + 1; // row stride of cm: rows land in distinct banks
 constexpr int F_SPAN_CAP = 4096;            // tile-column span of the slot table
@@ -72,7 +72,8 @@ struct FlatSmem
     int rowacc0[TD + 1];
     int rowcsr0[TD];
     int rowrun[TD];
-    int win_nnz;
+    int paircnt[FW]; // entries of each warp's rows (row windows)
+    int rowwin, win_begin, win_end;
 };
 
 struct Window
@@ -185,44 +186,72 @@ __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Windo
                 if (count) // each pair once, in the first window
                     n_fma += len;
             }
-            ent[lane] = make_int4(fs, len, rq * F_CM_STRIDE, 0);
-            enta[lane] = a;
-            __syncwarp();
-            const int nb = min(32, total - q0);
-            for (int j = 0; j < nb; j += GROUP)
-            {
-                int4 ge[GROUP];
-                int gcol[GROUP];
-                double gb[GROUP];
-#pragma unroll
-                for (int u = 0; u < GROUP; ++u)
+            // items of at most 32 B entries: an entry whose B row is longer
+            // than a warp becomes one item per 32 entries of the row, so the
+            // loads of every item are issued ahead like any other
+            auto run_items = [&](int nb) {
+                for (int j = 0; j < nb; j += GROUP)
                 {
-                    ge[u] = ent[(j + u) & 31];
-                    if (j + u >= nb)
-                        ge[u].y = 0;
-                }
+                    int4 ge[GROUP];
+                    int gcol[GROUP];
+                    double gb[GROUP];
 #pragma unroll
-                for (int u = 0; u < GROUP; ++u)
-                {
-                    gcol[u] = 0;
-                    gb[u] = 0.0;
-                    if (lane < ge[u].y)
+                    for (int u = 0; u < GROUP; ++u)
                     {
-                        gcol[u] = __ldg(B.csr_col + ge[u].x + lane);
-                        gb[u] = __ldg(B.csr_val + ge[u].x + lane);
+                        ge[u] = ent[(j + u) & 31];
+                        if (j + u >= nb)
+                            ge[u].y = 0;
                     }
-                }
 #pragma unroll
-                for (int u = 0; u < GROUP; ++u)
+                    for (int u = 0; u < GROUP; ++u)
+                    {
+                        gcol[u] = 0;
+                        gb[u] = 0.0;
+                        if (lane < ge[u].y)
+                        {
+                            gcol[u] = __ldg(B.csr_col + ge[u].x + lane);
+                            gb[u] = __ldg(B.csr_val + ge[u].x + lane);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < GROUP; ++u)
+                        if (lane < ge[u].y)
+                            flat_add<SAFE, CHECK, ACC>(S, W, S.cm + ge[u].z, gcol[u],
+                                                       enta[(j + u) & 31], gb[u]);
+                }
+            };
+            if (!__any_sync(FULL, len > 32))
+            {
+                ent[lane] = make_int4(fs, len, rq * F_CM_STRIDE, 0);
+                enta[lane] = a;
+                __syncwarp();
+                run_items(min(32, total - q0));
+            }
+            else
+            {
+                const int nch = (len + 31) >> 5;
+                const int cincl = warp_incl_scan(nch);
+                const int ctotal = __shfl_sync(FULL, cincl, 31);
+                for (int i0 = 0; i0 < ctotal; i0 += 32)
                 {
-                    const double au = enta[(j + u) & 31];
-                    const uint32_t *cmr = S.cm + ge[u].z;
-                    if (lane < ge[u].y)
-                        flat_add<SAFE, CHECK, ACC>(S, W, cmr, gcol[u], au, gb[u]);
-                    if (ge[u].y > 32) // rows longer than a warp (uniform branch)
-                        for (int f = 32 + lane; f < ge[u].y; f += 32)
-                            flat_add<SAFE, CHECK, ACC>(S, W, cmr, __ldg(B.csr_col + ge[u].x + f), au,
-                                                  __ldg(B.csr_val + ge[u].x + f));
+                    const int qi = i0 + lane;
+                    int ow = 0;
+#pragma unroll
+                    for (int b = 16; b > 0; b >>= 1)
+                        if (__shfl_sync(FULL, cincl, ow + b - 1) <= qi)
+                            ow += b;
+                    ow = min(ow, 31);
+                    const int k = qi - (__shfl_sync(FULL, cincl, ow) - __shfl_sync(FULL, nch, ow));
+                    const int ofs = __shfl_sync(FULL, fs, ow), olen = __shfl_sync(FULL, len, ow);
+                    const int orq = __shfl_sync(FULL, rq, ow);
+                    const double oa = __shfl_sync(FULL, a, ow);
+                    __syncwarp(); // the previous items are consumed
+                    ent[lane] = qi < ctotal ? make_int4(ofs + 32 * k, min(32, olen - 32 * k),
+                                                        orq * F_CM_STRIDE, 0)
+                                            : make_int4(0, 0, 0, 0);
+                    enta[lane] = oa;
+                    __syncwarp();
+                    run_items(min(32, ctotal - i0));
                 }
             }
             __syncwarp(); // the next batch overwrites this warp's list
@@ -259,30 +288,75 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
     int4 *ent = S.ent[warp];
     double *enta = S.enta[warp];
 
+    // Row windows: a tile row with more entries than the accumulator holds,
+    // but few enough C tiles for one slot table, is processed in groups of
+    // warps (row pairs) whose entries fit - every product is computed once,
+    // warps outside the group wait, and the SM's other CTAs use the issue
+    // slots.  Otherwise (or for the tile output) windows of C tiles are used
+    // and the warps walk their A entries once per window.
+    // (window state lives in shared memory: registers are the kernel's limit)
+    if (tid == 0)
+    {
+        S.rowwin = 0;
+        S.win_begin = 0;
+        S.win_end = FW;
+    }
+    if (c_val == nullptr && csr_rowptr != nullptr && cs1 - cs0 <= F_SLOT_CAP &&
+        __ldg(c_tile_nnz + cs1) - __ldg(c_tile_nnz + cs0) > ACC)
+    {
+        if (tid < FW)
+        {
+            const int ra = min(tid * RPW, nrows), rb = min(tid * RPW + RPW, nrows);
+            S.paircnt[tid] = __ldg(csr_rowptr + I * TD + rb) - __ldg(csr_rowptr + I * TD + ra);
+        }
+        const int ok = __syncthreads_and(tid >= FW || S.paircnt[tid] <= ACC);
+        if (tid == 0)
+            S.rowwin = ok;
+    }
+    __syncthreads();
+
     for (int w0 = cs0; w0 < cs1;)
     {
-        // ---- window [w0, w1): longest run of <= F_SLOT_CAP tiles, <= F_ACC_CAP entries
-        const int base_nnz = __ldg(c_tile_nnz + w0);
-        bool ok = false;
-        if (tid < F_SLOT_CAP && w0 + tid < cs1)
-            ok = __ldg(c_tile_nnz + w0 + tid + 1) - base_nnz <= ACC;
-        const int nW = __syncthreads_count(ok);
-        if (nW == 0)
+        int nW;
+        if (S.rowwin)
         {
+            // ---- row window: warps [win_begin, win_end), all C tiles of the tile row
             if (tid == 0)
-                set_error(err, DERR_NUM_BOUNDS); // a C tile holds at most 256 entries
-            return;
+            {
+                const int wa = S.win_begin;
+                int e = wa + 1, sum = S.paircnt[wa];
+                while (e < FW && sum + S.paircnt[e] <= ACC)
+                    sum += S.paircnt[e++];
+                S.win_end = e;
+            }
+            __syncthreads();
+            nW = cs1 - cs0;
+        }
+        else
+        {
+            // ---- window [w0, w1): longest run of <= F_SLOT_CAP tiles, <= ACC entries
+            const int base_nnz = __ldg(c_tile_nnz + w0);
+            bool ok = false;
+            if (tid < F_SLOT_CAP && w0 + tid < cs1)
+                ok = __ldg(c_tile_nnz + w0 + tid + 1) - base_nnz <= ACC;
+            nW = __syncthreads_count(ok);
+            if (nW == 0)
+            {
+                if (tid == 0)
+                    set_error(err, DERR_NUM_BOUNDS); // a C tile holds at most 256 entries
+                return;
+            }
         }
         const int w1 = w0 + nW;
-        if (tid == 0)
-            S.win_nnz = __ldg(c_tile_nnz + w1) - base_nnz;
         {
             // two rows' masks per 32-bit word (c_mask rows are 32-byte aligned per tile)
             const uint32_t *src = reinterpret_cast<const uint32_t *>(c_mask + (size_t)w0 * TD);
             for (int i = tid; i < nW * (TD / 2); i += F_THREADS)
             {
-                const uint32_t v = __ldg(src + i);
                 const int s = i >> 3, r = (i & 7) * 2;
+                // rows outside the row window count as empty
+                const bool in = r / RPW >= S.win_begin && r / RPW < S.win_end;
+                const uint32_t v = in ? __ldg(src + i) : 0u;
                 S.cm[r * F_CM_STRIDE + s] = v & 0xFFFFu;
                 S.cm[(r + 1) * F_CM_STRIDE + s] = v >> 16;
             }
@@ -343,18 +417,20 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
         }
         if (tid < nrows && csr_rowptr != nullptr)
             S.rowcsr0[tid] = __ldg(csr_rowptr + I * TD + tid) + S.rowrun[tid];
-        for (int i = tid; i < S.win_nnz; i += F_THREADS)
+        __syncthreads(); // rowacc0 complete
+        for (int i = tid; i < S.rowacc0[TD]; i += F_THREADS)
             S.acc[i] = 0.0;
         __syncthreads();
 
         // ---- products: warp-private, no CTA barrier
-        if (r0 < nrows)
+        if (r0 < nrows && warp >= S.win_begin && warp < S.win_end)
         {
-            // count each pair once, in the first window
+            // each pair counted once: in the first tile window, in its row window
+            const bool count = S.rowwin || w0 == cs0;
             if (W.table && nW == cs1 - cs0)
-                n_fma += warp_products<SAFE, false, ACC>(S, W, A, B, a0, a1, r0, r1, w0 == cs0, ent, enta);
+                n_fma += warp_products<SAFE, false, ACC>(S, W, A, B, a0, a1, r0, r1, count, ent, enta);
             else
-                n_fma += warp_products<SAFE, true, ACC>(S, W, A, B, a0, a1, r0, r1, w0 == cs0, ent, enta);
+                n_fma += warp_products<SAFE, true, ACC>(S, W, A, B, a0, a1, r0, r1, count, ent, enta);
         }
         __syncthreads();
 
@@ -417,7 +493,17 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
         if (tid < TD)
             S.rowrun[tid] += S.rowtot[tid];
         __syncthreads();
-        w0 = w1;
+        if (S.rowwin)
+        {
+            if (S.win_end >= FW)
+                break;
+            __syncthreads(); // every thread has read win_end
+            if (tid == 0)
+                S.win_begin = S.win_end;
+            __syncthreads();
+        }
+        else
+            w0 = w1;
     }
     if (counters != nullptr)
     {
@@ -456,14 +542,11 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
             cfg.csr_col, cfg.csr_val, cfg.counters, ws.err.as<int>());
         return RTT_OK;
     };
-    const bool large = S.max_tr_nnz > ACC_SMALL;
-    const size_t sm_small = sizeof(FlatSmem<ACC_SMALL>), sm_large = sizeof(FlatSmem<ACC_LARGE>);
+    const size_t smem = sizeof(FlatSmem<ACC_SMALL>);
     if (cfg.conflict_safe)
-        RTT_CHECK(large ? launch(k_numeric_flat<true, ACC_LARGE, CTAS_LARGE>, sm_large)
-                        : launch(k_numeric_flat<true, ACC_SMALL, CTAS_SMALL>, sm_small));
+        RTT_CHECK(launch(k_numeric_flat<true, ACC_SMALL, CTAS_SMALL>, smem));
     else
-        RTT_CHECK(large ? launch(k_numeric_flat<false, ACC_LARGE, CTAS_LARGE>, sm_large)
-                        : launch(k_numeric_flat<false, ACC_SMALL, CTAS_SMALL>, sm_small));
+        RTT_CHECK(launch(k_numeric_flat<false, ACC_SMALL, CTAS_SMALL>, smem));
     ws.launches++;
     if (cfg.ev_end != nullptr)
         RTT_CUDA(cudaEventRecord(cfg.ev_end, s));

@@ -252,7 +252,6 @@ struct SymbolicOut
     DevBuf tile_cnt;    // numtile ints, nnz per C tile
     int numtile = 0;
     long long nnz = 0;
-    int max_tr_nnz = 0; // entries of the largest C tile row
     int tilem = 0, tilen = 0, m = 0, n = 0;
     void release();
     DevCTiles view();

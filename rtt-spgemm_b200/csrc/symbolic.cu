@@ -20,8 +20,6 @@
 // counts and the tile row total come out of the masks with popc.
 #include "rtt_internal.cuh"
 
-#include <cub/device/device_reduce.cuh>
-
 #include <climits>
 
 namespace rtt
@@ -481,20 +479,7 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
     long long *tr64 = S.c_rowptr.as<long long>();
     RTT_CHECK(scan_exclusive_i64(ws, S.c_tr_nnz.as<int>(), tr64, tilem));
     long long nnz = 0;
-    S.max_tr_nnz = 0;
-    if (tilem > 0)
-    {
-        // largest tile row (entries): the numeric step sizes its accumulator by it
-        size_t bytes = 0;
-        int *dmax = S.count_tmp.as<int>(); // step-1 counts are consumed by now
-        RTT_CUDA(cub::DeviceReduce::Max(nullptr, bytes, S.c_tr_nnz.as<int>(), dmax, tilem, s));
-        RTT_CHECK(ws.scan_tmp.ensure(bytes, s));
-        RTT_CUDA(cub::DeviceReduce::Max(ws.scan_tmp.p, bytes, S.c_tr_nnz.as<int>(), dmax, tilem, s));
-        RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 12, dmax, sizeof(int), cudaMemcpyDeviceToHost, s));
-    }
-    RTT_CHECK(read_i64(ws, tr64 + tilem, &nnz)); // syncs: the max has landed too
-    if (tilem > 0)
-        S.max_tr_nnz = ws.h_scalars[12];
+    RTT_CHECK(read_i64(ws, tr64 + tilem, &nnz));
     RTT_CHECK(check_device_error(ws, "symbolic step 2"));
     S.nnz = nnz;
     if (nnz > (long long)INT_MAX)
