@@ -392,6 +392,12 @@ RTT_API int rtt_spgemm_batched_symbolic(rtt_context ctx, int count, const rtt_cs
                                         const rtt_csr_view *B, long long *nnz_c,
                                         long long *nnz_total);
 
+/* Device CSR transpose (A^T of a device CSR view into caller-owned device
+ * arrays of A->cols + 1 and A->nnz entries; rows sorted).  The serving loop
+ * uses it to turn A*A^T requests into A*B instances of one batch. */
+RTT_API int rtt_csr_transpose(rtt_context ctx, const rtt_csr_view *A, int *t_row_ptr,
+                              int *t_col_idx, double *t_values);
+
 /* Writes the products of the last batched symbolic.  c_row_ptr: the
  * instances' row pointers one after another (instance i's A_i.rows + 1
  * entries, starting at 0, at offset sum_{j<i} (A_j.rows + 1)); c_col_idx /

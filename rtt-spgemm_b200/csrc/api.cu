@@ -1350,6 +1350,40 @@ int rtt_spgemm_batched_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, do
     return RTT_OK;
 }
 
+int rtt_csr_transpose(rtt_context c, const rtt_csr_view *A, int *t_row_ptr, int *t_col_idx,
+                      double *t_values)
+{
+    if (c == nullptr || A == nullptr || !view_ok(*A) || t_row_ptr == nullptr ||
+        (A->nnz > 0 && (t_col_idx == nullptr || t_values == nullptr)))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "csr_transpose: bad arguments");
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    Workspace &ws = c->ws;
+    cudaStream_t s = ws.stream;
+    // the transpose lands in the context's scratch, then in the caller's arrays
+    DevBuf trp, tci, tva;
+    int st = csr_transpose_device(ws, A->rows, A->cols, (int)A->nnz, A->row_ptr, A->col_idx,
+                                  A->values, trp, tci, tva);
+    if (st == RTT_OK)
+    {
+        cudaError_t e = cudaMemcpyAsync(t_row_ptr, trp.p, sizeof(int) * ((size_t)A->cols + 1),
+                                        cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess && A->nnz > 0)
+            e = cudaMemcpyAsync(t_col_idx, tci.p, sizeof(int) * (size_t)A->nnz,
+                                cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess && A->nnz > 0)
+            e = cudaMemcpyAsync(t_values, tva.p, sizeof(double) * (size_t)A->nnz,
+                                cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess)
+            st = rtt::cuda_fail(e, "csr_transpose copy");
+    }
+    trp.release();
+    tci.release();
+    tva.release();
+    return st;
+}
+
 int rtt_spgemm_tiles_view(rtt_context c, SMatrix *out)
 {
     if (c == nullptr || out == nullptr)

@@ -348,6 +348,20 @@ class Context:
         finally:
             self._borrowed = None
 
+    def transpose(self, a):
+        """A^T of a device CSR tuple, as a device CSR tuple (new tensors)."""
+        import torch
+
+        rows, cols, rp, ci, va = a
+        trp = torch.empty(cols + 1, dtype=torch.int32, device=rp.device)
+        tci = torch.empty(max(int(ci.numel()), 1), dtype=torch.int32, device=rp.device)
+        tva = torch.empty(max(int(ci.numel()), 1), dtype=torch.float64, device=rp.device)
+        v = self._view(*a)
+        check(lib().rtt_csr_transpose(self.handle, C.byref(v), C.c_void_p(trp.data_ptr()),
+                                      C.c_void_p(tci.data_ptr()), C.c_void_p(tva.data_ptr())))
+        n = int(ci.numel())
+        return (cols, rows, trp, tci[:n], tva[:n])
+
     def stats(self) -> dict:
         st = Stats()
         check(lib().rtt_context_get_stats(self.handle, C.byref(st)))

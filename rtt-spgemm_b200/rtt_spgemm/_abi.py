@@ -34,6 +34,7 @@ EXPORTS = [
     "rtt_spgemm_numeric", "rtt_spgemm_tiles_view", "rtt_spgemm_csr_host",
     "rtt_tile2csr_device_noalloc", "rtt_csr_to_hybrid_tiles", "rtt_hybrid_tiles_destroy",
     "rtt_plan_tail_queue", "rtt_spgemm_batched_symbolic", "rtt_spgemm_batched_numeric",
+    "rtt_csr_transpose",
 ]
 
 
@@ -171,6 +172,7 @@ def lib() -> C.CDLL:
     L.rtt_spgemm_batched_symbolic.argtypes = [C.c_void_p, C.c_int, P(CsrView), P(CsrView),
                                               P(C.c_longlong), P(C.c_longlong)]
     L.rtt_spgemm_batched_numeric.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.rtt_csr_transpose.argtypes = [C.c_void_p, P(CsrView), C.c_void_p, C.c_void_p, C.c_void_p]
     _LIB = L
     return L
 

@@ -1,0 +1,249 @@
+"""Serving loop: SpGEMM requests of different sizes, batched as they arrive.
+
+The north star's served form (the reference has none; it runs one product per
+process): requests C = A^2 or C = A*A^T arrive over time; whenever a worker is
+free it takes every request that has arrived and fits the device pool, and
+runs them as ONE batched product (rtt_spgemm_batched_symbolic / _numeric: one
+csr2tile, one symbolic and one numeric pass over the block diagonal of the
+batch).  Two workers, each with its own context and CUDA stream, keep two
+batches in flight, so requests that arrive while one batch is on the GPU are
+admitted into the next one as soon as a worker and pool memory free up, and
+the two batches' work overlaps on the device.
+
+Admission is bounded by memory: a request reserves, for the time its batch
+runs, its operands plus the exact upper bound of the symbolic phase for C
+(nnzCub entries of 12 bytes: C cannot have more entries than products) plus
+its row pointer, against a fixed pool.  Operands that a request marks with a
+reuse key stay resident on the device (with A^T for A*A^T requests) and are
+not copied again.
+
+Latency of a request = time its result is on the device minus its arrival.
+"""
+from __future__ import annotations
+
+import threading
+import time
+from collections import OrderedDict, deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import Context, spgemm_batched
+from .generators import CSR
+
+
+@dataclass
+class Request:
+    a: CSR                    # host CSR operand
+    op: str = "A2"            # "A2" (C = A*A) or "AAT" (C = A*A^T)
+    key: object = None        # reuse key: keep the device operands resident
+    arrival: float = 0.0      # seconds after the start of the run
+    done: float = -1.0
+    result: tuple = None      # device (rowptr, col, val) of C
+    bound: int = field(default=0, repr=False)
+
+
+def product_bound(a: CSR, op: str) -> int:
+    """Upper bound of C's bytes from the structure alone: nnz(C) <= nnzCub."""
+    if op == "A2":
+        cub = int(np.diff(a.rowptr).astype(np.int64)[a.col].sum())
+    else:  # A * A^T: row i's products = sum over k in A(i) of nnz(A^T row k) = colcount(k)
+        cc = np.bincount(a.col, minlength=a.n).astype(np.int64)
+        cub = int(cc[a.col].sum())
+    return 12 * cub + 4 * (a.m + 1)
+
+
+class Server:
+    def __init__(self, device: int = 0, pool_bytes: float = 120e9, max_batch: int = 512,
+                 workers: int = 2, config: dict | None = None, keep_results: bool = True):
+        import torch
+
+        self.torch = torch
+        self.device = torch.device("cuda", device)
+        self.pool = float(pool_bytes)
+        self.max_batch = max_batch
+        self.config = config
+        self.nworkers = workers
+        self.keep_results = keep_results
+        self.resident: OrderedDict = OrderedDict()
+        self.lock = threading.Lock()
+
+    # -- operands -------------------------------------------------------
+    def _upload(self, a: CSR, ctx: Context):
+        t = self.torch
+        d = self.device
+        va = (a.m, a.n, t.from_numpy(a.rowptr).to(d, non_blocking=True),
+              t.from_numpy(a.col).to(d, non_blocking=True),
+              t.from_numpy(a.val).to(d, non_blocking=True))
+        return va
+
+    def _operands(self, r: Request, ctx: Context):
+        with self.lock:
+            hit = self.resident.get(r.key) if r.key is not None else None
+            if hit is not None:
+                self.resident.move_to_end(r.key)
+        if hit is None:
+            a = self._upload(r.a, ctx)
+            at = ctx.transpose(a) if r.op == "AAT" else None
+            hit = (a, at)
+            if r.key is not None:
+                with self.lock:
+                    self.resident[r.key] = hit
+        a, at = hit
+        if r.op == "AAT" and at is None:
+            at = ctx.transpose(a)
+            with self.lock:
+                if r.key is not None:
+                    self.resident[r.key] = (a, at)
+        return a, (at if r.op == "AAT" else a)
+
+    # -- the loop ---------------------------------------------------------
+    def run(self, requests: list[Request]) -> dict:
+        """Serve requests (sorted by arrival) in real time; returns latency
+        percentiles and throughput."""
+        for r in requests:
+            r.bound = product_bound(r.a, r.op) + 12 * r.a.nnz + 4 * (r.a.m + 1)
+        pending = deque()
+        nxt = 0
+        reserved = [0.0]
+        done = [0]
+        cv = threading.Condition()
+        t0 = time.perf_counter()
+        n = len(requests)
+
+        def take_batch():
+            # called with cv held: admit arrived requests that fit the pool
+            nonlocal nxt
+            now = time.perf_counter() - t0
+            while nxt < n and requests[nxt].arrival <= now:
+                pending.append(requests[nxt])
+                nxt += 1
+            batch, need = [], 0.0
+            while pending and len(batch) < self.max_batch:
+                r = pending[0]
+                if batch and reserved[0] + need + r.bound > self.pool:
+                    break
+                if not batch and reserved[0] + r.bound > self.pool and reserved[0] > 0:
+                    break  # wait for memory to free up
+                batch.append(pending.popleft())
+                need += r.bound
+            reserved[0] += need
+            return batch, need
+
+        def worker():
+            torch = self.torch
+            torch.cuda.set_device(self.device)
+            stream = torch.cuda.Stream(device=self.device)
+            ctx = Context(self.device.index or 0, self.config)
+            ctx.set_stream(stream.cuda_stream)
+            with torch.cuda.stream(stream):
+                while True:
+                    with cv:
+                        batch, need = take_batch()
+                        while not batch:
+                            if nxt >= n and not pending:
+                                ctx.close()
+                                return
+                            wait = 0.0005
+                            if nxt < n and not pending:
+                                wait = max(0.0, requests[nxt].arrival - (time.perf_counter() - t0))
+                            cv.wait(timeout=min(wait, 0.01) if wait > 0 else 0.0005)
+                            batch, need = take_batch()
+                    As, Bs = [], []
+                    for r in batch:
+                        a, b = self._operands(r, ctx)
+                        As.append(a)
+                        Bs.append(b)
+                    outs = spgemm_batched(ctx, As, Bs)
+                    stream.synchronize()
+                    t = time.perf_counter() - t0
+                    for r, o in zip(batch, outs):
+                        r.done = t
+                        r.result = o if self.keep_results else None
+                    with cv:
+                        reserved[0] -= need
+                        done[0] += len(batch)
+                        cv.notify_all()
+
+        threads = [threading.Thread(target=worker) for _ in range(self.nworkers)]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+        span = max(r.done for r in requests) if requests else 0.0
+        return summarize(requests, span)
+
+
+def serve_plain(requests: list[Request], device: int = 0, config: dict | None = None) -> dict:
+    """The plain path under the same arrivals: one product per call, FIFO."""
+    import torch
+
+    dev = torch.device("cuda", device)
+    ctx = Context(device, config)
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    resident = {}
+    t0 = time.perf_counter()
+    for r in requests:
+        now = time.perf_counter() - t0
+        if r.arrival > now:
+            time.sleep(r.arrival - now)
+        a = resident.get(r.key) if r.key is not None else None
+        if a is None:
+            a = (r.a.m, r.a.n, torch.from_numpy(r.a.rowptr).to(dev),
+                 torch.from_numpy(r.a.col).to(dev), torch.from_numpy(r.a.val).to(dev))
+            if r.key is not None:
+                resident[r.key] = a
+        nnz, _ = ctx.symbolic(a, None, 1 if r.op == "AAT" else 0)
+        rp = torch.empty(r.a.m + 1, dtype=torch.int32, device=dev)
+        ci = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+        va = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
+        ctx.numeric(rp, ci, va)
+        stream.synchronize()
+        r.done = time.perf_counter() - t0
+        r.result = (rp, ci[:nnz], va[:nnz])
+    ctx.close()
+    return summarize(requests, max(r.done for r in requests) if requests else 0.0)
+
+
+def summarize(requests, span: float) -> dict:
+    lat = np.array([r.done - r.arrival for r in requests]) * 1e3
+    return {"requests": len(requests), "seconds": span,
+            "spgemms_per_s": len(requests) / span if span > 0 else 0.0,
+            "p50_ms": float(np.percentile(lat, 50)) if lat.size else 0.0,
+            "p99_ms": float(np.percentile(lat, 99)) if lat.size else 0.0}
+
+
+def poisson_requests(count: int, rate: float, n_lo: int, n_hi: int, reuse: float = 0.3,
+                     aat_share: float = 0.5, seed: int = 0) -> list[Request]:
+    """The served configuration's request stream: Poisson arrivals, mixed A^2 /
+    A*A^T, n log-uniform in [n_lo, n_hi], nnz/row 4..64 from the generators
+    (2-D / 3-D stencils, R-MAT, banded plus scatter); a share of requests
+    reuses an earlier request's A (its reuse key)."""
+    from . import generators as G
+
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=count))
+    reqs = []
+    for i in range(count):
+        if reqs and rng.random() < reuse:
+            j = int(rng.integers(0, len(reqs)))
+            src = reqs[j]
+            reqs.append(Request(src.a, src.op, src.key, float(t[i])))
+            continue
+        n = int(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi))))
+        kind = int(rng.integers(0, 4))
+        if kind == 0:
+            side = max(4, int(round(np.sqrt(n))))
+            a = G.laplacian_2d(side)
+        elif kind == 1:
+            side = max(3, int(round(n ** (1 / 3))))
+            a = G.stencil_27(side, int(rng.integers(0, 1 << 30)))
+        elif kind == 2:
+            scale = max(8, int(np.log2(n)))
+            a = G.rmat(scale, int(rng.integers(4, 17)), seed=int(rng.integers(0, 1 << 30)))
+        else:
+            a = G.banded_scatter(n, int(rng.integers(2, 32)), seed=int(rng.integers(0, 1 << 30)))
+        op = "AAT" if rng.random() < aat_share else "A2"
+        reqs.append(Request(a, op, ("req", i), float(t[i])))
+    return reqs

@@ -83,7 +83,7 @@ def test_bad_arguments_rejected_before_device_work():
     assert lib.rtt_tile2csr(C.byref(R.SMatrix()), 12, 1) == 1  # malformed / bad tile_dim
     cfg = R.Config()
     lib.rtt_config_default(C.byref(cfg))
-    assert cfg.dmma_pair_cutoff == 3072 and cfg.fused_csr_output == 1
+    assert cfg.dmma_pair_cutoff == 0 and cfg.fused_csr_output == 1  # DMMA opt-in
 
 
 def test_generators_shapes():
