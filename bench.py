@@ -38,6 +38,9 @@ WORKLOADS = {
     "stencil27_96_brick": "3-D 27-point stencil, 96^3 grid, 2x2x4 brick ordering, C = A^2",
     "laplacian2d_256": "2-D 5-point Laplacian, 256^2 grid (n=65,536), C = A^2",
     "stencil27_80": "3-D 27-point stencil, 80^3 grid (n=512,000), C = A^2 (profiling size)",
+    "served": "Poisson request stream (2,000 req/s) of mixed A^2 / A*A^T products, n log-uniform "
+              "in [4,096, n_max], 2-D/3-D stencils, R-MAT, banded+scatter, 30% reuse a resident A; "
+              "120 GB pool; served (batched as they arrive) vs plain one-call FIFO",
     "batched": "independent A_i^2: n_i log-uniform in [2,000, 200,000], banded (half-bandwidth "
                "8..64, band kept w.p. 0.5) + 0..4 random entries per row; batched form vs one "
                "call per product",
@@ -267,6 +270,37 @@ def run_batched(args) -> None:
     ctx.close()
 
 
+def run_served(args) -> None:
+    """Serving loop against the plain path under the same Poisson arrivals."""
+    import torch
+    from rtt_spgemm import serve
+
+    torch.cuda.set_device(0)
+    # warm both paths up on a short stream of small requests
+    warm = serve.poisson_requests(16, 2000.0, 256, 4096, seed=args.seed + 7)
+    serve.Server(keep_results=False).run(warm)
+    serve.serve_plain(serve.poisson_requests(16, 2000.0, 256, 4096, seed=args.seed + 7))
+    mk = lambda: serve.poisson_requests(args.serve_count, 2000.0, 4096, args.serve_nmax,
+                                        reuse=0.3, seed=args.seed)
+    reqs = mk()
+    served = serve.Server(pool_bytes=120e9, keep_results=False).run(reqs)
+    plain_reqs = mk()
+    plain = serve.serve_plain(plain_reqs)
+    for r in plain_reqs:
+        r.result = None
+    line = {
+        "metric": "SpGEMMs/s (served)", "value": served["spgemms_per_s"], "unit": "SpGEMMs/s",
+        "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": served["seconds"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generators, Poisson arrivals)",
+        "config": {"workload": "served", "description": WORKLOADS["served"],
+                   "requests": len(reqs), "n_max": args.serve_nmax, "rate_per_s": 2000.0},
+        "served": served, "plain": plain,
+        "served_over_plain": served["spgemms_per_s"] / max(plain["spgemms_per_s"], 1e-9),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args) -> None:
     import torch
     import rtt_spgemm as R
@@ -423,6 +457,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--batch-count", type=int, default=128)
+    ap.add_argument("--serve-count", type=int, default=200)
+    ap.add_argument("--serve-nmax", type=int, default=262144)
     ap.add_argument("--wave-rows", type=int, default=4_000_000)
     ap.add_argument("--staging", action="store_true",
                     help="TMA-staged numeric kernel instead of the default flat one")
@@ -434,6 +470,8 @@ def main() -> None:
         run_reference(args)
     elif args.workload == "batched":
         run_batched(args)
+    elif args.workload == "served":
+        run_served(args)
     else:
         run_ours(args)
 
