@@ -316,8 +316,16 @@ typedef struct
      * streamed by TMA bulk copies through a shared-memory stage ring (the
      * kernel that also runs the DMMA pairs). */
     int b_staging;
+    /* Early split of heavy C tile rows.  A tile row that needs several
+     * windows of C tiles walks all its products once per window; when that
+     * walk exceeds split_target products the row is cut into tasks of
+     * consecutive windows of about split_target products each, which
+     * persistent CTAs take from a device queue.  0 = the default (2^20);
+     * negative = never split (each tile row's CTA runs its windows in
+     * sequence).  Every setting gives bitwise the same C. */
+    int split_target;
     /* Reserved, must be zero. */
-    int reserved[6];
+    int reserved[5];
 } rtt_config;
 
 RTT_API void rtt_config_default(rtt_config *config);
@@ -342,6 +350,10 @@ typedef struct
     double csr2tile_ms;
     double symbolic_ms;
     double numeric_kernel_ms;
+    /* Window tasks of the last numeric step: C tile rows that need several
+     * windows of C tiles are cut into windows that persistent CTAs take from
+     * a device queue (the early split of src/dmma_tile_early_split.h). */
+    long long split_windows;
 } rtt_stats;
 
 /* A context owns a CUDA stream handle (borrowed), workspace and the state

@@ -797,6 +797,7 @@ int rtt_spgemm_tile(SMatrix *A, SMatrix *B, SMatrix *C)
     nc.write_tiles = true;
     nc.conflict_safe = true; // caller tiles may repeat a coordinate
     nc.b_staging = c->cfg.b_staging != 0;
+    nc.split_target = c->cfg.split_target;
     RTT_CHECK(numeric_select_device(c->ws, dA, dB, c->S, nc));
     RTT_CHECK(check_device_error(c->ws, "spgemm_tile numeric"));
     cudaStream_t s = c->ws.stream;
@@ -1142,6 +1143,7 @@ int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_
     RTT_CHECK(effective_cutoff(c, c->A.view(), TB.view(), &nc.dmma_pair_cutoff));
     nc.counters = c->counters.as<long long>();
     nc.b_staging = c->cfg.b_staging != 0;
+    nc.split_target = c->cfg.split_target;
     if (c->cfg.stage_timing)
     {
         nc.ev_begin = ws.ev[3];
@@ -1172,7 +1174,7 @@ int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_
                                        S.tilem, TD, nullptr, -1, c_row_ptr, c_col_idx, c_values,
                                        false));
     }
-    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars64 + 2, c->counters.p, sizeof(long long) * 2,
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars64 + 2, c->counters.p, sizeof(long long) * 3,
                              cudaMemcpyDeviceToHost, ws.stream));
     RTT_CHECK(check_device_error(ws, "numeric"));
     if (c->cfg.stage_timing && c->S.numtile > 0)
@@ -1186,6 +1188,7 @@ int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_
     // the numeric kernels count every (a_ik, b_kj) pair once: sum over A
     // entries of nnz(B(k, :)), the reference's nnzCub
     c->stats.nnz_cub = ws.h_scalars64[3];
+    c->stats.split_windows = ws.h_scalars64[4];
     c->stats.kernel_launches = ws.launches;
     c->stats.host_syncs = ws.syncs;
     return RTT_OK;

@@ -51,8 +51,8 @@ constexpr int F_THREADS = FW * 32;
 // slots at three CTAs per SM, one window for tile rows up to 4608 entries,
 // measured slower on banded batches than this one with row windows: the
 // kernel lives on warps in flight.)
-constexpr int ACC_SMALL = 2048, CTAS_SMALL = 5;
-constexpr int F_SLOT_CAP = 128;             // C tiles per window
+constexpr int ACC_SMALL = FLAT_ACC, CTAS_SMALL = 5;
+constexpr int F_SLOT_CAP = FLAT_SLOT_CAP;   // C tiles per window
 constexpr int F_CM_STRIDE = F_SLOT_CAP + 1; // row stride of cm: rows land in distinct banks
 constexpr int F_SPAN_CAP = 4096;            // tile-column span of the slot table
 constexpr int GROUP = 2;                    // B rows loaded together
@@ -74,6 +74,7 @@ struct FlatSmem
     int rowrun[TD];
     int paircnt[FW]; // entries of each warp's rows (row windows)
     int rowwin, win_begin, win_end;
+    int task;        // window task taken from the queue (split tile rows)
 };
 
 struct Window
@@ -130,7 +131,7 @@ __device__ __forceinline__ void flat_add(FlatSmem<ACC> &S, const Window &W, cons
 
 // The warp's products for one window: every A entry (r, k) of its rows r0, r1
 // times B's row k.  Returns the number of products when count is set.
-template <bool SAFE, bool CHECK, int ACC>
+template <bool SAFE, bool CHECK, int ACC, bool NARROW>
 __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Window &W, const DevTiles &A,
                                                    const DevTiles &B, int a0, int a1, int r0,
                                                    int r1, bool count, int4 *ent, double *enta)
@@ -185,6 +186,15 @@ __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Windo
                 }
                 if (count) // each pair once, in the first window
                     n_fma += len;
+                // one window of several: a long sorted B row contributes only
+                // its columns inside the window's tile-column range
+                if (NARROW && CHECK && !SAFE && len > 32)
+                {
+                    const int lo = W.Jlo * TD, hi = (W.Jlo + W.Jspan + 1) * TD;
+                    const int sb = lower_bound(B.csr_col, fs, fs + len, lo);
+                    len = lower_bound(B.csr_col, sb, fs + len, hi) - sb;
+                    fs = sb;
+                }
             }
             // items of at most 32 B entries: an entry whose B row is longer
             // than a warp becomes one item per 32 entries of the row, so the
@@ -260,7 +270,225 @@ __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Windo
     return n_fma;
 }
 
-template <bool SAFE, int ACC, int MIN_CTAS>
+// ---------------------------------------------------------------------------
+// Split execution of heavy tile rows (the early split of the reference's
+// numeric step, src/dmma_tile_early_split.h:152-229, applied to C tile rows).
+//
+// A tile row is heavy when its C tiles need more than one window (more than
+// F_SLOT_CAP tiles, or more than ACC entries that row windows cannot divide).
+// One CTA would walk its A entries once per window, one window after another,
+// and become the tail of the launch (an R-MAT hub row has hundreds of
+// windows).  Instead k_win_plan cuts every heavy tile row into windows up
+// front and queues them as tasks; the first CTAs of the numeric launch are
+// persistent workers that take tasks from the queue, and the CTA of a heavy
+// tile row itself exits.  Each task knows, for each of its rows, how many
+// entries the row has in the tiles before the window, so it writes its part
+// of C's CSR without waiting for the other windows.  Every output entry is
+// still summed by one warp in the fixed (K, k) order: bitwise the same result.
+struct WinTask
+{
+    int I, w0, w1, pad; // tile row, C tiles [w0, w1)
+    int run[TD];        // per row: entries in the tile row's tiles before w0
+};
+static_assert(sizeof(WinTask) == 80, "task record layout");
+
+struct WinQueue
+{
+    int count;    // tasks written by the plan
+    int head;     // next task to take
+    int overflow; // some heavy tile row found no room and kept its own CTA
+    int pad;
+};
+
+constexpr int PLAN_WARPS = 8;
+// Products walked by one window task (about a millisecond of one CTA): tile
+// rows whose windows together walk fewer are not split.
+constexpr long long SPLIT_TARGET = 1ll << 20;
+
+// Window starts of a heavy tile row, chosen so that the tiles can be cut
+// independently: tile t starts a window when t is the row's first tile, when
+// t - cs0 is a multiple of F_SLOT_CAP, or when the entries before t cross a
+// multiple of H = ACC - 256.  A window then holds <= F_SLOT_CAP tiles and
+// fewer than H entries before its last tile, which adds at most 256.
+template <int ACC>
+__device__ __forceinline__ bool win_cut(const int *c_tile_nnz, int cs0, int cs1, int P0, int t)
+{
+    constexpr int H = ACC - 256;
+    if (t >= cs1)
+        return false;
+    if (t == cs0 || (t - cs0) % F_SLOT_CAP == 0)
+        return true;
+    return (__ldg(c_tile_nnz + t) - P0) / H != (__ldg(c_tile_nnz + t - 1) - P0) / H;
+}
+
+// One warp per C tile row: decide heavy or not, and queue the windows of a
+// heavy one.  heavy[I] = 1 tells the numeric kernel's CTA for I to exit.
+template <int ACC>
+__global__ void __launch_bounds__(PLAN_WARPS * 32)
+    k_win_plan(int tilem, int m, DevTiles A, DevTiles B,
+               const int *__restrict__ c_tile_ptr, const int *__restrict__ c_tile_nnz,
+               const uint16_t *__restrict__ c_mask, const int *__restrict__ csr_rowptr,
+               uint8_t *__restrict__ heavy, WinTask *__restrict__ tasks, int cap,
+               long long target, WinQueue *q, long long *counters)
+{
+    const int lane = lane_id();
+    const int I = blockIdx.x * PLAN_WARPS + (threadIdx.x >> 5);
+    if (I >= tilem)
+        return;
+    const int cs0 = __ldg(c_tile_ptr + I), cs1 = __ldg(c_tile_ptr + I + 1);
+    const int a0 = __ldg(A.tile_ptr + I), a1 = __ldg(A.tile_ptr + I + 1);
+    bool multi = false;
+    if (cs1 > cs0 && a0 < a1)
+    {
+        const int E = __ldg(c_tile_nnz + cs1) - __ldg(c_tile_nnz + cs0);
+        multi = cs1 - cs0 > F_SLOT_CAP || E > ACC;
+        if (multi && cs1 - cs0 <= F_SLOT_CAP && csr_rowptr != nullptr)
+        {
+            // the numeric kernel's row windows: every warp's rows fit
+            const int nrows = min(TD, m - I * TD);
+            int pc = 0;
+            if (lane < FW)
+            {
+                const int ra = min(lane * RPW, nrows), rb = min(lane * RPW + RPW, nrows);
+                pc = __ldg(csr_rowptr + I * TD + rb) - __ldg(csr_rowptr + I * TD + ra);
+            }
+            multi = __any_sync(FULL, pc > ACC);
+        }
+    }
+    if (!multi)
+    {
+        if (lane == 0)
+            heavy[I] = 0;
+        return;
+    }
+    const int P0 = __ldg(c_tile_nnz + cs0);
+    int nwin = 0;
+    for (int t0 = cs0; t0 < cs1; t0 += 32)
+        nwin += __popc(__ballot_sync(FULL, win_cut<ACC>(c_tile_nnz, cs0, cs1, P0, t0 + lane)));
+    // Cost of one window: the tile row's products, since every window walks
+    // all of them (the cost model of the reference's tail queue, products
+    // standing in for its scan/match terms).  A task takes g consecutive
+    // windows, about SPLIT_TARGET products of walking; a row whose windows all
+    // fit one task keeps its own CTA and the L1 reuse of its B rows.
+    long long P = 0;
+    for (int t = a0 + lane; t < a1; t += 32)
+    {
+        const int e0 = __ldg(A.tile_nnz + t), e1 = __ldg(A.tile_nnz + t + 1);
+        const int K = __ldg(A.tile_col + t);
+        for (int e = e0; e < e1; ++e)
+        {
+            const int k = K * TD + (A.col[e] & 15);
+            if (k < B.m)
+                P += __ldg(B.csr_rowptr + k + 1) - __ldg(B.csr_rowptr + k);
+        }
+    }
+    P = warp_sum(P);
+    const int g = (int)max(1ll, min((long long)nwin, target / max(P, 1ll)));
+    const int ntask = (nwin + g - 1) / g;
+    int base = -1;
+    if (ntask >= 2 && lane == 0)
+    {
+        // room for all the tasks, or none at all (then the row keeps its own CTA)
+        int old = *(volatile int *)&q->count;
+        for (int it = 0; it < (1 << 20); ++it)
+        {
+            if (old + ntask > cap)
+                break;
+            const int seen = atomicCAS(&q->count, old, old + ntask);
+            if (seen == old)
+            {
+                base = old;
+                break;
+            }
+            old = seen;
+        }
+        if (base < 0)
+            q->overflow = 1;
+        else if (counters != nullptr)
+            atomicAdd((unsigned long long *)&counters[2], (unsigned long long)ntask);
+    }
+    base = __shfl_sync(FULL, base, 0);
+    if (lane == 0)
+        heavy[I] = base >= 0;
+    if (base < 0)
+        return;
+    // the tasks: window bounds and the rows' entries before each window
+    int run[TD];
+#pragma unroll
+    for (int r = 0; r < TD; ++r)
+        run[r] = 0;
+    int widx = base, nw = 0; // tasks written, windows seen
+    for (int t0 = cs0; t0 < cs1; t0 += 32)
+    {
+        const int t = t0 + lane;
+        const bool cut = win_cut<ACC>(c_tile_nnz, cs0, cs1, P0, t);
+        const unsigned wbal = __ballot_sync(FULL, cut);
+        // a task starts at every g-th window
+        const bool start = cut && (nw + __popc(wbal & ((1u << lane) - 1u))) % g == 0;
+        nw += __popc(wbal);
+        uint32_t w[TD / 2];
+        if (t < cs1)
+        {
+            const uint4 *mp = reinterpret_cast<const uint4 *>(c_mask + (size_t)t * TD);
+            const uint4 u0 = __ldg(mp), u1 = __ldg(mp + 1);
+            w[0] = u0.x, w[1] = u0.y, w[2] = u0.z, w[3] = u0.w;
+            w[4] = u1.x, w[5] = u1.y, w[6] = u1.z, w[7] = u1.w;
+        }
+        else
+        {
+#pragma unroll
+            for (int p = 0; p < TD / 2; ++p)
+                w[p] = 0u;
+        }
+        // per row pair: two 16-bit counts in one word (a chunk adds <= 512)
+        int excl[TD / 2], tot[TD / 2];
+#pragma unroll
+        for (int p = 0; p < TD / 2; ++p)
+        {
+            const int pc = __popc(w[p] & 0xFFFFu) | (__popc(w[p] >> 16) << 16);
+            const int incl = warp_incl_scan(pc);
+            excl[p] = incl - pc;
+            tot[p] = __shfl_sync(FULL, incl, 31);
+        }
+        const unsigned bal = __ballot_sync(FULL, start);
+        if (start)
+        {
+            WinTask *tk = tasks + widx + __popc(bal & ((1u << lane) - 1u));
+            tk->I = I;
+            tk->w0 = t;
+            tk->pad = 0;
+            const unsigned later = lane == 31 ? 0u : bal & (0xFFFFFFFFu << (lane + 1));
+            if (later) // the task ends at the next start in this chunk
+                tk->w1 = t0 + __ffs(later) - 1;
+#pragma unroll
+            for (int p = 0; p < TD / 2; ++p)
+            {
+                tk->run[2 * p] = run[2 * p] + (excl[p] & 0xFFFF);
+                tk->run[2 * p + 1] = run[2 * p + 1] + (excl[p] >> 16);
+            }
+        }
+        // the last task of the chunks before ends at this chunk's first start
+        if (bal != 0u && widx > base && lane == __ffs(bal) - 1)
+            tasks[widx - 1].w1 = t;
+        widx += __popc(bal);
+#pragma unroll
+        for (int p = 0; p < TD / 2; ++p)
+        {
+            run[2 * p] += tot[p] & 0xFFFF;
+            run[2 * p + 1] += tot[p] >> 16;
+        }
+    }
+    if (lane == 0)
+        tasks[widx - 1].w1 = cs1;
+}
+
+// WORKER: the persistent CTAs that take window tasks from the queue (launched
+// on a second stream, ahead of the tile-row CTAs); otherwise one CTA per C
+// tile row, which exits if its row was split.  NARROW: some tile row has
+// several windows, so long sorted B rows are cut to each window's columns
+// (compiled out when every tile row fits one window: the registers are the
+// kernel's limit).
+template <bool SAFE, int ACC, int MIN_CTAS, bool WORKER, bool NARROW>
 __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
     k_numeric_flat(DevTiles A, DevTiles B, int tilem, long long nnzC,
                    const int *__restrict__ c_tile_ptr, const int *__restrict__ c_tile_col,
@@ -268,242 +496,277 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
                    uint8_t *__restrict__ c_ptr, uint8_t *__restrict__ c_colb,
                    double *__restrict__ c_val, const int *__restrict__ csr_rowptr,
                    int *__restrict__ csr_col, double *__restrict__ csr_val, long long *counters,
-                   int *err)
+                   int *err, const uint8_t *__restrict__ heavy, const WinTask *__restrict__ tasks,
+                   WinQueue *q)
 {
     extern __shared__ __align__(128) unsigned char dyn[];
     FlatSmem<ACC> &S = *reinterpret_cast<FlatSmem<ACC> *>(dyn);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int I = blockIdx.x;
-    if (I >= tilem)
-        return;
-    const int a0 = __ldg(A.tile_ptr + I), a1 = __ldg(A.tile_ptr + I + 1);
-    const int cs0 = __ldg(c_tile_ptr + I), cs1 = __ldg(c_tile_ptr + I + 1);
-    if (cs0 == cs1 || a0 == a1)
-        return; // no C tiles in this tile row (uniform)
-    if (tid < TD)
-        S.rowrun[tid] = 0;
-    const int nrows = min(TD, A.m - I * TD);
     const int r0 = warp * RPW, r1 = r0 + RPW - 1;
     long long n_fma = 0;
     int4 *ent = S.ent[warp];
     double *enta = S.enta[warp];
-
-    // Row windows: a tile row with more entries than the accumulator holds,
-    // but few enough C tiles for one slot table, is processed in groups of
-    // warps (row pairs) whose entries fit - every product is computed once,
-    // warps outside the group wait, and the SM's other CTAs use the issue
-    // slots.  Otherwise (or for the tile output) windows of C tiles are used
-    // and the warps walk their A entries once per window.
-    // (window state lives in shared memory: registers are the kernel's limit)
-    if (tid == 0)
+    constexpr bool worker = WORKER;
+    for (;;)
     {
-        S.rowwin = 0;
-        S.win_begin = 0;
-        S.win_end = FW;
-    }
-    if (c_val == nullptr && csr_rowptr != nullptr && cs1 - cs0 <= F_SLOT_CAP &&
-        __ldg(c_tile_nnz + cs1) - __ldg(c_tile_nnz + cs0) > ACC)
-    {
-        if (tid < FW)
+        int I, wbeg = 0, wend = 0;
+        if (worker)
         {
-            const int ra = min(tid * RPW, nrows), rb = min(tid * RPW + RPW, nrows);
-            S.paircnt[tid] = __ldg(csr_rowptr + I * TD + rb) - __ldg(csr_rowptr + I * TD + ra);
-        }
-        const int ok = __syncthreads_and(tid >= FW || S.paircnt[tid] <= ACC);
-        if (tid == 0)
-            S.rowwin = ok;
-    }
-    __syncthreads();
-
-    for (int w0 = cs0; w0 < cs1;)
-    {
-        int nW;
-        if (S.rowwin)
-        {
-            // ---- row window: warps [win_begin, win_end), all C tiles of the tile row
+            __syncthreads(); // the previous task is done with shared memory
             if (tid == 0)
-            {
-                const int wa = S.win_begin;
-                int e = wa + 1, sum = S.paircnt[wa];
-                while (e < FW && sum + S.paircnt[e] <= ACC)
-                    sum += S.paircnt[e++];
-                S.win_end = e;
-            }
+                S.task = atomicAdd(&q->head, 1);
             __syncthreads();
-            nW = cs1 - cs0;
-        }
-        else
-        {
-            // ---- window [w0, w1): longest run of <= F_SLOT_CAP tiles, <= ACC entries
-            const int base_nnz = __ldg(c_tile_nnz + w0);
-            bool ok = false;
-            if (tid < F_SLOT_CAP && w0 + tid < cs1)
-                ok = __ldg(c_tile_nnz + w0 + tid + 1) - base_nnz <= ACC;
-            nW = __syncthreads_count(ok);
-            if (nW == 0)
-            {
-                if (tid == 0)
-                    set_error(err, DERR_NUM_BOUNDS); // a C tile holds at most 256 entries
-                return;
-            }
-        }
-        const int w1 = w0 + nW;
-        {
-            // two rows' masks per 32-bit word (c_mask rows are 32-byte aligned per tile)
-            const uint32_t *src = reinterpret_cast<const uint32_t *>(c_mask + (size_t)w0 * TD);
-            for (int i = tid; i < nW * (TD / 2); i += F_THREADS)
-            {
-                const int s = i >> 3, r = (i & 7) * 2;
-                // rows outside the row window count as empty
-                const bool in = r / RPW >= S.win_begin && r / RPW < S.win_end;
-                const uint32_t v = in ? __ldg(src + i) : 0u;
-                S.cm[r * F_CM_STRIDE + s] = v & 0xFFFFu;
-                S.cm[(r + 1) * F_CM_STRIDE + s] = v >> 16;
-            }
-        }
-        for (int i = tid; i < nW; i += F_THREADS)
-            S.cJ[i] = __ldg(c_tile_col + w0 + i);
-        {
-            // the slot table covers the window's tile-column span only
-            const int span = __ldg(c_tile_col + w1 - 1) - __ldg(c_tile_col + w0) + 1;
-            for (int i = tid; i < min((span + 3) / 4, F_SPAN_CAP / 4); i += F_THREADS)
-                reinterpret_cast<uint32_t *>(S.slot8)[i] = 0xFFFFFFFFu;
-        }
-        __syncthreads();
-        Window W;
-        W.Jlo = S.cJ[0];
-        W.Jspan = S.cJ[nW - 1] - W.Jlo;
-        W.nW = nW;
-        W.table = W.Jspan < F_SPAN_CAP;
-        if (W.table)
-            for (int i = tid; i < nW; i += F_THREADS)
-                S.slot8[S.cJ[i] - W.Jlo] = (uint8_t)i;
-        // accumulator bases: (row r, slot s) starts at the entries of rows < r
-        // plus those of row r in slots < s.  Thread (r = tid / 16, part =
-        // tid % 16) owns a run of slots: sum, half-warp scan, write.
-        {
-            static_assert(F_THREADS == TD * 16, "one half-warp per row");
-            const int r = tid >> 4, part = tid & 15;
-            const int per = (nW + 15) >> 4;
-            const int s0 = min(part * per, nW), s1 = min(s0 + per, nW);
-            uint32_t *cmr = S.cm + r * F_CM_STRIDE;
-            int sum = 0;
-            for (int s = s0; s < s1; ++s)
-                sum += __popc(cmr[s]);
-            const int incl = half_incl_scan(sum);
-            if (part == 15)
-                S.rowtot[r] = incl;
-            __syncthreads();
-            int racc = 0; // entries of rows < r
-            for (int q = 0; q < r; ++q)
-                racc += S.rowtot[q];
-            if (tid == 0)
-            {
-                int t = 0;
-                for (int q = 0; q < TD; ++q)
-                {
-                    S.rowacc0[q] = t;
-                    t += S.rowtot[q];
-                }
-                S.rowacc0[TD] = t;
-            }
-            int run = racc + incl - sum;
-            for (int s = s0; s < s1; ++s)
-            {
-                const uint32_t m = cmr[s];
-                cmr[s] = ((uint32_t)run << 16) | m;
-                run += __popc(m);
-            }
-        }
-        if (tid < nrows && csr_rowptr != nullptr)
-            S.rowcsr0[tid] = __ldg(csr_rowptr + I * TD + tid) + S.rowrun[tid];
-        __syncthreads(); // rowacc0 complete
-        for (int i = tid; i < S.rowacc0[TD]; i += F_THREADS)
-            S.acc[i] = 0.0;
-        __syncthreads();
-
-        // ---- products: warp-private, no CTA barrier
-        if (r0 < nrows && warp >= S.win_begin && warp < S.win_end)
-        {
-            // each pair counted once: in the first tile window, in its row window
-            const bool count = S.rowwin || w0 == cs0;
-            if (W.table && nW == cs1 - cs0)
-                n_fma += warp_products<SAFE, false, ACC>(S, W, A, B, a0, a1, r0, r1, count, ent, enta);
-            else
-                n_fma += warp_products<SAFE, true, ACC>(S, W, A, B, a0, a1, r0, r1, count, ent, enta);
-        }
-        __syncthreads();
-
-        // ---- write-out of the window: each warp its own rows
-        if (csr_col != nullptr)
-        {
-#pragma unroll
-            for (int rr = 0; rr < RPW; ++rr)
-            {
-                const int r = r0 + rr;
-                if (r >= nrows)
-                    break;
-                const int b0 = S.rowacc0[r], b1 = S.rowacc0[r + 1];
-                const long long dst = (long long)S.rowcsr0[r] - b0;
-                if (dst + b1 > nnzC)
-                {
-                    if (lane == 0)
-                        set_error(err, DERR_NUM_BOUNDS);
-                    continue;
-                }
-                for (int p = b0 + lane; p < b1; p += 32)
-                {
-                    csr_val[dst + p] = S.acc[p];
-                    csr_col[dst + p] = S.ccol[p];
-                }
-            }
-        }
-        if (c_val != nullptr)
-        {
-            for (int it = tid; it < nW * TD; it += F_THREADS)
-            {
-                const int s = it >> 4, r = it & 15;
-                const uint32_t w = S.cm[r * F_CM_STRIDE + s];
-                const uint32_t m = w & 0xFFFFu;
-                const int abase = (int)(w >> 16);
-                const int t = w0 + s;
-                int pre = 0;
-                for (int rr = 0; rr < r; ++rr)
-                    pre += __popc(S.cm[rr * F_CM_STRIDE + s] & 0xFFFFu);
-                c_ptr[(size_t)t * TD + r] = (uint8_t)pre;
-                const long long tpos = (long long)__ldg(c_tile_nnz + t) + pre;
-                uint32_t mm = m;
-                int k = 0;
-                while (mm)
-                {
-                    const int c = __clz(mm) - 16;
-                    mm &= ~(0x8000u >> c);
-                    if (tpos + k >= nnzC)
-                    {
-                        set_error(err, DERR_NUM_BOUNDS);
-                        break;
-                    }
-                    c_colb[tpos + k] = (uint8_t)c;
-                    c_val[tpos + k] = S.acc[abase + k];
-                    ++k;
-                }
-            }
-        }
-        __syncthreads();
-        if (tid < TD)
-            S.rowrun[tid] += S.rowtot[tid];
-        __syncthreads();
-        if (S.rowwin)
-        {
-            if (S.win_end >= FW)
+            const int tk = S.task;
+            if (tk >= __ldg(&q->count))
                 break;
-            __syncthreads(); // every thread has read win_end
-            if (tid == 0)
-                S.win_begin = S.win_end;
-            __syncthreads();
+            I = __ldg(&tasks[tk].I);
+            wbeg = __ldg(&tasks[tk].w0);
+            wend = __ldg(&tasks[tk].w1);
+            if (tid < TD)
+                S.rowrun[tid] = __ldg(&tasks[tk].run[tid]);
+            if (I < 0 || I >= tilem)
+                break; // not a task of this product (uniform)
         }
         else
-            w0 = w1;
+        {
+            I = blockIdx.x;
+            if (I >= tilem || (heavy != nullptr && heavy[I]))
+                break;
+        }
+        const int a0 = __ldg(A.tile_ptr + I), a1 = __ldg(A.tile_ptr + I + 1);
+        const int cs0 = __ldg(c_tile_ptr + I), cs1 = __ldg(c_tile_ptr + I + 1);
+        if (cs0 == cs1 || a0 == a1)
+            break; // no C tiles in this tile row (uniform)
+        if (!worker)
+        {
+            wbeg = cs0;
+            wend = cs1;
+            if (tid < TD)
+                S.rowrun[tid] = 0;
+        }
+        else if (wbeg < cs0 || wend > cs1)
+            break;
+        const int nrows = min(TD, A.m - I * TD);
+
+        // Row windows: a tile row with more entries than the accumulator holds,
+        // but few enough C tiles for one slot table, is processed in groups of
+        // warps (row pairs) whose entries fit - every product is computed once,
+        // warps outside the group wait, and the SM's other CTAs use the issue
+        // slots.  Otherwise (or for the tile output) windows of C tiles are used
+        // and the warps walk their A entries once per window.
+        // (window state lives in shared memory: registers are the kernel's limit)
+        if (tid == 0)
+        {
+            S.rowwin = 0;
+            S.win_begin = 0;
+            S.win_end = FW;
+        }
+        if (!worker && c_val == nullptr && csr_rowptr != nullptr && cs1 - cs0 <= F_SLOT_CAP &&
+            __ldg(c_tile_nnz + cs1) - __ldg(c_tile_nnz + cs0) > ACC)
+        {
+            if (tid < FW)
+            {
+                const int ra = min(tid * RPW, nrows), rb = min(tid * RPW + RPW, nrows);
+                S.paircnt[tid] = __ldg(csr_rowptr + I * TD + rb) - __ldg(csr_rowptr + I * TD + ra);
+            }
+            const int ok = __syncthreads_and(tid >= FW || S.paircnt[tid] <= ACC);
+            if (tid == 0)
+                S.rowwin = ok;
+        }
+        __syncthreads();
+
+        for (int w0 = wbeg; w0 < wend;)
+        {
+            int nW;
+            if (S.rowwin)
+            {
+                // ---- row window: warps [win_begin, win_end), all C tiles of the tile row
+                if (tid == 0)
+                {
+                    const int wa = S.win_begin;
+                    int e = wa + 1, sum = S.paircnt[wa];
+                    while (e < FW && sum + S.paircnt[e] <= ACC)
+                        sum += S.paircnt[e++];
+                    S.win_end = e;
+                }
+                __syncthreads();
+                nW = cs1 - cs0;
+            }
+            else
+            {
+                // ---- window [w0, w1): longest run of <= F_SLOT_CAP tiles, <= ACC entries
+                const int base_nnz = __ldg(c_tile_nnz + w0);
+                bool ok = false;
+                if (tid < F_SLOT_CAP && w0 + tid < wend)
+                    ok = __ldg(c_tile_nnz + w0 + tid + 1) - base_nnz <= ACC;
+                nW = __syncthreads_count(ok);
+                if (nW == 0)
+                {
+                    if (tid == 0)
+                        set_error(err, DERR_NUM_BOUNDS); // a C tile holds at most 256 entries
+                    return;
+                }
+            }
+            const int w1 = w0 + nW;
+            {
+                // two rows' masks per 32-bit word (c_mask rows are 32-byte aligned per tile)
+                const uint32_t *src = reinterpret_cast<const uint32_t *>(c_mask + (size_t)w0 * TD);
+                for (int i = tid; i < nW * (TD / 2); i += F_THREADS)
+                {
+                    const int s = i >> 3, r = (i & 7) * 2;
+                    // rows outside the row window count as empty
+                    const bool in = r / RPW >= S.win_begin && r / RPW < S.win_end;
+                    const uint32_t v = in ? __ldg(src + i) : 0u;
+                    S.cm[r * F_CM_STRIDE + s] = v & 0xFFFFu;
+                    S.cm[(r + 1) * F_CM_STRIDE + s] = v >> 16;
+                }
+            }
+            for (int i = tid; i < nW; i += F_THREADS)
+                S.cJ[i] = __ldg(c_tile_col + w0 + i);
+            {
+                // the slot table covers the window's tile-column span only
+                const int span = __ldg(c_tile_col + w1 - 1) - __ldg(c_tile_col + w0) + 1;
+                for (int i = tid; i < min((span + 3) / 4, F_SPAN_CAP / 4); i += F_THREADS)
+                    reinterpret_cast<uint32_t *>(S.slot8)[i] = 0xFFFFFFFFu;
+            }
+            __syncthreads();
+            Window W;
+            W.Jlo = S.cJ[0];
+            W.Jspan = S.cJ[nW - 1] - W.Jlo;
+            W.nW = nW;
+            W.table = W.Jspan < F_SPAN_CAP;
+            if (W.table)
+                for (int i = tid; i < nW; i += F_THREADS)
+                    S.slot8[S.cJ[i] - W.Jlo] = (uint8_t)i;
+            // accumulator bases: (row r, slot s) starts at the entries of rows < r
+            // plus those of row r in slots < s.  Thread (r = tid / 16, part =
+            // tid % 16) owns a run of slots: sum, half-warp scan, write.
+            {
+                static_assert(F_THREADS == TD * 16, "one half-warp per row");
+                const int r = tid >> 4, part = tid & 15;
+                const int per = (nW + 15) >> 4;
+                const int s0 = min(part * per, nW), s1 = min(s0 + per, nW);
+                uint32_t *cmr = S.cm + r * F_CM_STRIDE;
+                int sum = 0;
+                for (int s = s0; s < s1; ++s)
+                    sum += __popc(cmr[s]);
+                const int incl = half_incl_scan(sum);
+                if (part == 15)
+                    S.rowtot[r] = incl;
+                __syncthreads();
+                int racc = 0; // entries of rows < r
+                for (int q = 0; q < r; ++q)
+                    racc += S.rowtot[q];
+                if (tid == 0)
+                {
+                    int t = 0;
+                    for (int q = 0; q < TD; ++q)
+                    {
+                        S.rowacc0[q] = t;
+                        t += S.rowtot[q];
+                    }
+                    S.rowacc0[TD] = t;
+                }
+                int run = racc + incl - sum;
+                for (int s = s0; s < s1; ++s)
+                {
+                    const uint32_t m = cmr[s];
+                    cmr[s] = ((uint32_t)run << 16) | m;
+                    run += __popc(m);
+                }
+            }
+            if (tid < nrows && csr_rowptr != nullptr)
+                S.rowcsr0[tid] = __ldg(csr_rowptr + I * TD + tid) + S.rowrun[tid];
+            __syncthreads(); // rowacc0 complete
+            for (int i = tid; i < S.rowacc0[TD]; i += F_THREADS)
+                S.acc[i] = 0.0;
+            __syncthreads();
+
+            // ---- products: warp-private, no CTA barrier
+            if (r0 < nrows && warp >= S.win_begin && warp < S.win_end)
+            {
+                // each pair counted once: in the first tile window, in its row window
+                const bool count = S.rowwin || w0 == cs0;
+                if (W.table && nW == cs1 - cs0)
+                    n_fma += warp_products<SAFE, false, ACC, NARROW>(S, W, A, B, a0, a1, r0, r1, count, ent, enta);
+                else
+                    n_fma += warp_products<SAFE, true, ACC, NARROW>(S, W, A, B, a0, a1, r0, r1, count, ent, enta);
+            }
+            __syncthreads();
+
+            // ---- write-out of the window: each warp its own rows
+            if (csr_col != nullptr)
+            {
+#pragma unroll
+                for (int rr = 0; rr < RPW; ++rr)
+                {
+                    const int r = r0 + rr;
+                    if (r >= nrows)
+                        break;
+                    const int b0 = S.rowacc0[r], b1 = S.rowacc0[r + 1];
+                    const long long dst = (long long)S.rowcsr0[r] - b0;
+                    if (dst + b1 > nnzC)
+                    {
+                        if (lane == 0)
+                            set_error(err, DERR_NUM_BOUNDS);
+                        continue;
+                    }
+                    for (int p = b0 + lane; p < b1; p += 32)
+                    {
+                        csr_val[dst + p] = S.acc[p];
+                        csr_col[dst + p] = S.ccol[p];
+                    }
+                }
+            }
+            if (c_val != nullptr)
+            {
+                for (int it = tid; it < nW * TD; it += F_THREADS)
+                {
+                    const int s = it >> 4, r = it & 15;
+                    const uint32_t w = S.cm[r * F_CM_STRIDE + s];
+                    const uint32_t m = w & 0xFFFFu;
+                    const int abase = (int)(w >> 16);
+                    const int t = w0 + s;
+                    int pre = 0;
+                    for (int rr = 0; rr < r; ++rr)
+                        pre += __popc(S.cm[rr * F_CM_STRIDE + s] & 0xFFFFu);
+                    c_ptr[(size_t)t * TD + r] = (uint8_t)pre;
+                    const long long tpos = (long long)__ldg(c_tile_nnz + t) + pre;
+                    uint32_t mm = m;
+                    int k = 0;
+                    while (mm)
+                    {
+                        const int c = __clz(mm) - 16;
+                        mm &= ~(0x8000u >> c);
+                        if (tpos + k >= nnzC)
+                        {
+                            set_error(err, DERR_NUM_BOUNDS);
+                            break;
+                        }
+                        c_colb[tpos + k] = (uint8_t)c;
+                        c_val[tpos + k] = S.acc[abase + k];
+                        ++k;
+                    }
+                }
+            }
+            __syncthreads();
+            if (tid < TD)
+                S.rowrun[tid] += S.rowtot[tid];
+            __syncthreads();
+            if (S.rowwin)
+            {
+                if (S.win_end >= FW)
+                    break;
+                __syncthreads(); // every thread has read win_end
+                if (tid == 0)
+                    S.win_begin = S.win_end;
+                __syncthreads();
+            }
+            else
+                w0 = w1;
+        }
+        if (!worker)
+            break;
     }
     if (counters != nullptr)
     {
@@ -530,24 +793,68 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
         RTT_CHECK(csr_rowptr_device(ws, S, cfg.csr_rowptr));
     if (S.numtile == 0 || S.tilem == 0)
         return RTT_OK;
+    // window tasks of heavy tile rows: at most one per F_SLOT_CAP tiles, plus
+    // two per ACC - 256 entries (a cut on the entry count), plus one per row
+    const long long cap_ll = (long long)S.tilem + S.numtile / F_SLOT_CAP +
+                             2 * S.nnz / (ACC_SMALL - 256) + 16;
+    const int cap = (int)std::min<long long>(cap_ll, 1 << 26);
+    RTT_CHECK(S.w_task.ensure(sizeof(WinTask) * (size_t)cap, s));
+    RTT_CHECK(S.w_heavy.ensure((size_t)S.tilem + 16, s));
+    RTT_CHECK(S.w_queue.ensure(sizeof(WinQueue), s));
     if (cfg.ev_begin != nullptr)
         RTT_CUDA(cudaEventRecord(cfg.ev_begin, s));
-    auto launch = [&](auto kern, size_t smem) -> int {
+    const int *fused_rowptr = cfg.csr_col ? cfg.csr_rowptr : nullptr;
+    // split and narrowing only matter when some tile row has several windows
+    const bool split = cfg.split_target >= 0 && S.multi_window;
+    const long long target = cfg.split_target > 0 ? cfg.split_target : SPLIT_TARGET;
+    if (split)
+    {
+        RTT_CUDA(cudaMemsetAsync(S.w_queue.p, 0, sizeof(WinQueue), s));
+        k_win_plan<ACC_SMALL><<<(S.tilem + PLAN_WARPS - 1) / PLAN_WARPS, PLAN_WARPS * 32, 0, s>>>(
+            S.tilem, S.m, A, B, S.c_tile_ptr.as<int>(), S.c_tile_nnz.as<int>(),
+            S.c_mask.as<uint16_t>(), fused_rowptr, S.w_heavy.as<uint8_t>(),
+            S.w_task.as<WinTask>(), cap, target, S.w_queue.as<WinQueue>(), cfg.counters);
+        ws.launches++;
+    }
+    auto launch = [&](auto kern, int grid, cudaStream_t st, size_t smem) -> int {
         RTT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<S.tilem, F_THREADS, smem, s>>>(
+        kern<<<grid, F_THREADS, smem, st>>>(
             A, B, S.tilem, S.nnz, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(),
             S.c_mask.as<uint16_t>(), S.c_tile_nnz.as<int>(), S.c_ptr.as<uint8_t>(),
             cfg.write_tiles ? S.c_col.as<uint8_t>() : nullptr,
-            cfg.write_tiles ? S.c_val.as<double>() : nullptr, cfg.csr_col ? cfg.csr_rowptr : nullptr,
-            cfg.csr_col, cfg.csr_val, cfg.counters, ws.err.as<int>());
+            cfg.write_tiles ? S.c_val.as<double>() : nullptr, fused_rowptr, cfg.csr_col,
+            cfg.csr_val, cfg.counters, ws.err.as<int>(),
+            split ? S.w_heavy.as<uint8_t>() : nullptr, S.w_task.as<WinTask>(),
+            S.w_queue.as<WinQueue>());
+        ws.launches++;
         return RTT_OK;
     };
     const size_t smem = sizeof(FlatSmem<ACC_SMALL>);
-    if (cfg.conflict_safe)
-        RTT_CHECK(launch(k_numeric_flat<true, ACC_SMALL, CTAS_SMALL>, smem));
-    else
-        RTT_CHECK(launch(k_numeric_flat<false, ACC_SMALL, CTAS_SMALL>, smem));
-    ws.launches++;
+    if (split)
+    {
+        // The workers go first, on the side stream, so that the split rows'
+        // tasks start while the tile-row CTAs run (the reference's heavy grid
+        // enqueued before its light grid, src/dmma_tile_early_split.h:13-27).
+        // One wave of resident CTAs; with an empty queue they exit at once.
+        auto wk = cfg.conflict_safe ? k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, true, true>
+                                    : k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, true, true>;
+        int per_sm = 0, sms = 0;
+        RTT_CUDA(cudaFuncSetAttribute(wk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        RTT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk, F_THREADS, smem));
+        RTT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws.device));
+        RTT_CUDA(cudaEventRecord(ws.fork_ev, s));
+        RTT_CUDA(cudaStreamWaitEvent(ws.side, ws.fork_ev, 0));
+        RTT_CHECK(launch(wk, std::max(1, per_sm * sms), ws.side, smem));
+        RTT_CUDA(cudaEventRecord(ws.join_ev, ws.side));
+    }
+    auto light = cfg.conflict_safe
+                     ? (S.multi_window ? k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, false, true>
+                                       : k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, false, false>)
+                     : (S.multi_window ? k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, true>
+                                       : k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, false>);
+    RTT_CHECK(launch(light, S.tilem, s, smem));
+    if (split)
+        RTT_CUDA(cudaStreamWaitEvent(s, ws.join_ev, 0));
     if (cfg.ev_end != nullptr)
         RTT_CUDA(cudaEventRecord(cfg.ev_end, s));
     return RTT_OK;

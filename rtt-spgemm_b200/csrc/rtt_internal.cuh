@@ -205,6 +205,10 @@ struct Workspace
     int launches = 0;
     int syncs = 0;
     cudaEvent_t ev[6] = {};  // stage timing events (recorded on stream)
+    // second stream for work that overlaps the main one (forked and joined
+    // with the two events inside one call)
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     int init(int dev);
     void destroy();
 };
@@ -242,6 +246,11 @@ int tiles_to_col_major(Workspace &ws, const TileBufs &rowmajor, TileBufs &out);
 int csr_transpose_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
                          const double *val, DevBuf &t_rowptr, DevBuf &t_col, DevBuf &t_val);
 
+// Accumulator slots and C tiles per window of the flat numeric kernel (the
+// symbolic step flags tile rows beyond either).
+constexpr int FLAT_ACC = 2048;
+constexpr int FLAT_SLOT_CAP = 128;
+
 struct SymbolicOut
 {
     DevBuf c_tile_ptr, c_tile_col, c_tile_row, c_tile_nnz, c_mask, c_ptr, c_col, c_val;
@@ -250,6 +259,11 @@ struct SymbolicOut
     DevBuf c_tr_nnz;    // tilem ints, nnz per C tile row
     DevBuf count_tmp;   // tilem + 1 ints
     DevBuf tile_cnt;    // numtile ints, nnz per C tile
+    // numeric split of heavy tile rows: window tasks, per-tile-row flag, queue
+    DevBuf w_task, w_heavy, w_queue, w_flag;
+    // some C tile row needs more than one window of the flat numeric kernel
+    // (set by the symbolic step; true when unknown)
+    bool multi_window = true;
     int numtile = 0;
     long long nnz = 0;
     int tilem = 0, tilen = 0, m = 0, n = 0;
@@ -263,11 +277,12 @@ struct NumericConfig
 {
     int dmma_pair_cutoff = 3072;
     bool b_staging = true;          // TMA staging of B tile rows in the numeric step
+    int split_target = 0;           // products per window task (0 = default, < 0 = no split)
     bool write_tiles = true;
     int *csr_rowptr = nullptr;  // fused CSR output when csr_col != nullptr
     int *csr_col = nullptr;
     double *csr_val = nullptr;
-    long long *counters = nullptr; // device [0] dmma pairs, [1] sparse pairs
+    long long *counters = nullptr; // device [0] dmma pairs, [1] sparse pairs, [2] split windows
     cudaEvent_t ev_begin = nullptr; // recorded around the numeric kernel when set
     cudaEvent_t ev_end = nullptr;
     bool conflict_safe = false;     // B rows may repeat a column: accumulate with shared atomics

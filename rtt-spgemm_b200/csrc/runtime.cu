@@ -100,6 +100,11 @@ int Workspace::init(int dev)
     for (cudaEvent_t &e : ev)
         if (e == nullptr)
             RTT_CUDA(cudaEventCreate(&e));
+    if (side == nullptr)
+        RTT_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    for (cudaEvent_t *e : {&fork_ev, &join_ev})
+        if (*e == nullptr)
+            RTT_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     return RTT_OK;
 }
 
@@ -119,6 +124,15 @@ void Workspace::destroy()
             cudaEventDestroy(e);
             e = nullptr;
         }
+    for (cudaEvent_t *e : {&fork_ev, &join_ev})
+        if (*e != nullptr)
+        {
+            cudaEventDestroy(*e);
+            *e = nullptr;
+        }
+    if (side != nullptr)
+        cudaStreamDestroy(side);
+    side = nullptr;
 }
 
 namespace
@@ -235,7 +249,7 @@ void SymbolicOut::release()
 {
     DevBuf *all[] = {&c_tile_ptr, &c_tile_col, &c_tile_row, &c_tile_nnz, &c_mask, &c_ptr,
                      &c_col, &c_val, &c_row_cnt, &c_rowptr, &c_tr_nnz, &count_tmp,
-                     &tile_cnt};
+                     &tile_cnt, &w_task, &w_heavy, &w_queue, &w_flag};
     for (DevBuf *b : all)
         b->release();
 }

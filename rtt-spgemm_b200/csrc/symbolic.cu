@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
     k_sym_rows(DevTiles A, DevTiles B, const int *__restrict__ c_tile_ptr,
                int *__restrict__ c_tile_col, int *__restrict__ c_tile_row,
                uint16_t *__restrict__ c_mask, int *__restrict__ c_tile_cnt,
-               int *__restrict__ c_row_cnt, int *__restrict__ c_tr_nnz, int *err)
+               int *__restrict__ c_row_cnt, int *__restrict__ c_tr_nnz, int *multi, int *err)
 {
     __shared__ CtaSmem2 S;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -429,7 +429,12 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
         atomicAdd(&tot, run0 + run1);
     __syncthreads();
     if (tid == 0)
+    {
         c_tr_nnz[I] = tot;
+        // the numeric step needs more than one window of C tiles here
+        if (cend - cbeg > FLAT_SLOT_CAP || tot > FLAT_ACC)
+            atomicOr(multi, 1);
+    }
 }
 
 } // namespace
@@ -467,14 +472,19 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
     RTT_CHECK(S.c_rowptr.ensure(sizeof(long long) * (size_t)(tilem + 1), s));
     RTT_CHECK(S.c_tr_nnz.ensure(sizeof(int) * (size_t)(tilem + 1), s));
     RTT_CHECK(S.tile_cnt.ensure(sizeof(int) * (nt + 1), s));
+    RTT_CHECK(S.w_flag.ensure(sizeof(int), s));
+    RTT_CUDA(cudaMemsetAsync(S.w_flag.p, 0, sizeof(int), s));
     if (tilem > 0)
     {
         k_sym_rows<<<tilem, S2_THREADS, 0, s>>>(
             A, B, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(), S.c_tile_row.as<int>(),
             S.c_mask.as<uint16_t>(), S.tile_cnt.as<int>(), S.c_row_cnt.as<int>(),
-            S.c_tr_nnz.as<int>(), ws.err.as<int>());
+            S.c_tr_nnz.as<int>(), S.w_flag.as<int>(), ws.err.as<int>());
         ws.launches++;
     }
+    // read with nnz(C) below (one synchronisation for both)
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 12, S.w_flag.p, sizeof(int), cudaMemcpyDeviceToHost,
+                             s));
     // exact sizes: nnz(C) as int64 over tile rows first (int32 overflow check)
     long long *tr64 = S.c_rowptr.as<long long>();
     RTT_CHECK(scan_exclusive_i64(ws, S.c_tr_nnz.as<int>(), tr64, tilem));
@@ -482,6 +492,7 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
     RTT_CHECK(read_i64(ws, tr64 + tilem, &nnz));
     RTT_CHECK(check_device_error(ws, "symbolic step 2"));
     S.nnz = nnz;
+    S.multi_window = ws.h_scalars[12] != 0;
     if (nnz > (long long)INT_MAX)
         return fail(RTT_ERR_UNREPRESENTABLE, "nnz(C) = " + std::to_string(nnz) +
                                                  " exceeds the int32 offsets of SMatrix / CSR");

@@ -114,6 +114,45 @@ def test_wide_and_crowded_tile_rows(orc):
     ctx.close()
 
 
+# C tile rows with more tiles than one slot window (banded plus scatter,
+# R-MAT hubs, unsorted random rows): several windows per tile row
+MANY_WINDOW_CASES = {
+    "banded": CASES["banded"],
+    "rmat_12": CASES["rmat_12"],
+    "banded_20k": lambda: G.banded_scatter(20000, 24, seed=11),
+    "unsorted_wide": lambda: G.random_csr(3000, 3000, 0.01, seed=12, sort=False),
+}
+
+
+@pytest.mark.parametrize("case", list(MANY_WINDOW_CASES))
+def test_many_window_rows_fused_equals_tiles(case, orc):
+    """C written as CSR directly by the numeric kernel or as tiles converted by
+    tile2csr, with heavy tile rows split into window tasks or not: every entry
+    is summed in the same order, so all four are bitwise equal, and they match
+    the oracle."""
+    A = MANY_WINDOW_CASES[case]()
+    runs = {}
+    for name, cfg in (("fused", dict(fused_csr_output=1)), ("tiled", dict(fused_csr_output=0)),
+                      ("fused_split1", dict(fused_csr_output=1, split_target=1)),
+                      ("tiled_split1", dict(fused_csr_output=0, split_target=1)),
+                      ("fused_split64k", dict(fused_csr_output=1, split_target=1 << 16)),
+                      ("fused_nosplit", dict(fused_csr_output=1, split_target=-1))):
+        ctx = R.Context(0, cfg)
+        runs[name] = _run(ctx, A)
+        # split_target 1: every multi-window row becomes one task per window
+        if "split1" in name:
+            assert ctx.stats()["split_windows"] > 0, name
+        if "nosplit" in name:
+            assert ctx.stats()["split_windows"] == 0, name
+        ctx.close()
+    fused = runs["fused"]
+    for name, other in runs.items():
+        assert np.array_equal(fused[0], other[0]) and np.array_equal(fused[1], other[1]), name
+        assert np.array_equal(fused[2].view(np.int64), other[2].view(np.int64)), name
+    erp, ecol, evals, eabs = orc.spgemm_csr(A, A)
+    assert_csr_close(fused[0], fused[1], fused[2], erp, ecol, evals, eabs, f"{case}: ")
+
+
 def test_deterministic_and_reusable(orc):
     """Two runs on one context give bitwise-identical values (no atomics in
     the value accumulation), and the context can switch problems."""
