@@ -1100,7 +1100,7 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
     dB.csr_col = c->b_ci;
     dB.csr_val = c->b_va;
     dB.nnz = (int)c->b_nnz;
-    RTT_CHECK(map_device_error(symbolic_device(ws, c->A.view(), dB, c->S)));
+    RTT_CHECK(map_device_error(symbolic_device(ws, c->A.view(), dB, c->S, !c->b_dups)));
     if (timing)
     {
         float t01 = 0.f, t12 = 0.f;

@@ -271,7 +271,10 @@ struct SymbolicOut
     DevCTiles view();
 };
 
-int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S);
+// b_sorted: B's CSR rows have strictly increasing columns (lets the walk of a
+// wide tile row's windows cut long B rows to each window)
+int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
+                    bool b_sorted = false);
 
 struct NumericConfig
 {

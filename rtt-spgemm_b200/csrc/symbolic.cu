@@ -117,7 +117,8 @@ __device__ __forceinline__ void fill_bitmap(const DevTiles &A, const DevTiles &B
     }
 }
 
-__global__ void __launch_bounds__(SYM_WARPS * 32) k_sym_count(DevTiles A, DevTiles B, int *cnt)
+__global__ void __launch_bounds__(SYM_WARPS * 32)
+    k_sym_count(DevTiles A, DevTiles B, int *cnt, int *multi)
 {
     __shared__ WarpSmem1 sm[SYM_WARPS];
     const int lane = lane_id(), wi = threadIdx.x >> 5;
@@ -148,11 +149,20 @@ __global__ void __launch_bounds__(SYM_WARPS * 32) k_sym_count(DevTiles A, DevTil
         }
     }
     if (lane == 0)
+    {
         cnt[I] = count;
+        // step 2 will need more than one window for this tile row
+        if (count > S2_SLOTS || (hi >= 0 && (long long)hi - lo + 1 > WBITS))
+            atomicOr(multi, 1);
+    }
 }
 
 // Step 2.  Outputs per C tile: column, tile row, 16 row masks and entry
-// count; per scalar row: entry count; per tile row: entry total.
+// count; per scalar row: entry count; per tile row: entry total.  NARROW:
+// some tile row has several windows and B's rows are sorted, so long B rows
+// are cut to each window's columns (compiled out otherwise: it costs the
+// single-window walk registers and issue slots).
+template <bool NARROW>
 __global__ void __launch_bounds__(S2_THREADS, 5)
     k_sym_rows(DevTiles A, DevTiles B, const int *__restrict__ c_tile_ptr,
                int *__restrict__ c_tile_col, int *__restrict__ c_tile_row,
@@ -262,6 +272,8 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
         const int nb = S.nb;
         wend = S.wend;
         const int wlen = wend - w;
+        // one window of several: long sorted B rows are cut to its columns
+        const bool narrow = NARROW && (w > lo || wend <= hi);
         if (cbase + nb > cend)
         {
             if (tid == 0)
@@ -338,6 +350,12 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
                         {
                             fs = min(max(__ldg(B.csr_rowptr + k), 0), B.nnz);
                             len = min(max(__ldg(B.csr_rowptr + k + 1), fs), B.nnz) - fs;
+                        }
+                        if (narrow && len > 32)
+                        {
+                            const int sb = lower_bound(B.csr_col, fs, fs + len, w * TD);
+                            len = lower_bound(B.csr_col, sb, fs + len, wend * TD) - sb;
+                            fs = sb;
                         }
                     }
                     ent[lane] = make_int4(fs, len, sh, 0);
@@ -439,7 +457,8 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
 
 } // namespace
 
-int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S)
+int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
+                    bool b_sorted)
 {
     cudaStream_t s = ws.stream;
     if (A.n != B.m)
@@ -452,14 +471,22 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
     RTT_CHECK(S.count_tmp.ensure(sizeof(int) * (size_t)(tilem + 1), s));
     RTT_CHECK(S.c_tile_ptr.ensure(sizeof(int) * (size_t)(tilem + 1), s));
     int *cnt = S.count_tmp.as<int>();
+    // flags: [0] some tile row needs several step-2 windows, [1] several
+    // numeric windows
+    RTT_CHECK(S.w_flag.ensure(sizeof(int) * 2, s));
+    RTT_CUDA(cudaMemsetAsync(S.w_flag.p, 0, sizeof(int) * 2, s));
     if (tilem > 0)
     {
-        k_sym_count<<<ceil_div(tilem, SYM_WARPS), SYM_WARPS * 32, 0, s>>>(A, B, cnt);
+        k_sym_count<<<ceil_div(tilem, SYM_WARPS), SYM_WARPS * 32, 0, s>>>(A, B, cnt,
+                                                                          S.w_flag.as<int>());
         ws.launches++;
     }
     RTT_CHECK(scan_exclusive_int(ws, cnt, S.c_tile_ptr.as<int>(), tilem));
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 13, S.w_flag.p, sizeof(int), cudaMemcpyDeviceToHost,
+                             s));
     int numtile = 0;
     RTT_CHECK(read_int(ws, S.c_tile_ptr.as<int>() + tilem, &numtile));
+    const bool sym_multi = ws.h_scalars[13] != 0;
     RTT_CHECK(check_device_error(ws, "symbolic step 1"));
     S.numtile = numtile;
     const size_t nt = (size_t)numtile;
@@ -472,19 +499,18 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
     RTT_CHECK(S.c_rowptr.ensure(sizeof(long long) * (size_t)(tilem + 1), s));
     RTT_CHECK(S.c_tr_nnz.ensure(sizeof(int) * (size_t)(tilem + 1), s));
     RTT_CHECK(S.tile_cnt.ensure(sizeof(int) * (nt + 1), s));
-    RTT_CHECK(S.w_flag.ensure(sizeof(int), s));
-    RTT_CUDA(cudaMemsetAsync(S.w_flag.p, 0, sizeof(int), s));
     if (tilem > 0)
     {
-        k_sym_rows<<<tilem, S2_THREADS, 0, s>>>(
+        auto kern = b_sorted && sym_multi ? k_sym_rows<true> : k_sym_rows<false>;
+        kern<<<tilem, S2_THREADS, 0, s>>>(
             A, B, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(), S.c_tile_row.as<int>(),
             S.c_mask.as<uint16_t>(), S.tile_cnt.as<int>(), S.c_row_cnt.as<int>(),
-            S.c_tr_nnz.as<int>(), S.w_flag.as<int>(), ws.err.as<int>());
+            S.c_tr_nnz.as<int>(), S.w_flag.as<int>() + 1, ws.err.as<int>());
         ws.launches++;
     }
     // read with nnz(C) below (one synchronisation for both)
-    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 12, S.w_flag.p, sizeof(int), cudaMemcpyDeviceToHost,
-                             s));
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 12, S.w_flag.as<int>() + 1, sizeof(int),
+                             cudaMemcpyDeviceToHost, s));
     // exact sizes: nnz(C) as int64 over tile rows first (int32 overflow check)
     long long *tr64 = S.c_rowptr.as<long long>();
     RTT_CHECK(scan_exclusive_i64(ws, S.c_tr_nnz.as<int>(), tr64, tilem));
