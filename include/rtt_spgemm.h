@@ -255,6 +255,39 @@ RTT_API int rtt_plan_tail_queue(int ntasks, const int *scans, const int *matches
                                 const rtt_tail_cost_model *model, int *chunks_out,
                                 rtt_tail_plan *plan);
 
+/* Early split (the reference's DmmaTileEarlySplitPlan,
+ * src/dmma_tile_early_split.h:72-97): the tail-queue partition exposed as a
+ * bounded grid of persistent heavy CTAs, at most ceil(sm_count / 2) of them,
+ * enqueued before the light grid. */
+typedef struct
+{
+    int reason;      /* DmmaTileEarlySplitGateReason: 0 default off, 1 enabled,
+                        2 invalid topology, 3 base fallback, 4 worker cap overflow */
+    int base_reason; /* the tail-queue planner's reason (rtt_tail_plan.reason) */
+    long long output_tasks, ordinary_tasks, heavy_tasks, chunks;
+    int sm_count;
+    int global_heavy_worker_block_cap; /* ceil(sm_count / 2) */
+    int heavy_worker_blocks;           /* min(chunks, cap) */
+    int reduction_worker_blocks;       /* min(heavy_tasks, cap) with workspace reduction */
+    long long descriptor_bytes, heavy_flag_bytes, partial_workspace_bytes;
+    int exact_parent_partition;        /* every task is ordinary or heavy exactly once */
+} rtt_early_split_plan;
+
+/* The reference's early-split policy defaults (DmmaTileEarlySplitPolicy,
+ * src/dmma_tile_early_split.h:33-43): enabled = 0, admission 684947.875,
+ * chunk target 342473.938, 8 chunks, heavy fraction 0.001, 131072 records,
+ * 512 MiB of partial workspace, workspace reduction on. */
+RTT_API void rtt_early_split_policy_default(rtt_tail_policy *policy);
+
+/* Replaces dmma_plan_tile_early_split (src/dmma_tile_early_split.h:152-229):
+ * the tail-queue plan of rtt_plan_tail_queue (with the policy forced on) plus
+ * the heavy-worker bound.  chunks_out[i] receives task i's chunk count (0 =
+ * ordinary; all 0 unless reason == 1).  sm_count <= 0 gives reason 2. */
+RTT_API int rtt_plan_early_split(int ntasks, const int *scans, const int *matches,
+                                 const int *output_nnz, const rtt_tail_policy *policy,
+                                 const rtt_tail_cost_model *model, int sm_count,
+                                 int *chunks_out, rtt_early_split_plan *plan);
+
 /* Frees the arrays of a hybrid tile matrix and zeroes it (the reference's
  * destroy_hybrid_tile_matrix, src/dmma_tiles.h:64-79). */
 RTT_API void rtt_hybrid_tiles_destroy(rtt_hybrid_tiles *tiles);

@@ -277,6 +277,50 @@ def plan_tail_queue(scans, matches, output_nnz, policy: dict, model: dict):
     return ch.astype(np.int32), plan
 
 
+EARLY_SPLIT_POLICY = dict(enabled=0, admission_threshold=684947.875, chunk_target=342473.938,
+                          max_chunks=8, max_heavy_fraction=0.001, record_capacity=131072,
+                          workspace_limit_bytes=512 * 1024 * 1024, workspace_reduction=1)
+
+
+def plan_early_split(scans, matches, output_nnz, policy: dict, model: dict, sm_count: int):
+    """Restatement of dmma_plan_tile_early_split (src/dmma_tile_early_split.h:152-229):
+    the tail-queue partition (plan_tail_queue with the policy switched on), a
+    global cap of ceil(sm_count / 2) persistent heavy CTAs (:98-110) and the
+    exact-parent-partition check (:127-150).  Returns (chunks per task, plan)."""
+    n = len(scans)
+    plan = dict(reason=0, base_reason=0, output_tasks=n, ordinary_tasks=n, heavy_tasks=0,
+                chunks=0, sm_count=sm_count, global_heavy_worker_block_cap=0,
+                heavy_worker_blocks=0, reduction_worker_blocks=0, descriptor_bytes=0,
+                heavy_flag_bytes=0, partial_workspace_bytes=0, exact_parent_partition=1)
+    zero = np.zeros(n, np.int32)
+    if not policy["enabled"]:
+        return zero, plan
+    if sm_count <= 0:
+        plan["reason"] = 2
+        return zero, plan
+    ch, base = plan_tail_queue(scans, matches, output_nnz, {**policy, "enabled": 1}, model)
+    plan["base_reason"] = base["reason"]
+    if base["reason"] != 1:
+        plan["reason"] = 3
+        return zero, plan
+    cap = (sm_count + 1) // 2
+    plan.update(reason=1, ordinary_tasks=base["ordinary_tasks"], heavy_tasks=base["heavy_tasks"],
+                chunks=base["chunks"], global_heavy_worker_block_cap=cap,
+                heavy_worker_blocks=min(base["chunks"], cap),
+                reduction_worker_blocks=min(base["heavy_tasks"], cap) if policy["workspace_reduction"] else 0,
+                descriptor_bytes=base["descriptor_bytes"], heavy_flag_bytes=base["heavy_flag_bytes"],
+                partial_workspace_bytes=base["partial_workspace_bytes"])
+    exact = (plan["ordinary_tasks"] + plan["heavy_tasks"] == n and not np.any(ch == 1)
+             and int((ch > 0).sum()) == plan["heavy_tasks"])
+    plan["exact_parent_partition"] = int(exact)
+    if not exact or plan["heavy_worker_blocks"] <= 0:
+        plan.update(reason=3, ordinary_tasks=n, heavy_tasks=0, chunks=0, heavy_worker_blocks=0,
+                    reduction_worker_blocks=0, descriptor_bytes=0, heavy_flag_bytes=0,
+                    partial_workspace_bytes=0)
+        return zero, plan
+    return ch, plan
+
+
 def build(reference: bool = True) -> None:
     """Compile liboracle.so (and the reference libraries where the reference
     checkout exists)."""
@@ -515,6 +559,33 @@ class Reference(_Base):
             policy["workspace_reduction"], model["intercept"], model["scan"], model["match"],
             model["output"], ch.ctypes.data, summ.ctypes.data)
         return ch[:n], (reason, summ)
+
+    def plan_early_split(self, scans, matches, output_nnz, policy: dict, model: dict,
+                         sm_count: int):
+        """The reference's dmma_plan_tile_early_split (via ref_plan_tile_early_split)."""
+        L = self.lib
+        L.ref_plan_tile_early_split.argtypes = [
+            C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double,
+            C.c_int, C.c_double, C.c_int, C.c_longlong, C.c_int, C.c_double, C.c_double,
+            C.c_double, C.c_double, C.c_int, C.c_void_p, C.c_void_p]
+        sc = np.ascontiguousarray(scans, np.int32)
+        mt = np.ascontiguousarray(matches, np.int32)
+        on = np.ascontiguousarray(output_nnz, np.int32)
+        n = sc.size
+        ch = np.zeros(max(n, 1), np.int32)
+        summ = np.zeros(11, np.int64)
+        reason = L.ref_plan_tile_early_split(
+            n, sc.ctypes.data, mt.ctypes.data, on.ctypes.data, int(policy["enabled"]),
+            policy["admission_threshold"], policy["chunk_target"], policy["max_chunks"],
+            policy["max_heavy_fraction"], policy["record_capacity"],
+            policy["workspace_limit_bytes"], policy["workspace_reduction"], model["intercept"],
+            model["scan"], model["match"], model["output"], sm_count, ch.ctypes.data,
+            summ.ctypes.data)
+        keys = ("base_reason", "ordinary_tasks", "heavy_tasks", "chunks",
+                "global_heavy_worker_block_cap", "heavy_worker_blocks", "reduction_worker_blocks",
+                "descriptor_bytes", "heavy_flag_bytes", "partial_workspace_bytes",
+                "exact_parent_partition")
+        return ch[:n], dict(reason=reason, **{k: int(v) for k, v in zip(keys, summ)})
 
     def spgemm_serialref(self, a, b):
         rp = np.zeros(a.m + 1, dtype=np.int32)

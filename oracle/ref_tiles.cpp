@@ -11,6 +11,7 @@
  *   spgemm_spa (structure, OpenMP)           src/spgemm_serialref_spa_new.h:7
  *   csr_to_hybrid_tiles                      src/dmma_tiles.h:243
  *   dmma_plan_tile_tail_queue                src/dmma_tile_tail_queue.h:190
+ *   dmma_plan_tile_early_split               src/dmma_tile_early_split.h:152
  * The output is built into oracle/_ref/ and never shipped with the product.
  */
 #include <unistd.h>
@@ -22,6 +23,7 @@
 #include "spgemm-cpu.h"
 #include "tile2csr.h"
 #include "dmma_tile_tail_queue.h"
+#include "dmma_tile_early_split.h"
 #include "spgemm_serialref_spa_new.h"
 
 namespace
@@ -178,6 +180,59 @@ int ref_plan_tile_tail_queue(int ntasks, const int *scans, const int *matches, c
     summary[2] = (long long)plan.descriptor_bytes;
     summary[3] = (long long)plan.partial_workspace_bytes;
     summary[4] = (long long)plan.heavy_flag_bytes;
+    return (int)plan.reason;
+}
+
+/* Early-split planner: same task arrays; returns the gate reason and writes
+ * the admitted chunk count per task, summary = {base reason, ordinary,
+ * heavy, chunks, cap, heavy workers, reduction workers, descriptor bytes,
+ * heavy flag bytes, partial workspace bytes, exact parent partition}. */
+int ref_plan_tile_early_split(int ntasks, const int *scans, const int *matches,
+                              const int *out_nnz, int enabled, double admission_threshold,
+                              double chunk_target, int max_chunks, double max_heavy_fraction,
+                              int record_capacity, long long workspace_limit_bytes,
+                              int workspace_reduction, double m_intercept, double m_scan,
+                              double m_match, double m_output, int sm_count, int *chunks_out,
+                              long long *summary)
+{
+    std::vector<DmmaTileTailQueueExactTask> tasks((size_t)ntasks);
+    for (int i = 0; i < ntasks; ++i)
+    {
+        tasks[(size_t)i].task = i;
+        tasks[(size_t)i].scans = scans[i];
+        tasks[(size_t)i].matches = matches[i];
+        tasks[(size_t)i].output_nnz = out_nnz[i];
+    }
+    DmmaTileEarlySplitPolicy policy;
+    policy.enabled = enabled != 0;
+    policy.admission_threshold = admission_threshold;
+    policy.chunk_target = chunk_target;
+    policy.max_chunks = max_chunks;
+    policy.max_heavy_fraction = max_heavy_fraction;
+    policy.record_capacity = record_capacity;
+    policy.workspace_limit_bytes = (std::size_t)workspace_limit_bytes;
+    policy.workspace_reduction = workspace_reduction != 0;
+    DmmaTileTailQueueCostModel model;
+    model.intercept = m_intercept;
+    model.scan = m_scan;
+    model.match = m_match;
+    model.output = m_output;
+    DmmaTileEarlySplitPlan plan = dmma_plan_tile_early_split(tasks, policy, model, sm_count);
+    for (int i = 0; i < ntasks; ++i)
+        chunks_out[i] = 0;
+    for (const auto &h : plan.heavy)
+        chunks_out[h.task] = h.chunks;
+    summary[0] = (long long)plan.base_reason;
+    summary[1] = (long long)plan.ordinary_tasks;
+    summary[2] = (long long)plan.heavy_tasks;
+    summary[3] = (long long)plan.chunks;
+    summary[4] = (long long)plan.global_heavy_worker_block_cap;
+    summary[5] = (long long)plan.heavy_worker_blocks;
+    summary[6] = (long long)plan.reduction_worker_blocks;
+    summary[7] = (long long)plan.descriptor_bytes;
+    summary[8] = (long long)plan.heavy_flag_bytes;
+    summary[9] = (long long)plan.partial_workspace_bytes;
+    summary[10] = plan.exact_parent_partition ? 1 : 0;
     return (int)plan.reason;
 }
 

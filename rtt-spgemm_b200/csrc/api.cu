@@ -975,6 +975,100 @@ int rtt_plan_tail_queue(int ntasks, const int *scans, const int *matches, const 
     return RTT_OK;
 }
 
+void rtt_early_split_policy_default(rtt_tail_policy *p)
+{
+    if (p == nullptr)
+        return;
+    std::memset(p, 0, sizeof(*p));
+    p->enabled = 0;
+    p->admission_threshold = 684947.875;
+    p->chunk_target = 342473.938;
+    p->max_chunks = 8;
+    p->max_heavy_fraction = 0.001;
+    p->record_capacity = 131072;
+    p->workspace_limit_bytes = 512ll * 1024 * 1024;
+    p->workspace_reduction = 1;
+}
+
+int rtt_plan_early_split(int ntasks, const int *scans, const int *matches,
+                         const int *output_nnz, const rtt_tail_policy *policy,
+                         const rtt_tail_cost_model *model, int sm_count, int *chunks_out,
+                         rtt_early_split_plan *plan)
+{
+    if (ntasks < 0 || policy == nullptr || model == nullptr || plan == nullptr ||
+        (ntasks > 0 && chunks_out == nullptr))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "plan_early_split: bad arguments");
+    std::memset(plan, 0, sizeof(*plan));
+    plan->output_tasks = ntasks;
+    plan->ordinary_tasks = ntasks;
+    plan->sm_count = sm_count;
+    plan->exact_parent_partition = 1;
+    auto all_ordinary = [&]() {
+        for (int i = 0; i < ntasks; ++i)
+            chunks_out[i] = 0;
+    };
+    all_ordinary();
+    if (!policy->enabled)
+        return RTT_OK; // default off
+    if (sm_count <= 0)
+    {
+        plan->reason = 2; // invalid topology
+        return RTT_OK;
+    }
+    // the partition is the tail-queue plan's, with the policy switched on
+    rtt_tail_policy base = *policy;
+    base.enabled = 1;
+    rtt_tail_plan tp;
+    RTT_CHECK(rtt_plan_tail_queue(ntasks, scans, matches, output_nnz, &base, model, chunks_out,
+                                  &tp));
+    plan->base_reason = tp.reason;
+    if (tp.reason != 1)
+    {
+        plan->reason = 3; // base fallback: the all-ordinary partition, no heavy records
+        all_ordinary();
+        return RTT_OK;
+    }
+    // at most ceil(sm_count / 2) persistent heavy CTAs (a pressure bound)
+    const long long cap = ((long long)sm_count + 1) / 2;
+    if (cap <= 0 || cap > INT_MAX)
+    {
+        plan->reason = 4;
+        all_ordinary();
+        return RTT_OK;
+    }
+    plan->reason = 1;
+    plan->ordinary_tasks = tp.ordinary_tasks;
+    plan->heavy_tasks = tp.heavy_tasks;
+    plan->chunks = tp.chunks;
+    plan->global_heavy_worker_block_cap = (int)cap;
+    plan->heavy_worker_blocks = (int)std::min<long long>(tp.chunks, cap);
+    plan->reduction_worker_blocks =
+        policy->workspace_reduction ? (int)std::min<long long>(tp.heavy_tasks, cap) : 0;
+    plan->descriptor_bytes = tp.descriptor_bytes;
+    plan->heavy_flag_bytes = tp.heavy_flag_bytes;
+    plan->partial_workspace_bytes = tp.partial_workspace_bytes;
+    // each heavy task owns >= 2 chunks and the parts cover every task once
+    long long heavy = 0;
+    bool ok = plan->ordinary_tasks + plan->heavy_tasks == plan->output_tasks;
+    for (int i = 0; i < ntasks; ++i)
+    {
+        heavy += chunks_out[i] > 0;
+        ok = ok && chunks_out[i] != 1;
+    }
+    ok = ok && heavy == plan->heavy_tasks;
+    plan->exact_parent_partition = ok ? 1 : 0;
+    if (!ok || plan->heavy_worker_blocks <= 0)
+    {
+        plan->reason = 3;
+        plan->ordinary_tasks = ntasks;
+        plan->heavy_tasks = plan->chunks = 0;
+        plan->heavy_worker_blocks = plan->reduction_worker_blocks = 0;
+        plan->descriptor_bytes = plan->heavy_flag_bytes = plan->partial_workspace_bytes = 0;
+        all_ordinary();
+    }
+    return RTT_OK;
+}
+
 void rtt_hybrid_tiles_destroy(rtt_hybrid_tiles *h)
 {
     if (h == nullptr)

@@ -27,14 +27,15 @@ from types import SimpleNamespace
 import numpy as np
 
 from . import generators
-from ._abi import (EXPORTS, LIB_PATH, RTT_OP_AAT, RTT_OP_AB, Config, CsrView, HybridTiles,
-                   RttError, SMatrix, Stats, TailCostModel, TailPlan, TailPolicy, build, check,
-                   lib)
+from ._abi import (EXPORTS, LIB_PATH, RTT_OP_AAT, RTT_OP_AB, Config, CsrView, EarlySplitPlan,
+                   HybridTiles, RttError, SMatrix, Stats, TailCostModel, TailPlan, TailPolicy,
+                   build, check, lib)
 from .generators import CSR
 
 __all__ = ["CSR", "Context", "RttError", "build", "csr2tile_col_major", "csr2tile_row_major",
            "generators", "lib", "spgemm_csr_host", "spgemm_tile", "tile16_to_tile8", "tile2csr",
            "tile2csr_device_noalloc", "csr_to_hybrid_tiles", "plan_tail_queue",
+           "plan_early_split", "early_split_policy_default",
            "TAIL_POLICY_DEFAULT", "TAIL_MODEL_DEFAULT", "spgemm_batched",
            "EXPORTS", "LIB_PATH", "RTT_OP_AB", "RTT_OP_AAT"]
 
@@ -239,6 +240,31 @@ def plan_tail_queue(scans, matches, output_nnz, policy: dict | None = None,
                                     C.byref(pol), C.byref(mod), _ptr(chunks, C.c_int),
                                     C.byref(plan)))
     return chunks[:n], {k: getattr(plan, k) for k, _ in TailPlan._fields_}
+
+
+def early_split_policy_default() -> dict:
+    """The reference's early-split policy defaults (rtt_early_split_policy_default)."""
+    pol = TailPolicy()
+    lib().rtt_early_split_policy_default(C.byref(pol))
+    return {k: getattr(pol, k) for k, _ in TailPolicy._fields_}
+
+
+def plan_early_split(scans, matches, output_nnz, policy: dict | None = None,
+                     model: dict | None = None, sm_count: int = 148):
+    """Replacement of dmma_plan_tile_early_split (reference
+    src/dmma_tile_early_split.h:152).  Returns (chunks per task, plan dict)."""
+    sc = np.ascontiguousarray(scans, dtype=np.int32)
+    mt = np.ascontiguousarray(matches, dtype=np.int32)
+    on = np.ascontiguousarray(output_nnz, dtype=np.int32)
+    n = int(sc.shape[0])
+    pol = TailPolicy(**{**early_split_policy_default(), **(policy or {})})
+    mod = TailCostModel(**{**TAIL_MODEL_DEFAULT, **(model or {})})
+    chunks = np.zeros(max(n, 1), np.int32)
+    plan = EarlySplitPlan()
+    check(lib().rtt_plan_early_split(n, _ptr(sc, C.c_int), _ptr(mt, C.c_int), _ptr(on, C.c_int),
+                                     C.byref(pol), C.byref(mod), int(sm_count),
+                                     _ptr(chunks, C.c_int), C.byref(plan)))
+    return chunks[:n], {k: getattr(plan, k) for k, _ in EarlySplitPlan._fields_}
 
 
 def tile2csr_device_noalloc(tiles: dict, rowptr, col=None, val=None, tile_dim: int = 16,

@@ -34,7 +34,7 @@ EXPORTS = [
     "rtt_spgemm_numeric", "rtt_spgemm_tiles_view", "rtt_spgemm_csr_host",
     "rtt_tile2csr_device_noalloc", "rtt_csr_to_hybrid_tiles", "rtt_hybrid_tiles_destroy",
     "rtt_plan_tail_queue", "rtt_spgemm_batched_symbolic", "rtt_spgemm_batched_numeric",
-    "rtt_csr_transpose",
+    "rtt_csr_transpose", "rtt_early_split_policy_default", "rtt_plan_early_split",
 ]
 
 
@@ -104,6 +104,15 @@ class TailPlan(C.Structure):
         ("heavy_fraction", C.c_double), ("average_chunks", C.c_double)]
 
 
+class EarlySplitPlan(C.Structure):
+    _fields_ = [("reason", C.c_int), ("base_reason", C.c_int)] + [(k, C.c_longlong) for k in (
+        "output_tasks", "ordinary_tasks", "heavy_tasks", "chunks")] + [(k, C.c_int) for k in (
+        "sm_count", "global_heavy_worker_block_cap", "heavy_worker_blocks",
+        "reduction_worker_blocks")] + [(k, C.c_longlong) for k in (
+        "descriptor_bytes", "heavy_flag_bytes", "partial_workspace_bytes")] + [
+        ("exact_parent_partition", C.c_int)]
+
+
 class Stats(C.Structure):
     _fields_ = [("nnz_a", C.c_longlong), ("nnz_b", C.c_longlong), ("nnz_c", C.c_longlong),
                 ("nnz_cub", C.c_longlong), ("tiles_a", C.c_longlong),
@@ -150,6 +159,11 @@ def lib() -> C.CDLL:
                                           P(HybridTiles)]
     L.rtt_plan_tail_queue.argtypes = [C.c_int, P(C.c_int), P(C.c_int), P(C.c_int),
                                       P(TailPolicy), P(TailCostModel), P(C.c_int), P(TailPlan)]
+    L.rtt_early_split_policy_default.argtypes = [P(TailPolicy)]
+    L.rtt_early_split_policy_default.restype = None
+    L.rtt_plan_early_split.argtypes = [C.c_int, P(C.c_int), P(C.c_int), P(C.c_int),
+                                       P(TailPolicy), P(TailCostModel), C.c_int, P(C.c_int),
+                                       P(EarlySplitPlan)]
     L.rtt_hybrid_tiles_destroy.argtypes = [P(HybridTiles)]
     L.rtt_hybrid_tiles_destroy.restype = None
     L.rtt_tile2csr_device_noalloc.argtypes = [P(SMatrix), C.c_int, C.c_int, C.c_longlong,

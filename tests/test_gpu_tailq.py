@@ -8,7 +8,7 @@ import pytest
 
 import oracle as O
 import rtt_spgemm as R
-from test_oracle_pin import TAIL_CASES, TAIL_MODEL, TAIL_POLICY, tail_tasks
+from test_oracle_pin import EARLY_CASES, TAIL_CASES, TAIL_MODEL, TAIL_POLICY, early_case, tail_tasks
 
 pytestmark = pytest.mark.gpu
 
@@ -33,3 +33,17 @@ def test_tail_planner_disabled_and_empty():
     assert plan["reason"] == 0 and list(ch) == [0, 0]
     ch, plan = R.plan_tail_queue([], [], [])
     assert plan["reason"] == 4 and plan["output_tasks"] == 0
+
+
+@pytest.mark.parametrize("case", list(EARLY_CASES))
+def test_early_split_planner_matches_oracle(case):
+    pol, mod, sms, (s, m, o) = early_case(case)
+    ch, plan = R.plan_early_split(s, m, o, pol, mod, sms)
+    want_ch, want = O.plan_early_split(s, m, o, pol, mod, sms)
+    assert np.array_equal(ch, want_ch), case
+    for k, v in want.items():
+        assert plan[k] == v, (case, k)
+
+
+def test_early_split_policy_defaults():
+    assert R.early_split_policy_default() == pytest.approx(O.EARLY_SPLIT_POLICY)

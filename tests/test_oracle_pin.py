@@ -251,3 +251,45 @@ def test_tail_planner_oracle_matches_reference(ref, case):
     assert np.array_equal(ch, rch)
     assert [plan["heavy_tasks"], plan["chunks"], plan["descriptor_bytes"],
             plan["partial_workspace_bytes"], plan["heavy_flag_bytes"]] == list(summ)
+
+
+# ---------------------------------------------------------------- early-split planner
+EARLY_CASES = {
+    # (policy overrides, sm_count, tasks)
+    "default_off": (dict(enabled=0), 148, dict(n=2000, seed=11)),
+    "reference_defaults": (dict(enabled=1), 148, dict(n=3000, seed=12)),
+    "enabled": (dict(enabled=1, admission_threshold=256.0, chunk_target=256.0,
+                     max_heavy_fraction=0.5), 148, dict(n=5000, seed=13, heavy_rate=0.02)),
+    "small_gpu": (dict(enabled=1, admission_threshold=256.0, chunk_target=256.0,
+                       max_heavy_fraction=0.5), 3, dict(n=5000, seed=14, heavy_rate=0.05)),
+    "no_reduction": (dict(enabled=1, admission_threshold=256.0, chunk_target=100.0,
+                          max_heavy_fraction=1.0, workspace_reduction=0), 148,
+                     dict(n=4000, seed=15, heavy_rate=0.1)),
+    "invalid_topology": (dict(enabled=1, admission_threshold=256.0, max_heavy_fraction=0.5), 0,
+                         dict(n=500, seed=16)),
+    "negative_sms": (dict(enabled=1), -4, dict(n=500, seed=17)),
+    "base_fraction_gate": (dict(enabled=1, admission_threshold=256.0, chunk_target=256.0), 148,
+                           dict(n=3000, seed=18, heavy_rate=0.2)),
+    "base_invalid_task": (dict(enabled=1, admission_threshold=256.0, max_heavy_fraction=1.0), 148,
+                          dict(n=2000, seed=19, invalid_at=7)),
+}
+
+
+def early_case(case):
+    import oracle as O
+    pol, sms, tk = EARLY_CASES[case]
+    return {**O.EARLY_SPLIT_POLICY, **pol}, dict(TAIL_MODEL), sms, tail_tasks(**tk)
+
+
+@pytest.mark.parametrize("case", list(EARLY_CASES))
+def test_early_split_oracle_matches_reference(ref, case):
+    """dmma_plan_tile_early_split (src/dmma_tile_early_split.h:152) compiled
+    from the reference against the oracle restatement: gate reasons, worker
+    bounds, byte counts and the admitted chunks per task."""
+    import oracle as O
+    pol, mod, sms, (s, m, o) = early_case(case)
+    ch, plan = O.plan_early_split(s, m, o, pol, mod, sms)
+    rch, rplan = ref.plan_early_split(s, m, o, pol, mod, sms)
+    assert np.array_equal(ch, rch), case
+    for k, v in rplan.items():
+        assert plan[k] == v, (case, k, plan[k], v)
