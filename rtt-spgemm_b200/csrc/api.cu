@@ -635,6 +635,9 @@ int rtt_context_set_stream(rtt_context c, void *stream)
 {
     if (c == nullptr)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    // buffers allocated in the order of the old stream are complete before
+    // the new stream uses them
+    RTT_CUDA(cudaStreamSynchronize(c->ws.stream));
     c->ws.stream = static_cast<cudaStream_t>(stream);
     return RTT_OK;
 }
@@ -1159,9 +1162,12 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
         c->b_alias = false;
         if (op == RTT_OP_AAT)
         {
+            RTT_CHECK(c->bt_rowptr.ensure(sizeof(int) * ((size_t)A->cols + 1), ws.stream));
+            RTT_CHECK(c->bt_col.ensure(sizeof(int) * (size_t)A->nnz + 16, ws.stream));
+            RTT_CHECK(c->bt_val.ensure(sizeof(double) * (size_t)A->nnz + 16, ws.stream));
             RTT_CHECK(csr_transpose_device(ws, A->rows, A->cols, (int)A->nnz, A->row_ptr,
-                                           A->col_idx, A->values, c->bt_rowptr, c->bt_col,
-                                           c->bt_val));
+                                           A->col_idx, A->values, c->bt_rowptr.as<int>(),
+                                           c->bt_col.as<int>(), c->bt_val.as<double>()));
             RTT_CHECK(map_device_error(csr2tile_device(ws, A->cols, A->rows, (int)A->nnz,
                                                        c->bt_rowptr.as<int>(), c->bt_col.as<int>(),
                                                        c->bt_val.as<double>(), c->B, true, false)));
@@ -1308,11 +1314,12 @@ int assemble(rtt_context c, int count, const rtt_csr_view *V, const std::vector<
     Workspace &ws = c->ws;
     cudaStream_t s = ws.stream;
     const int total_rows = row_off[(size_t)count];
-    std::vector<int> rows((size_t)count), nnz_off((size_t)count + 1, 0);
+    std::vector<int> rows((size_t)count), cols((size_t)count), nnz_off((size_t)count + 1, 0);
     std::vector<const void *> tab((size_t)count * 3);
     for (int i = 0; i < count; ++i)
     {
         rows[(size_t)i] = V[i].rows;
+        cols[(size_t)i] = V[i].cols;
         nnz_off[(size_t)i + 1] = nnz_off[(size_t)i] + (int)V[i].nnz;
         tab[(size_t)i] = V[i].row_ptr;
         tab[(size_t)count + i] = V[i].col_idx;
@@ -1320,17 +1327,20 @@ int assemble(rtt_context c, int count, const rtt_csr_view *V, const std::vector<
     }
     const int nnz = nnz_off[(size_t)count];
     // device copy of the tables: pointers first (8-byte aligned), then ints
-    DevBuf tabd;
-    const size_t ints = (size_t)count * 3 + 2;
+    // (grow-only scratch: no cudaFree, which would wait for every stream)
+    DevBuf &tabd = ws.tmp[0];
+    const size_t ints = (size_t)count * 4 + 2;
     RTT_CHECK(tabd.ensure(sizeof(void *) * tab.size() + sizeof(int) * ints, s));
     char *base = tabd.as<char>();
     int *d_rows = reinterpret_cast<int *>(base + sizeof(void *) * tab.size());
     int *d_rowoff = d_rows + count, *d_coladd = d_rowoff + count + 1, *d_nnzoff = d_coladd + count;
+    int *d_cols = d_nnzoff + count + 1;
     std::vector<int> packed;
     packed.insert(packed.end(), rows.begin(), rows.end());
     packed.insert(packed.end(), row_off.begin(), row_off.end());
     packed.insert(packed.end(), col_add.begin(), col_add.begin() + count);
     packed.insert(packed.end(), nnz_off.begin(), nnz_off.end());
+    packed.insert(packed.end(), cols.begin(), cols.end());
     RTT_CUDA(cudaMemcpyAsync(base, tab.data(), sizeof(void *) * tab.size(), cudaMemcpyHostToDevice, s));
     RTT_CUDA(cudaMemcpyAsync(d_rows, packed.data(), sizeof(int) * packed.size(), cudaMemcpyHostToDevice, s));
     RTT_CHECK(rp.ensure(sizeof(int) * ((size_t)total_rows + 1), s));
@@ -1340,10 +1350,8 @@ int assemble(rtt_context c, int count, const rtt_csr_view *V, const std::vector<
     RTT_CHECK(batch_assemble_device(ws, count, total_rows, reinterpret_cast<const int *const *>(tp),
                                     reinterpret_cast<const int *const *>(tp + count),
                                     reinterpret_cast<const double *const *>(tp + 2 * count),
-                                    d_rows, d_rowoff, d_coladd, d_nnzoff, rp.as<int>(),
+                                    d_rows, d_cols, d_rowoff, d_coladd, d_nnzoff, rp.as<int>(),
                                     col.as<int>(), val.as<double>()));
-    RTT_CUDA(cudaStreamSynchronize(s)); // the tables are released on return
-    tabd.release();
     return RTT_OK;
 }
 } // namespace
@@ -1456,29 +1464,11 @@ int rtt_csr_transpose(rtt_context c, const rtt_csr_view *A, int *t_row_ptr, int 
     RTT_CUDA(cudaSetDevice(c->ws.device));
     Workspace &ws = c->ws;
     cudaStream_t s = ws.stream;
-    // the transpose lands in the context's scratch, then in the caller's arrays
-    DevBuf trp, tci, tva;
-    int st = csr_transpose_device(ws, A->rows, A->cols, (int)A->nnz, A->row_ptr, A->col_idx,
-                                  A->values, trp, tci, tva);
-    if (st == RTT_OK)
-    {
-        cudaError_t e = cudaMemcpyAsync(t_row_ptr, trp.p, sizeof(int) * ((size_t)A->cols + 1),
-                                        cudaMemcpyDeviceToDevice, s);
-        if (e == cudaSuccess && A->nnz > 0)
-            e = cudaMemcpyAsync(t_col_idx, tci.p, sizeof(int) * (size_t)A->nnz,
-                                cudaMemcpyDeviceToDevice, s);
-        if (e == cudaSuccess && A->nnz > 0)
-            e = cudaMemcpyAsync(t_values, tva.p, sizeof(double) * (size_t)A->nnz,
-                                cudaMemcpyDeviceToDevice, s);
-        if (e == cudaSuccess)
-            e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess)
-            st = rtt::cuda_fail(e, "csr_transpose copy");
-    }
-    trp.release();
-    tci.release();
-    tva.release();
-    return st;
+    // straight into the caller's arrays; the scratch is the context's own
+    RTT_CHECK(csr_transpose_device(ws, A->rows, A->cols, (int)A->nnz, A->row_ptr, A->col_idx,
+                                   A->values, t_row_ptr, t_col_idx, t_values));
+    RTT_CUDA(cudaStreamSynchronize(s));
+    return RTT_OK;
 }
 
 int rtt_spgemm_tiles_view(rtt_context c, SMatrix *out)

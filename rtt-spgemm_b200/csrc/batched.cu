@@ -33,14 +33,18 @@ __device__ __forceinline__ int instance_of(const int *__restrict__ off, int coun
     return lo;
 }
 
-// One warp per row of the block-diagonal matrix.
+// One warp per row of the block-diagonal matrix.  Every instance's row
+// pointer is checked against its own entry count and every column against its
+// own width before anything is written: a broken instance sets the device
+// error word (the batch fails as a whole) and cannot write outside its part.
 __global__ void k_batch_assemble(int count, int total_rows, const int *const *__restrict__ rp_tab,
                                  const int *const *__restrict__ ci_tab,
                                  const double *const *__restrict__ va_tab,
-                                 const int *__restrict__ rows, const int *__restrict__ row_off,
+                                 const int *__restrict__ rows, const int *__restrict__ cols,
+                                 const int *__restrict__ row_off,
                                  const int *__restrict__ col_add, const int *__restrict__ nnz_off,
                                  int *__restrict__ out_rp, int *__restrict__ out_col,
-                                 double *__restrict__ out_val)
+                                 double *__restrict__ out_val, int *err)
 {
     const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -62,15 +66,28 @@ __global__ void k_batch_assemble(int count, int total_rows, const int *const *__
         return;
     }
     const int *rp = rp_tab[i];
-    const int b = rp[j], e = rp[j + 1], base = nnz_off[i];
+    const int base = nnz_off[i], nnz_i = nnz_off[i + 1] - base;
+    int b = rp[j], e = rp[j + 1];
+    if (b < 0 || e < b || e > nnz_i)
+    {
+        if (lane == 0)
+            set_error(err, DERR_CSR_ROWPTR);
+        b = e = min(max(b, 0), nnz_i);
+    }
     if (lane == 0)
         out_rp[r] = base + b;
     const int *ci = ci_tab[i];
     const double *va = va_tab[i];
-    const int add = col_add[i];
+    const int add = col_add[i], ncols = cols[i];
     for (int k = b + lane; k < e; k += 32)
     {
-        out_col[base + k] = ci[k] + add;
+        int cc = ci[k];
+        if ((unsigned)cc >= (unsigned)ncols)
+        {
+            set_error(err, DERR_CSR_COL);
+            cc = 0;
+        }
+        out_col[base + k] = cc + add;
         out_val[base + k] = va[k];
     }
 }
@@ -143,12 +160,12 @@ inline int warps_grid(long long warps) { return (int)((warps * 32 + 255) / 256);
 
 int batch_assemble_device(Workspace &ws, int count, int total_rows, const int *const *rp_tab,
                           const int *const *ci_tab, const double *const *va_tab, const int *rows,
-                          const int *row_off, const int *col_add, const int *nnz_off, int *out_rp,
-                          int *out_col, double *out_val)
+                          const int *cols, const int *row_off, const int *col_add,
+                          const int *nnz_off, int *out_rp, int *out_col, double *out_val)
 {
     k_batch_assemble<<<warps_grid((long long)total_rows + 1), 256, 0, ws.stream>>>(
-        count, total_rows, rp_tab, ci_tab, va_tab, rows, row_off, col_add, nnz_off, out_rp,
-        out_col, out_val);
+        count, total_rows, rp_tab, ci_tab, va_tab, rows, cols, row_off, col_add, nnz_off, out_rp,
+        out_col, out_val, ws.err.as<int>());
     ws.launches++;
     RTT_CUDA(cudaGetLastError());
     return RTT_OK;

@@ -628,53 +628,32 @@ int tiles_to_col_major(Workspace &ws, const TileBufs &rm, TileBufs &out)
 }
 
 int csr_transpose_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
-                         const double *val, DevBuf &t_rowptr, DevBuf &t_col, DevBuf &t_val)
+                         const double *val, int *t_rowptr, int *t_col, double *t_val)
 {
     cudaStream_t s = ws.stream;
-    RTT_CHECK(t_rowptr.ensure(sizeof(int) * (size_t)(n + 1), s));
-    RTT_CHECK(t_col.ensure(sizeof(int) * (size_t)nnz + 16, s));
-    RTT_CHECK(t_val.ensure(sizeof(double) * (size_t)nnz + 16, s));
-    DevBuf rows, iota, keys, order;
-    int st = RTT_OK;
-    do
+    // grow-only scratch of the workspace: no cudaMalloc / cudaFree (which
+    // would wait for every stream of the device) once it has grown
+    const size_t bytes = sizeof(int) * (size_t)nnz + 16;
+    for (DevBuf &b : ws.tmp)
+        RTT_CHECK(b.ensure(bytes, s));
+    int *rows = ws.tmp[0].as<int>(), *iota = ws.tmp[1].as<int>();
+    int *keys = ws.tmp[2].as<int>(), *order = ws.tmp[3].as<int>();
+    if (m > 0)
     {
-        if ((st = rows.ensure(sizeof(int) * (size_t)nnz + 16, s)) != RTT_OK)
-            break;
-        if ((st = iota.ensure(sizeof(int) * (size_t)nnz + 16, s)) != RTT_OK)
-            break;
-        if ((st = keys.ensure(sizeof(int) * (size_t)nnz + 16, s)) != RTT_OK)
-            break;
-        if ((st = order.ensure(sizeof(int) * (size_t)nnz + 16, s)) != RTT_OK)
-            break;
-        if (m > 0)
-        {
-            k_row_ids<<<grid_for(m, 256), 256, 0, s>>>(m, rowptr, rows.as<int>());
-            ws.launches++;
-        }
-        if (nnz > 0)
-        {
-            k_iota<<<grid_for(nnz, 256), 256, 0, s>>>(iota.as<int>(), nnz);
-            ws.launches++;
-            if ((st = sort_pairs(ws, col, keys.as<int>(), iota.as<int>(), order.as<int>(), nnz, n)) !=
-                RTT_OK)
-                break;
-            k_gather_transpose<<<grid_for(nnz, 256), 256, 0, s>>>(
-                nnz, order.as<int>(), rows.as<int>(), val, t_col.as<int>(), t_val.as<double>());
-            ws.launches++;
-        }
-        k_lower_bound_ptr<<<grid_for(n + 1, 256), 256, 0, s>>>(keys.as<int>(), nnz, n,
-                                                              t_rowptr.as<int>());
+        k_row_ids<<<grid_for(m, 256), 256, 0, s>>>(m, rowptr, rows);
         ws.launches++;
-        cudaError_t e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess)
-            st = cuda_fail(e, "csr transpose");
-    } while (0);
-    cudaStreamSynchronize(s);
-    rows.release();
-    iota.release();
-    keys.release();
-    order.release();
-    return st;
+    }
+    if (nnz > 0)
+    {
+        k_iota<<<grid_for(nnz, 256), 256, 0, s>>>(iota, nnz);
+        ws.launches++;
+        RTT_CHECK(sort_pairs(ws, col, keys, iota, order, nnz, n));
+        k_gather_transpose<<<grid_for(nnz, 256), 256, 0, s>>>(nnz, order, rows, val, t_col, t_val);
+        ws.launches++;
+    }
+    k_lower_bound_ptr<<<grid_for(n + 1, 256), 256, 0, s>>>(keys, nnz, n, t_rowptr);
+    ws.launches++;
+    return RTT_OK;
 }
 
 } // namespace rtt

@@ -200,6 +200,7 @@ struct Workspace
     cudaStream_t stream = nullptr;
     DevBuf err;        // int device error word
     DevBuf scan_tmp;   // CUB temp storage
+    DevBuf tmp[4];     // grow-only scratch of the transpose and the batch tables
     int *h_scalars = nullptr; // pinned, 16 ints
     long long *h_scalars64 = nullptr; // pinned, 8 long long
     int launches = 0;
@@ -243,8 +244,10 @@ int build_tile_csc(Workspace &ws, TileBufs &t);
 // rearrange row-major tiles into the csr2tile_col_major layout (data in CSC order)
 int tiles_to_col_major(Workspace &ws, const TileBufs &rowmajor, TileBufs &out);
 // CSR transpose on the device
+// A^T of a device CSR into caller-sized arrays (n + 1, nnz, nnz), sorted rows;
+// enqueued on ws.stream, scratch from ws.tmp
 int csr_transpose_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
-                         const double *val, DevBuf &t_rowptr, DevBuf &t_col, DevBuf &t_val);
+                         const double *val, int *t_rowptr, int *t_col, double *t_val);
 
 // Accumulator slots and C tiles per window of the flat numeric kernel (the
 // symbolic step flags tile rows beyond either).
@@ -318,8 +321,8 @@ int tile2csr_fill_device(Workspace &ws, const int *tile_ptr, const int *tile_col
 // batched products (block-diagonal operands)
 int batch_assemble_device(Workspace &ws, int count, int total_rows, const int *const *rp_tab,
                           const int *const *ci_tab, const double *const *va_tab, const int *rows,
-                          const int *row_off, const int *col_add, const int *nnz_off, int *out_rp,
-                          int *out_col, double *out_val);
+                          const int *cols, const int *row_off, const int *col_add,
+                          const int *nnz_off, int *out_rp, int *out_col, double *out_val);
 int batch_count_device(Workspace &ws, int count, const int *row_off, const int *rows,
                        const int *row_cnt, long long *nnz);
 int batch_split_device(Workspace &ws, int count, int total_rows, const int *row_off,

@@ -32,22 +32,36 @@ int cuda_fail(cudaError_t e, const char *what)
     return fail(RTT_ERR_CUDA, m);
 }
 
+// Grow-only buffers from the device's stream-ordered pool: a regrow frees
+// and allocates in the order of stream s, without the device-wide
+// synchronisation of cudaFree / cudaMalloc, so contexts that run on other
+// streams (the serving loop's workers) do not wait for each other's kernels.
+// The pool keeps freed memory for reuse (release threshold raised in
+// Workspace::init).
 int DevBuf::ensure(size_t bytes, cudaStream_t s)
 {
-    (void)s;
     if (bytes == 0)
         bytes = 16;
     if (bytes <= cap)
         return RTT_OK;
     if (p != nullptr)
     {
-        cudaFree(p);
+        if (cudaFreeAsync(p, s) != cudaSuccess)
+        {
+            cudaGetLastError();
+            cudaFree(p);
+        }
         p = nullptr;
         cap = 0;
     }
     // round up so that repeated slightly-larger requests do not thrash
     size_t want = bytes + bytes / 8 + 256;
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = cudaMallocAsync(&p, want, s);
+    if (e != cudaSuccess)
+    {
+        cudaGetLastError();
+        e = cudaMalloc(&p, want);
+    }
     if (e != cudaSuccess)
     {
         cudaGetLastError();
@@ -90,6 +104,16 @@ int Workspace::init(int dev)
     if (prop.major < 10)
         return fail(RTT_ERR_NO_DEVICE, "this library is built for sm_100a (B200); found sm_" +
                                            std::to_string(prop.major * 10 + prop.minor));
+    {
+        // keep memory freed to the default pool cached in this process
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+        {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    }
     RTT_CHECK(err.ensure(sizeof(int) * 4, stream));
     RTT_CUDA(cudaMemset(err.p, 0, sizeof(int) * 4));
     if (h_scalars == nullptr)

@@ -17,6 +17,12 @@ its row pointer, against a fixed pool.  Operands that a request marks with a
 reuse key stay resident on the device (with A^T for A*A^T requests) and are
 not copied again.
 
+A batch's product is one CSR with int32 offsets, so a batch also keeps the
+sum of its requests' entry bounds (nnzCub) within 2^31 - 1.  A request whose
+own result cannot be represented, or any other failing request, is finished
+with its error recorded (Request.error) instead of a result; a failing batch
+is retried one request at a time so that only the failing request fails.
+
 Latency of a request = time its result is on the device minus its arrival.
 """
 from __future__ import annotations
@@ -28,8 +34,10 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import Context, spgemm_batched
+from . import Context, RttError, spgemm_batched
 from .generators import CSR
+
+INT32_MAX = 2**31 - 1
 
 
 @dataclass
@@ -40,17 +48,31 @@ class Request:
     arrival: float = 0.0      # seconds after the start of the run
     done: float = -1.0
     result: tuple = None      # device (rowptr, col, val) of C
+    error: str = None         # set instead of result when the product failed
     bound: int = field(default=0, repr=False)
+    entries: int = field(default=0, repr=False)
+
+
+def product_cub(a: CSR, op: str) -> int:
+    """nnzCub of the request: the products, an upper bound of nnz(C).  Raises
+    ValueError for a CSR the library would reject (row pointer not monotone
+    or past the entries, a column outside [0, n), A^2 of a non-square A)."""
+    rp, col = np.asarray(a.rowptr), np.asarray(a.col)
+    if (rp.size != a.m + 1 or rp[0] < 0 or np.any(np.diff(rp) < 0) or rp[-1] > col.size
+            or (col.size and (col.min() < 0 or col.max() >= a.n))):
+        raise ValueError("invalid CSR operand")
+    if op == "A2" and a.m != a.n:
+        raise ValueError("A^2 of a non-square matrix")
+    if op == "A2":
+        return int(np.diff(a.rowptr).astype(np.int64)[a.col].sum())
+    # A * A^T: row i's products = sum over k in A(i) of nnz(A^T row k) = colcount(k)
+    cc = np.bincount(a.col, minlength=a.n).astype(np.int64)
+    return int(cc[a.col].sum())
 
 
 def product_bound(a: CSR, op: str) -> int:
     """Upper bound of C's bytes from the structure alone: nnz(C) <= nnzCub."""
-    if op == "A2":
-        cub = int(np.diff(a.rowptr).astype(np.int64)[a.col].sum())
-    else:  # A * A^T: row i's products = sum over k in A(i) of nnz(A^T row k) = colcount(k)
-        cc = np.bincount(a.col, minlength=a.n).astype(np.int64)
-        cub = int(cc[a.col].sum())
-    return 12 * cub + 4 * (a.m + 1)
+    return 12 * product_cub(a, op) + 4 * (a.m + 1)
 
 
 class Server:
@@ -97,12 +119,39 @@ class Server:
                     self.resident[r.key] = (a, at)
         return a, (at if r.op == "AAT" else a)
 
+    def _run_batch(self, ctx, stream, batch, t0):
+        try:
+            As, Bs = [], []
+            for r in batch:
+                a, b = self._operands(r, ctx)
+                As.append(a)
+                Bs.append(b)
+            outs = spgemm_batched(ctx, As, Bs)
+            stream.synchronize()
+        except RttError as e:
+            if len(batch) > 1:  # find the failing request(s): one at a time
+                for r in batch:
+                    self._run_batch(ctx, stream, [r], t0)
+                return
+            batch[0].error = str(e)
+            batch[0].done = time.perf_counter() - t0
+            return
+        t = time.perf_counter() - t0
+        for r, o in zip(batch, outs):
+            r.done = t
+            r.result = o if self.keep_results else None
+
     # -- the loop ---------------------------------------------------------
     def run(self, requests: list[Request]) -> dict:
         """Serve requests (sorted by arrival) in real time; returns latency
         percentiles and throughput."""
         for r in requests:
-            r.bound = product_bound(r.a, r.op) + 12 * r.a.nnz + 4 * (r.a.m + 1)
+            try:
+                r.entries = product_cub(r.a, r.op)
+            except ValueError as e:  # rejected at admission, finished on arrival
+                r.error, r.done = str(e), r.arrival
+                continue
+            r.bound = 12 * r.entries + 4 * (r.a.m + 1) + 12 * r.a.nnz + 4 * (r.a.m + 1)
         pending = deque()
         nxt = 0
         reserved = [0.0]
@@ -116,13 +165,17 @@ class Server:
             nonlocal nxt
             now = time.perf_counter() - t0
             while nxt < n and requests[nxt].arrival <= now:
-                pending.append(requests[nxt])
+                if requests[nxt].error is None:
+                    pending.append(requests[nxt])
                 nxt += 1
-            batch, need = [], 0.0
+            batch, need, entries = [], 0.0, 0
             while pending and len(batch) < self.max_batch:
                 r = pending[0]
                 if batch and reserved[0] + need + r.bound > self.pool:
                     break
+                if batch and entries + r.entries > INT32_MAX:
+                    break  # the batch's C must keep int32 offsets
+                entries += r.entries
                 if not batch and reserved[0] + r.bound > self.pool and reserved[0] > 0:
                     break  # wait for memory to free up
                 batch.append(pending.popleft())
@@ -149,17 +202,7 @@ class Server:
                                 wait = max(0.0, requests[nxt].arrival - (time.perf_counter() - t0))
                             cv.wait(timeout=min(wait, 0.01) if wait > 0 else 0.0005)
                             batch, need = take_batch()
-                    As, Bs = [], []
-                    for r in batch:
-                        a, b = self._operands(r, ctx)
-                        As.append(a)
-                        Bs.append(b)
-                    outs = spgemm_batched(ctx, As, Bs)
-                    stream.synchronize()
-                    t = time.perf_counter() - t0
-                    for r, o in zip(batch, outs):
-                        r.done = t
-                        r.result = o if self.keep_results else None
+                    self._run_batch(ctx, stream, batch, t0)
                     with cv:
                         reserved[0] -= need
                         done[0] += len(batch)
@@ -194,14 +237,17 @@ def serve_plain(requests: list[Request], device: int = 0, config: dict | None = 
                  torch.from_numpy(r.a.col).to(dev), torch.from_numpy(r.a.val).to(dev))
             if r.key is not None:
                 resident[r.key] = a
-        nnz, _ = ctx.symbolic(a, None, 1 if r.op == "AAT" else 0)
-        rp = torch.empty(r.a.m + 1, dtype=torch.int32, device=dev)
-        ci = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
-        va = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
-        ctx.numeric(rp, ci, va)
-        stream.synchronize()
+        try:
+            nnz, _ = ctx.symbolic(a, None, 1 if r.op == "AAT" else 0)
+            rp = torch.empty(r.a.m + 1, dtype=torch.int32, device=dev)
+            ci = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+            va = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
+            ctx.numeric(rp, ci, va)
+            stream.synchronize()
+            r.result = (rp, ci[:nnz], va[:nnz])
+        except RttError as e:
+            r.error = str(e)
         r.done = time.perf_counter() - t0
-        r.result = (rp, ci[:nnz], va[:nnz])
     ctx.close()
     return summarize(requests, max(r.done for r in requests) if requests else 0.0)
 
@@ -209,6 +255,7 @@ def serve_plain(requests: list[Request], device: int = 0, config: dict | None = 
 def summarize(requests, span: float) -> dict:
     lat = np.array([r.done - r.arrival for r in requests]) * 1e3
     return {"requests": len(requests), "seconds": span,
+            "failed": sum(r.error is not None for r in requests),
             "spgemms_per_s": len(requests) / span if span > 0 else 0.0,
             "p50_ms": float(np.percentile(lat, 50)) if lat.size else 0.0,
             "p99_ms": float(np.percentile(lat, 99)) if lat.size else 0.0}

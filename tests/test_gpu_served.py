@@ -35,3 +35,36 @@ def test_served_results_equal_alone_and_oracle(orc, pool):
             B = r.a if r.op == "A2" else r.a.transpose()
             erp, ecol, evals, eabs = orc.spgemm_csr(r.a, B)
             assert_csr_close(rp, ci, va, erp, ecol, evals, eabs, f"request {i} ({r.op}): ")
+
+
+def test_served_batches_bounded_by_int32_entries(monkeypatch):
+    """A batch's C keeps int32 offsets: with the cap lowered to a few
+    thousand products per batch the loop cuts many small batches, and every
+    result is still the plain path's, bit for bit."""
+    from rtt_spgemm import serve
+
+    monkeypatch.setattr(serve, "INT32_MAX", 5000)
+    reqs = serve.poisson_requests(12, rate=2000.0, n_lo=200, n_hi=2000, reuse=0.0, seed=5)
+    alone = serve.poisson_requests(12, rate=2000.0, n_lo=200, n_hi=2000, reuse=0.0, seed=5)
+    serve.Server(workers=2).run(reqs)
+    serve.serve_plain(alone)
+    for r, p in zip(reqs, alone):
+        assert r.error is None and r.result is not None
+        for x, y in zip(r.result, p.result):
+            assert np.array_equal(_host(x).view(np.uint8), _host(y).view(np.uint8))
+
+
+def test_served_failing_request_does_not_stop_the_loop():
+    """A request the library rejects (a column index past n) is finished with
+    its error; the requests batched with it get their results."""
+    from rtt_spgemm import serve
+    from rtt_spgemm.generators import CSR
+
+    reqs = serve.poisson_requests(8, rate=1e6, n_lo=300, n_hi=1000, reuse=0.0, seed=6)
+    bad = CSR(4, 4, np.array([0, 1, 2, 3, 4], np.int32), np.array([0, 1, 9, 3], np.int32),
+              np.ones(4))
+    reqs.insert(3, serve.Request(bad, "A2", None, reqs[3].arrival))
+    stats = serve.Server(workers=1).run(reqs)
+    assert stats["failed"] == 1
+    assert reqs[3].error is not None and reqs[3].result is None
+    assert all(r.result is not None for i, r in enumerate(reqs) if i != 3)
