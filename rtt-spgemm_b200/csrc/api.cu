@@ -1200,7 +1200,9 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
     dB.csr_col = c->b_ci;
     dB.csr_val = c->b_va;
     dB.nnz = (int)c->b_nnz;
-    RTT_CHECK(map_device_error(symbolic_device(ws, c->A.view(), dB, c->S, !c->b_dups)));
+    DevTiles dA = c->A.view();
+    dA.csr_rowptr = A->row_ptr; // A's row lengths: the symbolic step balances hub rows
+    RTT_CHECK(map_device_error(symbolic_device(ws, dA, dB, c->S, !c->b_dups)));
     if (timing)
     {
         float t01 = 0.f, t12 = 0.f;

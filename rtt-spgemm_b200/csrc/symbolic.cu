@@ -49,8 +49,9 @@ struct CtaSmem2
     int wordpre[WWORDS];
     uint8_t slot8[WBITS];                // window column -> slot
     uint32_t mw[S2_WARPS * S2_STRIDE];   // per warp and slot: row 2w (low 16), 2w+1 (high 16)
-    int4 ent[S2_WARPS][32];              // per warp: B row start, length, mask shift, -
+    int4 ent[S2_WARPS][32];              // per warp: B row start, length, mask shift, mask row
     int lo, hi, nb, wend;
+    int share;                           // the warps share the A entries (unbalanced rows)
 };
 
 // Window bounds [lo, hi] of the tile columns reachable from tile row I.
@@ -212,6 +213,25 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
     __syncthreads();
     const int lo = S.lo, hi = S.hi;
     const bool clip = hi >= 0 && (long long)hi - lo + 1 > WBITS;
+    if (NARROW)
+    {
+        // Row pairs with very different A entry counts (an R-MAT hub row):
+        // all warps share the walk.  Balanced rows keep the warp-private walk,
+        // whose mask words no other warp touches.
+        int pc = 0;
+        if (tid < S2_WARPS && A.csr_rowptr != nullptr)
+        {
+            const int ra = min(2 * tid, nrows), rb = min(2 * tid + 2, nrows);
+            pc = __ldg(A.csr_rowptr + I * TD + rb) - __ldg(A.csr_rowptr + I * TD + ra);
+        }
+        int tot = pc;
+        for (int o = 4; o > 0; o >>= 1)
+            tot += __shfl_xor_sync(FULL, tot, o);
+        const bool skew = tid < S2_WARPS && pc > 32 && 2 * S2_WARPS * pc > 5 * tot;
+        const int any = __syncthreads_or(skew);
+        if (tid == 0)
+            S.share = any;
+    }
     int cbase = cbeg;
     for (long long wl = lo; hi >= 0 && wl <= hi;)
     {
@@ -305,9 +325,95 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
             mw[i] = 0u;
         __syncthreads();
 
-        // ---- masks: warp-private walk over the warp's A entries
-        if (r0 < nrows)
+        // ---- masks
+        if (NARROW && S.share)
         {
+            // several windows: a hub row would leave one warp walking while
+            // seven wait, so all warps share the tile row's A entries (the
+            // masks combine by OR, in any order); warp w takes every
+            // S2_WARPS-th A tile, so short tile rows are shared too
+            for (int t0 = a0; t0 < a1; t0 += S2_WARPS * 32)
+            {
+                const int t = t0 + lane * S2_WARPS + warp;
+                int n = 0, tn0 = 0, K = 0;
+                if (t < a1)
+                {
+                    tn0 = __ldg(A.tile_nnz + t);
+                    n = __ldg(A.tile_nnz + t + 1) - tn0;
+                    K = __ldg(A.tile_col + t);
+                }
+                const int incl = warp_incl_scan(n);
+                const int total = __shfl_sync(FULL, incl, 31);
+                for (int q0 = 0; q0 < total; q0 += 32)
+                {
+                    const int q = q0 + lane;
+                    int own = 0;
+#pragma unroll
+                    for (int b = 16; b > 0; b >>= 1)
+                        if (__shfl_sync(FULL, incl, own + b - 1) <= q)
+                            own += b;
+                    own = min(own, 31);
+                    const int o_incl = __shfl_sync(FULL, incl, own);
+                    const int o_n = __shfl_sync(FULL, n, own);
+                    const int o_tn0 = __shfl_sync(FULL, tn0, own);
+                    const int o_K = __shfl_sync(FULL, K, own);
+                    int fs = 0, len = 0, sh = 0, rb = 0;
+                    if (q < total)
+                    {
+                        const int pc = A.col[o_tn0 + q - (o_incl - o_n)]; // (row << 4) | col
+                        const int r = pc >> 4, k = o_K * TD + (pc & 15);
+                        if (r < nrows && k < B.m)
+                        {
+                            fs = min(max(__ldg(B.csr_rowptr + k), 0), B.nnz);
+                            len = min(max(__ldg(B.csr_rowptr + k + 1), fs), B.nnz) - fs;
+                            if (narrow && len > 32)
+                            {
+                                const int sb = lower_bound(B.csr_col, fs, fs + len, w * TD);
+                                len = lower_bound(B.csr_col, sb, fs + len, wend * TD) - sb;
+                                fs = sb;
+                            }
+                            sh = (r & 1) * 16;
+                            rb = (r >> 1) * S2_STRIDE;
+                        }
+                    }
+                    ent[lane] = make_int4(fs, len, sh, rb);
+                    __syncwarp();
+                    const int nbat = min(32, total - q0);
+                    auto mark = [&](int col, int sh, int rb) {
+                        const int d = (col >> 4) - w;
+                        if ((unsigned)d < (unsigned)wlen)
+                        {
+                            const int sl = S.slot8[d];
+                            if (sl != 255)
+                                atomicOr(&S.mw[rb + sl], (0x8000u >> (col & 15)) << sh);
+                        }
+                    };
+                    for (int j = 0; j < nbat; j += 2)
+                    {
+                        int4 e0 = ent[j], e1 = ent[(j + 1) & 31];
+                        if (j + 1 >= nbat)
+                            e1.y = 0;
+                        const int c0 = lane < e0.y ? __ldg(B.csr_col + e0.x + lane) : -1;
+                        const int c1 = lane < e1.y ? __ldg(B.csr_col + e1.x + lane) : -1;
+                        if (c0 >= 0)
+                            mark(c0, e0.z, e0.w);
+                        if (e0.y > 32) // rows longer than a warp (uniform branch)
+                            for (int f = 32 + lane; f < e0.y; f += 32)
+                                mark(__ldg(B.csr_col + e0.x + f), e0.z, e0.w);
+                        if (c1 >= 0)
+                            mark(c1, e1.z, e1.w);
+                        if (e1.y > 32)
+                            for (int f = 32 + lane; f < e1.y; f += 32)
+                                mark(__ldg(B.csr_col + e1.x + f), e1.z, e1.w);
+                    }
+                    __syncwarp(); // the next batch overwrites this warp's list
+                }
+            }
+            __syncthreads(); // every warp's rows are complete
+        }
+        else if (r0 < nrows)
+        {
+            // one window: warp-private walk over the warp's own A entries
             for (int t0 = a0; t0 < a1; t0 += 32)
             {
                 const int t = t0 + lane;
