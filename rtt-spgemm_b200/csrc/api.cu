@@ -627,8 +627,14 @@ void rtt_context_destroy(rtt_context c)
         if (c->hstage_ev[b] != nullptr)
             cudaEventDestroy(c->hstage_ev[b]);
     }
+    const int dev = c->ws.device;
     c->ws.destroy();
     delete c;
+    // hand the memory this context freed back to the driver
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+        cudaMemPoolTrimTo(pool, 0);
+    cudaGetLastError();
 }
 
 int rtt_context_set_stream(rtt_context c, void *stream)

@@ -75,13 +75,16 @@ __global__ void k_validate_csr(int m, int n, int nnz, const int *__restrict__ ro
 
 // -------------------------------------------------------------- fast path
 __global__ void __launch_bounds__(256) k_c2t_count(int m, int tilem, const int *__restrict__ rowptr,
-                                                   const int *__restrict__ col, int *__restrict__ cnt)
+                                                   const int *__restrict__ col, int *__restrict__ cnt,
+                                                   const uint8_t *__restrict__ heavy)
 {
     const int lane = threadIdx.x & 31, hl = lane & 15;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int I = gw * 2 + (lane >> 4);
+    // heavy tile rows are counted by k_c2t_heavy_count
+    const bool mine = I < tilem && !(heavy != nullptr && heavy[I]);
     int p = 0, e = 0;
-    if (I < tilem && I * TD + hl < m)
+    if (mine && I * TD + hl < m)
     {
         p = rowptr[I * TD + hl];
         e = rowptr[I * TD + hl + 1];
@@ -102,7 +105,7 @@ __global__ void __launch_bounds__(256) k_c2t_count(int m, int tilem, const int *
             cur = p < e ? (__ldg(col + p) >> 4) : INT_MAX;
         }
     }
-    if (I < tilem && hl == 0)
+    if (mine && hl == 0)
         cnt[I] = count;
 }
 
@@ -114,12 +117,14 @@ __global__ void __launch_bounds__(256) k_c2t_fill(int m, int tilem, const int *_
                                                   int *__restrict__ o_tnnz, uint8_t *__restrict__ o_ptr,
                                                   uint8_t *__restrict__ o_col,
                                                   double *__restrict__ o_val,
-                                                  uint16_t *__restrict__ o_mask, int packed, int *err)
+                                                  uint16_t *__restrict__ o_mask, int packed, int *err,
+                                                  const uint8_t *__restrict__ heavy)
 {
     const int lane = threadIdx.x & 31, hl = lane & 15;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int I = gw * 2 + (lane >> 4);
-    const bool tr_ok = I < tilem;
+    // heavy tile rows are filled by k_c2t_heavy_fill
+    const bool tr_ok = I < tilem && !(heavy != nullptr && heavy[I]);
     int p = 0, e = 0, base = 0, t = 0, tend = 0;
     if (tr_ok)
     {
@@ -177,6 +182,310 @@ __global__ void __launch_bounds__(256) k_c2t_fill(int m, int tilem, const int *_
             ++t;
             p = q;
             cur = p < e ? (__ldg(col + p) >> 4) : INT_MAX;
+        }
+    }
+}
+
+// ------------------------------------------------ fast path, heavy tile rows
+// A tile row holding a row with thousands of entries (an R-MAT hub) spans
+// thousands of tile columns; the half-warp above takes them one per step and
+// becomes the tail of the launch.  Such tile rows get a CTA each: the tile
+// columns of the 16 rows become a bitmap, a tile's index is the rank of its
+// bit, and since each row's tile columns are non-decreasing, the entries of
+// one (tile, row) are one run in the row (at most 16 entries unless columns
+// repeat), found and written by the thread that holds its first entry.  Entry
+// order inside a (tile, row) stays the CSR order, as on the half-warp path.
+constexpr int HV_ENTRIES = 2048;            // tile rows with more entries take this path
+constexpr int HV_WORDS = 4096;              // bitmap words: 131072 tile columns
+constexpr int HV_THREADS = 256;
+constexpr int HV_CHUNK = 2048;              // tiles written per pass
+
+struct HeavySmem
+{
+    uint32_t bits[HV_WORDS];
+    int pre[HV_WORDS + 1];      // set bits before each word
+    uint8_t cnt[HV_CHUNK][TD];  // entries per (tile of the pass, row)
+    int tbase[HV_CHUNK + 1];    // entries of the pass's tiles before each tile
+    int rs[TD + 1], re[TD];     // rows' entry ranges in the pass
+    int rpre[TD + 1];           // prefix of the ranges' lengths
+    int jlo, count;
+};
+
+// First entry of [b, e) whose tile column is >= J (the row's tile columns are
+// non-decreasing).
+__device__ __forceinline__ int tile_lower_bound(const int *col, int b, int e, int J)
+{
+    while (b < e)
+    {
+        const int mid = (b + e) >> 1;
+        if ((__ldg(col + mid) >> 4) < J)
+            b = mid + 1;
+        else
+            e = mid;
+    }
+    return b;
+}
+
+// Marks heavy tile rows (flag and list); thread per tile row.
+__global__ void k_c2t_heavy_mark(int m, int tilem, const int *__restrict__ rowptr,
+                                 const int *__restrict__ col, uint8_t *__restrict__ heavy,
+                                 int *__restrict__ list, int *__restrict__ count)
+{
+    const int I = blockIdx.x * blockDim.x + threadIdx.x;
+    if (I >= tilem)
+        return;
+    const int r0 = I * TD, r1 = min(r0 + TD, m);
+    bool hv = rowptr[r1] - rowptr[r0] > HV_ENTRIES;
+    if (hv)
+    {
+        int lo = INT_MAX, hi = -1;
+        for (int r = r0; r < r1; ++r)
+        {
+            const int b = rowptr[r], e = rowptr[r + 1];
+            if (b < e)
+            {
+                lo = min(lo, __ldg(col + b) >> 4);
+                hi = max(hi, __ldg(col + e - 1) >> 4);
+            }
+        }
+        hv = hi >= lo && hi - lo < HV_WORDS * 32;
+    }
+    heavy[I] = hv;
+    if (hv)
+        list[atomicAdd(count, 1)] = I;
+}
+
+// The heavy tile row's tile-column bitmap and the set bits before each word.
+__device__ void heavy_bitmap(HeavySmem &S, int I, int m, const int *__restrict__ rowptr,
+                             const int *__restrict__ col)
+{
+    const int tid = threadIdx.x;
+    const int r0 = I * TD, r1 = min(r0 + TD, m);
+    if (tid == 0)
+        S.jlo = INT_MAX;
+    for (int i = tid; i < HV_WORDS; i += HV_THREADS)
+        S.bits[i] = 0u;
+    __syncthreads();
+    if (tid < r1 - r0)
+    {
+        const int b = rowptr[r0 + tid];
+        if (b < rowptr[r0 + tid + 1])
+            atomicMin(&S.jlo, __ldg(col + b) >> 4);
+    }
+    __syncthreads();
+    const int jlo = S.jlo;
+    const int s0 = rowptr[r0], s1 = rowptr[r1];
+    for (int j = s0 + tid; j < s1; j += HV_THREADS)
+    {
+        const int d = (__ldg(col + j) >> 4) - jlo;
+        if ((unsigned)d < (unsigned)(HV_WORDS * 32)) // checked by the mark kernel
+            atomicOr(&S.bits[d >> 5], 1u << (d & 31));
+    }
+    __syncthreads();
+    if (tid < 32)
+    {
+        int run = 0;
+        for (int q0 = 0; q0 < HV_WORDS; q0 += 32)
+        {
+            const int v = __popc(S.bits[q0 + tid]);
+            const int incl = warp_incl_scan(v);
+            S.pre[q0 + tid] = run + incl - v;
+            run += __shfl_sync(FULL, incl, 31);
+        }
+        if (tid == 0)
+        {
+            S.pre[HV_WORDS] = run;
+            S.count = run;
+        }
+    }
+    __syncthreads();
+}
+
+// Tile column of the k-th set bit.
+__device__ __forceinline__ int heavy_select(const HeavySmem &S, int k)
+{
+    int lo = 0, hi = HV_WORDS - 1; // last word with pre <= k
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (S.pre[mid] <= k)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    uint32_t w = S.bits[lo];
+    for (int i = S.pre[lo]; i < k; ++i)
+        w &= w - 1;
+    return S.jlo + lo * 32 + __ffs(w) - 1;
+}
+
+__device__ __forceinline__ int heavy_rank(const HeavySmem &S, int J)
+{
+    const int d = J - S.jlo;
+    return S.pre[d >> 5] + __popc(S.bits[d >> 5] & ((1u << (d & 31)) - 1u));
+}
+
+__global__ void __launch_bounds__(HV_THREADS)
+    k_c2t_heavy_count(int m, const int *__restrict__ list, const int *__restrict__ count,
+                      const int *__restrict__ rowptr, const int *__restrict__ col,
+                      int *__restrict__ cnt)
+{
+    extern __shared__ __align__(16) unsigned char hv_dyn[];
+    HeavySmem &S = *reinterpret_cast<HeavySmem *>(hv_dyn);
+    const int n = *count;
+    for (int li = blockIdx.x; li < n; li += gridDim.x)
+    {
+        const int I = list[li];
+        heavy_bitmap(S, I, m, rowptr, col);
+        if (threadIdx.x == 0)
+            cnt[I] = S.count;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(HV_THREADS)
+    k_c2t_heavy_fill(int m, const int *__restrict__ list, const int *__restrict__ count,
+                     const int *__restrict__ rowptr, const int *__restrict__ col,
+                     const double *__restrict__ val, const int *__restrict__ tile_ptr,
+                     int *__restrict__ o_tcol, int *__restrict__ o_trow,
+                     int *__restrict__ o_tnnz, uint8_t *__restrict__ o_ptr,
+                     uint8_t *__restrict__ o_col, double *__restrict__ o_val,
+                     uint16_t *__restrict__ o_mask, int packed, int *err)
+{
+    extern __shared__ __align__(16) unsigned char hv_dyn[];
+    HeavySmem &S = *reinterpret_cast<HeavySmem *>(hv_dyn);
+    const int tid = threadIdx.x;
+    const int n = *count;
+    for (int li = blockIdx.x; li < n; li += gridDim.x)
+    {
+        const int I = list[li];
+        const int r0 = I * TD, nr = min(TD, m - r0);
+        heavy_bitmap(S, I, m, rowptr, col);
+        const int ntiles = S.count, t0 = tile_ptr[I];
+        if (t0 + ntiles != tile_ptr[I + 1])
+        {
+            if (tid == 0)
+                set_error(err, DERR_C2T_OVERFLOW);
+            __syncthreads();
+            continue;
+        }
+        int base = rowptr[r0]; // entries of the tile row before the pass
+        for (int k0 = 0; k0 < ntiles; k0 += HV_CHUNK)
+        {
+            const int k1 = min(k0 + HV_CHUNK, ntiles), nk = k1 - k0;
+            // the pass's entries: per row, the run of tile columns [Ja, Jb]
+            if (tid < TD)
+            {
+                int b = 0, e = 0;
+                if (tid < nr)
+                {
+                    const int Ja = heavy_select(S, k0), Jb = heavy_select(S, k1 - 1);
+                    const int rb = rowptr[r0 + tid], rend = rowptr[r0 + tid + 1];
+                    b = tile_lower_bound(col, rb, rend, Ja);
+                    e = tile_lower_bound(col, b, rend, Jb + 1);
+                }
+                S.rs[tid] = b;
+                S.re[tid] = e;
+            }
+            for (int i = tid; i < nk * TD; i += HV_THREADS)
+                S.cnt[i >> 4][i & 15] = 0;
+            __syncthreads();
+            if (tid == 0)
+            {
+                int t = 0;
+                for (int r = 0; r < TD; ++r)
+                {
+                    S.rpre[r] = t;
+                    t += S.re[r] - S.rs[r];
+                }
+                S.rpre[TD] = t;
+            }
+            __syncthreads();
+            const int total = S.rpre[TD];
+            // pass 1: run lengths per (tile, row); a run starts where the
+            // tile column changes inside the row
+            for (int i = tid; i < total; i += HV_THREADS)
+            {
+                int r = 0;
+                while (S.rpre[r + 1] <= i)
+                    ++r;
+                const int j = S.rs[r] + (i - S.rpre[r]);
+                const int J = __ldg(col + j) >> 4;
+                if (j == S.rs[r] || (__ldg(col + j - 1) >> 4) != J)
+                {
+                    int e = j + 1;
+                    while (e < S.re[r] && (__ldg(col + e) >> 4) == J)
+                        ++e;
+                    if (e - j > 255) // repeated columns beyond a u8 row offset
+                        set_error(err, DERR_C2T_OVERFLOW);
+                    S.cnt[heavy_rank(S, J) - k0][r] = (uint8_t)min(e - j, 255);
+                }
+            }
+            __syncthreads();
+            // per tile: row offsets, size, column, tile row, empty masks
+            for (int t = tid; t < nk; t += HV_THREADS)
+            {
+                int run = 0;
+                const size_t g = (size_t)(t0 + k0 + t);
+#pragma unroll
+                for (int r = 0; r < TD; ++r)
+                {
+                    o_ptr[g * TD + r] = (uint8_t)run;
+                    if (S.cnt[t][r] == 0)
+                        o_mask[g * TD + r] = 0;
+                    run += S.cnt[t][r];
+                }
+                S.tbase[t + 1] = run;
+                o_tcol[g] = heavy_select(S, k0 + t);
+                o_trow[g] = I;
+            }
+            __syncthreads();
+            if (tid < 32)
+            {
+                int acc = 0;
+                for (int q0 = 0; q0 < nk; q0 += 32)
+                {
+                    const int v = q0 + tid < nk ? S.tbase[q0 + tid + 1] : 0;
+                    const int incl = warp_incl_scan(v);
+                    if (q0 + tid < nk)
+                        S.tbase[q0 + tid] = acc + incl - v;
+                    acc += __shfl_sync(FULL, incl, 31);
+                }
+                if (tid == 0)
+                    S.tbase[nk] = acc;
+            }
+            __syncthreads();
+            for (int t = tid; t < nk; t += HV_THREADS)
+                o_tnnz[t0 + k0 + t] = base + S.tbase[t];
+            // pass 2: each run's first entry writes the run and its mask
+            for (int i = tid; i < total; i += HV_THREADS)
+            {
+                int r = 0;
+                while (S.rpre[r + 1] <= i)
+                    ++r;
+                const int j = S.rs[r] + (i - S.rpre[r]);
+                const int J = __ldg(col + j) >> 4;
+                if (j == S.rs[r] || (__ldg(col + j - 1) >> 4) != J)
+                {
+                    const int t = heavy_rank(S, J) - k0;
+                    int off = 0;
+                    for (int rr = 0; rr < r; ++rr)
+                        off += S.cnt[t][rr];
+                    int dst = base + S.tbase[t] + off;
+                    const int len = S.cnt[t][r]; // the run, as counted in pass 1
+                    uint16_t mk = 0;
+                    for (int e = j; e < j + len; ++e, ++dst)
+                    {
+                        const int cc = __ldg(col + e) & 15;
+                        mk |= (uint16_t)(0x8000u >> cc);
+                        o_col[dst] = (uint8_t)(packed ? ((r << 4) | cc) : cc);
+                        o_val[dst] = __ldg(val + e);
+                    }
+                    o_mask[(size_t)(t0 + k0 + t) * TD + r] = mk;
+                }
+            }
+            base += S.tbase[nk];
+            __syncthreads();
         }
     }
 }
@@ -518,9 +827,36 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
     out.dup_cols = ws.h_scalars[6] != 0 || unsorted;
 
     int *cnt = out.tmp0.as<int>();
+    // heavy tile rows (a CTA each) are listed on the device; their kernels
+    // take the list length from device memory, so no host read is needed
+    uint8_t *heavy = nullptr;
+    int *hv_list = nullptr, *hv_count = flags + 3;
+    int hv_grid = 0;
+    const size_t hv_smem = sizeof(HeavySmem);
+    if (!generic)
+    {
+        RTT_CHECK(out.tmp2.ensure((size_t)tilem + 16, s));
+        RTT_CHECK(out.tmp3.ensure(sizeof(int) * (size_t)tilem + 16, s));
+        heavy = out.tmp2.as<uint8_t>();
+        hv_list = out.tmp3.as<int>();
+        RTT_CUDA(cudaMemsetAsync(hv_count, 0, sizeof(int), s));
+        k_c2t_heavy_mark<<<grid_for(tilem, 256), 256, 0, s>>>(m, tilem, rowptr, col, heavy,
+                                                              hv_list, hv_count);
+        ws.launches++;
+        int sms = 0;
+        RTT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws.device));
+        hv_grid = std::min(tilem, 2 * sms);
+        RTT_CUDA(cudaFuncSetAttribute(k_c2t_heavy_count, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)hv_smem));
+        RTT_CUDA(cudaFuncSetAttribute(k_c2t_heavy_fill, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)hv_smem));
+        k_c2t_heavy_count<<<hv_grid, HV_THREADS, hv_smem, s>>>(m, hv_list, hv_count, rowptr, col,
+                                                               cnt);
+        ws.launches++;
+    }
     if (!generic)
         k_c2t_count<<<grid_for((long long)ceil_div(tilem, 2) * 32, 256), 256, 0, s>>>(m, tilem, rowptr,
-                                                                                   col, cnt);
+                                                                                   col, cnt, heavy);
     else
         k_c2t_count_generic<<<grid_for((long long)tilem * 32, 256), 256, 0, s>>>(m, tilem, rowptr,
                                                                                col, cnt);
@@ -543,7 +879,7 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
             m, tilem, rowptr, col, val, out.tile_ptr.as<int>(), out.tile_col.as<int>(),
             out.tile_row.as<int>(), out.tile_nnz.as<int>(), out.ptr.as<uint8_t>(),
             out.col.as<uint8_t>(), out.val.as<double>(), out.mask.as<uint16_t>(), packed_col ? 1 : 0,
-            ws.err.as<int>());
+            ws.err.as<int>(), heavy);
     else
         k_c2t_fill_generic<<<grid_for((long long)tilem * 32, 128), 128, 0, s>>>(
             m, tilem, rowptr, col, val, out.tile_ptr.as<int>(), out.tile_col.as<int>(),
@@ -551,6 +887,15 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
             out.col.as<uint8_t>(), out.val.as<double>(), out.mask.as<uint16_t>(), packed_col ? 1 : 0,
             ws.err.as<int>());
     ws.launches++;
+    if (!generic)
+    {
+        k_c2t_heavy_fill<<<hv_grid, HV_THREADS, hv_smem, s>>>(
+            m, hv_list, hv_count, rowptr, col, val, out.tile_ptr.as<int>(), out.tile_col.as<int>(),
+            out.tile_row.as<int>(), out.tile_nnz.as<int>(), out.ptr.as<uint8_t>(),
+            out.col.as<uint8_t>(), out.val.as<double>(), out.mask.as<uint16_t>(),
+            packed_col ? 1 : 0, ws.err.as<int>());
+        ws.launches++;
+    }
     k_set_int<<<1, 1, 0, s>>>(out.tile_nnz.as<int>() + numtile, nnz);
     ws.launches++;
     if (sort_within_rows && unsorted && numtile > 0)

@@ -105,11 +105,14 @@ int Workspace::init(int dev)
         return fail(RTT_ERR_NO_DEVICE, "this library is built for sm_100a (B200); found sm_" +
                                            std::to_string(prop.major * 10 + prop.minor));
     {
-        // keep memory freed to the default pool cached in this process
+        // the default pool keeps up to 8 GiB of freed memory for reuse (a
+        // regrow then costs no driver allocation); above that it returns
+        // memory at synchronisations, so it does not starve other
+        // allocators of the process (a framework's caching allocator)
         cudaMemPool_t pool;
         if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
         {
-            uint64_t keep = UINT64_MAX;
+            uint64_t keep = 8ull << 30;
             cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         }
         cudaGetLastError();
@@ -136,6 +139,8 @@ void Workspace::destroy()
 {
     err.release();
     scan_tmp.release();
+    for (DevBuf &b : tmp)
+        b.release();
     if (h_scalars != nullptr)
         cudaFreeHost(h_scalars);
     if (h_scalars64 != nullptr)

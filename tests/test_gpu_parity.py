@@ -21,6 +21,25 @@ def _empty(m, n):
     return G.CSR(m, n, np.zeros(m + 1, np.int32), np.zeros(0, np.int32), np.zeros(0))
 
 
+def _hub_rows(m, n, hubs, hub_len, other_len, seed, dup_every=0):
+    """Rows of other_len random sorted columns plus hub rows of hub_len: tile
+    rows above 2048 entries take csr2tile's CTA-per-tile-row path.  dup_every
+    repeats every dup_every-th hub column a few times (sorted, so the tile
+    columns stay non-decreasing)."""
+    rng = np.random.default_rng(seed)
+    rows = []
+    for i in range(m):
+        k = hub_len if i in hubs else other_len
+        c = np.sort(rng.choice(n, size=min(k, n), replace=False))
+        if dup_every and i in hubs:
+            c = np.sort(np.concatenate([c, np.repeat(c[::dup_every], 3)]))
+        rows.append(c)
+    rp = np.zeros(m + 1, np.int32)
+    rp[1:] = np.cumsum([len(c) for c in rows])
+    col = np.concatenate(rows).astype(np.int32)
+    return G.CSR(m, n, rp, col, rng.uniform(-1, 1, col.size))
+
+
 CASES = {
     "lap2d_16": lambda: G.laplacian_2d(16),
     "lap2d_64": lambda: G.laplacian_2d(64),
@@ -37,8 +56,14 @@ CASES = {
     "empty_0x0": lambda: _empty(0, 0),
     "empty_10x10": lambda: _empty(10, 10),
     "one": lambda: G.CSR(1, 1, np.array([0, 1], np.int32), np.array([0], np.int32), np.array([2.5])),
+    # heavy tile rows: one pass, many passes (> 2048 tiles), repeated columns,
+    # and a column span past the bitmap (back to the half-warp path)
+    "hub_rows": lambda: _hub_rows(70, 60000, {3, 17, 40}, 5000, 20, seed=7),
+    "hub_many_tiles": lambda: _hub_rows(40, 1000000, {5}, 40000, 30, seed=8),
+    "hub_dups": lambda: _hub_rows(40, 20000, {1, 2}, 3000, 10, seed=9, dup_every=5),
+    "hub_wide_span": lambda: _hub_rows(20, 3000000, {4}, 6000, 5, seed=10),
 }
-SQUARE = [k for k in CASES if k not in ("rand_rect",)]
+SQUARE = [k for k in CASES if k != "rand_rect" and not k.startswith("hub")]
 
 ROW_KEYS = ["m", "n", "tilem", "tilen", "numtile", "tile_ptr", "tile_columnidx", "tile_rowidx",
             "tile_nnz", "tile_csr_Ptr", "tile_csr_Col", "tile_csr_Value", "mask"]
