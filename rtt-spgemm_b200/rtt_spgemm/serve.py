@@ -89,6 +89,32 @@ class Server:
         self.keep_results = keep_results
         self.resident: OrderedDict = OrderedDict()
         self.lock = threading.Lock()
+        # one (stream, context) per worker, kept across run() calls: their
+        # grow-only device buffers stay sized for the traffic seen so far
+        self._slots = []
+
+    def _slot(self, i):
+        torch = self.torch
+        with self.lock:
+            while len(self._slots) <= i:
+                stream = torch.cuda.Stream(device=self.device)
+                ctx = Context(self.device.index or 0, self.config)
+                ctx.set_stream(stream.cuda_stream)
+                self._slots.append((stream, ctx))
+            return self._slots[i]
+
+    def close(self):
+        """Release the workers' contexts and the resident operands."""
+        for _, ctx in self._slots:
+            ctx.close()
+        self._slots = []
+        self.resident.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     # -- operands -------------------------------------------------------
     def _upload(self, a: CSR, ctx: Context):
@@ -183,19 +209,16 @@ class Server:
             reserved[0] += need
             return batch, need
 
-        def worker():
+        def worker(i):
             torch = self.torch
             torch.cuda.set_device(self.device)
-            stream = torch.cuda.Stream(device=self.device)
-            ctx = Context(self.device.index or 0, self.config)
-            ctx.set_stream(stream.cuda_stream)
+            stream, ctx = self._slot(i)
             with torch.cuda.stream(stream):
                 while True:
                     with cv:
                         batch, need = take_batch()
                         while not batch:
                             if nxt >= n and not pending:
-                                ctx.close()
                                 return
                             wait = 0.0005
                             if nxt < n and not pending:
@@ -208,7 +231,7 @@ class Server:
                         done[0] += len(batch)
                         cv.notify_all()
 
-        threads = [threading.Thread(target=worker) for _ in range(self.nworkers)]
+        threads = [threading.Thread(target=worker, args=(i,)) for i in range(self.nworkers)]
         for th in threads:
             th.start()
         for th in threads:
@@ -217,12 +240,16 @@ class Server:
         return summarize(requests, span)
 
 
-def serve_plain(requests: list[Request], device: int = 0, config: dict | None = None) -> dict:
-    """The plain path under the same arrivals: one product per call, FIFO."""
+def serve_plain(requests: list[Request], device: int = 0, config: dict | None = None,
+                keep_results: bool = True, ctx: Context | None = None) -> dict:
+    """The plain path under the same arrivals: one product per call, FIFO.
+    A caller-owned ctx is used and kept (its buffers stay grown)."""
     import torch
 
     dev = torch.device("cuda", device)
-    ctx = Context(device, config)
+    own = ctx is None
+    if own:
+        ctx = Context(device, config)
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
     resident = {}
@@ -244,11 +271,12 @@ def serve_plain(requests: list[Request], device: int = 0, config: dict | None = 
             va = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
             ctx.numeric(rp, ci, va)
             stream.synchronize()
-            r.result = (rp, ci[:nnz], va[:nnz])
+            r.result = (rp, ci[:nnz], va[:nnz]) if keep_results else None
         except RttError as e:
             r.error = str(e)
         r.done = time.perf_counter() - t0
-    ctx.close()
+    if own:
+        ctx.close()
     return summarize(requests, max(r.done for r in requests) if requests else 0.0)
 
 
