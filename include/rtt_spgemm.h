@@ -288,6 +288,25 @@ RTT_API int rtt_plan_early_split(int ntasks, const int *scans, const int *matche
                                  const rtt_tail_cost_model *model, int sm_count,
                                  int *chunks_out, rtt_early_split_plan *plan);
 
+/* Row / inner (K) reorder plan of A (the reference's DmmaReorderPlan,
+ * src/dmma_reorder.h:173-224, reduced to its maps and counters).  Maps are
+ * host arrays malloc'd by rtt_reorder_plan_build (rtt_reorder_plan_destroy
+ * frees them); new = old_to_new[old], old = new_to_old[new]. */
+typedef struct
+{
+    int rows, cols, nnz;
+    int active_rows, active_inner; /* rows / columns reached by the traversal */
+    int components, levels;        /* components traversed, traversal levels */
+    int accepted;                  /* 1: the proposal has fewer 8x4 A tiles and is the plan;
+                                      0: the plan is the identity */
+    long long tiles_before;        /* distinct 8x4 tiles of A as given */
+    long long tiles_after;         /* ... under the plan (never more than tiles_before) */
+    long long proposal_tiles;      /* ... under the traversal's proposal */
+    long long moved_rows, moved_inner;
+    int *row_old_to_new, *row_new_to_old;
+    int *inner_old_to_new, *inner_new_to_old;
+} rtt_reorder_plan;
+
 /* Frees the arrays of a hybrid tile matrix and zeroes it (the reference's
  * destroy_hybrid_tile_matrix, src/dmma_tiles.h:64-79). */
 RTT_API void rtt_hybrid_tiles_destroy(rtt_hybrid_tiles *tiles);
@@ -442,6 +461,27 @@ RTT_API int rtt_spgemm_batched_symbolic(rtt_context ctx, int count, const rtt_cs
  * uses it to turn A*A^T requests into A*B instances of one batch. */
 RTT_API int rtt_csr_transpose(rtt_context ctx, const rtt_csr_view *A, int *t_row_ptr,
                               int *t_col_idx, double *t_values);
+
+/* Replaces build_dmma_reorder_plan (src/dmma_reorder.h:2651) for a device CSR
+ * A: a bipartite Cuthill-McKee traversal of A's rows and columns proposes a
+ * joint row / K order, committed only if it cuts A's distinct 8x4 tiles (the
+ * reference's exact commit rule, :1671-1727), else the identity.  The
+ * reference's fine passes that pack 8x4 tensor-core groups are not
+ * performed, so its permutations are not reproduced; the commit guarantee
+ * is.  With A' = P A Q^T and B' = Q B, C' = A' B' = P C.  Uses the context's
+ * tile buffers as scratch (a following product starts with
+ * rtt_spgemm_symbolic). */
+RTT_API int rtt_reorder_plan_build(rtt_context ctx, const rtt_csr_view *A, rtt_reorder_plan *plan);
+RTT_API void rtt_reorder_plan_destroy(rtt_reorder_plan *plan);
+
+/* Device CSR permutation: out row i = A row row_new_to_old[i] (NULL: i), each
+ * column c replaced by col_old_to_new[c] (NULL: c) and every row sorted by
+ * its new columns (stable).  Maps are device arrays and must be
+ * permutations (else RTT_ERR_DEVICE_CHECK); out_row_ptr has A->rows + 1
+ * entries, out_col_idx / out_values A->nnz. */
+RTT_API int rtt_csr_permute(rtt_context ctx, const rtt_csr_view *A, const int *row_new_to_old,
+                            const int *col_old_to_new, int *out_row_ptr, int *out_col_idx,
+                            double *out_values);
 
 /* Writes the products of the last batched symbolic.  c_row_ptr: the
  * instances' row pointers one after another (instance i's A_i.rows + 1

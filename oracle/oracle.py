@@ -221,6 +221,74 @@ def csr_to_hybrid_tiles(csr, tile_rows: int, tile_cols: int, col_major: bool,
     return d
 
 
+def tiles_8x4(a, row_old_to_new=None, col_old_to_new=None) -> int:
+    """Distinct 8x4 tiles of A under row / column maps: the quantity of the
+    reference's exact reorder commit rule (src/dmma_reorder.h:1671-1727)."""
+    rows = np.repeat(np.arange(a.m), np.diff(a.rowptr))
+    cols = np.asarray(a.col, np.int64)
+    if row_old_to_new is not None:
+        rows = np.asarray(row_old_to_new)[rows]
+    if col_old_to_new is not None:
+        cols = np.asarray(col_old_to_new)[cols]
+    keys = (rows.astype(np.int64) // 8) * ((a.n + 3) // 4) + cols // 4
+    return int(np.unique(keys).size)
+
+
+def reorder_cm(a, max_components: int = 256):
+    """Restatement of the reorder proposal of this build (rtt_reorder_plan_build):
+    a breadth-first traversal alternating rows and columns, each level ordered
+    by (position of the earliest-placed neighbour, degree, index); components
+    start at the unplaced row of least (degree, index); unreached rows and
+    columns follow in index order.  Returns (row_old_to_new, col_old_to_new,
+    components, levels).  Pure Python: small inputs only."""
+    m, n = a.m, a.n
+    rp = np.asarray(a.rowptr, np.int64)
+    col = np.asarray(a.col, np.int64)
+    deg_r = np.diff(rp)
+    rows_of = np.repeat(np.arange(m), deg_r)
+    o = np.lexsort((rows_of, col))
+    tcol_rows = rows_of[o]
+    tp = np.zeros(n + 1, np.int64)
+    tp[1:] = np.cumsum(np.bincount(col, minlength=n))
+    deg_c = np.diff(tp)
+    adj_r = [col[rp[i]:rp[i + 1]] for i in range(m)]
+    adj_c = [tcol_rows[tp[j]:tp[j + 1]] for j in range(n)]
+    pos = [np.full(m, -1, np.int64), np.full(n, -1, np.int64)]
+    deg = [deg_r, deg_c]
+    adj = [adj_r, adj_c]
+    placed = [0, 0]
+    comps = levels = 0
+    for _ in range(max_components):
+        cand = np.nonzero((pos[0] == -1) & (deg_r > 0))[0]
+        if cand.size == 0:
+            break
+        r0 = int(cand[np.lexsort((cand, deg_r[cand]))[0]])
+        comps += 1
+        pos[0][r0] = placed[0]
+        placed[0] += 1
+        front, side = [r0], 0
+        while front:
+            other = 1 - side
+            claim = {}
+            for v in front:
+                pv = pos[side][v]
+                for u in adj[side][v]:
+                    u = int(u)
+                    if pos[other][u] == -1:
+                        claim[u] = min(claim.get(u, 1 << 62), pv)
+            new = sorted(claim, key=lambda u: (claim[u], deg[other][u], u))
+            for i, u in enumerate(new):
+                pos[other][u] = placed[other] + i
+            placed[other] += len(new)
+            if new:
+                levels += 1
+            front, side = new, other
+    for s in (0, 1):
+        rest = np.nonzero(pos[s] == -1)[0]
+        pos[s][rest] = placed[s] + np.arange(rest.size)
+    return pos[0], pos[1], comps, levels
+
+
 def plan_tail_queue(scans, matches, output_nnz, policy: dict, model: dict):
     """Restatement of dmma_plan_tile_tail_queue (src/dmma_tile_tail_queue.h:190-291)
     with the chunk rule of :148-176 in numpy float32 (round-to-nearest, no

@@ -1463,6 +1463,43 @@ int rtt_spgemm_batched_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, do
     return RTT_OK;
 }
 
+int rtt_reorder_plan_build(rtt_context c, const rtt_csr_view *A, rtt_reorder_plan *plan)
+{
+    if (c == nullptr || A == nullptr || plan == nullptr || !view_ok(*A))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "reorder_plan_build: bad arguments");
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    // the traversal trusts A's structure: validate it like csr2tile does
+    RTT_CHECK(map_device_error(csr2tile_device(c->ws, A->rows, A->cols, (int)A->nnz, A->row_ptr,
+                                               A->col_idx, A->values, c->A, true, false)));
+    c->have_symbolic = false; // the context's A tiles were reused as scratch
+    return rtt::reorder_plan_device(c->ws, *A, plan);
+}
+
+void rtt_reorder_plan_destroy(rtt_reorder_plan *plan)
+{
+    if (plan == nullptr)
+        return;
+    std::free(plan->row_old_to_new);
+    std::free(plan->row_new_to_old);
+    std::free(plan->inner_old_to_new);
+    std::free(plan->inner_new_to_old);
+    std::memset(plan, 0, sizeof(*plan));
+}
+
+int rtt_csr_permute(rtt_context c, const rtt_csr_view *A, const int *row_new_to_old,
+                    const int *col_old_to_new, int *out_row_ptr, int *out_col_idx,
+                    double *out_values)
+{
+    if (c == nullptr || A == nullptr || !view_ok(*A) || out_row_ptr == nullptr ||
+        (A->nnz > 0 && (out_col_idx == nullptr || out_values == nullptr)))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "csr_permute: bad arguments");
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    RTT_CHECK(rtt::csr_permute_device(c->ws, *A, row_new_to_old, col_old_to_new, out_row_ptr,
+                                      out_col_idx, out_values));
+    RTT_CUDA(cudaStreamSynchronize(c->ws.stream));
+    return RTT_OK;
+}
+
 int rtt_csr_transpose(rtt_context c, const rtt_csr_view *A, int *t_row_ptr, int *t_col_idx,
                       double *t_values)
 {

@@ -244,6 +244,11 @@ int build_tile_csc(Workspace &ws, TileBufs &t);
 // rearrange row-major tiles into the csr2tile_col_major layout (data in CSC order)
 int tiles_to_col_major(Workspace &ws, const TileBufs &rowmajor, TileBufs &out);
 // CSR transpose on the device
+// bipartite Cuthill-McKee reorder plan of a device CSR (host maps malloc'd)
+int reorder_plan_device(Workspace &ws, const rtt_csr_view &A, rtt_reorder_plan *plan);
+// device CSR with permuted rows and remapped (then sorted) columns
+int csr_permute_device(Workspace &ws, const rtt_csr_view &A, const int *row_new_to_old,
+                       const int *col_old_to_new, int *out_rp, int *out_col, double *out_val);
 // A^T of a device CSR into caller-sized arrays (n + 1, nnz, nnz), sorted rows;
 // enqueued on ws.stream, scratch from ws.tmp
 int csr_transpose_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,

@@ -28,8 +28,8 @@ import numpy as np
 
 from . import generators
 from ._abi import (EXPORTS, LIB_PATH, RTT_OP_AAT, RTT_OP_AB, Config, CsrView, EarlySplitPlan,
-                   HybridTiles, RttError, SMatrix, Stats, TailCostModel, TailPlan, TailPolicy,
-                   build, check, lib)
+                   HybridTiles, ReorderPlan, RttError, SMatrix, Stats, TailCostModel, TailPlan,
+                   TailPolicy, build, check, lib)
 from .generators import CSR
 
 __all__ = ["CSR", "Context", "RttError", "build", "csr2tile_col_major", "csr2tile_row_major",
@@ -373,6 +373,36 @@ class Context:
                                                    C.c_void_p(val.data_ptr())))
         finally:
             self._borrowed = None
+
+    def reorder_plan(self, a) -> dict:
+        """Row / inner reorder plan of a device CSR tuple (rtt_reorder_plan_build,
+        the reference's build_dmma_reorder_plan): counters and numpy maps."""
+        v = self._view(*a)
+        p = ReorderPlan()
+        check(lib().rtt_reorder_plan_build(self.handle, C.byref(v), C.byref(p)))
+        out = {k: getattr(p, k) for k, t in ReorderPlan._fields_ if t is not C.POINTER(C.c_int)}
+        for k, n in (("row_old_to_new", p.rows), ("row_new_to_old", p.rows),
+                     ("inner_old_to_new", p.cols), ("inner_new_to_old", p.cols)):
+            out[k] = np.ctypeslib.as_array(getattr(p, k), shape=(n,)).copy() if n else \
+                np.zeros(0, np.int32)
+        lib().rtt_reorder_plan_destroy(C.byref(p))
+        return out
+
+    def permute(self, a, row_new_to_old=None, col_old_to_new=None):
+        """rtt_csr_permute: rows taken in row_new_to_old order, columns mapped by
+        col_old_to_new (device int32 tensors or None), rows re-sorted."""
+        import torch
+
+        rows, cols, rp, ci, va = a
+        nnz = int(ci.numel())
+        orp = torch.empty(rows + 1, dtype=torch.int32, device=rp.device)
+        oci = torch.empty(max(nnz, 1), dtype=torch.int32, device=rp.device)
+        ova = torch.empty(max(nnz, 1), dtype=torch.float64, device=rp.device)
+        v = self._view(*a)
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        check(lib().rtt_csr_permute(self.handle, C.byref(v), ptr(row_new_to_old),
+                                    ptr(col_old_to_new), ptr(orp), ptr(oci), ptr(ova)))
+        return (rows, cols, orp, oci[:nnz], ova[:nnz])
 
     def transpose(self, a):
         """A^T of a device CSR tuple, as a device CSR tuple (new tensors)."""

@@ -35,6 +35,7 @@ EXPORTS = [
     "rtt_tile2csr_device_noalloc", "rtt_csr_to_hybrid_tiles", "rtt_hybrid_tiles_destroy",
     "rtt_plan_tail_queue", "rtt_spgemm_batched_symbolic", "rtt_spgemm_batched_numeric",
     "rtt_csr_transpose", "rtt_early_split_policy_default", "rtt_plan_early_split",
+    "rtt_reorder_plan_build", "rtt_reorder_plan_destroy", "rtt_csr_permute",
 ]
 
 
@@ -113,6 +114,15 @@ class EarlySplitPlan(C.Structure):
         ("exact_parent_partition", C.c_int)]
 
 
+class ReorderPlan(C.Structure):
+    _fields_ = [(k, C.c_int) for k in ("rows", "cols", "nnz", "active_rows", "active_inner",
+                                        "components", "levels", "accepted")] + [
+        (k, C.c_longlong) for k in ("tiles_before", "tiles_after", "proposal_tiles",
+                                    "moved_rows", "moved_inner")] + [
+        (k, C.POINTER(C.c_int)) for k in ("row_old_to_new", "row_new_to_old", "inner_old_to_new",
+                                          "inner_new_to_old")]
+
+
 class Stats(C.Structure):
     _fields_ = [("nnz_a", C.c_longlong), ("nnz_b", C.c_longlong), ("nnz_c", C.c_longlong),
                 ("nnz_cub", C.c_longlong), ("tiles_a", C.c_longlong),
@@ -187,6 +197,11 @@ def lib() -> C.CDLL:
                                               P(C.c_longlong), P(C.c_longlong)]
     L.rtt_spgemm_batched_numeric.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.rtt_csr_transpose.argtypes = [C.c_void_p, P(CsrView), C.c_void_p, C.c_void_p, C.c_void_p]
+    L.rtt_reorder_plan_build.argtypes = [C.c_void_p, P(CsrView), P(ReorderPlan)]
+    L.rtt_reorder_plan_destroy.argtypes = [P(ReorderPlan)]
+    L.rtt_reorder_plan_destroy.restype = None
+    L.rtt_csr_permute.argtypes = [C.c_void_p, P(CsrView), C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p]
     _LIB = L
     return L
 
