@@ -432,6 +432,19 @@ RTT_API int rtt_spgemm_symbolic(rtt_context ctx, const rtt_csr_view *A,
 RTT_API int rtt_spgemm_numeric(rtt_context ctx, int *c_row_ptr, int *c_col_idx,
                        double *c_values);
 
+/* Values-only update (the reference's dynamic-B "values-only" mode,
+ * src/main.cu:26-32, :1406-1453, for A and B): the same product as the last
+ * rtt_spgemm_symbolic, with new values for A (a_values, device, A's CSR order)
+ * and B (b_values, B's CSR order; NULL keeps B's values; ignored for
+ * C = A*A and C = A*A^T, whose B follows A).  The structure arrays given to
+ * rtt_spgemm_symbolic stay borrowed while such updates are made.  Skips
+ * csr2tile's counting and the symbolic phase: A's tiles (and B's) are refilled
+ * in place and the numeric step runs into the caller's C buffers, whose
+ * structure equals the first product's. */
+RTT_API int rtt_spgemm_numeric_values(rtt_context ctx, const double *a_values,
+                                      const double *b_values, int *c_row_ptr, int *c_col_idx,
+                                      double *c_values);
+
 /* Device pointers to C's 16x16 tiles from the last numeric (legacy SMatrix
  * layout, plain column bytes).  Valid until the next symbolic on ctx. */
 RTT_API int rtt_spgemm_tiles_view(rtt_context ctx, SMatrix *c_tiles_device);

@@ -39,6 +39,10 @@ struct rtt_context_s
     const double *b_va = nullptr;
     long long b_nnz = 0;
     bool b_dups = false;
+    // A's structure as given to the last symbolic (values-only updates)
+    const int *a_rp = nullptr;
+    const int *a_ci = nullptr;
+    bool op_aat = false;
     // page-locked staging of the host-buffer entry points (created on first use)
     void *hstage[2] = {};
     cudaEvent_t hstage_ev[2] = {};
@@ -1152,6 +1156,9 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
         RTT_CUDA(cudaEventRecord(ws.ev[0], ws.stream));
     RTT_CHECK(map_device_error(csr2tile_device(ws, A->rows, A->cols, (int)A->nnz, A->row_ptr,
                                                A->col_idx, A->values, c->A, true, false)));
+    c->a_rp = A->row_ptr;
+    c->a_ci = A->col_idx;
+    c->op_aat = op == RTT_OP_AAT;
     if (op == RTT_OP_AB && B == nullptr)
     {
         if (A->rows != A->cols)
@@ -1232,6 +1239,39 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
         *tiles_c = c->S.numtile;
     c->have_symbolic = true;
     return RTT_OK;
+}
+
+int rtt_spgemm_numeric_values(rtt_context c, const double *a_values, const double *b_values,
+                              int *c_row_ptr, int *c_col_idx, double *c_values)
+{
+    if (c == nullptr || a_values == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "numeric_values: NULL argument");
+    if (!c->have_symbolic || c->bat_active)
+        return rtt::fail(RTT_ERR_STATE, "rtt_spgemm_numeric_values before rtt_spgemm_symbolic");
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    Workspace &ws = c->ws;
+    // A's tiles take the new values (same structure, same tile order)
+    RTT_CHECK(map_device_error(csr2tile_refill_device(ws, c->a_rp, c->a_ci, a_values, c->A, true)));
+    if (c->b_alias)
+        c->b_va = a_values;
+    else if (c->op_aat)
+    {
+        // B = A^T again, values only (its structure is unchanged)
+        RTT_CHECK(csr_transpose_device(ws, c->A.m, c->A.n, c->A.nnz, c->a_rp, c->a_ci, a_values,
+                                       c->bt_rowptr.as<int>(), c->bt_col.as<int>(),
+                                       c->bt_val.as<double>()));
+        RTT_CHECK(map_device_error(csr2tile_refill_device(ws, c->bt_rowptr.as<int>(),
+                                                          c->bt_col.as<int>(),
+                                                          c->bt_val.as<double>(), c->B, true)));
+        c->b_va = c->bt_val.as<double>();
+    }
+    else if (b_values != nullptr)
+    {
+        RTT_CHECK(map_device_error(
+            csr2tile_refill_device(ws, c->b_rp, c->b_ci, b_values, c->B, true)));
+        c->b_va = b_values;
+    }
+    return rtt_spgemm_numeric(c, c_row_ptr, c_col_idx, c_values);
 }
 
 int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_values)

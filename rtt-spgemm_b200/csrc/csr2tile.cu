@@ -825,6 +825,7 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
     const bool unsorted = ws.h_scalars[5] != 0;
     // rows that are unsorted may hide repeated columns too
     out.dup_cols = ws.h_scalars[6] != 0 || unsorted;
+    out.generic = generic;
 
     int *cnt = out.tmp0.as<int>();
     // heavy tile rows (a CTA each) are listed on the device; their kernels
@@ -905,6 +906,52 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
             out.val.as<double>());
         ws.launches++;
     }
+    return RTT_OK;
+}
+
+int csr2tile_refill_device(Workspace &ws, const int *rowptr, const int *col, const double *val,
+                           TileBufs &t, bool packed_col)
+{
+    cudaStream_t s = ws.stream;
+    const int m = t.m, tilem = t.tilem;
+    if (m == 0 || t.nnz == 0)
+        return RTT_OK;
+    // the fill kernels of the first build, with the new values: they rewrite
+    // the structure arrays with the same bytes and the values in tile order
+    if (!t.generic)
+    {
+        RTT_CHECK(t.tmp1.ensure(sizeof(int) * 4, s));
+        RTT_CHECK(t.tmp2.ensure((size_t)tilem + 16, s));
+        RTT_CHECK(t.tmp3.ensure(sizeof(int) * (size_t)tilem + 16, s));
+        uint8_t *heavy = t.tmp2.as<uint8_t>();
+        int *hv_list = t.tmp3.as<int>(), *hv_count = t.tmp1.as<int>() + 3;
+        RTT_CUDA(cudaMemsetAsync(hv_count, 0, sizeof(int), s));
+        k_c2t_heavy_mark<<<grid_for(tilem, 256), 256, 0, s>>>(m, tilem, rowptr, col, heavy,
+                                                              hv_list, hv_count);
+        k_c2t_fill<<<grid_for((long long)ceil_div(tilem, 2) * 32, 256), 256, 0, s>>>(
+            m, tilem, rowptr, col, val, t.tile_ptr.as<int>(), t.tile_col.as<int>(),
+            t.tile_row.as<int>(), t.tile_nnz.as<int>(), t.ptr.as<uint8_t>(), t.col.as<uint8_t>(),
+            t.val.as<double>(), t.mask.as<uint16_t>(), packed_col ? 1 : 0, ws.err.as<int>(), heavy);
+        int sms = 0;
+        RTT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws.device));
+        const size_t hv_smem = sizeof(HeavySmem);
+        RTT_CUDA(cudaFuncSetAttribute(k_c2t_heavy_fill, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)hv_smem));
+        k_c2t_heavy_fill<<<std::min(tilem, 2 * sms), HV_THREADS, hv_smem, s>>>(
+            m, hv_list, hv_count, rowptr, col, val, t.tile_ptr.as<int>(), t.tile_col.as<int>(),
+            t.tile_row.as<int>(), t.tile_nnz.as<int>(), t.ptr.as<uint8_t>(), t.col.as<uint8_t>(),
+            t.val.as<double>(), t.mask.as<uint16_t>(), packed_col ? 1 : 0, ws.err.as<int>());
+        ws.launches += 3;
+    }
+    else
+    {
+        k_c2t_fill_generic<<<grid_for((long long)tilem * 32, 128), 128, 0, s>>>(
+            m, tilem, rowptr, col, val, t.tile_ptr.as<int>(), t.tile_col.as<int>(),
+            t.tile_row.as<int>(), t.tile_nnz.as<int>(), t.ptr.as<uint8_t>(), t.col.as<uint8_t>(),
+            t.val.as<double>(), t.mask.as<uint16_t>(), packed_col ? 1 : 0, ws.err.as<int>());
+        ws.launches++;
+    }
+    RTT_CUDA(cudaGetLastError());
     return RTT_OK;
 }
 

@@ -233,12 +233,17 @@ struct TileBufs
     DevBuf tmp0, tmp1, tmp2, tmp3;
     int m = 0, n = 0, tilem = 0, tilen = 0, numtile = 0, nnz = 0;
     bool dup_cols = false; // some row may repeat a column (set by csr2tile_device)
+    bool generic = false;  // built by the generic (unsorted tile columns) path
     void release();
     DevTiles view() const;
 };
 
 int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
                     const double *val, TileBufs &out, bool packed_col, bool sort_within_rows);
+// values-only update: tiles built by csr2tile_device (sort_within_rows false)
+// from a CSR of the same structure get the values val (no host round trip)
+int csr2tile_refill_device(Workspace &ws, const int *rowptr, const int *col, const double *val,
+                           TileBufs &t, bool packed_col);
 // tile CSC index (column lists) over row-major tiles
 int build_tile_csc(Workspace &ws, TileBufs &t);
 // rearrange row-major tiles into the csr2tile_col_major layout (data in CSC order)

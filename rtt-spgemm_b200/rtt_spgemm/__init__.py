@@ -353,6 +353,14 @@ class Context:
         finally:
             self._borrowed = None
 
+    def numeric_values(self, a_values, b_values, rowptr, col, val):
+        """rtt_spgemm_numeric_values: the last symbolic's product with new values
+        of A (device tensor in A's CSR order) and of B (or None).  The caller
+        keeps the structure tensors given to symbolic() alive meanwhile."""
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        check(lib().rtt_spgemm_numeric_values(self.handle, ptr(a_values), ptr(b_values),
+                                              ptr(rowptr), ptr(col), ptr(val)))
+
     def batched_symbolic(self, As, Bs=None):
         """Batched form: As (and Bs) are lists of (rows, cols, rowptr, col, val)
         device tuples.  Returns (nnz per instance, total nnz).  The operands

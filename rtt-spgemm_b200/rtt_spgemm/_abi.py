@@ -36,6 +36,7 @@ EXPORTS = [
     "rtt_plan_tail_queue", "rtt_spgemm_batched_symbolic", "rtt_spgemm_batched_numeric",
     "rtt_csr_transpose", "rtt_early_split_policy_default", "rtt_plan_early_split",
     "rtt_reorder_plan_build", "rtt_reorder_plan_destroy", "rtt_csr_permute",
+    "rtt_spgemm_numeric_values",
 ]
 
 
@@ -197,6 +198,8 @@ def lib() -> C.CDLL:
                                               P(C.c_longlong), P(C.c_longlong)]
     L.rtt_spgemm_batched_numeric.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.rtt_csr_transpose.argtypes = [C.c_void_p, P(CsrView), C.c_void_p, C.c_void_p, C.c_void_p]
+    L.rtt_spgemm_numeric_values.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p]
     L.rtt_reorder_plan_build.argtypes = [C.c_void_p, P(CsrView), P(ReorderPlan)]
     L.rtt_reorder_plan_destroy.argtypes = [P(ReorderPlan)]
     L.rtt_reorder_plan_destroy.restype = None
