@@ -398,6 +398,32 @@ def run_ours(args) -> None:
     achieved = abytes / (num_ms * 1e-3) / 1e9
     traffic = None if args.staging or args.unfused else load_traffic(args.workload)
 
+    # repeated product with the same structure and new values (values-only
+    # update, rtt_spgemm_numeric_values): no csr2tile counting, no symbolic
+    upd = None
+    if not args.staging and not args.unfused and not args.no_update:
+        nnz_u, _ = ctx.symbolic(a_view)
+        urp = torch.empty(A.m + 1, dtype=torch.int32, device=dev)
+        uci = torch.empty(max(nnz_u, 1), dtype=torch.int32, device=dev)
+        uva = torch.empty(max(nnz_u, 1), dtype=torch.float64, device=dev)
+        ctx.numeric(urp, uci, uva)
+        new_vals = va * 0.5
+        for _ in range(args.warmup):
+            ctx.numeric_values(new_vals, None, urp, uci, uva)
+        u0 = torch.cuda.Event(enable_timing=True)
+        u1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        u0.record(stream)
+        for _ in range(args.steps):
+            ctx.numeric_values(new_vals, None, urp, uci, uva)
+        u1.record(stream)
+        torch.cuda.synchronize(dev)
+        u_ms = shards.max_over_ranks(u0.elapsed_time(u1) / args.steps)
+        upd = {"value": shards.replica_throughput(world, flops, u_ms), "unit": "GFLOP/s",
+               "ms_per_step": u_ms,
+               "what": "same structure, new values of A: tiles refilled, numeric step only"}
+        del urp, uci, uva
+
     # end to end through the host-buffer C-ABI call (rtt_spgemm_csr_host):
     # H2D of A from pinned memory, the product, D2H of C into malloc'd arrays
     e2e = None
@@ -458,6 +484,7 @@ def run_ours(args) -> None:
         "clocks": clocks,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "values_only_update": upd,
     }
     print(json.dumps(line), flush=True)
 
@@ -474,6 +501,8 @@ def main() -> None:
     ap.add_argument("--unfused", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-update", action="store_true",
+                    help="skip the values-only update timing")
     ap.add_argument("--batch-count", type=int, default=128)
     ap.add_argument("--serve-count", type=int, default=200)
     ap.add_argument("--serve-nmax", type=int, default=262144)
