@@ -38,6 +38,8 @@ WORKLOADS = {
     "stencil27_96_brick": "3-D 27-point stencil, 96^3 grid, 2x2x4 brick ordering, C = A^2",
     "laplacian2d_256": "2-D 5-point Laplacian, 256^2 grid (n=65,536), C = A^2",
     "stencil27_80": "3-D 27-point stencil, 80^3 grid (n=512,000), C = A^2 (profiling size)",
+    "rmat16_aat": "R-MAT 2^16, 16 edges/row, (a,b,c,d)=(.57,.19,.19,.05), C = A*A^T (the R-MAT "
+                  "config's generator at the largest scale whose C fits int32 offsets)",
     "served": "Poisson request stream (2,000 req/s) of mixed A^2 / A*A^T products, n log-uniform "
               "in [4,096, n_max], 2-D/3-D stencils, R-MAT, banded+scatter, 30% reuse a resident A; "
               "120 GB pool; served (batched as they arrive) vs plain one-call FIFO",
@@ -57,10 +59,19 @@ def make_workload(name: str, seed: int):
         return G.laplacian_2d(256)
     if name == "stencil27_80":
         return G.stencil_27(80, seed)
+    if name == "rmat16_aat":
+        return G.rmat(16, 16, seed=seed + 1)
     raise SystemExit(f"unknown workload {name}")
 
 
-def nnz_cub(A) -> int:
+def workload_aat(name: str) -> bool:
+    return name.endswith("_aat")
+
+
+def nnz_cub(A, aat: bool = False) -> int:
+    if aat:  # B = A^T: nnz(B row k) = entries of A's column k
+        cc = np.bincount(A.col, minlength=A.n).astype(np.int64)
+        return int(cc[A.col].sum())
     return int(np.diff(A.rowptr).astype(np.int64)[A.col].sum())
 
 
@@ -140,11 +151,11 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline_port(A, flops: float) -> dict:
+def cpu_baseline_port(A, flops: float, B=None) -> dict:
     import oracle
     orc = oracle.Oracle()
     t0 = time.perf_counter()
-    orc.spgemm_csr(A, A, with_abs=False)
+    orc.spgemm_csr(A, A if B is None else B, with_abs=False)
     dt = time.perf_counter() - t0
     return {"value": flops / dt / 1e9, "unit": "GFLOP/s", "cores": orc.threads(), "kind": "port",
             "sample": "full product, FP64 OpenMP row SPA restating spgemm_serialref "
@@ -159,14 +170,16 @@ def run_reference(args) -> None:
         return
     import oracle
     A = make_workload(args.workload, args.seed)
+    aat = workload_aat(args.workload)
+    B = A.transpose() if aat else A
     from rtt_spgemm import generators as G
     if oracle.reference_available():
         ref = oracle.Reference()
-        b_tiles = ref.csr2tile_col_major(A)  # B prepared once, outside the timed steps
+        b_tiles = ref.csr2tile_col_major(B)  # B prepared once, outside the timed steps
         rows = min(A.m, args.ref_tile_rows * 16)
         rp = A.rowptr[: rows + 1].copy()
         As = G.CSR(rows, A.n, rp, A.col[: rp[-1]].copy(), A.val[: rp[-1]].copy())
-        flops = 2.0 * int(np.diff(A.rowptr).astype(np.int64)[As.col].sum())
+        flops = 2.0 * int(np.diff(B.rowptr).astype(np.int64)[As.col].sum())
         times = []
         for i in range(args.warmup + args.steps):
             t0 = time.perf_counter()
@@ -182,8 +195,8 @@ def run_reference(args) -> None:
                   f"the in-tile column fix at the call site); B's csr2tile_col_major done once "
                   f"before timing")
     else:
-        flops = 2.0 * nnz_cub(A)
-        cb = cpu_baseline_port(A, flops)
+        flops = 2.0 * nnz_cub(A, aat)
+        cb = cpu_baseline_port(A, flops, B if aat else None)
         t, kind, cores, sample = cb["seconds"], "port", cb["cores"], cb["sample"]
     value = flops / t / 1e9
     line = {"impl": "reference", "metric": "SpGEMM GFLOP/s", "value": value, "unit": "GFLOP/s",
@@ -337,7 +350,9 @@ def run_ours(args) -> None:
                                 device_id=dev)
 
     A = make_workload(args.workload, args.seed)
-    cub = nnz_cub(A)
+    aat = workload_aat(args.workload)
+    op = R.RTT_OP_AAT if aat else R.RTT_OP_AB
+    cub = nnz_cub(A, aat)
     flops = 2.0 * cub
     stream = torch.cuda.current_stream(dev)
     ctx = R.Context(local, {"stage_timing": 1, "dmma_pair_cutoff": args.dmma_cutoff,
@@ -350,7 +365,7 @@ def run_ours(args) -> None:
     a_view = (A.m, A.n, rp, ci, va)
 
     def step():
-        nnz, _ = ctx.symbolic(a_view)
+        nnz, _ = ctx.symbolic(a_view, None, op)
         crp = torch.empty(A.m + 1, dtype=torch.int32, device=dev)
         cci = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
         cva = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
@@ -402,7 +417,7 @@ def run_ours(args) -> None:
     # update, rtt_spgemm_numeric_values): no csr2tile counting, no symbolic
     upd = None
     if not args.staging and not args.unfused and not args.no_update:
-        nnz_u, _ = ctx.symbolic(a_view)
+        nnz_u, _ = ctx.symbolic(a_view, None, op)
         urp = torch.empty(A.m + 1, dtype=torch.int32, device=dev)
         uci = torch.empty(max(nnz_u, 1), dtype=torch.int32, device=dev)
         uva = torch.empty(max(nnz_u, 1), dtype=torch.float64, device=dev)
@@ -432,14 +447,14 @@ def run_ours(args) -> None:
         pin_ci = torch.from_numpy(A.col).pin_memory()
         pin_va = torch.from_numpy(A.val).pin_memory()
         Ah = R.CSR(A.m, A.n, pin_rp.numpy(), pin_ci.numpy(), pin_va.numpy())
-        ctx.spgemm_csr_host(Ah)  # warm
+        ctx.spgemm_csr_host(Ah, None, op)  # warm
         torch.cuda.synchronize(dev)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         n_e2e = max(1, min(3, args.steps))
         e0.record(stream)
         for _ in range(n_e2e):
-            Ch = ctx.spgemm_csr_host(Ah)
+            Ch = ctx.spgemm_csr_host(Ah, None, op)
         e1.record(stream)
         torch.cuda.synchronize(dev)
         e2e_ms = shards.max_over_ranks(e0.elapsed_time(e1) / n_e2e)
@@ -449,7 +464,7 @@ def run_ours(args) -> None:
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_port(A, flops)
+        cpu = cpu_baseline_port(A, flops, A.transpose() if aat else None)
         cpu.pop("seconds", None)
 
     if dist:
