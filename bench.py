@@ -364,7 +364,19 @@ def run_ours(args) -> None:
     va = torch.from_numpy(A.val).to(dev)
     a_view = (A.m, A.n, rp, ci, va)
 
+    # L2 (126 MB): inputs larger than it are re-read from HBM every step; a
+    # smaller input gets a 256 MB buffer written before each step (inside the
+    # timed region, about 0.04 ms) so that no step starts with it in L2
+    a_bytes = 4 * (A.m + 1) + 12 * A.nnz
+    flush = None if a_bytes > 126e6 else torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    l2_note = ("inputs larger than L2 (A CSR %.0f MB > 126 MB), no flush" % (a_bytes / 1e6)
+               if flush is None else
+               "inputs smaller than L2 (A CSR %.0f MB): 256 MB written before each step, "
+               "inside the timed region" % (a_bytes / 1e6))
+
     def step():
+        if flush is not None:
+            flush.fill_(1)
         nnz, _ = ctx.symbolic(a_view, None, op)
         crp = torch.empty(A.m + 1, dtype=torch.int32, device=dev)
         cci = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
@@ -481,8 +493,7 @@ def run_ours(args) -> None:
                    "n": A.m, "nnz_a": A.nnz, "nnz_c": nnz_c, "nnz_cub": cub, "flops": flops,
                    "tiles_a": st["tiles_a"], "tiles_c": st["tiles_c"],
                    "alg_bytes": abytes, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (A CSR %.0f MB > 126 MB), no flush" %
-                         ((4 * (A.m + 1) + 12 * A.nnz) / 1e6),
+                   "l2": l2_note,
                    "dmma_pair_cutoff": args.dmma_cutoff, "fused_tile2csr": not args.unfused,
                    "b_staging": bool(args.staging)},
         "roofline": {"bound": "hbm",
