@@ -238,9 +238,15 @@ def run_batched(args) -> None:
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
 
+    tuner = None
+    if args.tune:
+        from rtt_spgemm import autotune
+        tuner = autotune.Tuner(ROOT / "gpurun_out" / "tune.json"
+                               if (ROOT / "gpurun_out").is_dir() else None)
+
     def batched():
         for w in waves:
-            R.spgemm_batched(ctx, [views[i] for i in w])
+            R.spgemm_batched(ctx, [views[i] for i in w], tuner=tuner)
 
     def plain():
         for v in views:
@@ -262,7 +268,10 @@ def run_batched(args) -> None:
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1) / args.steps
 
+    base_cfg = {"stage_timing": 0, "dmma_pair_cutoff": args.dmma_cutoff,
+                "b_staging": 1 if args.staging else 0}
     ms_b = timed(batched)
+    ctx.configure(base_cfg)  # the plain arm keeps the given configuration
     ms_p = timed(plain)
     n = len(As)
     line = {
@@ -278,6 +287,7 @@ def run_batched(args) -> None:
         "plain": {"spgemms_per_s": n / (ms_p * 1e-3), "ms_per_step": ms_p,
                   "gflops": flops / (ms_p * 1e-3) / 1e9},
         "batched_over_plain": ms_p / ms_b,
+        "tuned": (list(tuner.table.get("devices", {}).values()) or [{}])[0] if tuner else None,
     }
     print(json.dumps(line), flush=True)
     ctx.close()
@@ -529,6 +539,8 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-update", action="store_true",
                     help="skip the values-only update timing")
+    ap.add_argument("--tune", action="store_true",
+                    help="batched: configurations chosen by the autotuner (tuned in warm-up)")
     ap.add_argument("--batch-count", type=int, default=128)
     ap.add_argument("--serve-count", type=int, default=200)
     ap.add_argument("--serve-nmax", type=int, default=262144)

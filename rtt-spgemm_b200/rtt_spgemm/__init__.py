@@ -305,13 +305,18 @@ class Context:
         check(lib().rtt_context_create(C.byref(h), device))
         self.handle = h
         self.device = device
+        self.configure(config)
+        if stream is not None:
+            check(lib().rtt_context_set_stream(self.handle, C.c_void_p(stream)))
+
+    def configure(self, config: dict | None = None):
+        """rtt_config from the defaults plus the given fields."""
         cfg = Config()
         lib().rtt_config_default(C.byref(cfg))
         for k, v in (config or {}).items():
             setattr(cfg, k, int(v))
         check(lib().rtt_context_set_config(self.handle, C.byref(cfg)))
-        if stream is not None:
-            check(lib().rtt_context_set_stream(self.handle, C.c_void_p(stream)))
+        self.config = {k: getattr(cfg, k) for k, _ in Config._fields_ if k != "reserved"}
 
     def close(self):
         if self.handle:
@@ -444,12 +449,15 @@ class Context:
                    _adopt(sc.columnindex, sc.nnz, np.int32), _adopt(sc.value, sc.nnz, np.float64))
 
 
-def spgemm_batched(ctx: "Context", As, Bs=None):
+def spgemm_batched(ctx: "Context", As, Bs=None, tuner=None):
     """C_i = A_i * B_i (or A_i^2) for a list of device CSR tuples, through one
     pipeline run.  Returns per-instance (rowptr, col, val) device tensor views
-    of three concatenated output buffers."""
+    of three concatenated output buffers.  With a tuner (autotune.Tuner) the
+    context takes the tuned configuration of the batch's shape class first."""
     import torch
 
+    if tuner is not None:
+        tuner.configure_batch(ctx, As, Bs)
     nnz, total = ctx.batched_symbolic(As, Bs)
     dev = As[0][2].device
     rows = [int(a[0]) for a in As]
