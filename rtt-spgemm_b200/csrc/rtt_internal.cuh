@@ -274,6 +274,8 @@ struct SymbolicOut
     DevBuf tile_cnt;    // numtile ints, nnz per C tile
     // numeric split of heavy tile rows: window tasks, per-tile-row flag, queue
     DevBuf w_task, w_heavy, w_queue, w_flag;
+    // symbolic step 2: heavy tile rows (flag per tile row, list)
+    DevBuf s2_heavy, s2_list;
     // some C tile row needs more than one window of the flat numeric kernel
     // (set by the symbolic step; true when unknown)
     bool multi_window = true;

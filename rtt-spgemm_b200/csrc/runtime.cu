@@ -278,7 +278,7 @@ void SymbolicOut::release()
 {
     DevBuf *all[] = {&c_tile_ptr, &c_tile_col, &c_tile_row, &c_tile_nnz, &c_mask, &c_ptr,
                      &c_col, &c_val, &c_row_cnt, &c_rowptr, &c_tr_nnz, &count_tmp,
-                     &tile_cnt, &w_task, &w_heavy, &w_queue, &w_flag};
+                     &tile_cnt, &w_task, &w_heavy, &w_queue, &w_flag, &s2_heavy, &s2_list};
     for (DevBuf *b : all)
         b->release();
 }

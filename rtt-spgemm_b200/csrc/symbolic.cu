@@ -40,19 +40,43 @@ struct WarpSmem1
 
 constexpr int S2_WARPS = 8;              // warps per CTA, two rows each
 constexpr int S2_THREADS = S2_WARPS * 32;
+constexpr int S2_PAIRS = TD / 2;         // row pairs of a tile row
+// Heavy tile rows (several windows and an R-MAT hub among their rows: one
+// row pair with more than HEAVY_PAIR A entries and 2.5x the mean) run in a
+// CTA of S2_HEAVY_WARPS warps that all share the walk.
+constexpr int S2_HEAVY_WARPS = 32;
+constexpr int HEAVY_PAIR = 1024;
 constexpr int S2_SLOTS = 254;            // C tiles per window (slot 255 = none)
-constexpr int S2_STRIDE = 257;           // odd stride: the warps' mask rows in distinct banks
+constexpr int S2_STRIDE = 257;           // odd stride: the pairs' mask rows in distinct banks
 
+template <int NW>
 struct CtaSmem2
 {
     uint32_t bitmap[WWORDS];
     int wordpre[WWORDS];
     uint8_t slot8[WBITS];                // window column -> slot
-    uint32_t mw[S2_WARPS * S2_STRIDE];   // per warp and slot: row 2w (low 16), 2w+1 (high 16)
-    int4 ent[S2_WARPS][32];              // per warp: B row start, length, mask shift, mask row
+    uint32_t mw[S2_PAIRS * S2_STRIDE];   // per row pair and slot: row 2p (low 16), 2p+1 (high 16)
+    int4 ent[NW][32];                    // per warp: B row start, length, mask shift, mask row
     int lo, hi, nb, wend;
     int share;                           // the warps share the A entries (unbalanced rows)
 };
+
+// Row pairs with very different A entry counts: with NW warps, the pair
+// counts and whether one pair holds > 2.5x the mean (and > min_pair).
+__device__ __forceinline__ bool skewed_pairs(const DevTiles &A, int I, int nrows, int lane,
+                                             int min_pair)
+{
+    int pc = 0;
+    if (lane < S2_PAIRS && A.csr_rowptr != nullptr)
+    {
+        const int ra = min(2 * lane, nrows), rb = min(2 * lane + 2, nrows);
+        pc = __ldg(A.csr_rowptr + I * TD + rb) - __ldg(A.csr_rowptr + I * TD + ra);
+    }
+    int tot = pc;
+    for (int o = 4; o > 0; o >>= 1)
+        tot += __shfl_xor_sync(FULL, tot, o);
+    return __any_sync(FULL, lane < S2_PAIRS && pc > min_pair && 2 * S2_PAIRS * pc > 5 * tot);
+}
 
 // Window bounds [lo, hi] of the tile columns reachable from tile row I.
 __device__ __forceinline__ void row_window(const DevTiles &A, const DevTiles &B, int a0, int a1,
@@ -119,7 +143,8 @@ __device__ __forceinline__ void fill_bitmap(const DevTiles &A, const DevTiles &B
 }
 
 __global__ void __launch_bounds__(SYM_WARPS * 32)
-    k_sym_count(DevTiles A, DevTiles B, int *cnt, int *multi)
+    k_sym_count(DevTiles A, DevTiles B, int *cnt, int *multi, uint8_t *heavy, int *list,
+                int *list_count)
 {
     __shared__ WarpSmem1 sm[SYM_WARPS];
     const int lane = lane_id(), wi = threadIdx.x >> 5;
@@ -149,12 +174,22 @@ __global__ void __launch_bounds__(SYM_WARPS * 32)
             __syncwarp();
         }
     }
+    // step 2 will need more than one window for this tile row; with an
+    // unbalanced row pair it becomes a heavy row (a wide CTA of its own)
+    const bool multi_win = count > S2_SLOTS || (hi >= 0 && (long long)hi - lo + 1 > WBITS);
+    const bool hv = multi_win && heavy != nullptr &&
+                    skewed_pairs(A, I, min(TD, A.m - I * TD), lane, HEAVY_PAIR);
     if (lane == 0)
     {
         cnt[I] = count;
-        // step 2 will need more than one window for this tile row
-        if (count > S2_SLOTS || (hi >= 0 && (long long)hi - lo + 1 > WBITS))
+        if (multi_win)
             atomicOr(multi, 1);
+        if (heavy != nullptr)
+        {
+            heavy[I] = hv;
+            if (hv)
+                list[atomicAdd(list_count, 1)] = I;
+        }
     }
 }
 
@@ -162,24 +197,29 @@ __global__ void __launch_bounds__(SYM_WARPS * 32)
 // count; per scalar row: entry count; per tile row: entry total.  NARROW:
 // some tile row has several windows and B's rows are sorted, so long B rows
 // are cut to each window's columns (compiled out otherwise: it costs the
-// single-window walk registers and issue slots).
-template <bool NARROW>
-__global__ void __launch_bounds__(S2_THREADS, 5)
+// single-window walk registers and issue slots).  NW warps per CTA: 8 for
+// the tile rows in order (a heavy one is skipped when heavy[] marks it), or
+// S2_HEAVY_WARPS for the heavy rows of list[] (all warps share the walk).
+template <bool NARROW, int NW>
+__global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
     k_sym_rows(DevTiles A, DevTiles B, const int *__restrict__ c_tile_ptr,
                int *__restrict__ c_tile_col, int *__restrict__ c_tile_row,
                uint16_t *__restrict__ c_mask, int *__restrict__ c_tile_cnt,
-               int *__restrict__ c_row_cnt, int *__restrict__ c_tr_nnz, int *multi, int *err)
+               int *__restrict__ c_row_cnt, int *__restrict__ c_tr_nnz, int *multi, int *err,
+               const uint8_t *__restrict__ heavy, const int *__restrict__ list)
 {
-    __shared__ CtaSmem2 S;
+    static_assert(NW == S2_WARPS || NW == S2_HEAVY_WARPS, "CTA shapes");
+    constexpr int NT = NW * 32;
+    __shared__ CtaSmem2<NW> S;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int I = blockIdx.x;
-    if (I >= A.tilem)
+    const int I = list != nullptr ? list[blockIdx.x] : (int)blockIdx.x;
+    if (I >= A.tilem || (list == nullptr && heavy != nullptr && heavy[I]))
         return;
     const int a0 = __ldg(A.tile_ptr + I), a1 = __ldg(A.tile_ptr + I + 1);
     const int cbeg = __ldg(c_tile_ptr + I), cend = __ldg(c_tile_ptr + I + 1);
     const int nrows = min(TD, A.m - I * TD);
-    const int r0 = warp * 2, r1 = r0 + 1;
-    uint32_t *mw = S.mw + warp * S2_STRIDE;
+    const int r0 = warp * 2, r1 = r0 + 1; // warp-private walk (NW == S2_WARPS) and counts
+    uint32_t *mw = S.mw + min(warp, S2_PAIRS - 1) * S2_STRIDE;
     int4 *ent = S.ent[warp];
     int run0 = 0, run1 = 0; // entries of rows r0, r1 so far
 
@@ -192,7 +232,7 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
     __syncthreads();
     {
         int lo = INT_MAX, hi = -1;
-        for (int a = a0 + tid; a < a1; a += S2_THREADS)
+        for (int a = a0 + tid; a < a1; a += NT)
         {
             const int K = __ldg(A.tile_col + a);
             const int b0 = __ldg(B.tile_ptr + K), b1 = __ldg(B.tile_ptr + K + 1);
@@ -213,25 +253,20 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
     __syncthreads();
     const int lo = S.lo, hi = S.hi;
     const bool clip = hi >= 0 && (long long)hi - lo + 1 > WBITS;
-    if (NARROW)
+    if (NARROW && NW == S2_WARPS)
     {
         // Row pairs with very different A entry counts (an R-MAT hub row):
         // all warps share the walk.  Balanced rows keep the warp-private walk,
         // whose mask words no other warp touches.
-        int pc = 0;
-        if (tid < S2_WARPS && A.csr_rowptr != nullptr)
+        if (warp == 0)
         {
-            const int ra = min(2 * tid, nrows), rb = min(2 * tid + 2, nrows);
-            pc = __ldg(A.csr_rowptr + I * TD + rb) - __ldg(A.csr_rowptr + I * TD + ra);
+            const bool skew = skewed_pairs(A, I, nrows, lane, 32);
+            if (lane == 0)
+                S.share = skew;
         }
-        int tot = pc;
-        for (int o = 4; o > 0; o >>= 1)
-            tot += __shfl_xor_sync(FULL, tot, o);
-        const bool skew = tid < S2_WARPS && pc > 32 && 2 * S2_WARPS * pc > 5 * tot;
-        const int any = __syncthreads_or(skew);
-        if (tid == 0)
-            S.share = any;
     }
+    if (NW != S2_WARPS && tid == 0)
+        S.share = 1;
     int cbase = cbeg;
     for (long long wl = lo; hi >= 0 && wl <= hi;)
     {
@@ -239,10 +274,10 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
         int wend = (int)min((long long)hi + 1, wl + WBITS);
         const int nwords = (wend - w + 31) >> 5; // bitmap words the window can touch
         // ---- C tiles of the window: bitmap of the B tile columns in [w, wend)
-        for (int i = tid; i < nwords; i += S2_THREADS)
+        for (int i = tid; i < nwords; i += NT)
             S.bitmap[i] = 0u;
         __syncthreads();
-        for (int a = a0 + warp; a < a1; a += S2_WARPS)
+        for (int a = a0 + warp; a < a1; a += NW)
         {
             const int K = __ldg(A.tile_col + a);
             int b0 = __ldg(B.tile_ptr + K), b1 = __ldg(B.tile_ptr + K + 1);
@@ -300,10 +335,10 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
                 set_error(err, DERR_SYM_OVERFLOW);
             return;
         }
-        for (int i = tid; i < (wlen + 3) / 4; i += S2_THREADS)
+        for (int i = tid; i < (wlen + 3) / 4; i += NT)
             reinterpret_cast<uint32_t *>(S.slot8)[i] = 0xFFFFFFFFu;
         __syncthreads();
-        for (int q = tid; q < nwords; q += S2_THREADS)
+        for (int q = tid; q < nwords; q += NT)
         {
             uint32_t bits = S.bitmap[q];
             int slot = S.wordpre[q];
@@ -321,20 +356,20 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
                 ++slot;
             }
         }
-        for (int i = lane; i < nb; i += 32)
-            mw[i] = 0u;
+        for (int i = tid; i < S2_PAIRS * S2_STRIDE; i += NT)
+            S.mw[i] = 0u;
         __syncthreads();
 
         // ---- masks
-        if (NARROW && S.share)
+        if ((NARROW || NW != S2_WARPS) && S.share)
         {
             // several windows: a hub row would leave one warp walking while
             // seven wait, so all warps share the tile row's A entries (the
             // masks combine by OR, in any order); warp w takes every
-            // S2_WARPS-th A tile, so short tile rows are shared too
-            for (int t0 = a0; t0 < a1; t0 += S2_WARPS * 32)
+            // NW-th A tile, so short tile rows are shared too
+            for (int t0 = a0; t0 < a1; t0 += NW * 32)
             {
-                const int t = t0 + lane * S2_WARPS + warp;
+                const int t = t0 + lane * NW + warp;
                 int n = 0, tn0 = 0, K = 0;
                 if (t < a1)
                 {
@@ -411,7 +446,7 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
             }
             __syncthreads(); // every warp's rows are complete
         }
-        else if (r0 < nrows)
+        else if (NW == S2_WARPS && r0 < nrows)
         {
             // one window: warp-private walk over the warp's own A entries
             for (int t0 = a0; t0 < a1; t0 += 32)
@@ -499,7 +534,8 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
                 }
             }
         }
-        // per-row counts of the window (each warp its own rows)
+        // per-row counts of the window (warp w counts rows 2w, 2w + 1)
+        if (warp < S2_PAIRS)
         {
             int c0 = 0, c1 = 0;
             for (int i = lane; i < nb; i += 32)
@@ -513,17 +549,17 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
         }
         __syncthreads();
         // ---- outputs of the window: masks (coalesced u16), tile counts
-        for (int i = tid; i < nb * TD; i += S2_THREADS)
+        for (int i = tid; i < nb * TD; i += NT)
         {
             const int sl = i >> 4, r = i & 15;
             const uint32_t v = S.mw[(r >> 1) * S2_STRIDE + sl];
             c_mask[(size_t)(cbase + sl) * TD + r] = (uint16_t)((v >> ((r & 1) * 16)) & 0xFFFFu);
         }
-        for (int sl = tid; sl < nb; sl += S2_THREADS)
+        for (int sl = tid; sl < nb; sl += NT)
         {
             int c = 0;
 #pragma unroll
-            for (int wv = 0; wv < S2_WARPS; ++wv)
+            for (int wv = 0; wv < S2_PAIRS; ++wv)
                 c += __popc(S.mw[wv * S2_STRIDE + sl]);
             c_tile_cnt[cbase + sl] = c;
         }
@@ -549,7 +585,7 @@ __global__ void __launch_bounds__(S2_THREADS, 5)
     if (tid == 0)
         tot = 0;
     __syncthreads();
-    if (lane == 0)
+    if (lane == 0 && warp < S2_PAIRS)
         atomicAdd(&tot, run0 + run1);
     __syncthreads();
     if (tid == 0)
@@ -578,21 +614,25 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
     RTT_CHECK(S.c_tile_ptr.ensure(sizeof(int) * (size_t)(tilem + 1), s));
     int *cnt = S.count_tmp.as<int>();
     // flags: [0] some tile row needs several step-2 windows, [1] several
-    // numeric windows
-    RTT_CHECK(S.w_flag.ensure(sizeof(int) * 2, s));
-    RTT_CUDA(cudaMemsetAsync(S.w_flag.p, 0, sizeof(int) * 2, s));
+    // numeric windows, [2] heavy tile rows listed for the wide step-2 CTA
+    RTT_CHECK(S.w_flag.ensure(sizeof(int) * 3, s));
+    RTT_CUDA(cudaMemsetAsync(S.w_flag.p, 0, sizeof(int) * 3, s));
+    RTT_CHECK(S.s2_heavy.ensure((size_t)tilem + 16, s));
+    RTT_CHECK(S.s2_list.ensure(sizeof(int) * (size_t)tilem + 16, s));
     if (tilem > 0)
     {
-        k_sym_count<<<ceil_div(tilem, SYM_WARPS), SYM_WARPS * 32, 0, s>>>(A, B, cnt,
-                                                                          S.w_flag.as<int>());
+        k_sym_count<<<ceil_div(tilem, SYM_WARPS), SYM_WARPS * 32, 0, s>>>(
+            A, B, cnt, S.w_flag.as<int>(), S.s2_heavy.as<uint8_t>(), S.s2_list.as<int>(),
+            S.w_flag.as<int>() + 2);
         ws.launches++;
     }
     RTT_CHECK(scan_exclusive_int(ws, cnt, S.c_tile_ptr.as<int>(), tilem));
-    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 13, S.w_flag.p, sizeof(int), cudaMemcpyDeviceToHost,
-                             s));
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 13, S.w_flag.p, sizeof(int) * 3,
+                             cudaMemcpyDeviceToHost, s));
     int numtile = 0;
     RTT_CHECK(read_int(ws, S.c_tile_ptr.as<int>() + tilem, &numtile));
     const bool sym_multi = ws.h_scalars[13] != 0;
+    const int n_heavy = ws.h_scalars[15];
     RTT_CHECK(check_device_error(ws, "symbolic step 1"));
     S.numtile = numtile;
     const size_t nt = (size_t)numtile;
@@ -607,12 +647,32 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
     RTT_CHECK(S.tile_cnt.ensure(sizeof(int) * (nt + 1), s));
     if (tilem > 0)
     {
-        auto kern = b_sorted && sym_multi ? k_sym_rows<true> : k_sym_rows<false>;
+        if (n_heavy > 0)
+        {
+            // heavy rows: one wide CTA each, on the side stream, alongside
+            // the tile-row CTAs (which skip them)
+            RTT_CUDA(cudaEventRecord(ws.fork_ev, s));
+            RTT_CUDA(cudaStreamWaitEvent(ws.side, ws.fork_ev, 0));
+            auto wide = b_sorted ? k_sym_rows<true, S2_HEAVY_WARPS>
+                                 : k_sym_rows<false, S2_HEAVY_WARPS>;
+            wide<<<n_heavy, S2_HEAVY_WARPS * 32, 0, ws.side>>>(
+                A, B, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(), S.c_tile_row.as<int>(),
+                S.c_mask.as<uint16_t>(), S.tile_cnt.as<int>(), S.c_row_cnt.as<int>(),
+                S.c_tr_nnz.as<int>(), S.w_flag.as<int>() + 1, ws.err.as<int>(), nullptr,
+                S.s2_list.as<int>());
+            RTT_CUDA(cudaEventRecord(ws.join_ev, ws.side));
+            ws.launches++;
+        }
+        auto kern = b_sorted && sym_multi ? k_sym_rows<true, S2_WARPS>
+                                          : k_sym_rows<false, S2_WARPS>;
         kern<<<tilem, S2_THREADS, 0, s>>>(
             A, B, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(), S.c_tile_row.as<int>(),
             S.c_mask.as<uint16_t>(), S.tile_cnt.as<int>(), S.c_row_cnt.as<int>(),
-            S.c_tr_nnz.as<int>(), S.w_flag.as<int>() + 1, ws.err.as<int>());
+            S.c_tr_nnz.as<int>(), S.w_flag.as<int>() + 1, ws.err.as<int>(),
+            n_heavy > 0 ? S.s2_heavy.as<uint8_t>() : nullptr, nullptr);
         ws.launches++;
+        if (n_heavy > 0)
+            RTT_CUDA(cudaStreamWaitEvent(s, ws.join_ev, 0));
     }
     // read with nnz(C) below (one synchronisation for both)
     RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 12, S.w_flag.as<int>() + 1, sizeof(int),

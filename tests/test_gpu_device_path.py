@@ -121,6 +121,8 @@ MANY_WINDOW_CASES = {
     "rmat_12": CASES["rmat_12"],
     "banded_20k": lambda: G.banded_scatter(20000, 24, seed=11),
     "unsorted_wide": lambda: G.random_csr(3000, 3000, 0.01, seed=12, sort=False),
+    # hub rows with > 1024 A entries per row pair: symbolic step 2's wide CTA
+    "rmat_14": lambda: G.rmat(14, 16, seed=2),
 }
 
 
