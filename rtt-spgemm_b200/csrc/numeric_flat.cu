@@ -188,7 +188,7 @@ __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Windo
                     n_fma += len;
                 // one window of several: a long sorted B row contributes only
                 // its columns inside the window's tile-column range
-                if (NARROW && CHECK && !SAFE && len > 32)
+                if (NARROW && CHECK && !SAFE && len > NARROW_MIN)
                 {
                     const int lo = W.Jlo * TD, hi = (W.Jlo + W.Jspan + 1) * TD;
                     const int sb = lower_bound(B.csr_col, fs, fs + len, lo);

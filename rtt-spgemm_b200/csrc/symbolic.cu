@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
                         {
                             fs = min(max(__ldg(B.csr_rowptr + k), 0), B.nnz);
                             len = min(max(__ldg(B.csr_rowptr + k + 1), fs), B.nnz) - fs;
-                            if (narrow && len > 32)
+                            if (narrow && len > NARROW_MIN)
                             {
                                 const int sb = lower_bound(B.csr_col, fs, fs + len, w * TD);
                                 len = lower_bound(B.csr_col, sb, fs + len, wend * TD) - sb;
@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
                             fs = min(max(__ldg(B.csr_rowptr + k), 0), B.nnz);
                             len = min(max(__ldg(B.csr_rowptr + k + 1), fs), B.nnz) - fs;
                         }
-                        if (narrow && len > 32)
+                        if (narrow && len > NARROW_MIN)
                         {
                             const int sb = lower_bound(B.csr_col, fs, fs + len, w * TD);
                             len = lower_bound(B.csr_col, sb, fs + len, wend * TD) - sb;
