@@ -376,8 +376,15 @@ typedef struct
      * negative = never split (each tile row's CTA runs its windows in
      * sequence).  Every setting gives bitwise the same C. */
     int split_target;
+    /* Replay the numeric phase as a CUDA graph when nonzero (the default).
+     * rtt_spgemm_numeric, rtt_spgemm_numeric_values and
+     * rtt_spgemm_batched_numeric capture their launches on the second call
+     * in a row with the same shapes, pointers, configuration and workspace,
+     * and replay that graph while those stay the same.  Off with
+     * stage_timing or fused_csr_output == 0. */
+    int cuda_graphs;
     /* Reserved, must be zero. */
-    int reserved[5];
+    int reserved[4];
 } rtt_config;
 
 RTT_API void rtt_config_default(rtt_config *config);
@@ -406,6 +413,9 @@ typedef struct
      * windows of C tiles are cut into windows that persistent CTAs take from
      * a device queue (the early split of src/dmma_tile_early_split.h). */
     long long split_windows;
+    /* 1 when the last numeric phase ran as a launch of a captured CUDA graph
+     * (cuda_graphs), else 0. */
+    int graph_launched;
 } rtt_stats;
 
 /* A context owns a CUDA stream handle (borrowed), workspace and the state

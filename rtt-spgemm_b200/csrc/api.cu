@@ -14,8 +14,33 @@
 #include <climits>
 #include <cstdlib>
 #include <cstring>
+#include <cstdint>
 #include <mutex>
 #include <vector>
+
+namespace rtt
+{
+// One captured numeric phase.  The key lists every host-side input that its
+// launches baked in: shapes and flags of the tiles and of C, the operand and
+// output pointers, the configuration, the stream and the allocation epoch
+// (which covers every workspace pointer).
+struct GraphSlot
+{
+    std::vector<long long> key;
+    bool warm = false; // the last call ran eagerly with this key
+    cudaGraphExec_t exec = nullptr;
+    int launches = 0; // kernels in the graph
+    void reset()
+    {
+        if (exec != nullptr)
+            cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        key.clear();
+        warm = false;
+        launches = 0;
+    }
+};
+} // namespace rtt
 
 struct rtt_context_s
 {
@@ -28,6 +53,7 @@ struct rtt_context_s
     rtt::DevBuf out_rp, out_col, out_val;  // host-buffer product output
     rtt::DevBuf counters;
     rtt::DevBuf maxnnz;
+    rtt::DevBuf vflags; // flags of the values-only update's CSR validation
     rtt::SymbolicOut S;
     rtt_stats stats;
     bool have_symbolic = false;
@@ -53,11 +79,25 @@ struct rtt_context_s
     int bat_count = 0, bat_rows = 0;
     // offsets (in ints) of the device meta arrays inside bat_meta
     size_t bat_rows_off = 0, bat_rowoff_off = 0, bat_sec_off = 0, bat_colsub_off = 0;
+    // CUDA graphs of the numeric phase: numeric, values-only update, batched
+    rtt::GraphSlot graph[3];
+    cudaStream_t cap_stream = nullptr; // capture stream (never the legacy one)
+    int cut_cached = -1; // effective DMMA cutoff of the current tiles (-1: unknown)
 };
 
 namespace
 {
 using namespace rtt;
+
+// The context's own device buffers (tiles, C and workspace aside).
+std::vector<DevBuf *> own_buffers(rtt_context c)
+{
+    return {&c->bt_rowptr, &c->bt_col,    &c->bt_val,     &c->in_rp,     &c->in_col,
+            &c->in_val,    &c->in2_rp,    &c->in2_col,    &c->in2_val,   &c->out_rp,
+            &c->out_col,   &c->out_val,   &c->counters,   &c->maxnnz,    &c->bat_a_rp,
+            &c->bat_a_col, &c->bat_a_val, &c->bat_b_rp,   &c->bat_b_col, &c->bat_b_val,
+            &c->bat_meta,  &c->bat_big_rp, &c->bat_nnz,  &c->vflags};
+}
 
 std::mutex g_mutex;
 int g_device = 0;
@@ -499,6 +539,11 @@ int effective_cutoff(rtt_context c, const DevTiles &A, const DevTiles &B, int *c
     *cutoff = c->cfg.dmma_pair_cutoff;
     if (*cutoff <= 0)
         return RTT_OK;
+    if (c->cut_cached >= 0)
+    {
+        *cutoff = c->cut_cached;
+        return RTT_OK;
+    }
     RTT_CHECK(c->counters.ensure(sizeof(long long) * 4, c->ws.stream));
     RTT_CHECK(c->maxnnz.ensure(sizeof(int) * 2, c->ws.stream));
     RTT_CHECK(max_tile_nnz_device(c->ws, A.tile_nnz, A.numtile, c->maxnnz.as<int>()));
@@ -509,6 +554,7 @@ int effective_cutoff(rtt_context c, const DevTiles &A, const DevTiles &B, int *c
     c->ws.syncs++;
     if ((long long)c->ws.h_scalars[10] * c->ws.h_scalars[11] < (long long)*cutoff)
         *cutoff = 0;
+    c->cut_cached = *cutoff; // tile sizes change only with a new symbolic
     return RTT_OK;
 }
 
@@ -518,6 +564,209 @@ DevTiles view_with_rowdata(const TileBufs &T)
     v.row_data = T.row_data.p ? T.row_data.as<int>() : nullptr;
     v.csc_data = T.csc_data.p ? T.csc_data.as<int>() : nullptr;
     return v;
+}
+
+inline long long as_key(const void *p) { return (long long)(intptr_t)p; }
+
+// Host-side inputs of the numeric launches (GraphSlot::key), outputs excluded.
+void numeric_key(rtt_context c, std::vector<long long> &k)
+{
+    const TileBufs &TB = c->b_alias ? c->A : c->B;
+    const TileBufs *both[2] = {&c->A, &TB};
+    for (const TileBufs *T : both)
+        for (long long v : {(long long)T->m, (long long)T->n, (long long)T->tilem,
+                            (long long)T->tilen, (long long)T->numtile, (long long)T->nnz,
+                            (long long)T->dup_cols, (long long)T->generic})
+            k.push_back(v);
+    const SymbolicOut &S = c->S;
+    for (long long v : {(long long)S.numtile, S.nnz, (long long)S.tilem, (long long)S.tilen,
+                        (long long)S.m, (long long)S.n, (long long)S.multi_window})
+        k.push_back(v);
+    for (long long v : {as_key(c->b_rp), as_key(c->b_ci), as_key(c->b_va), c->b_nnz,
+                        (long long)c->b_dups, (long long)c->b_alias, (long long)c->op_aat,
+                        as_key(c->a_rp), as_key(c->a_ci), (long long)c->cut_cached,
+                        (long long)c->bat_active, (long long)c->bat_count,
+                        (long long)c->bat_rows})
+        k.push_back(v);
+    const int *cfg = reinterpret_cast<const int *>(&c->cfg);
+    k.insert(k.end(), cfg, cfg + sizeof(rtt_config) / sizeof(int));
+    // every device buffer of the context: a regrown one changes its address
+    auto put = [&](const DevBuf &b) { k.push_back(as_key(b.p)); };
+    c->A.each(put);
+    c->B.each(put);
+    c->S.each(put);
+    for (const DevBuf *b : own_buffers(c))
+        put(*b);
+    const Workspace &ws = c->ws;
+    put(ws.err);
+    put(ws.scan_tmp);
+    for (const DevBuf &b : ws.tmp)
+        put(b);
+    for (long long v : {as_key(ws.h_scalars), as_key(ws.h_scalars64), as_key(ws.side)})
+        k.push_back(v);
+}
+
+// Runs enqueue (device work on ws.stream, with no host read and no sync)
+// either eagerly or as a CUDA graph: the second call in a row with the same
+// key captures it (on a private stream: the legacy default stream cannot
+// capture) and launches the graph; later calls with that key replay it.
+// A capture that fails, because a workspace buffer had to grow, runs eagerly.
+template <class F>
+int run_phase(rtt_context c, int slot, const std::vector<long long> &head, bool allow,
+              F &&enqueue)
+{
+    Workspace &ws = c->ws;
+    GraphSlot &g = c->graph[slot];
+    // the call's own inputs (head), then the context's state
+    auto make_key = [&]() {
+        std::vector<long long> k = head;
+        numeric_key(c, k);
+        k.push_back(as_key(ws.stream));
+        return k;
+    };
+    c->stats.graph_launched = 0;
+    if (!allow || c->cfg.cuda_graphs == 0 || c->cfg.stage_timing != 0)
+    {
+        g.reset();
+        return enqueue();
+    }
+    std::vector<long long> key = make_key();
+    if (g.exec != nullptr && key == g.key)
+    {
+        RTT_CUDA(cudaGraphLaunch(g.exec, ws.stream));
+        ws.launches += g.launches;
+        c->stats.graph_launched = 1;
+        return RTT_OK;
+    }
+    auto eager = [&]() -> int {
+        g.reset();
+        RTT_CHECK(enqueue());
+        g.key = make_key(); // with the addresses of buffers that grew inside enqueue
+        g.warm = true;
+        return RTT_OK;
+    };
+    if (!g.warm || key != g.key)
+        return eager();
+    if (c->cap_stream == nullptr)
+        RTT_CUDA(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+    cudaStream_t user = ws.stream;
+    const int launches0 = ws.launches;
+    ws.stream = c->cap_stream;
+    freeze_growth(true);
+    cudaGraph_t graph = nullptr;
+    int rc = RTT_ERR_CUDA;
+    cudaError_t e = cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess)
+    {
+        rc = enqueue();
+        e = cudaStreamEndCapture(c->cap_stream, &graph);
+    }
+    freeze_growth(false);
+    ws.stream = user;
+    const int captured = ws.launches - launches0;
+    ws.launches = launches0;
+    cudaGraphExec_t exec = nullptr;
+    if (rc == RTT_OK && e == cudaSuccess && graph != nullptr)
+        e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph != nullptr)
+        cudaGraphDestroy(graph);
+    if (rc != RTT_OK || e != cudaSuccess || exec == nullptr)
+    {
+        if (exec != nullptr)
+            cudaGraphExecDestroy(exec);
+        cudaGetLastError();
+        cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(ws.side, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone)
+            return fail(RTT_ERR_CUDA, "side stream left in a failed graph capture");
+        return eager();
+    }
+    g.exec = exec;
+    g.key = std::move(key);
+    g.launches = captured;
+    g.warm = false;
+    RTT_CUDA(cudaGraphLaunch(exec, user));
+    ws.launches += captured;
+    c->stats.graph_launched = 1;
+    return RTT_OK;
+}
+
+// Device work of the numeric step into C's CSR (c_row_ptr, c_col_idx,
+// c_values), counters copied to ws.h_scalars64[2..4]; no host reads unless
+// fused_csr_output == 0 (tile2csr sizes its output on the host).
+int numeric_enqueue(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_values, int cutoff)
+{
+    Workspace &ws = c->ws;
+    const TileBufs &TB = c->b_alias ? c->A : c->B;
+    RTT_CHECK(c->counters.ensure(sizeof(long long) * 4, ws.stream));
+    RTT_CUDA(cudaMemsetAsync(c->counters.p, 0, sizeof(long long) * 4, ws.stream));
+    NumericConfig nc;
+    nc.dmma_pair_cutoff = cutoff;
+    nc.counters = c->counters.as<long long>();
+    nc.b_staging = c->cfg.b_staging != 0;
+    nc.split_target = c->cfg.split_target;
+    if (c->cfg.stage_timing)
+    {
+        nc.ev_begin = ws.ev[3];
+        nc.ev_end = ws.ev[4];
+    }
+    const bool fused = c->cfg.fused_csr_output != 0;
+    nc.write_tiles = !fused || c->cfg.keep_tiles != 0;
+    if (fused)
+    {
+        nc.csr_rowptr = c_row_ptr;
+        nc.csr_col = c_col_idx;
+        nc.csr_val = c_values;
+    }
+    DevTiles dB = TB.view();
+    dB.csr_rowptr = c->b_rp;
+    dB.csr_col = c->b_ci;
+    dB.csr_val = c->b_va;
+    dB.nnz = (int)c->b_nnz;
+    nc.conflict_safe = c->b_dups;
+    RTT_CHECK(numeric_select_device(ws, c->A.view(), dB, c->S, nc));
+    if (!fused)
+    {
+        SymbolicOut &S = c->S;
+        RTT_CHECK(csr_rowptr_device(ws, S, c_row_ptr));
+        RTT_CHECK(tile2csr_fill_device(ws, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(),
+                                       S.c_tile_nnz.as<int>(), S.c_ptr.as<uint8_t>(),
+                                       S.c_col.as<uint8_t>(), S.c_val.as<double>(), S.m, S.n,
+                                       S.tilem, TD, nullptr, -1, c_row_ptr, c_col_idx, c_values,
+                                       false));
+    }
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars64 + 2, c->counters.p, sizeof(long long) * 3,
+                             cudaMemcpyDeviceToHost, ws.stream));
+    return RTT_OK;
+}
+
+// After numeric_enqueue (eager or graph): device checks, then the statistics.
+int numeric_finish(rtt_context c)
+{
+    Workspace &ws = c->ws;
+    RTT_CHECK(check_device_error(ws, "numeric"));
+    if (c->cfg.stage_timing && c->S.numtile > 0)
+    {
+        float tn = 0.f;
+        RTT_CUDA(cudaEventElapsedTime(&tn, ws.ev[3], ws.ev[4]));
+        c->stats.numeric_kernel_ms = tn;
+    }
+    c->stats.dmma_pairs = ws.h_scalars64[2];
+    c->stats.sparse_pairs = ws.h_scalars64[3];
+    // the numeric kernels count every (a_ik, b_kj) pair once: sum over A
+    // entries of nnz(B(k, :)), the reference's nnzCub
+    c->stats.nnz_cub = ws.h_scalars64[3];
+    c->stats.split_windows = ws.h_scalars64[4];
+    c->stats.kernel_launches = ws.launches;
+    c->stats.host_syncs = ws.syncs;
+    return RTT_OK;
+}
+
+int numeric_args_ok(rtt_context c, const int *c_row_ptr, const int *c_col_idx,
+                    const double *c_values)
+{
+    if (c_row_ptr == nullptr || (c->S.nnz > 0 && (c_col_idx == nullptr || c_values == nullptr)))
+        return fail(RTT_ERR_INVALID_ARGUMENT, "NULL output buffer");
+    return RTT_OK;
 }
 
 } // namespace
@@ -570,6 +819,7 @@ void rtt_config_default(rtt_config *config)
     config->fused_csr_output = 1;
     config->keep_tiles = 0;
     config->b_staging = 0;
+    config->cuda_graphs = 1;
 }
 
 int rtt_set_device(int device)
@@ -613,16 +863,14 @@ void rtt_context_destroy(rtt_context c)
         return;
     cudaSetDevice(c->ws.device);
     cudaStreamSynchronize(c->ws.stream);
+    for (rtt::GraphSlot &g : c->graph)
+        g.reset();
+    if (c->cap_stream != nullptr)
+        cudaStreamDestroy(c->cap_stream);
     c->A.release();
     c->B.release();
     c->S.release();
-    rtt::DevBuf *bufs[] = {&c->bt_rowptr, &c->bt_col, &c->bt_val, &c->in_rp, &c->in_col,
-                           &c->in_val, &c->in2_rp, &c->in2_col, &c->in2_val, &c->out_rp,
-                           &c->out_col, &c->out_val, &c->counters, &c->maxnnz,
-                           &c->bat_a_rp, &c->bat_a_col, &c->bat_a_val, &c->bat_b_rp,
-                           &c->bat_b_col, &c->bat_b_val, &c->bat_meta, &c->bat_big_rp,
-                           &c->bat_nnz};
-    for (rtt::DevBuf *b : bufs)
+    for (rtt::DevBuf *b : own_buffers(c))
         b->release();
     for (int b = 0; b < 2; ++b)
     {
@@ -662,6 +910,7 @@ int rtt_context_set_config(rtt_context c, const rtt_config *config)
         if (r != 0)
             return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "reserved config fields must be zero");
     c->cfg = *config;
+    c->cut_cached = -1;
     return RTT_OK;
 }
 
@@ -1147,6 +1396,7 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
     RTT_CUDA(cudaSetDevice(c->ws.device));
     c->have_symbolic = false;
     c->bat_active = false;
+    c->cut_cached = -1;
     c->ws.launches = 0;
     c->ws.syncs = 0;
     std::memset(&c->stats, 0, sizeof(c->stats));
@@ -1248,30 +1498,59 @@ int rtt_spgemm_numeric_values(rtt_context c, const double *a_values, const doubl
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "numeric_values: NULL argument");
     if (!c->have_symbolic || c->bat_active)
         return rtt::fail(RTT_ERR_STATE, "rtt_spgemm_numeric_values before rtt_spgemm_symbolic");
+    RTT_CHECK(numeric_args_ok(c, c_row_ptr, c_col_idx, c_values));
     RTT_CUDA(cudaSetDevice(c->ws.device));
     Workspace &ws = c->ws;
-    // A's tiles take the new values (same structure, same tile order)
-    RTT_CHECK(map_device_error(csr2tile_refill_device(ws, c->a_rp, c->a_ci, a_values, c->A, true)));
+    // The kernels below index by the structure arrays given to symbolic,
+    // which the caller keeps unchanged: check once more on the device that
+    // they still form valid CSRs before anything indexes by them (one sync).
+    // The fast csr2tile fill also needs tile columns that never decrease in
+    // a row, as at the first build.
+    RTT_CHECK(c->vflags.ensure(sizeof(int) * 4, ws.stream));
+    const char *changed = "values-only update: the CSR structure changed since symbolic";
+    RTT_CHECK(map_device_error(validate_csr_device(ws, c->A.m, c->A.n, c->A.nnz, c->a_rp,
+                                                   c->a_ci, c->vflags.as<int>())));
+    if (!c->A.generic && ws.h_scalars[4] != 0)
+        return rtt::fail(RTT_ERR_INVALID_CSR, changed);
+    if (!c->b_alias && !c->op_aat)
+    {
+        RTT_CHECK(map_device_error(validate_csr_device(ws, c->B.m, c->B.n, c->B.nnz, c->b_rp,
+                                                       c->b_ci, c->vflags.as<int>())));
+        if (!c->B.generic && ws.h_scalars[4] != 0)
+            return rtt::fail(RTT_ERR_INVALID_CSR, changed);
+    }
+    // B's values for the numeric step: A's (A*A), A^T's (rebuilt below) or new
     if (c->b_alias)
         c->b_va = a_values;
     else if (c->op_aat)
-    {
-        // B = A^T again, values only (its structure is unchanged)
-        RTT_CHECK(csr_transpose_device(ws, c->A.m, c->A.n, c->A.nnz, c->a_rp, c->a_ci, a_values,
-                                       c->bt_rowptr.as<int>(), c->bt_col.as<int>(),
-                                       c->bt_val.as<double>()));
-        RTT_CHECK(map_device_error(csr2tile_refill_device(ws, c->bt_rowptr.as<int>(),
-                                                          c->bt_col.as<int>(),
-                                                          c->bt_val.as<double>(), c->B, true)));
         c->b_va = c->bt_val.as<double>();
-    }
     else if (b_values != nullptr)
-    {
-        RTT_CHECK(map_device_error(
-            csr2tile_refill_device(ws, c->b_rp, c->b_ci, b_values, c->B, true)));
         c->b_va = b_values;
-    }
-    return rtt_spgemm_numeric(c, c_row_ptr, c_col_idx, c_values);
+    int cutoff = 0;
+    const TileBufs &TB = c->b_alias ? c->A : c->B;
+    RTT_CHECK(effective_cutoff(c, c->A.view(), TB.view(), &cutoff));
+    std::vector<long long> key{1, as_key(a_values), as_key(b_values), as_key(c_row_ptr),
+                               as_key(c_col_idx), as_key(c_values)};
+    RTT_CHECK(run_phase(c, 1, key, c->cfg.fused_csr_output != 0, [&]() -> int {
+        // A's tiles take the new values (same structure, same tile order)
+        RTT_CHECK(map_device_error(
+            csr2tile_refill_device(ws, c->a_rp, c->a_ci, a_values, c->A, true)));
+        if (!c->b_alias && c->op_aat)
+        {
+            // B = A^T again, values only (its structure is unchanged)
+            RTT_CHECK(csr_transpose_device(ws, c->A.m, c->A.n, c->A.nnz, c->a_rp, c->a_ci,
+                                           a_values, c->bt_rowptr.as<int>(), c->bt_col.as<int>(),
+                                           c->bt_val.as<double>()));
+            RTT_CHECK(map_device_error(csr2tile_refill_device(ws, c->bt_rowptr.as<int>(),
+                                                              c->bt_col.as<int>(),
+                                                              c->bt_val.as<double>(), c->B, true)));
+        }
+        else if (!c->b_alias && b_values != nullptr)
+            RTT_CHECK(map_device_error(
+                csr2tile_refill_device(ws, c->b_rp, c->b_ci, b_values, c->B, true)));
+        return numeric_enqueue(c, c_row_ptr, c_col_idx, c_values, cutoff);
+    }));
+    return numeric_finish(c);
 }
 
 int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_values)
@@ -1280,66 +1559,16 @@ int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "ctx is NULL");
     if (!c->have_symbolic)
         return rtt::fail(RTT_ERR_STATE, "rtt_spgemm_numeric before rtt_spgemm_symbolic");
-    if (c_row_ptr == nullptr || (c->S.nnz > 0 && (c_col_idx == nullptr || c_values == nullptr)))
-        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "NULL output buffer");
+    RTT_CHECK(numeric_args_ok(c, c_row_ptr, c_col_idx, c_values));
     RTT_CUDA(cudaSetDevice(c->ws.device));
-    Workspace &ws = c->ws;
+    int cutoff = 0;
     const TileBufs &TB = c->b_alias ? c->A : c->B;
-    RTT_CHECK(c->counters.ensure(sizeof(long long) * 4, ws.stream));
-    RTT_CUDA(cudaMemsetAsync(c->counters.p, 0, sizeof(long long) * 4, ws.stream));
-    NumericConfig nc;
-    RTT_CHECK(effective_cutoff(c, c->A.view(), TB.view(), &nc.dmma_pair_cutoff));
-    nc.counters = c->counters.as<long long>();
-    nc.b_staging = c->cfg.b_staging != 0;
-    nc.split_target = c->cfg.split_target;
-    if (c->cfg.stage_timing)
-    {
-        nc.ev_begin = ws.ev[3];
-        nc.ev_end = ws.ev[4];
-    }
-    const bool fused = c->cfg.fused_csr_output != 0;
-    nc.write_tiles = !fused || c->cfg.keep_tiles != 0;
-    if (fused)
-    {
-        nc.csr_rowptr = c_row_ptr;
-        nc.csr_col = c_col_idx;
-        nc.csr_val = c_values;
-    }
-    DevTiles dB = TB.view();
-    dB.csr_rowptr = c->b_rp;
-    dB.csr_col = c->b_ci;
-    dB.csr_val = c->b_va;
-    dB.nnz = (int)c->b_nnz;
-    nc.conflict_safe = c->b_dups;
-    RTT_CHECK(numeric_select_device(ws, c->A.view(), dB, c->S, nc));
-    if (!fused)
-    {
-        SymbolicOut &S = c->S;
-        RTT_CHECK(csr_rowptr_device(ws, S, c_row_ptr));
-        RTT_CHECK(tile2csr_fill_device(ws, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(),
-                                       S.c_tile_nnz.as<int>(), S.c_ptr.as<uint8_t>(),
-                                       S.c_col.as<uint8_t>(), S.c_val.as<double>(), S.m, S.n,
-                                       S.tilem, TD, nullptr, -1, c_row_ptr, c_col_idx, c_values,
-                                       false));
-    }
-    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars64 + 2, c->counters.p, sizeof(long long) * 3,
-                             cudaMemcpyDeviceToHost, ws.stream));
-    RTT_CHECK(check_device_error(ws, "numeric"));
-    if (c->cfg.stage_timing && c->S.numtile > 0)
-    {
-        float tn = 0.f;
-        RTT_CUDA(cudaEventElapsedTime(&tn, ws.ev[3], ws.ev[4]));
-        c->stats.numeric_kernel_ms = tn;
-    }
-    c->stats.dmma_pairs = ws.h_scalars64[2];
-    c->stats.sparse_pairs = ws.h_scalars64[3];
-    // the numeric kernels count every (a_ik, b_kj) pair once: sum over A
-    // entries of nnz(B(k, :)), the reference's nnzCub
-    c->stats.nnz_cub = ws.h_scalars64[3];
-    c->stats.split_windows = ws.h_scalars64[4];
-    c->stats.kernel_launches = ws.launches;
-    c->stats.host_syncs = ws.syncs;
-    return RTT_OK;
+    RTT_CHECK(effective_cutoff(c, c->A.view(), TB.view(), &cutoff));
+    std::vector<long long> key{0, as_key(c_row_ptr), as_key(c_col_idx), as_key(c_values)};
+    RTT_CHECK(run_phase(c, 0, key, c->cfg.fused_csr_output != 0, [&]() -> int {
+        return numeric_enqueue(c, c_row_ptr, c_col_idx, c_values, cutoff);
+    }));
+    return numeric_finish(c);
 }
 
 // ------------------------------------------------------------ batched products
@@ -1491,16 +1720,30 @@ int rtt_spgemm_batched_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, do
         return rtt::fail(RTT_ERR_STATE, "rtt_spgemm_batched_numeric before rtt_spgemm_batched_symbolic");
     if (c_row_ptr == nullptr)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "NULL output buffer");
+    RTT_CHECK(numeric_args_ok(c, c_row_ptr, c_col_idx, c_values));
     RTT_CUDA(cudaSetDevice(c->ws.device));
     cudaStream_t s = c->ws.stream;
     RTT_CHECK(c->bat_big_rp.ensure(sizeof(int) * ((size_t)c->bat_rows + 1), s));
-    RTT_CHECK(rtt_spgemm_numeric(c, c->bat_big_rp.as<int>(), c_col_idx, c_values));
-    const int *meta_d = c->bat_meta.as<int>();
-    RTT_CHECK(batch_split_device(c->ws, c->bat_count, c->bat_rows, meta_d + c->bat_rowoff_off,
-                                 meta_d + c->bat_rows_off, meta_d + c->bat_sec_off,
-                                 meta_d + c->bat_colsub_off, c->bat_big_rp.as<int>(), c_row_ptr,
-                                 c_col_idx));
-    return RTT_OK;
+    int cutoff = 0;
+    const TileBufs &TB = c->b_alias ? c->A : c->B;
+    RTT_CHECK(effective_cutoff(c, c->A.view(), TB.view(), &cutoff));
+    std::vector<long long> key{2,
+                               as_key(c_row_ptr),
+                               as_key(c_col_idx),
+                               as_key(c_values),
+                               (long long)c->bat_rows_off,
+                               (long long)c->bat_rowoff_off,
+                               (long long)c->bat_sec_off,
+                               (long long)c->bat_colsub_off};
+    RTT_CHECK(run_phase(c, 2, key, c->cfg.fused_csr_output != 0, [&]() -> int {
+        RTT_CHECK(numeric_enqueue(c, c->bat_big_rp.as<int>(), c_col_idx, c_values, cutoff));
+        const int *meta_d = c->bat_meta.as<int>();
+        return batch_split_device(c->ws, c->bat_count, c->bat_rows, meta_d + c->bat_rowoff_off,
+                                  meta_d + c->bat_rows_off, meta_d + c->bat_sec_off,
+                                  meta_d + c->bat_colsub_off, c->bat_big_rp.as<int>(),
+                                  c_row_ptr, c_col_idx);
+    }));
+    return numeric_finish(c);
 }
 
 int rtt_reorder_plan_build(rtt_context c, const rtt_csr_view *A, rtt_reorder_plan *plan)

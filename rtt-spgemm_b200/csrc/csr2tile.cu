@@ -955,6 +955,21 @@ int csr2tile_refill_device(Workspace &ws, const int *rowptr, const int *col, con
     return RTT_OK;
 }
 
+int validate_csr_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
+                        int *flags)
+{
+    RTT_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * 3, ws.stream));
+    if (m > 0)
+    {
+        k_validate_csr<<<grid_for(m, 256), 256, 0, ws.stream>>>(m, n, nnz, rowptr, col,
+                                                                ws.err.as<int>(), flags);
+        ws.launches++;
+    }
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 4, flags, sizeof(int) * 3, cudaMemcpyDeviceToHost,
+                             ws.stream));
+    return check_device_error(ws, "csr validate");
+}
+
 int build_tile_csc(Workspace &ws, TileBufs &t)
 {
     cudaStream_t s = ws.stream;

@@ -223,6 +223,8 @@ int check_device_error(Workspace &ws, const char *stage);
 // copy one int / int64 from device to host (syncs)
 int read_int(Workspace &ws, const int *d, int *h);
 int read_i64(Workspace &ws, const long long *d, long long *h);
+// while on, DevBuf growth on this thread fails with RTT_ERR_STATE (graph capture)
+void freeze_growth(bool on);
 
 // ------------------------------------------------------------- kernel hosts
 // csr2tile: row-major tiles of a device CSR.  Output arrays allocated from bufs.
@@ -236,6 +238,16 @@ struct TileBufs
     bool generic = false;  // built by the generic (unsorted tile columns) path
     void release();
     DevTiles view() const;
+    // every device buffer of the struct (release, CUDA-graph keys)
+    template <class F>
+    void each(F &&f) const
+    {
+        const DevBuf *all[] = {&tile_ptr, &tile_col, &tile_row, &tile_nnz, &ptr, &col,
+                               &val,      &mask,     &csc_ptr,  &csc_row,  &csc_data,
+                               &row_data, &tmp0,     &tmp1,     &tmp2,     &tmp3};
+        for (const DevBuf *b : all)
+            f(*b);
+    }
 };
 
 int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
@@ -244,6 +256,12 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
 // from a CSR of the same structure get the values val (no host round trip)
 int csr2tile_refill_device(Workspace &ws, const int *rowptr, const int *col, const double *val,
                            TileBufs &t, bool packed_col);
+// k_validate_csr on the device, then the host reads the error word (syncs):
+// RTT_ERR_DEVICE_CHECK code 101/102 for a malformed CSR; flags: 3 device ints
+// (tile column / column decreases in a row, repeated column), copied to
+// ws.h_scalars[4..6]
+int validate_csr_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
+                        int *flags);
 // tile CSC index (column lists) over row-major tiles
 int build_tile_csc(Workspace &ws, TileBufs &t);
 // rearrange row-major tiles into the csr2tile_col_major layout (data in CSC order)
@@ -293,6 +311,17 @@ struct SymbolicOut
     int tilem = 0, tilen = 0, m = 0, n = 0;
     void release();
     DevCTiles view();
+    // every device buffer of the struct (release, CUDA-graph keys)
+    template <class F>
+    void each(F &&f) const
+    {
+        const DevBuf *all[] = {&c_tile_ptr, &c_tile_col, &c_tile_row, &c_tile_nnz, &c_mask,
+                               &c_ptr,      &c_col,      &c_val,      &c_row_cnt,  &c_rowptr,
+                               &c_tr_nnz,   &count_tmp,  &tile_cnt,   &w_task,     &w_heavy,
+                               &w_queue,    &w_flag,     &s2_heavy,   &s2_list};
+        for (const DevBuf *b : all)
+            f(*b);
+    }
 };
 
 // b_sorted: B's CSR rows have strictly increasing columns (lets the walk of a

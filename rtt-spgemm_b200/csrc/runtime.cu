@@ -32,6 +32,15 @@ int cuda_fail(cudaError_t e, const char *what)
     return fail(RTT_ERR_CUDA, m);
 }
 
+// Growth is refused on a thread that is capturing a CUDA graph (a captured
+// cudaMallocAsync would hand the buffer to the graph).
+namespace
+{
+thread_local bool g_growth_frozen = false;
+} // namespace
+
+void freeze_growth(bool on) { g_growth_frozen = on; }
+
 // Grow-only buffers from the device's stream-ordered pool: a regrow frees
 // and allocates in the order of stream s, without the device-wide
 // synchronisation of cudaFree / cudaMalloc, so contexts that run on other
@@ -44,6 +53,8 @@ int DevBuf::ensure(size_t bytes, cudaStream_t s)
         bytes = 16;
     if (bytes <= cap)
         return RTT_OK;
+    if (g_growth_frozen)
+        return fail(RTT_ERR_STATE, "device buffer growth inside a CUDA graph capture");
     if (p != nullptr)
     {
         if (cudaFreeAsync(p, s) != cudaSuccess)
@@ -242,10 +253,7 @@ int read_i64(Workspace &ws, const long long *d, long long *h)
 
 void TileBufs::release()
 {
-    DevBuf *all[] = {&tile_ptr, &tile_col, &tile_row, &tile_nnz, &ptr, &col, &val, &mask,
-                     &csc_ptr, &csc_row, &csc_data, &row_data, &tmp0, &tmp1, &tmp2, &tmp3};
-    for (DevBuf *b : all)
-        b->release();
+    each([](const DevBuf &b) { const_cast<DevBuf &>(b).release(); });
 }
 
 DevTiles TileBufs::view() const
@@ -276,11 +284,7 @@ DevTiles TileBufs::view() const
 
 void SymbolicOut::release()
 {
-    DevBuf *all[] = {&c_tile_ptr, &c_tile_col, &c_tile_row, &c_tile_nnz, &c_mask, &c_ptr,
-                     &c_col, &c_val, &c_row_cnt, &c_rowptr, &c_tr_nnz, &count_tmp,
-                     &tile_cnt, &w_task, &w_heavy, &w_queue, &w_flag, &s2_heavy, &s2_list};
-    for (DevBuf *b : all)
-        b->release();
+    each([](const DevBuf &b) { const_cast<DevBuf &>(b).release(); });
 }
 
 DevCTiles SymbolicOut::view()

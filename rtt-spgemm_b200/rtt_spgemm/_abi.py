@@ -71,7 +71,8 @@ class CsrView(C.Structure):
 class Config(C.Structure):
     _fields_ = [("dmma_pair_cutoff", C.c_int), ("fused_csr_output", C.c_int),
                 ("keep_tiles", C.c_int), ("stage_timing", C.c_int), ("b_staging", C.c_int),
-                ("split_target", C.c_int), ("reserved", C.c_int * 5)]
+                ("split_target", C.c_int), ("cuda_graphs", C.c_int),
+                ("reserved", C.c_int * 4)]
 
 
 class HybridTiles(C.Structure):
@@ -131,7 +132,8 @@ class Stats(C.Structure):
                 ("dmma_pairs", C.c_longlong), ("sparse_pairs", C.c_longlong),
                 ("kernel_launches", C.c_int), ("host_syncs", C.c_int),
                 ("csr2tile_ms", C.c_double), ("symbolic_ms", C.c_double),
-                ("numeric_kernel_ms", C.c_double), ("split_windows", C.c_longlong)]
+                ("numeric_kernel_ms", C.c_double), ("split_windows", C.c_longlong),
+                ("graph_launched", C.c_int)]
 
 
 def build(verbose: bool = False) -> Path:
