@@ -216,6 +216,48 @@ RTT_API int rtt_csr_to_hybrid_tiles(const SMatrix *csr, int tile_rows, int tile_
                                     int col_major, int dense_threshold, int build_csc,
                                     rtt_hybrid_tiles *out);
 
+/* Operand roles of the Super16 index (the reference's rtt::super16::OperandRole,
+ * src/super16_symbolic.cuh:64-68). */
+#define RTT_SUPER16_A8X4 1
+#define RTT_SUPER16_B4X8 2
+
+/* The reference's Super16 16x16 parent index over hybrid leaf tiles
+ * (rtt::super16::DeviceIndexView, src/super16_symbolic.cuh:85-106), field for
+ * field, as host arrays.  A parent is the 16x16 block of 2 x 4 A leaves (8x4)
+ * or 4 x 2 B leaves (4x8).  Parents of a parent row are in increasing column
+ * order; a parent's leaves (child_leaf_ids[child_ptr[p] ..]) are listed leaf
+ * row by leaf row, each in leaf-column order; child_mask bit
+ * child_row * col_group + leaf_col % col_group marks a present leaf
+ * (col_group 4 for A, 2 for B); boolean_row_masks[16 p + r] has bit c set when
+ * (r, c) of the parent is structurally nonzero (LSB = column 0).  B also gets
+ * the parent CSC (rows in increasing order per column), NULL for A. */
+typedef struct
+{
+    unsigned int role;
+    int rows, cols;
+    unsigned int parent_row_count, parent_col_count, parent_count;
+    unsigned long long *row_ptr;       /* parent_row_count + 1 */
+    unsigned int *col_idx;             /* parent_count */
+    unsigned long long *child_ptr;     /* parent_count + 1 */
+    unsigned char *child_mask;         /* parent_count */
+    unsigned int *child_leaf_ids;      /* num_tiles of the leaves */
+    unsigned short *boolean_row_masks; /* parent_count * 16 */
+    unsigned long long *col_ptr;       /* B4x8: parent_col_count + 1 */
+    unsigned int *row_idx;             /* B4x8: parent_count */
+    unsigned int *csc_parent_ids;      /* B4x8: parent_count */
+} rtt_super16_index;
+
+/* Replaces build_device_index (src/super16_symbolic.cuh:2123-2323): the
+ * Super16 index of leaf tiles from rtt_csr_to_hybrid_tiles (8x4 for
+ * RTT_SUPER16_A8X4, 4x8 for RTT_SUPER16_B4X8), built on the GPU, returned in
+ * malloc'd arrays (free with rtt_super16_index_destroy).  Leaf rows must list
+ * strictly increasing tile columns inside [0, tile_col_count) (as
+ * rtt_csr_to_hybrid_tiles writes them); otherwise RTT_ERR_INVALID_ARGUMENT.
+ * out is untouched on failure. */
+RTT_API int rtt_super16_index_build(const rtt_hybrid_tiles *leaf, unsigned int role,
+                                    rtt_super16_index *out);
+RTT_API void rtt_super16_index_destroy(rtt_super16_index *index);
+
 /* Tail-queue admission (the reference's DmmaTileTailQueuePolicy / CostModel /
  * Plan, src/dmma_tile_tail_queue.h:20-121; enabled is the policy switch). */
 typedef struct

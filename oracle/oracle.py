@@ -221,6 +221,64 @@ def csr_to_hybrid_tiles(csr, tile_rows: int, tile_cols: int, col_major: bool,
     return d
 
 
+def super16_index(leaf: dict, role: int) -> dict:
+    """Restatement of build_device_index (src/super16_symbolic.cuh:2123-2323)
+    over hybrid leaf tiles.  A parent groups RG x CG leaves: 2 x 4 of the 8x4
+    A leaves (role 1), 4 x 2 of the 4x8 B leaves (role 2) (:2145-2160).  Per
+    parent row the parent columns are the distinct leaf_col // CG of its leaf
+    rows (:674-718); a parent's leaves are listed leaf row by leaf row in leaf
+    order, and child_mask bit child_row * CG + leaf_col % CG marks each
+    (:720-789); the 16 Boolean rows have bit c for column c of the parent
+    (:797-864); B also gets its parent CSC ordered by (column, row)
+    (:866-907, :2262-2311)."""
+    a_role = role == 1
+    RG, CG = (2, 4) if a_role else (4, 2)
+    def arr(k, dt):  # absent arrays of an empty leaf matrix
+        return np.zeros(0, dt) if leaf[k] is None else np.asarray(leaf[k], dt)
+
+    trp, tci, masks = arr("tile_row_ptr", np.int64), arr("tile_col_idx", np.int64), arr("masks", np.uint64)
+    lrows, nt = int(leaf["tile_row_count"]), int(leaf["num_tiles"])
+    prows = 0 if lrows == 0 else 1 + (lrows - 1) // RG
+    pcols = 0 if leaf["tile_col_count"] == 0 else 1 + (int(leaf["tile_col_count"]) - 1) // CG
+    lrow = np.repeat(np.arange(lrows, dtype=np.int64), np.diff(trp))
+    prow, pcol, child = lrow // RG, tci // CG, lrow % RG
+    W = max(pcols, 1)
+    ukey, parent = np.unique(prow * W + pcol, return_inverse=True)
+    pc = ukey.size
+    row_ptr = np.concatenate([[0], np.cumsum(np.bincount(ukey // W, minlength=prows))])
+    order = np.lexsort((np.arange(nt), child, parent))
+    child_ptr = np.concatenate([[0], np.cumsum(np.bincount(parent, minlength=pc))])
+    child_mask = np.zeros(pc, np.uint8)
+    np.bitwise_or.at(child_mask, parent, (1 << (child * CG + tci % CG)).astype(np.uint8))
+    rows = np.zeros(pc * 16, np.uint16)
+    if a_role:
+        for lr in range(8):  # leaf row lr of the leaf is parent row 8 child + lr
+            bits = ((masks >> np.uint64(4 * lr)) & np.uint64(0xF)) << (4 * (tci % 4)).astype(np.uint64)
+            np.bitwise_or.at(rows, parent * 16 + child * 8 + lr, bits.astype(np.uint16))
+    else:
+        for k in range(4):  # leaf row k is parent row 4 child + k
+            bits = np.zeros(nt, np.uint64)
+            for c in range(8):
+                bits |= ((masks >> np.uint64(4 * c + k)) & np.uint64(1)) << np.uint64(c)
+            bits <<= (8 * (tci % 2)).astype(np.uint64)
+            np.bitwise_or.at(rows, parent * 16 + child * 4 + k, bits.astype(np.uint16))
+    d = {"role": role, "rows": int(leaf["rows"]), "cols": int(leaf["cols"]),
+         "parent_row_count": prows, "parent_col_count": pcols, "parent_count": pc,
+         "row_ptr": row_ptr.astype(np.uint64), "col_idx": (ukey % W).astype(np.uint32),
+         "child_ptr": child_ptr.astype(np.uint64), "child_mask": child_mask,
+         "child_leaf_ids": order.astype(np.uint32), "boolean_row_masks": rows,
+         "col_ptr": None, "row_idx": None, "csc_parent_ids": None}
+    if not a_role:
+        p_row = np.repeat(np.arange(prows, dtype=np.int64), np.diff(row_ptr))
+        ckey = (ukey % W) * max(prows, 1) + p_row
+        corder = np.argsort(ckey, kind="stable")
+        d["col_ptr"] = np.concatenate([[0], np.cumsum(np.bincount(ukey % W, minlength=pcols))]
+                                      ).astype(np.uint64)
+        d["row_idx"] = p_row[corder].astype(np.uint32)
+        d["csc_parent_ids"] = corder.astype(np.uint32)
+    return d
+
+
 def tiles_8x4(a, row_old_to_new=None, col_old_to_new=None) -> int:
     """Distinct 8x4 tiles of A under row / column maps: the quantity of the
     reference's exact reorder commit rule (src/dmma_reorder.h:1671-1727)."""
@@ -508,6 +566,9 @@ class Oracle(_Base):
                             dense_threshold=24, build_csc=False) -> dict:
         return csr_to_hybrid_tiles(csr, tile_rows, tile_cols, col_major, dense_threshold,
                                    build_csc)
+
+    def super16_index(self, leaf: dict, role: int) -> dict:
+        return super16_index(leaf, role)
 
     def nnzcub(self, a, b) -> int:
         return int(self.lib.orc_nnzcub(a.m, a.rowptr.ctypes.data, a.col.ctypes.data,

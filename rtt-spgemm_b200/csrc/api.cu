@@ -1209,6 +1209,60 @@ int rtt_csr_to_hybrid_tiles(const SMatrix *M, int tile_rows, int tile_cols, int 
                                                dense_threshold, build_csc, out));
 }
 
+int rtt_super16_index_build(const rtt_hybrid_tiles *L, unsigned int role, rtt_super16_index *out)
+{
+    if (L == nullptr || out == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "super16 index: NULL argument");
+    // leaf geometry and arrays (the checks of build_device_index,
+    // src/super16_symbolic.cuh:2128-2143, plus the sorted leaf rows its merge assumes)
+    const bool a_role = role == RTT_SUPER16_A8X4;
+    if (!a_role && role != RTT_SUPER16_B4X8)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "super16 index: role must be A8x4 or B4x8");
+    if ((a_role && (L->tile_rows != 8 || L->tile_cols != 4)) ||
+        (!a_role && (L->tile_rows != 4 || L->tile_cols != 8)))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "super16 index: leaf geometry does not fit the role");
+    if (L->rows < 0 || L->cols < 0 || L->tile_row_count < 0 || L->tile_col_count < 0 ||
+        L->num_tiles < 0 || L->tile_row_ptr == nullptr ||
+        (L->num_tiles > 0 && (L->tile_col_idx == nullptr || L->masks == nullptr ||
+                              L->tile_row_count == 0 || L->tile_col_count == 0)))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "super16 index: malformed leaf tiles");
+    if (L->tile_row_ptr[0] != 0 || L->tile_row_ptr[L->tile_row_count] != L->num_tiles)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "super16 index: bad leaf row pointer");
+    for (int r = 0; r < L->tile_row_count; ++r)
+    {
+        const int b = L->tile_row_ptr[r], e = L->tile_row_ptr[r + 1];
+        if (b > e || e > L->num_tiles)
+            return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "super16 index: bad leaf row pointer");
+        for (int t = b; t < e; ++t)
+        {
+            const int col = L->tile_col_idx[t];
+            if (col < 0 || col >= L->tile_col_count || (t > b && col <= L->tile_col_idx[t - 1]))
+                return rtt::fail(RTT_ERR_INVALID_ARGUMENT,
+                                 "super16 index: leaf columns must increase inside a leaf row");
+        }
+    }
+    std::lock_guard<std::mutex> lock(g_mutex);
+    rtt_context c = nullptr;
+    RTT_CHECK(default_context(&c));
+    return super16_index_host(c->ws, L, role, out);
+}
+
+void rtt_super16_index_destroy(rtt_super16_index *x)
+{
+    if (x == nullptr)
+        return;
+    std::free(x->row_ptr);
+    std::free(x->col_idx);
+    std::free(x->child_ptr);
+    std::free(x->child_mask);
+    std::free(x->child_leaf_ids);
+    std::free(x->boolean_row_masks);
+    std::free(x->col_ptr);
+    std::free(x->row_idx);
+    std::free(x->csc_parent_ids);
+    std::memset(x, 0, sizeof(*x));
+}
+
 int rtt_plan_tail_queue(int ntasks, const int *scans, const int *matches, const int *output_nnz,
                         const rtt_tail_policy *policy, const rtt_tail_cost_model *model,
                         int *chunks_out, rtt_tail_plan *plan)

@@ -19,6 +19,8 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
+#include <algorithm>
+
 #include <climits>
 #include <cstdlib>
 #include <cstring>
@@ -392,6 +394,339 @@ int csr_to_hybrid_host(Workspace &ws, const SMatrix *M, int tr, int tc, int col_
     if (st != RTT_OK)
     {
         rtt_hybrid_tiles_destroy(&h);
+        return st;
+    }
+    *out = h;
+    return RTT_OK;
+}
+
+// ------------------------------------------------------------- Super16 index
+// The 16x16 parent index over leaf tiles (reference build_device_index,
+// src/super16_symbolic.cuh:2123-2323).  A parent row covers RG leaf rows (2
+// for 8x4 A leaves, 4 for 4x8 B leaves) and a parent column CG leaf columns
+// (4 for A, 2 for B).  Each leaf row lists strictly increasing leaf columns,
+// so a parent row's parents are the merged quotients leaf column / CG of its
+// RG lists: one thread per parent row keeps one cursor per list.
+namespace
+{
+
+template <int RG, int CG>
+__device__ __forceinline__ int s16_next(const int *__restrict__ tcol, const int (&cur)[RG],
+                                        const int (&end)[RG])
+{
+    int nxt = INT_MAX;
+#pragma unroll
+    for (int c = 0; c < RG; ++c)
+        if (cur[c] < end[c])
+            nxt = min(nxt, tcol[cur[c]] / CG);
+    return nxt;
+}
+
+template <int RG>
+__device__ __forceinline__ void s16_open(int P, int lrows, const int *__restrict__ tptr, int (&cur)[RG],
+                                         int (&end)[RG])
+{
+#pragma unroll
+    for (int c = 0; c < RG; ++c)
+    {
+        const int lr = P * RG + c;
+        cur[c] = lr < lrows ? tptr[lr] : 0;
+        end[c] = lr < lrows ? tptr[lr + 1] : 0;
+    }
+}
+
+// parents per parent row
+template <int RG, int CG>
+__global__ void k_s16_count(int prows, int lrows, const int *__restrict__ tptr,
+                            const int *__restrict__ tcol, unsigned long long *__restrict__ cnt)
+{
+    const int P = blockIdx.x * blockDim.x + threadIdx.x;
+    if (P >= prows)
+        return;
+    int cur[RG], end[RG];
+    s16_open<RG>(P, lrows, tptr, cur, end);
+    unsigned long long n = 0;
+    for (int J = s16_next<RG, CG>(tcol, cur, end); J != INT_MAX; J = s16_next<RG, CG>(tcol, cur, end))
+    {
+        ++n;
+#pragma unroll
+        for (int c = 0; c < RG; ++c)
+            while (cur[c] < end[c] && tcol[cur[c]] / CG == J)
+                ++cur[c];
+    }
+    cnt[P] = n;
+}
+
+// parent columns, child pointers and masks, leaf ids (leaf row by leaf row)
+template <int RG, int CG>
+__global__ void k_s16_fill(int prows, int lrows, const int *__restrict__ tptr,
+                           const int *__restrict__ tcol, const unsigned long long *__restrict__ rowptr,
+                           unsigned *__restrict__ pcol, unsigned long long *__restrict__ cptr,
+                           unsigned char *__restrict__ cmask, unsigned *__restrict__ leaf_ids)
+{
+    const int P = blockIdx.x * blockDim.x + threadIdx.x;
+    if (P >= prows)
+        return;
+    int cur[RG], end[RG];
+    s16_open<RG>(P, lrows, tptr, cur, end);
+    unsigned long long p = rowptr[P];
+    // the parent row's leaves are the ids tptr[RG P] .. of its leaf rows
+    unsigned long long out = (unsigned long long)cur[0];
+    for (int J = s16_next<RG, CG>(tcol, cur, end); J != INT_MAX; J = s16_next<RG, CG>(tcol, cur, end))
+    {
+        unsigned mk = 0;
+        pcol[p] = (unsigned)J;
+        cptr[p] = out;
+#pragma unroll
+        for (int c = 0; c < RG; ++c)
+            while (cur[c] < end[c] && tcol[cur[c]] / CG == J)
+            {
+                const int id = cur[c]++;
+                mk |= 1u << (c * CG + tcol[id] % CG);
+                leaf_ids[out++] = (unsigned)id;
+            }
+        cmask[p] = (unsigned char)mk;
+        ++p;
+    }
+}
+
+__global__ void k_s16_set(unsigned long long *p, unsigned long long v) { *p = v; }
+
+// The 16 Boolean rows of every parent (thread per parent row r).  A leaves
+// are 8x4 with bit r * 4 + c; B leaves 4x8 with bit c * 4 + r.
+template <bool A_ROLE>
+__global__ void k_s16_rows(long long n, const unsigned long long *__restrict__ cptr,
+                           const unsigned char *__restrict__ cmask,
+                           const unsigned *__restrict__ leaf_ids, const unsigned *__restrict__ lmask,
+                           unsigned short *__restrict__ rows)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const long long p = i >> 4;
+    const int r = (int)(i & 15);
+    const unsigned occ = cmask[p];
+    const unsigned long long base = cptr[p];
+    unsigned res = 0;
+    if (A_ROLE)
+    {
+        // leaf (r / 8, t): its row r % 8 is 4 bits, columns 4 t .. 4 t + 3
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+        {
+            const int slot = (r >> 3) * 4 + t;
+            if ((occ >> slot) & 1u)
+            {
+                const unsigned m = lmask[leaf_ids[base + __popc(occ & ((1u << slot) - 1u))]];
+                res |= ((m >> ((r & 7) * 4)) & 0xFu) << (4 * t);
+            }
+        }
+    }
+    else
+    {
+        // leaf (r / 4, h): its row k = r % 4 is every fourth bit from k,
+        // columns 8 h .. 8 h + 7
+        const int k = r & 3;
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+        {
+            const int slot = (r >> 2) * 2 + h;
+            if ((occ >> slot) & 1u)
+            {
+                const unsigned m = lmask[leaf_ids[base + __popc(occ & ((1u << slot) - 1u))]] >> k;
+                unsigned row8 = 0;
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    row8 |= ((m >> (4 * c)) & 1u) << c;
+                res |= row8 << (8 * h);
+            }
+        }
+    }
+    rows[i] = (unsigned short)res;
+}
+
+// parent CSC of B: keys column * prows + row, sorted, then split
+__global__ void k_s16_csc_keys(int prows, const unsigned long long *__restrict__ rowptr,
+                               const unsigned *__restrict__ pcol,
+                               unsigned long long *__restrict__ keys, unsigned *__restrict__ ids)
+{
+    const int P = blockIdx.x * blockDim.x + threadIdx.x;
+    if (P >= prows)
+        return;
+    for (unsigned long long id = rowptr[P]; id < rowptr[P + 1]; ++id)
+    {
+        keys[id] = (unsigned long long)pcol[id] * (unsigned long long)prows + (unsigned long long)P;
+        ids[id] = (unsigned)id;
+    }
+}
+
+__global__ void k_s16_csc_rows(long long n, int prows, const unsigned long long *__restrict__ keys,
+                               unsigned *__restrict__ row_idx)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        row_idx[i] = (unsigned)(keys[i] % (unsigned long long)prows);
+}
+
+// col_ptr[c] = first sorted key of column c or later
+__global__ void k_s16_col_ptr(int pcols, int prows, long long n,
+                              const unsigned long long *__restrict__ keys,
+                              unsigned long long *__restrict__ col_ptr)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > pcols)
+        return;
+    const unsigned long long want = (unsigned long long)c * (unsigned long long)prows;
+    long long lo = 0, hi = n;
+    while (lo < hi)
+    {
+        const long long mid = (lo + hi) >> 1;
+        if (keys[mid] < want)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    col_ptr[c] = (unsigned long long)lo;
+}
+
+} // namespace
+
+int super16_index_host(Workspace &ws, const rtt_hybrid_tiles *L, unsigned role,
+                       rtt_super16_index *out)
+{
+    cudaStream_t s = ws.stream;
+    const bool a_role = role == RTT_SUPER16_A8X4;
+    const int RG = a_role ? 2 : 4, CG = a_role ? 4 : 2;
+    const int lrows = L->tile_row_count, nt = L->num_tiles;
+    const int prows = lrows == 0 ? 0 : 1 + (lrows - 1) / RG;
+    const int pcols = L->tile_col_count == 0 ? 0 : 1 + (L->tile_col_count - 1) / CG;
+    DevArrays D;
+    int *tptr = nullptr, *tcol = nullptr;
+    unsigned *lmask = nullptr;
+    unsigned long long *cnt = nullptr, *rowptr = nullptr;
+    RTT_CHECK(D.get(&tptr, (size_t)lrows + 1));
+    RTT_CHECK(D.get(&tcol, (size_t)nt));
+    RTT_CHECK(D.get(&lmask, (size_t)nt));
+    RTT_CHECK(D.get(&cnt, (size_t)prows + 1));
+    RTT_CHECK(D.get(&rowptr, (size_t)prows + 1));
+    RTT_CUDA(cudaMemcpyAsync(tptr, L->tile_row_ptr, sizeof(int) * ((size_t)lrows + 1),
+                             cudaMemcpyHostToDevice, s));
+    if (nt > 0)
+    {
+        RTT_CUDA(cudaMemcpyAsync(tcol, L->tile_col_idx, sizeof(int) * (size_t)nt,
+                                 cudaMemcpyHostToDevice, s));
+        RTT_CUDA(cudaMemcpyAsync(lmask, L->masks, sizeof(unsigned) * (size_t)nt,
+                                 cudaMemcpyHostToDevice, s));
+    }
+    RTT_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * ((size_t)prows + 1), s));
+    if (prows > 0)
+    {
+        if (a_role)
+            k_s16_count<2, 4><<<blocks(prows, 128), 128, 0, s>>>(prows, lrows, tptr, tcol, cnt);
+        else
+            k_s16_count<4, 2><<<blocks(prows, 128), 128, 0, s>>>(prows, lrows, tptr, tcol, cnt);
+    }
+    size_t bytes = 0;
+    RTT_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt, rowptr, prows + 1, s));
+    RTT_CHECK(ws.scan_tmp.ensure(bytes, s));
+    RTT_CUDA(cub::DeviceScan::ExclusiveSum(ws.scan_tmp.p, bytes, cnt, rowptr, prows + 1, s));
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars64, rowptr + prows, sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost, s));
+    RTT_CUDA(cudaStreamSynchronize(s));
+    const unsigned long long pc64 = (unsigned long long)ws.h_scalars64[0];
+    if (pc64 > 0xFFFFFFFFull || (!a_role && pc64 > (unsigned long long)INT_MAX))
+        return fail(RTT_ERR_UNREPRESENTABLE, "super16 index: too many parents");
+    const long long pc = (long long)pc64;
+
+    unsigned *pcol = nullptr, *leaf_ids = nullptr;
+    unsigned long long *cptr = nullptr;
+    unsigned char *cmask = nullptr;
+    unsigned short *brows = nullptr;
+    RTT_CHECK(D.get(&pcol, (size_t)pc));
+    RTT_CHECK(D.get(&cptr, (size_t)pc + 1));
+    RTT_CHECK(D.get(&cmask, (size_t)pc));
+    RTT_CHECK(D.get(&leaf_ids, (size_t)nt));
+    RTT_CHECK(D.get(&brows, (size_t)pc * 16));
+    if (prows > 0)
+    {
+        if (a_role)
+            k_s16_fill<2, 4><<<blocks(prows, 128), 128, 0, s>>>(prows, lrows, tptr, tcol, rowptr,
+                                                               pcol, cptr, cmask, leaf_ids);
+        else
+            k_s16_fill<4, 2><<<blocks(prows, 128), 128, 0, s>>>(prows, lrows, tptr, tcol, rowptr,
+                                                               pcol, cptr, cmask, leaf_ids);
+    }
+    k_s16_set<<<1, 1, 0, s>>>(cptr + pc, (unsigned long long)nt);
+    if (pc > 0)
+    {
+        if (a_role)
+            k_s16_rows<true><<<blocks(pc * 16, 256), 256, 0, s>>>(pc * 16, cptr, cmask, leaf_ids,
+                                                                 lmask, brows);
+        else
+            k_s16_rows<false><<<blocks(pc * 16, 256), 256, 0, s>>>(pc * 16, cptr, cmask, leaf_ids,
+                                                                  lmask, brows);
+    }
+    unsigned long long *col_ptr = nullptr;
+    unsigned *row_idx = nullptr, *csc_ids = nullptr;
+    if (!a_role)
+    {
+        unsigned long long *keys = nullptr, *skeys = nullptr;
+        unsigned *ids = nullptr;
+        RTT_CHECK(D.get(&keys, (size_t)pc));
+        RTT_CHECK(D.get(&skeys, (size_t)pc));
+        RTT_CHECK(D.get(&ids, (size_t)pc));
+        RTT_CHECK(D.get(&csc_ids, (size_t)pc));
+        RTT_CHECK(D.get(&row_idx, (size_t)pc));
+        RTT_CHECK(D.get(&col_ptr, (size_t)pcols + 1));
+        if (pc > 0)
+        {
+            k_s16_csc_keys<<<blocks(prows, 128), 128, 0, s>>>(prows, rowptr, pcol, keys, ids);
+            int kbits = 1;
+            const unsigned long long top = (unsigned long long)pcols * (unsigned long long)prows;
+            while (kbits < 64 && (top >> kbits) != 0)
+                ++kbits;
+            bytes = 0;
+            RTT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys, skeys, ids, csc_ids,
+                                                     (int)pc, 0, kbits, s));
+            RTT_CHECK(ws.scan_tmp.ensure(bytes, s));
+            RTT_CUDA(cub::DeviceRadixSort::SortPairs(ws.scan_tmp.p, bytes, keys, skeys, ids,
+                                                     csc_ids, (int)pc, 0, kbits, s));
+            k_s16_csc_rows<<<blocks(pc, 256), 256, 0, s>>>(pc, prows, skeys, row_idx);
+        }
+        k_s16_col_ptr<<<blocks((long long)pcols + 1, 256), 256, 0, s>>>(pcols, prows, pc, skeys,
+                                                                       col_ptr);
+    }
+    RTT_CUDA(cudaGetLastError());
+
+    rtt_super16_index h{};
+    h.role = role;
+    h.rows = L->rows;
+    h.cols = L->cols;
+    h.parent_row_count = (unsigned)prows;
+    h.parent_col_count = (unsigned)pcols;
+    h.parent_count = (unsigned)pc;
+    int st = to_host(&h.row_ptr, rowptr, (size_t)prows + 1, s);
+    if (st == RTT_OK)
+        st = to_host(&h.col_idx, pcol, (size_t)pc, s);
+    if (st == RTT_OK)
+        st = to_host(&h.child_ptr, cptr, (size_t)pc + 1, s);
+    if (st == RTT_OK)
+        st = to_host(&h.child_mask, cmask, (size_t)pc, s);
+    if (st == RTT_OK)
+        st = to_host(&h.child_leaf_ids, leaf_ids, (size_t)nt, s);
+    if (st == RTT_OK)
+        st = to_host(&h.boolean_row_masks, brows, (size_t)pc * 16, s);
+    if (st == RTT_OK && !a_role)
+    {
+        st = to_host(&h.col_ptr, col_ptr, (size_t)pcols + 1, s);
+        if (st == RTT_OK)
+            st = to_host(&h.row_idx, row_idx, (size_t)pc, s);
+        if (st == RTT_OK)
+            st = to_host(&h.csc_parent_ids, csc_ids, (size_t)pc, s);
+    }
+    if (st != RTT_OK)
+    {
+        rtt_super16_index_destroy(&h);
         return st;
     }
     *out = h;

@@ -385,6 +385,9 @@ int plan_tail_queue_device(Workspace &ws, int n, const int *d_scans, const int *
 // CSR (host arrays) -> hybrid leaf tiles on the device, results malloc'd into out
 int csr_to_hybrid_host(Workspace &ws, const SMatrix *M, int tile_rows, int tile_cols,
                        int col_major, int dense_threshold, int build_csc, rtt_hybrid_tiles *out);
+// Super16 parent index of validated host leaf tiles (role 1 = A8x4, 2 = B4x8)
+int super16_index_host(Workspace &ws, const rtt_hybrid_tiles *leaf, unsigned role,
+                       rtt_super16_index *out);
 // launch-only forms (no workspace, identity row order): the caller owns the
 // stream and the error word; row_cnt needs m entries cleared to zero
 int tile2csr_count_launch(cudaStream_t s, const int *tile_ptr, const int *tile_col,

@@ -27,14 +27,15 @@ from types import SimpleNamespace
 import numpy as np
 
 from . import generators
-from ._abi import (EXPORTS, LIB_PATH, RTT_OP_AAT, RTT_OP_AB, Config, CsrView, EarlySplitPlan,
+from ._abi import (EXPORTS, LIB_PATH, RTT_OP_AAT, RTT_OP_AB, RTT_SUPER16_A8X4, RTT_SUPER16_B4X8,
+                   Super16Index, Config, CsrView, EarlySplitPlan,
                    HybridTiles, ReorderPlan, RttError, SMatrix, Stats, TailCostModel, TailPlan,
                    TailPolicy, build, check, lib)
 from .generators import CSR
 
 __all__ = ["CSR", "Context", "RttError", "build", "csr2tile_col_major", "csr2tile_row_major",
            "generators", "lib", "spgemm_csr_host", "spgemm_tile", "tile16_to_tile8", "tile2csr",
-           "tile2csr_device_noalloc", "csr_to_hybrid_tiles", "plan_tail_queue",
+           "tile2csr_device_noalloc", "csr_to_hybrid_tiles", "super16_index", "plan_tail_queue",
            "plan_early_split", "early_split_policy_default",
            "TAIL_POLICY_DEFAULT", "TAIL_MODEL_DEFAULT", "spgemm_batched",
            "EXPORTS", "LIB_PATH", "RTT_OP_AB", "RTT_OP_AAT"]
@@ -214,6 +215,55 @@ def csr_to_hybrid_tiles(csr, tile_rows: int = 8, tile_cols: int = 4, col_major: 
                                         dense_threshold, int(build_csc), C.byref(h)))
     d = hybrid_dict(h)
     lib().rtt_hybrid_tiles_destroy(C.byref(h))
+    return d
+
+
+def _hybrid_struct(d: dict):
+    """A HybridTiles structure over the numpy arrays of a hybrid dict (kept
+    alive by the returned list)."""
+    h = HybridTiles()
+    for k in ("rows", "cols", "tile_rows", "tile_cols", "tile_row_count", "tile_col_count",
+              "num_tiles", "payload_size", "dense_tiles", "sparse_tiles"):
+        setattr(h, k, int(d[k]))
+    keep = []
+    types = {"masks": (np.uint32, C.c_uint), "values": (np.float64, C.c_double)}
+    for k in HYBRID_FIELDS:
+        if d.get(k) is None:
+            continue
+        nt, ct = types.get(k, (np.int32, C.c_int))
+        a = np.ascontiguousarray(d[k], dtype=nt)
+        if a.size == 0:
+            a = np.zeros(1, dtype=nt)
+        keep.append(a)
+        setattr(h, k, _ptr(a, ct))
+    return h, keep
+
+
+def super16_index(leaf: dict, role: int) -> dict:
+    """GPU replacement of build_device_index (reference
+    src/super16_symbolic.cuh:2123): the 16x16 parent index of hybrid leaf tiles
+    (a dict from csr_to_hybrid_tiles; 8x4 leaves for RTT_SUPER16_A8X4, 4x8 for
+    RTT_SUPER16_B4X8)."""
+    h, keep = _hybrid_struct(leaf)
+    x = Super16Index()
+    check(lib().rtt_super16_index_build(C.byref(h), role, C.byref(x)))
+    pc, pr, pcol, nt = x.parent_count, x.parent_row_count, x.parent_col_count, int(leaf["num_tiles"])
+    d = {k: getattr(x, k) for k in ("role", "rows", "cols", "parent_row_count",
+                                    "parent_col_count", "parent_count")}
+    d["row_ptr"] = _copy(x.row_ptr, pr + 1, np.uint64)
+    d["col_idx"] = _copy(x.col_idx, pc, np.uint32)
+    d["child_ptr"] = _copy(x.child_ptr, pc + 1, np.uint64)
+    d["child_mask"] = _copy(x.child_mask, pc, np.uint8)
+    d["child_leaf_ids"] = _copy(x.child_leaf_ids, nt, np.uint32)
+    d["boolean_row_masks"] = _copy(x.boolean_row_masks, pc * 16, np.uint16)
+    if role == RTT_SUPER16_B4X8:
+        d["col_ptr"] = _copy(x.col_ptr, pcol + 1, np.uint64)
+        d["row_idx"] = _copy(x.row_idx, pc, np.uint32)
+        d["csc_parent_ids"] = _copy(x.csc_parent_ids, pc, np.uint32)
+    else:
+        d["col_ptr"] = d["row_idx"] = d["csc_parent_ids"] = None
+    lib().rtt_super16_index_destroy(C.byref(x))
+    del keep
     return d
 
 

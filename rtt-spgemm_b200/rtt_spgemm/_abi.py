@@ -36,8 +36,11 @@ EXPORTS = [
     "rtt_plan_tail_queue", "rtt_spgemm_batched_symbolic", "rtt_spgemm_batched_numeric",
     "rtt_csr_transpose", "rtt_early_split_policy_default", "rtt_plan_early_split",
     "rtt_reorder_plan_build", "rtt_reorder_plan_destroy", "rtt_csr_permute",
-    "rtt_spgemm_numeric_values",
+    "rtt_spgemm_numeric_values", "rtt_super16_index_build", "rtt_super16_index_destroy",
 ]
+
+RTT_SUPER16_A8X4 = 1
+RTT_SUPER16_B4X8 = 2
 
 
 class RttError(RuntimeError):
@@ -86,6 +89,21 @@ class HybridTiles(C.Structure):
                 ("value_offsets", C.POINTER(C.c_int)), ("masks", C.POINTER(C.c_uint)),
                 ("values", C.POINTER(C.c_double)), ("tile_col_ptr", C.POINTER(C.c_int)),
                 ("tile_row_idx", C.POINTER(C.c_int)), ("csc_tile_ids", C.POINTER(C.c_int))]
+
+
+class Super16Index(C.Structure):
+    """rtt_super16_index = the reference's Super16 DeviceIndexView
+    (src/super16_symbolic.cuh:85-106) as host arrays."""
+
+    _fields_ = [("role", C.c_uint), ("rows", C.c_int), ("cols", C.c_int),
+                ("parent_row_count", C.c_uint), ("parent_col_count", C.c_uint),
+                ("parent_count", C.c_uint),
+                ("row_ptr", C.POINTER(C.c_ulonglong)), ("col_idx", C.POINTER(C.c_uint)),
+                ("child_ptr", C.POINTER(C.c_ulonglong)), ("child_mask", C.POINTER(C.c_ubyte)),
+                ("child_leaf_ids", C.POINTER(C.c_uint)),
+                ("boolean_row_masks", C.POINTER(C.c_ushort)),
+                ("col_ptr", C.POINTER(C.c_ulonglong)), ("row_idx", C.POINTER(C.c_uint)),
+                ("csc_parent_ids", C.POINTER(C.c_uint))]
 
 
 class TailPolicy(C.Structure):
@@ -179,6 +197,9 @@ def lib() -> C.CDLL:
                                        P(EarlySplitPlan)]
     L.rtt_hybrid_tiles_destroy.argtypes = [P(HybridTiles)]
     L.rtt_hybrid_tiles_destroy.restype = None
+    L.rtt_super16_index_build.argtypes = [P(HybridTiles), C.c_uint, P(Super16Index)]
+    L.rtt_super16_index_destroy.argtypes = [P(Super16Index)]
+    L.rtt_super16_index_destroy.restype = None
     L.rtt_tile2csr_device_noalloc.argtypes = [P(SMatrix), C.c_int, C.c_int, C.c_longlong,
                                               P(C.c_longlong), C.c_void_p]
     L.rtt_matrix_destroy.argtypes = [P(SMatrix), C.c_int]
