@@ -232,10 +232,27 @@ __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Windo
             };
             if (!__any_sync(FULL, len > 32))
             {
-                ent[lane] = make_int4(fs, len, rq * F_CM_STRIDE, 0);
-                enta[lane] = a;
-                __syncwarp();
-                run_items(min(32, total - q0));
+                if (NARROW && CHECK)
+                {
+                    // entries whose B row has nothing in this window (narrowed
+                    // to zero) are left out of the list, which keeps its order
+                    const unsigned live = __ballot_sync(FULL, len > 0);
+                    if (len > 0)
+                    {
+                        const int at = __popc(live & ((1u << lane) - 1u));
+                        ent[at] = make_int4(fs, len, rq * F_CM_STRIDE, 0);
+                        enta[at] = a;
+                    }
+                    __syncwarp();
+                    run_items(__popc(live));
+                }
+                else
+                {
+                    ent[lane] = make_int4(fs, len, rq * F_CM_STRIDE, 0);
+                    enta[lane] = a;
+                    __syncwarp();
+                    run_items(min(32, total - q0));
+                }
             }
             else
             {

@@ -411,9 +411,18 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
                             rb = (r >> 1) * S2_STRIDE;
                         }
                     }
-                    ent[lane] = make_int4(fs, len, sh, rb);
+                    int nbat = min(32, total - q0);
+                    if (NARROW)
+                    {
+                        // B rows with nothing in this window leave the list
+                        const unsigned live = __ballot_sync(FULL, len > 0);
+                        if (len > 0)
+                            ent[__popc(live & ((1u << lane) - 1u))] = make_int4(fs, len, sh, rb);
+                        nbat = __popc(live);
+                    }
+                    else
+                        ent[lane] = make_int4(fs, len, sh, rb);
                     __syncwarp();
-                    const int nbat = min(32, total - q0);
                     auto mark = [&](int col, int sh, int rb) {
                         const int d = (col >> 4) - w;
                         if ((unsigned)d < (unsigned)wlen)
@@ -499,9 +508,18 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
                             fs = sb;
                         }
                     }
-                    ent[lane] = make_int4(fs, len, sh, 0);
+                    int nbat = min(32, total - q0);
+                    if (NARROW)
+                    {
+                        // B rows with nothing in this window leave the list
+                        const unsigned live = __ballot_sync(FULL, len > 0);
+                        if (len > 0)
+                            ent[__popc(live & ((1u << lane) - 1u))] = make_int4(fs, len, sh, 0);
+                        nbat = __popc(live);
+                    }
+                    else
+                        ent[lane] = make_int4(fs, len, sh, 0);
                     __syncwarp();
-                    const int nbat = min(32, total - q0);
                     // one column of B row k into the mask of row r's C tile
                     auto mark = [&](int col, int sh) {
                         const int d = (col >> 4) - w;
