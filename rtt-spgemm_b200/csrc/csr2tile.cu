@@ -30,47 +30,97 @@ namespace
 // ------------------------------------------------------------ validation
 // flags[0]: some row's tile column decreases (needs the generic path)
 // flags[1]: some row's column decreases (entries not sorted inside rows)
+// flags[2]: some row repeats a column
+// One warp per 32 consecutive rows.  Rows of at most 256 entries: each lane
+// walks its own row.  A warp with a longer row walks the rows' entries, one
+// contiguous range, 32 at a time instead (a hub row costs len / 32 steps, not
+// len): a lane compares its entry with the one before unless the entry starts
+// a row; the row starts inside a step are one OR-reduced bit mask.
 __global__ void k_validate_csr(int m, int n, int nnz, const int *__restrict__ rowptr,
                                const int *__restrict__ col, int *err, int *flags)
 {
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r == 0 && (rowptr[0] != 0 || rowptr[m] != nnz))
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw == 0 && lane == 0 && (rowptr[0] != 0 || rowptr[m] != nnz))
         set_error(err, DERR_CSR_ROWPTR);
-    if (r >= m)
-        return;
-    int b = rowptr[r], e = rowptr[r + 1];
-    if (b < 0 || e < b || e > nnz)
+    if (gw * 32 >= m)
+        return; // whole warp
+    const int r = (int)(gw * 32) + lane;
+    int b = 0, e = 0;
+    bool bad = false;
+    if (r < m)
     {
-        set_error(err, DERR_CSR_ROWPTR);
+        b = rowptr[r];
+        e = rowptr[r + 1];
+        bad = b < 0 || e < b || e > nnz;
+    }
+    if (__any_sync(FULL, bad))
+    {
+        if (lane == 0)
+            set_error(err, DERR_CSR_ROWPTR);
         return;
     }
-    int prev = -1;
-    bool tile_dec = false, col_dec = false, col_dup = false;
-    for (int j = b; j < e; ++j)
+    const int rows = min(32, m - (int)(gw * 32));
+    const int lo = __shfl_sync(FULL, b, 0), hi = __shfl_sync(FULL, e, rows - 1);
+    bool col_bad = false, tile_dec = false, col_dec = false, col_dup = false;
+    if (__reduce_max_sync(FULL, (unsigned)(e - b)) <= 256)
     {
-        int c = col[j];
-        if (c < 0 || c >= n)
+        // short rows: each lane walks its own row (the warp's rows share
+        // their cache lines)
+        int prev = -1;
+        for (int j = b; j < e; ++j)
         {
-            set_error(err, DERR_CSR_COL);
-            return;
+            const int c = __ldg(col + j);
+            if (c < 0 || c >= n)
+            {
+                col_bad = true;
+                break;
+            }
+            if (prev >= 0)
+            {
+                tile_dec |= (c >> 4) < (prev >> 4);
+                col_dec |= c < prev;
+                col_dup |= c == prev;
+            }
+            prev = c;
         }
-        if (prev >= 0)
-        {
-            if ((c >> 4) < (prev >> 4))
-                tile_dec = true;
-            if (c < prev)
-                col_dec = true;
-            if (c == prev)
-                col_dup = true;
-        }
-        prev = c;
     }
-    if (tile_dec)
-        atomicOr(&flags[0], 1);
-    if (col_dec)
-        atomicOr(&flags[1], 1);
-    if (col_dup)
-        atomicOr(&flags[2], 1);
+    else
+    {
+        // a long row: the warp walks its rows' entry range 32 at a time
+        for (long long c0 = lo; c0 < hi; c0 += 32)
+        {
+            const bool here = r < m && b >= c0 && b < c0 + 32;
+            const unsigned starts = __reduce_or_sync(FULL, here ? 1u << (int)(b - c0) : 0u);
+            const int j = (int)c0 + lane;
+            if (j < hi)
+            {
+                const int c = __ldg(col + j);
+                if (c < 0 || c >= n)
+                    col_bad = true;
+                else if (((starts >> lane) & 1u) == 0)
+                {
+                    const int p = __ldg(col + j - 1); // same row, j - 1 >= lo
+                    tile_dec |= (c >> 4) < (p >> 4);
+                    col_dec |= c < p;
+                    col_dup |= c == p;
+                }
+            }
+        }
+    }
+    if (__any_sync(FULL, col_bad) && lane == 0)
+        set_error(err, DERR_CSR_COL);
+    const bool td = __any_sync(FULL, tile_dec), cd = __any_sync(FULL, col_dec),
+               dp = __any_sync(FULL, col_dup);
+    if (lane == 0)
+    {
+        if (td)
+            atomicOr(&flags[0], 1);
+        if (cd)
+            atomicOr(&flags[1], 1);
+        if (dp)
+            atomicOr(&flags[2], 1);
+    }
 }
 
 // -------------------------------------------------------------- fast path
@@ -816,8 +866,8 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
         RTT_CHECK(out.val.ensure(tiny, s));
         return RTT_OK;
     }
-    k_validate_csr<<<grid_for(m, 256), 256, 0, s>>>(m, n, nnz, rowptr, col, ws.err.as<int>(),
-                                                    flags);
+    k_validate_csr<<<grid_for((long long)ceil_div(m, 32) * 32, 256), 256, 0, s>>>(
+        m, n, nnz, rowptr, col, ws.err.as<int>(), flags);
     ws.launches++;
     RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 4, flags, sizeof(int) * 3, cudaMemcpyDeviceToHost, s));
     RTT_CHECK(check_device_error(ws, "csr2tile validate"));
@@ -961,8 +1011,8 @@ int validate_csr_device(Workspace &ws, int m, int n, int nnz, const int *rowptr,
     RTT_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * 3, ws.stream));
     if (m > 0)
     {
-        k_validate_csr<<<grid_for(m, 256), 256, 0, ws.stream>>>(m, n, nnz, rowptr, col,
-                                                                ws.err.as<int>(), flags);
+        k_validate_csr<<<grid_for((long long)ceil_div(m, 32) * 32, 256), 256, 0, ws.stream>>>(
+            m, n, nnz, rowptr, col, ws.err.as<int>(), flags);
         ws.launches++;
     }
     RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 4, flags, sizeof(int) * 3, cudaMemcpyDeviceToHost,

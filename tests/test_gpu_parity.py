@@ -224,6 +224,38 @@ def test_invalid_csr_rejected():
     assert e.value.status == 2
 
 
+def _with_long_row(n=2000, width=900, seed=5):
+    """Random CSR whose row 37 holds `width` sorted columns (the validation's
+    warp-wide walk of rows longer than 256 entries)."""
+    A = G.random_csr(n, n, 0.002, seed=seed)
+    rows = [A.col[A.rowptr[i]:A.rowptr[i + 1]] for i in range(n)]
+    vals = [A.val[A.rowptr[i]:A.rowptr[i + 1]] for i in range(n)]
+    rng = np.random.default_rng(seed)
+    rows[37] = np.sort(rng.choice(n, width, replace=False)).astype(np.int32)
+    vals[37] = rng.uniform(-1, 1, width)
+    rp = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int32)
+    return G.CSR(n, n, rp, np.concatenate(rows).astype(np.int32), np.concatenate(vals))
+
+
+def test_long_row_validation(orc):
+    """A row of 900 entries: sorted, with two columns swapped (generic
+    path), with a repeated column, and with a column out of range."""
+    A = _with_long_row()
+    assert_tiles_equal(R.csr2tile_row_major(A), orc.csr2tile_row_major(A), ROW_KEYS, "long row: ")
+    b = int(A.rowptr[37])
+    U = G.CSR(A.m, A.n, A.rowptr, A.col.copy(), A.val)
+    U.col[b + 100], U.col[b + 500] = U.col[b + 500], U.col[b + 100]  # tile columns decrease
+    assert_tiles_equal(R.csr2tile_row_major(U), orc.csr2tile_row_major(U), ROW_KEYS, "unsorted: ")
+    D = G.CSR(A.m, A.n, A.rowptr, A.col.copy(), A.val)
+    D.col[b + 301] = D.col[b + 300]  # repeated column (still non-decreasing)
+    assert_tiles_equal(R.csr2tile_row_major(D), orc.csr2tile_row_major(D), ROW_KEYS, "repeat: ")
+    X = G.CSR(A.m, A.n, A.rowptr, A.col.copy(), A.val)
+    X.col[b + 700] = A.n + 1
+    with pytest.raises(R.RttError) as e:
+        R.csr2tile_row_major(X)
+    assert e.value.status == 2
+
+
 def test_malformed_tiles_rejected(orc):
     A = G.laplacian_2d(16)
     a = orc.csr2tile_row_major(A)
