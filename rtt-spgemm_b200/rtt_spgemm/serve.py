@@ -10,6 +10,14 @@ batches in flight, so requests that arrive while one batch is on the GPU are
 admitted into the next one as soon as a worker and pool memory free up, and
 the two batches' work overlaps on the device.
 
+Repeated products of one A keep its tile structure resident: the first
+request that reuses a reuse key runs alone on a context of its own, whose
+csr2tile and symbolic state then stays on the device (least recently used
+first out, bounded in count and bytes); every later request with that key
+runs the numeric step only on that context (rtt_spgemm_numeric, or
+rtt_spgemm_numeric_values when the request brings other values of the same
+structure), without csr2tile or the symbolic phase.
+
 Admission is bounded by memory: a request reserves, for the time its batch
 runs, its operands plus the exact upper bound of the symbolic phase for C
 (nnzCub entries of 12 bytes: C cannot have more entries than products) plus
@@ -44,7 +52,7 @@ INT32_MAX = 2**31 - 1
 class Request:
     a: CSR                    # host CSR operand
     op: str = "A2"            # "A2" (C = A*A) or "AAT" (C = A*A^T)
-    key: object = None        # reuse key: keep the device operands resident
+    key: object = None        # reuse key of A's structure: operands (and tiles) stay resident
     arrival: float = 0.0      # seconds after the start of the run
     done: float = -1.0
     result: tuple = None      # device (rowptr, col, val) of C
@@ -75,9 +83,24 @@ def product_bound(a: CSR, op: str) -> int:
     return 12 * product_cub(a, op) + 4 * (a.m + 1)
 
 
+@dataclass
+class _Structure:
+    """A reuse key's resident tile structure: a context after its symbolic
+    phase on the key's A, with the device operand it borrows."""
+    ctx: Context
+    cur: CSR                  # the host operand whose values the device tiles hold
+    a: tuple                  # device operand (borrowed by ctx)
+    op: str
+    nnz: int
+    bytes: int
+    vals: object = None       # device values of the last values-only update (borrowed)
+    lock: threading.Lock = field(default_factory=threading.Lock)
+
+
 class Server:
     def __init__(self, device: int = 0, pool_bytes: float = 120e9, max_batch: int = 512,
-                 workers: int = 2, config: dict | None = None, keep_results: bool = True):
+                 workers: int = 2, config: dict | None = None, keep_results: bool = True,
+                 max_structures: int = 16, structure_bytes: float | None = None):
         import torch
 
         self.torch = torch
@@ -89,6 +112,11 @@ class Server:
         self.keep_results = keep_results
         self.resident: OrderedDict = OrderedDict()
         self.lock = threading.Lock()
+        # reuse key -> _Structure (LRU), bounded by count and by the bytes of
+        # their products' bounds
+        self.structures: OrderedDict = OrderedDict()
+        self.max_structures = max_structures
+        self.structure_bytes = pool_bytes / 4 if structure_bytes is None else structure_bytes
         # one (stream, context) per worker, kept across run() calls: their
         # grow-only device buffers stay sized for the traffic seen so far
         self._slots = []
@@ -104,10 +132,14 @@ class Server:
             return self._slots[i]
 
     def close(self):
-        """Release the workers' contexts and the resident operands."""
+        """Release the workers' contexts, the resident structures and operands."""
         for _, ctx in self._slots:
             ctx.close()
         self._slots = []
+        for st in self.structures.values():
+            with st.lock:
+                st.ctx.close()
+        self.structures.clear()
         self.resident.clear()
 
     def __del__(self):
@@ -126,26 +158,129 @@ class Server:
         return va
 
     def _operands(self, r: Request, ctx: Context):
+        """Device operands of a request.  A reuse key names a structure: a
+        request whose host operand is another object than the resident one
+        brings new values, which replace the resident values (and A^T)."""
         with self.lock:
             hit = self.resident.get(r.key) if r.key is not None else None
             if hit is not None:
                 self.resident.move_to_end(r.key)
-        if hit is None:
-            a = self._upload(r.a, ctx)
-            at = ctx.transpose(a) if r.op == "AAT" else None
-            hit = (a, at)
-            if r.key is not None:
-                with self.lock:
-                    self.resident[r.key] = hit
-        a, at = hit
+        if hit is not None and hit[2] is not r.a:
+            a0 = hit[0]
+            a = (a0[0], a0[1], a0[2], a0[3],
+                 self.torch.from_numpy(np.ascontiguousarray(r.a.val)).to(self.device,
+                                                                         non_blocking=True))
+            hit = (a, None, r.a)
+        elif hit is None:
+            hit = (self._upload(r.a, ctx), None, r.a)
+        a, at, src = hit
         if r.op == "AAT" and at is None:
             at = ctx.transpose(a)
+        if r.key is not None:
             with self.lock:
-                if r.key is not None:
-                    self.resident[r.key] = (a, at)
+                self.resident[r.key] = (a, at, src)
         return a, (at if r.op == "AAT" else a)
 
+    # -- resident tile structures -----------------------------------------
+    def _seen(self, r: Request) -> bool:
+        with self.lock:
+            return r.key is not None and r.key in self.resident
+
+    def _structure(self, r: Request):
+        with self.lock:
+            st = self.structures.get(r.key) if r.key is not None else None
+            if st is not None and st.op == r.op:
+                self.structures.move_to_end(r.key)
+                return st
+        return None
+
+    def _outputs(self, m: int, nnz: int):
+        t = self.torch
+        return (t.empty(m + 1, dtype=t.int32, device=self.device),
+                t.empty(max(nnz, 1), dtype=t.int32, device=self.device),
+                t.empty(max(nnz, 1), dtype=t.float64, device=self.device))
+
+    def _finish(self, r: Request, out, nnz: int, t0: float):
+        r.done = time.perf_counter() - t0
+        r.result = (out[0], out[1][:nnz], out[2][:nnz]) if self.keep_results else None
+
+    def _run_resident(self, st: _Structure, stream, r: Request, t0: float):
+        """Numeric step only, on the key's resident structure."""
+        with st.lock:
+            try:
+                st.ctx.set_stream(stream.cuda_stream)
+                out = self._outputs(r.a.m, st.nnz)
+                if r.a is st.cur:  # the values on the device
+                    st.ctx.numeric(*out)
+                else:  # other values of the same structure
+                    vals = self.torch.from_numpy(np.ascontiguousarray(r.a.val)).to(
+                        self.device, non_blocking=True)
+                    st.ctx.numeric_values(vals, None, *out)
+                    # the tiles (and, for A*A, B's values) now come from vals
+                    st.vals, st.cur = vals, r.a
+                stream.synchronize()
+            except RttError as e:
+                r.error, r.done = str(e), time.perf_counter() - t0
+                return
+        self._finish(r, out, st.nnz, t0)
+
+    def _build_resident(self, stream, r: Request, t0: float):
+        """Run a reused key's product alone on a context of its own and keep
+        that context's structure resident."""
+        with self.lock:
+            hit = self.resident.get(r.key)
+        if hit is not None and hit[2] is r.a:
+            a = hit[0]
+        elif hit is not None:  # the resident structure with the request's values
+            a = hit[0][:4] + (self.torch.from_numpy(np.ascontiguousarray(r.a.val)).to(
+                self.device, non_blocking=True),)
+        else:
+            a = self._upload(r.a, None)
+        ctx = Context(self.device.index or 0, self.config)
+        try:
+            ctx.set_stream(stream.cuda_stream)
+            nnz, _ = ctx.symbolic(a, None, 1 if r.op == "AAT" else 0)
+            out = self._outputs(r.a.m, nnz)
+            ctx.numeric(*out)
+            stream.synchronize()
+        except RttError as e:
+            ctx.close()
+            r.error, r.done = str(e), time.perf_counter() - t0
+            return
+        self._finish(r, out, nnz, t0)
+        st = _Structure(ctx, r.a, a, r.op, nnz, int(r.bound))
+        evict = []
+        with self.lock:
+            old = self.structures.pop(r.key, None)
+            if old is not None:
+                evict.append(old)
+            self.structures[r.key] = st
+            total = sum(x.bytes for x in self.structures.values())
+            while len(self.structures) > 1 and (len(self.structures) > self.max_structures
+                                                or total > self.structure_bytes):
+                _, x = self.structures.popitem(last=False)
+                total -= x.bytes
+                evict.append(x)
+        for x in evict:
+            with x.lock:  # not in use by another worker
+                x.ctx.close()
+
     def _run_batch(self, ctx, stream, batch, t0):
+        # keys seen before: the numeric step on their resident structure, or
+        # (first reuse) a product of their own that makes one resident
+        rest = []
+        for r in batch:
+            st = self._structure(r)
+            if st is not None:
+                self._run_resident(st, stream, r, t0)
+            elif self._seen(r) and r.bound <= self.structure_bytes:
+                self._build_resident(stream, r, t0)
+            else:
+                rest.append(r)
+        if rest:
+            self._run_batch_plain(ctx, stream, rest, t0)
+
+    def _run_batch_plain(self, ctx, stream, batch, t0):
         try:
             As, Bs = [], []
             for r in batch:
@@ -157,7 +292,7 @@ class Server:
         except RttError as e:
             if len(batch) > 1:  # find the failing request(s): one at a time
                 for r in batch:
-                    self._run_batch(ctx, stream, [r], t0)
+                    self._run_batch_plain(ctx, stream, [r], t0)
                 return
             batch[0].error = str(e)
             batch[0].done = time.perf_counter() - t0
@@ -258,12 +393,16 @@ def serve_plain(requests: list[Request], device: int = 0, config: dict | None = 
         now = time.perf_counter() - t0
         if r.arrival > now:
             time.sleep(r.arrival - now)
-        a = resident.get(r.key) if r.key is not None else None
-        if a is None:
+        hit = resident.get(r.key) if r.key is not None else None
+        if hit is None:
             a = (r.a.m, r.a.n, torch.from_numpy(r.a.rowptr).to(dev),
                  torch.from_numpy(r.a.col).to(dev), torch.from_numpy(r.a.val).to(dev))
-            if r.key is not None:
-                resident[r.key] = a
+        elif hit[1] is not r.a:  # the key's structure with new values
+            a = hit[0][:4] + (torch.from_numpy(np.ascontiguousarray(r.a.val)).to(dev),)
+        else:
+            a = hit[0]
+        if r.key is not None:
+            resident[r.key] = (a, r.a)
         try:
             nnz, _ = ctx.symbolic(a, None, 1 if r.op == "AAT" else 0)
             rp = torch.empty(r.a.m + 1, dtype=torch.int32, device=dev)

@@ -68,3 +68,41 @@ def test_served_failing_request_does_not_stop_the_loop():
     assert stats["failed"] == 1
     assert reqs[3].error is not None and reqs[3].result is None
     assert all(r.result is not None for i, r in enumerate(reqs) if i != 3)
+
+
+@pytest.mark.parametrize("max_structures", [16, 1])
+def test_served_resident_structures(max_structures):
+    """Keys used again keep their tile structure resident: later requests run
+    the numeric step only (the same A object) or a values-only update (a new
+    CSR with the same structure and other values).  Every result equals the
+    plain path's, bit for bit; with room for one structure the keys evict
+    each other and are rebuilt."""
+    from rtt_spgemm import generators as G
+    from rtt_spgemm import serve
+
+    bases = [(G.stencil_27(12, 4), "A2"), (G.rmat(10, 8, seed=2), "AAT"),
+             (G.banded_scatter(3000, 12, seed=6), "A2")]
+    rng = np.random.default_rng(1)
+
+    def stream():
+        reqs, t = [], 0.0
+        for i in range(18):
+            j = i % 3
+            a, op = bases[j]
+            if i >= 9 and i % 2 == 0:  # same structure, other values
+                a = G.CSR(a.m, a.n, a.rowptr, a.col, a.val * (1.0 + 0.5 * (i + 1)))
+            t += 0.002
+            reqs.append(serve.Request(a, op, ("key", j), t))
+        return reqs
+
+    reqs, alone = stream(), stream()
+    server = serve.Server(workers=2, max_structures=max_structures)
+    server.run(reqs[:3])  # one request per key: batched, operands now resident
+    server.run(reqs[3:])  # every key seen: resident structures from here on
+    assert 1 <= len(server.structures) <= max_structures
+    serve.serve_plain(alone)
+    for i, (r, p) in enumerate(zip(reqs, alone)):
+        assert r.error is None and p.error is None, (i, r.error, p.error)
+        for x, y in zip(r.result, p.result):
+            assert np.array_equal(_host(x).view(np.uint8), _host(y).view(np.uint8)), f"request {i}"
+    server.close()
