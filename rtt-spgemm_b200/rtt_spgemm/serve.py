@@ -10,13 +10,15 @@ batches in flight, so requests that arrive while one batch is on the GPU are
 admitted into the next one as soon as a worker and pool memory free up, and
 the two batches' work overlaps on the device.
 
-Repeated products of one A keep its tile structure resident: the first
-request that reuses a reuse key runs alone on a context of its own, whose
-csr2tile and symbolic state then stays on the device (least recently used
-first out, bounded in count and bytes); every later request with that key
-runs the numeric step only on that context (rtt_spgemm_numeric, or
+Repeated products of one A keep its tile structure resident: the request
+that uses a reuse key for the third time runs alone on a context of its own,
+whose csr2tile and symbolic state then stays on the device (least recently
+used first out, bounded in count and bytes; an evicted structure's context
+is kept for the next one); every later request with that key runs the
+numeric step only on that context (rtt_spgemm_numeric, or
 rtt_spgemm_numeric_values when the request brings other values of the same
-structure), without csr2tile or the symbolic phase.
+structure), without csr2tile or the symbolic phase.  Keys used once or twice
+stay in the batches.
 
 Admission is bounded by memory: a request reserves, for the time its batch
 runs, its operands plus the exact upper bound of the symbolic phase for C
@@ -117,6 +119,8 @@ class Server:
         self.structures: OrderedDict = OrderedDict()
         self.max_structures = max_structures
         self.structure_bytes = pool_bytes / 4 if structure_bytes is None else structure_bytes
+        self.uses: dict = {}     # reuse key -> requests seen with it
+        self._spare: list = []   # contexts of evicted structures, for the next one
         # one (stream, context) per worker, kept across run() calls: their
         # grow-only device buffers stay sized for the traffic seen so far
         self._slots = []
@@ -140,6 +144,9 @@ class Server:
             with st.lock:
                 st.ctx.close()
         self.structures.clear()
+        for ctx in self._spare:
+            ctx.close()
+        self._spare = []
         self.resident.clear()
 
     def __del__(self):
@@ -182,9 +189,14 @@ class Server:
         return a, (at if r.op == "AAT" else a)
 
     # -- resident tile structures -----------------------------------------
-    def _seen(self, r: Request) -> bool:
+    def _count(self, r: Request) -> int:
+        """Requests with r's reuse key before r (and count r)."""
+        if r.key is None:
+            return 0
         with self.lock:
-            return r.key is not None and r.key in self.resident
+            n = self.uses.get(r.key, 0)
+            self.uses[r.key] = n + 1
+        return n
 
     def _structure(self, r: Request):
         with self.lock:
@@ -236,7 +248,10 @@ class Server:
                 self.device, non_blocking=True),)
         else:
             a = self._upload(r.a, None)
-        ctx = Context(self.device.index or 0, self.config)
+        with self.lock:
+            ctx = self._spare.pop() if self._spare else None
+        if ctx is None:
+            ctx = Context(self.device.index or 0, self.config)
         try:
             ctx.set_stream(stream.cuda_stream)
             nnz, _ = ctx.symbolic(a, None, 1 if r.op == "AAT" else 0)
@@ -244,7 +259,8 @@ class Server:
             ctx.numeric(*out)
             stream.synchronize()
         except RttError as e:
-            ctx.close()
+            with self.lock:
+                self._spare.append(ctx)
             r.error, r.done = str(e), time.perf_counter() - t0
             return
         self._finish(r, out, nnz, t0)
@@ -263,17 +279,22 @@ class Server:
                 evict.append(x)
         for x in evict:
             with x.lock:  # not in use by another worker
+                with self.lock:
+                    if len(self._spare) < 4:
+                        self._spare.append(x.ctx)
+                        continue
                 x.ctx.close()
 
     def _run_batch(self, ctx, stream, batch, t0):
-        # keys seen before: the numeric step on their resident structure, or
-        # (first reuse) a product of their own that makes one resident
+        # keys with a resident structure: the numeric step on it; keys used
+        # twice before: a product of their own that makes one resident
         rest = []
         for r in batch:
+            uses = self._count(r)
             st = self._structure(r)
             if st is not None:
                 self._run_resident(st, stream, r, t0)
-            elif self._seen(r) and r.bound <= self.structure_bytes:
+            elif uses >= 2 and self.max_structures > 0 and r.bound <= self.structure_bytes:
                 self._build_resident(stream, r, t0)
             else:
                 rest.append(r)

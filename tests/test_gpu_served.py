@@ -72,7 +72,8 @@ def test_served_failing_request_does_not_stop_the_loop():
 
 @pytest.mark.parametrize("max_structures", [16, 1])
 def test_served_resident_structures(max_structures):
-    """Keys used again keep their tile structure resident: later requests run
+    """Keys used again keep their tile structure resident (from the third
+    use on); later requests run
     the numeric step only (the same A object) or a values-only update (a new
     CSR with the same structure and other values).  Every result equals the
     plain path's, bit for bit; with room for one structure the keys evict
@@ -97,8 +98,8 @@ def test_served_resident_structures(max_structures):
 
     reqs, alone = stream(), stream()
     server = serve.Server(workers=2, max_structures=max_structures)
-    server.run(reqs[:3])  # one request per key: batched, operands now resident
-    server.run(reqs[3:])  # every key seen: resident structures from here on
+    server.run(reqs[:6])  # two requests per key: batched, operands now resident
+    server.run(reqs[6:])  # resident structures from each key's third use on
     assert 1 <= len(server.structures) <= max_structures
     serve.serve_plain(alone)
     for i, (r, p) in enumerate(zip(reqs, alone)):
