@@ -24,6 +24,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -107,7 +108,7 @@ class ClockSampler:
     def __init__(self, uuid: str | None):
         self.uuid = uuid
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        self.path = Path(tempfile.gettempdir()) / f"rtt_clocks_{os.getpid()}.csv"
 
     def start(self):
         try:
@@ -241,8 +242,7 @@ def run_batched(args) -> None:
     tuner = None
     if args.tune:
         from rtt_spgemm import autotune
-        tuner = autotune.Tuner(ROOT / "gpurun_out" / "tune.json"
-                               if (ROOT / "gpurun_out").is_dir() else None)
+        tuner = autotune.Tuner(os.environ.get("RTT_TUNE_CACHE"))  # None: the per-user default
 
     def batched():
         for w in waves:

@@ -509,8 +509,8 @@ RTT_API int rtt_spgemm_csr_host(rtt_context ctx, const SMatrix *A, const SMatrix
                         int op, SMatrix *C);
 
 /* Batched form (no single reference function: it batches the device path
- * above over independent products, the north star's "many SpGEMMs of uneven
- * sizes in one launch").  count products C_i = A_i * B_i (B == NULL: C_i =
+ * above over independent products, many SpGEMMs of uneven sizes in one
+ * pipeline run).  count products C_i = A_i * B_i (B == NULL: C_i =
  * A_i^2, A_i square), device CSR views in; all instances run through ONE
  * csr2tile, ONE symbolic and ONE numeric pass over their block diagonal
  * (every instance padded to a multiple of 16 rows and columns).

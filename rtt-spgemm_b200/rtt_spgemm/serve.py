@@ -1,7 +1,7 @@
 """Serving loop: SpGEMM requests of different sizes, batched as they arrive.
 
-The north star's served form (the reference has none; it runs one product per
-process): requests C = A^2 or C = A*A^T arrive over time; whenever a worker is
+The served form of the product (the reference has none; it runs one product
+per process): requests C = A^2 or C = A*A^T arrive over time; whenever a worker is
 free it takes every request that has arrived and fits the device pool, and
 runs them as ONE batched product (rtt_spgemm_batched_symbolic / _numeric: one
 csr2tile, one symbolic and one numeric pass over the block diagonal of the
