@@ -303,6 +303,8 @@ struct SymbolicOut
     DevBuf w_task, w_heavy, w_queue, w_flag;
     // symbolic step 2: heavy tile rows (flag per tile row, list)
     DevBuf s2_heavy, s2_list;
+    // symbolic step 1: tile rows with many tile pairs (list for a wide CTA)
+    DevBuf s1_list;
     // some C tile row needs more than one window of the flat numeric kernel
     // (set by the symbolic step; true when unknown)
     bool multi_window = true;
@@ -318,7 +320,8 @@ struct SymbolicOut
         const DevBuf *all[] = {&c_tile_ptr, &c_tile_col, &c_tile_row, &c_tile_nnz, &c_mask,
                                &c_ptr,      &c_col,      &c_val,      &c_row_cnt,  &c_rowptr,
                                &c_tr_nnz,   &count_tmp,  &tile_cnt,   &w_task,     &w_heavy,
-                               &w_queue,    &w_flag,     &s2_heavy,   &s2_list};
+                               &w_queue,    &w_flag,     &s2_heavy,   &s2_list,
+                               &s1_list};
         for (const DevBuf *b : all)
             f(*b);
     }

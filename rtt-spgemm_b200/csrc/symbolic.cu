@@ -79,12 +79,14 @@ __device__ __forceinline__ bool skewed_pairs(const DevTiles &A, int I, int nrows
 }
 
 // Window bounds [lo, hi] of the tile columns reachable from tile row I.
+// pairs: the (A tile, B tile) pairs of the tile row, the work of its bitmap.
 __device__ __forceinline__ void row_window(const DevTiles &A, const DevTiles &B, int a0, int a1,
-                                           int &lo, int &hi)
+                                           int &lo, int &hi, long long &pairs)
 {
     const int lane = lane_id();
     lo = INT_MAX;
     hi = -1;
+    long long np = 0;
     for (int a = a0 + lane; a < a1; a += 32)
     {
         const int K = __ldg(A.tile_col + a);
@@ -93,10 +95,12 @@ __device__ __forceinline__ void row_window(const DevTiles &A, const DevTiles &B,
         {
             lo = min(lo, __ldg(B.tile_col + b0));
             hi = max(hi, __ldg(B.tile_col + b1 - 1));
+            np += b1 - b0;
         }
     }
     lo = warp_min(lo);
     hi = warp_max(hi);
+    pairs = warp_sum(np);
 }
 
 // Mark in the bitmap every tile column of B.row(K), K in A.row(I), that lies
@@ -142,9 +146,39 @@ __device__ __forceinline__ void fill_bitmap(const DevTiles &A, const DevTiles &B
     }
 }
 
+// Step 1 of a tile row with more pairs than this goes to k_sym_count_wide:
+// one warp would walk them alone while the rest of the grid has finished.
+constexpr long long S1_WIDE_PAIRS = 1 << 16;
+constexpr int S1_WIDE_WARPS = 16;
+
+// Step-1 outcome of tile row I: C tiles, the step-2 window flag and the
+// step-2 heavy list.
+__device__ __forceinline__ void step1_out(const DevTiles &A, int I, int count, int lo, int hi,
+                                          int lane, int *cnt, int *multi, uint8_t *heavy,
+                                          int *list, int *list_count)
+{
+    // step 2 will need more than one window for this tile row; with an
+    // unbalanced row pair it becomes a heavy row (a wide CTA of its own)
+    const bool multi_win = count > S2_SLOTS || (hi >= 0 && (long long)hi - lo + 1 > WBITS);
+    const bool hv = multi_win && heavy != nullptr &&
+                    skewed_pairs(A, I, min(TD, A.m - I * TD), lane, HEAVY_PAIR);
+    if (lane == 0)
+    {
+        cnt[I] = count;
+        if (multi_win)
+            atomicOr(multi, 1);
+        if (heavy != nullptr)
+        {
+            heavy[I] = hv;
+            if (hv)
+                list[atomicAdd(list_count, 1)] = I;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(SYM_WARPS * 32)
     k_sym_count(DevTiles A, DevTiles B, int *cnt, int *multi, uint8_t *heavy, int *list,
-                int *list_count)
+                int *list_count, int *wide, int *wide_count)
 {
     __shared__ WarpSmem1 sm[SYM_WARPS];
     const int lane = lane_id(), wi = threadIdx.x >> 5;
@@ -154,7 +188,14 @@ __global__ void __launch_bounds__(SYM_WARPS * 32)
     WarpSmem1 &S = sm[wi];
     const int a0 = __ldg(A.tile_ptr + I), a1 = __ldg(A.tile_ptr + I + 1);
     int lo, hi;
-    row_window(A, B, a0, a1, lo, hi);
+    long long pairs;
+    row_window(A, B, a0, a1, lo, hi, pairs);
+    if (pairs > S1_WIDE_PAIRS)
+    {
+        if (lane == 0)
+            wide[atomicAdd(wide_count, 1)] = I;
+        return;
+    }
     int count = 0;
     if (hi >= 0)
     {
@@ -174,22 +215,71 @@ __global__ void __launch_bounds__(SYM_WARPS * 32)
             __syncwarp();
         }
     }
-    // step 2 will need more than one window for this tile row; with an
-    // unbalanced row pair it becomes a heavy row (a wide CTA of its own)
-    const bool multi_win = count > S2_SLOTS || (hi >= 0 && (long long)hi - lo + 1 > WBITS);
-    const bool hv = multi_win && heavy != nullptr &&
-                    skewed_pairs(A, I, min(TD, A.m - I * TD), lane, HEAVY_PAIR);
-    if (lane == 0)
+    step1_out(A, I, count, lo, hi, lane, cnt, multi, heavy, list, list_count);
+}
+
+// Step 1 of the tile rows k_sym_count listed as wide: one CTA of
+// S1_WIDE_WARPS warps per tile row (persistent CTAs over the list), the
+// warps splitting its A tiles and OR-ing into one shared bitmap per window.
+__global__ void __launch_bounds__(S1_WIDE_WARPS * 32)
+    k_sym_count_wide(DevTiles A, DevTiles B, int *cnt, int *multi, uint8_t *heavy, int *list,
+                     int *list_count, const int *wide, const int *wide_count)
+{
+    __shared__ uint32_t bitmap[WWORDS];
+    __shared__ int s_start[S1_WIDE_WARPS][32], s_pre[S1_WIDE_WARPS][32];
+    __shared__ int s_lo, s_hi, s_count;
+    const int tid = threadIdx.x, lane = lane_id(), wi = tid >> 5;
+    const int n = *wide_count;
+    for (int li = blockIdx.x; li < n; li += gridDim.x)
     {
-        cnt[I] = count;
-        if (multi_win)
-            atomicOr(multi, 1);
-        if (heavy != nullptr)
+        const int I = wide[li];
+        const int a0 = __ldg(A.tile_ptr + I), a1 = __ldg(A.tile_ptr + I + 1);
+        if (tid == 0)
         {
-            heavy[I] = hv;
-            if (hv)
-                list[atomicAdd(list_count, 1)] = I;
+            s_lo = INT_MAX;
+            s_hi = -1;
+            s_count = 0;
         }
+        __syncthreads();
+        // this warp's share of the A tiles
+        const int per = (a1 - a0 + S1_WIDE_WARPS - 1) / S1_WIDE_WARPS;
+        const int b0 = min(a1, a0 + wi * per), b1 = min(a1, b0 + per);
+        {
+            int lo, hi;
+            long long pairs;
+            row_window(A, B, b0, b1, lo, hi, pairs);
+            if (lane == 0 && hi >= 0)
+            {
+                atomicMin(&s_lo, lo);
+                atomicMax(&s_hi, hi);
+            }
+        }
+        __syncthreads();
+        const int lo = s_lo, hi = s_hi;
+        if (hi >= 0)
+        {
+            const bool clip = (long long)hi - lo + 1 > WBITS;
+            for (long long w = lo; w <= hi; w += WBITS)
+            {
+                const int wend = (int)min((long long)hi + 1, w + WBITS);
+                const int nwords = (int)((wend - w + 31) >> 5);
+                for (int i = tid; i < nwords; i += S1_WIDE_WARPS * 32)
+                    bitmap[i] = 0;
+                __syncthreads();
+                fill_bitmap(A, B, b0, b1, (int)w, wend, clip, bitmap, s_start[wi], s_pre[wi]);
+                __syncthreads();
+                int c = 0;
+                for (int i = tid; i < nwords; i += S1_WIDE_WARPS * 32)
+                    c += __popc(bitmap[i]);
+                c = warp_sum(c);
+                if (lane == 0 && c)
+                    atomicAdd(&s_count, c);
+                __syncthreads();
+            }
+        }
+        if (wi == 0)
+            step1_out(A, I, s_count, lo, hi, lane, cnt, multi, heavy, list, list_count);
+        __syncthreads(); // s_* are reset for the next tile row
     }
 }
 
@@ -633,16 +723,25 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
     int *cnt = S.count_tmp.as<int>();
     // flags: [0] some tile row needs several step-2 windows, [1] several
     // numeric windows, [2] heavy tile rows listed for the wide step-2 CTA
-    RTT_CHECK(S.w_flag.ensure(sizeof(int) * 3, s));
-    RTT_CUDA(cudaMemsetAsync(S.w_flag.p, 0, sizeof(int) * 3, s));
+    // [3]: tile rows listed for the wide step-1 CTA
+    RTT_CHECK(S.w_flag.ensure(sizeof(int) * 4, s));
+    RTT_CUDA(cudaMemsetAsync(S.w_flag.p, 0, sizeof(int) * 4, s));
     RTT_CHECK(S.s2_heavy.ensure((size_t)tilem + 16, s));
     RTT_CHECK(S.s2_list.ensure(sizeof(int) * (size_t)tilem + 16, s));
+    RTT_CHECK(S.s1_list.ensure(sizeof(int) * (size_t)tilem + 16, s));
     if (tilem > 0)
     {
+        int *flag = S.w_flag.as<int>();
         k_sym_count<<<ceil_div(tilem, SYM_WARPS), SYM_WARPS * 32, 0, s>>>(
-            A, B, cnt, S.w_flag.as<int>(), S.s2_heavy.as<uint8_t>(), S.s2_list.as<int>(),
-            S.w_flag.as<int>() + 2);
-        ws.launches++;
+            A, B, cnt, flag, S.s2_heavy.as<uint8_t>(), S.s2_list.as<int>(), flag + 2,
+            S.s1_list.as<int>(), flag + 3);
+        int sms = 0;
+        RTT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws.device));
+        // persistent CTAs over the wide list (empty: they exit at once)
+        k_sym_count_wide<<<std::min(tilem, 2 * sms), S1_WIDE_WARPS * 32, 0, s>>>(
+            A, B, cnt, flag, S.s2_heavy.as<uint8_t>(), S.s2_list.as<int>(), flag + 2,
+            S.s1_list.as<int>(), flag + 3);
+        ws.launches += 2;
     }
     RTT_CHECK(scan_exclusive_int(ws, cnt, S.c_tile_ptr.as<int>(), tilem));
     RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 13, S.w_flag.p, sizeof(int) * 3,
