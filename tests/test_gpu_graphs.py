@@ -261,3 +261,24 @@ def test_values_update_checks_the_structure():
         ctx.numeric_values(vt, None, *out)
         _same(_host(out, nnz), want)
     ctx.close()
+
+
+@pytest.mark.parametrize("A", [G.CSR(5, 5, np.zeros(6, np.int32), np.zeros(0, np.int32), np.zeros(0)),
+                               G.CSR(1, 1, np.array([0, 1], np.int32), np.array([0], np.int32),
+                                     np.array([3.0]))], ids=["empty_5x5", "one_1x1"])
+def test_graphs_on_empty_and_tiny(A):
+    """Capture and replay of products with no entry and with one."""
+    want = _eager(A)
+    ctx = R.Context(0)
+    a = _dev(A)
+    nnz, _ = ctx.symbolic(a)
+    out = _outputs(A.m, nnz)
+    for _ in range(3):
+        ctx.numeric(*out)
+        _same(_host(out, nnz), want)
+    vt = torch.from_numpy(np.resize(A.val, max(A.nnz, 1))).to(DEV)  # same values
+    for _ in range(3):
+        ctx.numeric_values(vt, None, *out)
+        _same(_host(out, nnz), want)
+    assert ctx.stats()["graph_launched"] == 1
+    ctx.close()
