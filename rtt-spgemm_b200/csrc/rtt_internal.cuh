@@ -223,6 +223,9 @@ int check_device_error(Workspace &ws, const char *stage);
 // copy one int / int64 from device to host (syncs)
 int read_int(Workspace &ws, const int *d, int *h);
 int read_i64(Workspace &ws, const long long *d, long long *h);
+// the same reads with the device error word checked in the same synchronisation
+int read_int_checked(Workspace &ws, const int *d, int *h, const char *stage);
+int read_i64_checked(Workspace &ws, const long long *d, long long *h, const char *stage);
 // while on, DevBuf growth on this thread fails with RTT_ERR_STATE (graph capture)
 void freeze_growth(bool on);
 

@@ -215,13 +215,11 @@ int scan_exclusive_i64(Workspace &ws, const int *in, long long *out, int n)
     return RTT_OK;
 }
 
-int check_device_error(Workspace &ws, const char *stage)
+namespace
 {
-    RTT_CUDA(cudaGetLastError());
-    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 8, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost,
-                             ws.stream));
-    RTT_CUDA(cudaStreamSynchronize(ws.stream));
-    ws.syncs++;
+// The error word copied to ws.h_scalars[8] before the last synchronisation.
+int error_word_seen(Workspace &ws, const char *stage)
+{
     int code = ws.h_scalars[8];
     if (code != 0)
     {
@@ -230,6 +228,35 @@ int check_device_error(Workspace &ws, const char *stage)
                     std::string(stage) + ": device check failed, code " + std::to_string(code));
     }
     return RTT_OK;
+}
+} // namespace
+
+int check_device_error(Workspace &ws, const char *stage)
+{
+    RTT_CUDA(cudaGetLastError());
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 8, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost,
+                             ws.stream));
+    RTT_CUDA(cudaStreamSynchronize(ws.stream));
+    ws.syncs++;
+    return error_word_seen(ws, stage);
+}
+
+int read_int_checked(Workspace &ws, const int *d, int *h, const char *stage)
+{
+    RTT_CUDA(cudaGetLastError());
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 8, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost,
+                             ws.stream));
+    RTT_CHECK(read_int(ws, d, h));
+    return error_word_seen(ws, stage);
+}
+
+int read_i64_checked(Workspace &ws, const long long *d, long long *h, const char *stage)
+{
+    RTT_CUDA(cudaGetLastError());
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 8, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost,
+                             ws.stream));
+    RTT_CHECK(read_i64(ws, d, h));
+    return error_word_seen(ws, stage);
 }
 
 int read_int(Workspace &ws, const int *d, int *h)

@@ -747,10 +747,9 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
     RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 13, S.w_flag.p, sizeof(int) * 3,
                              cudaMemcpyDeviceToHost, s));
     int numtile = 0;
-    RTT_CHECK(read_int(ws, S.c_tile_ptr.as<int>() + tilem, &numtile));
+    RTT_CHECK(read_int_checked(ws, S.c_tile_ptr.as<int>() + tilem, &numtile, "symbolic step 1"));
     const bool sym_multi = ws.h_scalars[13] != 0;
     const int n_heavy = ws.h_scalars[15];
-    RTT_CHECK(check_device_error(ws, "symbolic step 1"));
     S.numtile = numtile;
     const size_t nt = (size_t)numtile;
     RTT_CHECK(S.c_tile_col.ensure(sizeof(int) * nt, s));
@@ -798,8 +797,7 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
     long long *tr64 = S.c_rowptr.as<long long>();
     RTT_CHECK(scan_exclusive_i64(ws, S.c_tr_nnz.as<int>(), tr64, tilem));
     long long nnz = 0;
-    RTT_CHECK(read_i64(ws, tr64 + tilem, &nnz));
-    RTT_CHECK(check_device_error(ws, "symbolic step 2"));
+    RTT_CHECK(read_i64_checked(ws, tr64 + tilem, &nnz, "symbolic step 2"));
     S.nnz = nnz;
     S.multi_window = ws.h_scalars[12] != 0;
     if (nnz > (long long)INT_MAX)
