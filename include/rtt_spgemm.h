@@ -556,6 +556,18 @@ RTT_API int rtt_csr_permute(rtt_context ctx, const rtt_csr_view *A, const int *r
 RTT_API int rtt_spgemm_batched_numeric(rtt_context ctx, int *c_row_ptr, int *c_col_idx,
                                        double *c_values);
 
+/* Values-only update of the last batch (Galerkin products, time steps: the
+ * same instances' structures, new values): a_values[i] holds instance i's
+ * new A values in its CSR order (b_values[i] its B values, or b_values ==
+ * NULL to keep B's, which a batch of A_i^2 takes from A).  The values are
+ * gathered into the block diagonal on the device, its tiles refilled and the
+ * numeric step run as in rtt_spgemm_batched_numeric (same outputs); neither
+ * csr2tile's counting nor the symbolic phase runs again, and a repeated call
+ * replays a CUDA graph (rtt_config.cuda_graphs). */
+RTT_API int rtt_spgemm_batched_numeric_values(rtt_context ctx, const double *const *a_values,
+                                              const double *const *b_values, int *c_row_ptr,
+                                              int *c_col_idx, double *c_values);
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,10 +77,15 @@ struct rtt_context_s
     rtt::DevBuf bat_meta, bat_big_rp, bat_nnz;
     bool bat_active = false;
     int bat_count = 0, bat_rows = 0;
+    // entry offsets of the instances in the block-diagonal A (and B), their
+    // largest entry count, and the device pointer table of a values-only update
+    std::vector<int> bat_a_off, bat_b_off;
+    int bat_a_max = 0, bat_b_max = 0;
+    rtt::DevBuf bat_vtab;
     // offsets (in ints) of the device meta arrays inside bat_meta
     size_t bat_rows_off = 0, bat_rowoff_off = 0, bat_sec_off = 0, bat_colsub_off = 0;
-    // CUDA graphs of the numeric phase: numeric, values-only update, batched
-    rtt::GraphSlot graph[3];
+    // CUDA graphs of the numeric phase
+    rtt::GraphSlot graph[4]; // numeric, values-only, batched, batched values-only
     cudaStream_t cap_stream = nullptr; // capture stream (never the legacy one)
     int cut_cached = -1; // effective DMMA cutoff of the current tiles (-1: unknown)
 };
@@ -96,7 +101,7 @@ std::vector<DevBuf *> own_buffers(rtt_context c)
             &c->in_val,    &c->in2_rp,    &c->in2_col,    &c->in2_val,   &c->out_rp,
             &c->out_col,   &c->out_val,   &c->counters,   &c->maxnnz,    &c->bat_a_rp,
             &c->bat_a_col, &c->bat_a_val, &c->bat_b_rp,   &c->bat_b_col, &c->bat_b_val,
-            &c->bat_meta,  &c->bat_big_rp, &c->bat_nnz,  &c->vflags};
+            &c->bat_meta,  &c->bat_big_rp, &c->bat_nnz,  &c->vflags,    &c->bat_vtab};
 }
 
 std::mutex g_mutex;
@@ -1640,7 +1645,8 @@ bool view_ok(const rtt_csr_view &v)
 // rows start at row_off[i] (multiples of 16), its columns are shifted by
 // col_add[i].  meta_base points at count * 3 pointer slots + int arrays.
 int assemble(rtt_context c, int count, const rtt_csr_view *V, const std::vector<int> &row_off,
-             const std::vector<int> &col_add, DevBuf &rp, DevBuf &col, DevBuf &val)
+             const std::vector<int> &col_add, DevBuf &rp, DevBuf &col, DevBuf &val,
+             std::vector<int> &nnz_off_out, int &max_nnz)
 {
     Workspace &ws = c->ws;
     cudaStream_t s = ws.stream;
@@ -1657,6 +1663,10 @@ int assemble(rtt_context c, int count, const rtt_csr_view *V, const std::vector<
         tab[(size_t)2 * count + i] = V[i].values;
     }
     const int nnz = nnz_off[(size_t)count];
+    max_nnz = 0;
+    for (int i = 0; i < count; ++i)
+        max_nnz = std::max(max_nnz, (int)V[i].nnz);
+    nnz_off_out = nnz_off;
     // device copy of the tables: pointers first (8-byte aligned), then ints
     // (grow-only scratch: no cudaFree, which would wait for every stream)
     DevBuf &tabd = ws.tmp[0];
@@ -1724,14 +1734,15 @@ int rtt_spgemm_batched_symbolic(rtt_context c, int count, const rtt_csr_view *A,
     Workspace &ws = c->ws;
     cudaStream_t s = ws.stream;
     // A's block diagonal (rows at row_off, columns shifted to col_off)
-    RTT_CHECK(assemble(c, count, A, row_off, col_off, c->bat_a_rp, c->bat_a_col, c->bat_a_val));
+    RTT_CHECK(assemble(c, count, A, row_off, col_off, c->bat_a_rp, c->bat_a_col, c->bat_a_val,
+                       c->bat_a_off, c->bat_a_max));
     rtt_csr_view va{(int)R, (int)K, annz, c->bat_a_rp.as<int>(), c->bat_a_col.as<int>(),
                     c->bat_a_val.as<double>()};
     rtt_csr_view vb{};
     if (B != nullptr)
     {
         RTT_CHECK(assemble(c, count, B, col_off, pcol_off, c->bat_b_rp, c->bat_b_col,
-                           c->bat_b_val));
+                           c->bat_b_val, c->bat_b_off, c->bat_b_max));
         vb = rtt_csr_view{(int)K, (int)P, bnnz, c->bat_b_rp.as<int>(), c->bat_b_col.as<int>(),
                           c->bat_b_val.as<double>()};
     }
@@ -1763,6 +1774,8 @@ int rtt_spgemm_batched_symbolic(rtt_context c, int count, const rtt_csr_view *A,
     c->bat_active = true;
     c->bat_count = count;
     c->bat_rows = (int)R;
+    if (B == nullptr)
+        c->bat_b_off.clear();
     return RTT_OK;
 }
 
@@ -1796,6 +1809,78 @@ int rtt_spgemm_batched_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, do
                                   meta_d + c->bat_rows_off, meta_d + c->bat_sec_off,
                                   meta_d + c->bat_colsub_off, c->bat_big_rp.as<int>(),
                                   c_row_ptr, c_col_idx);
+    }));
+    return numeric_finish(c);
+}
+
+int rtt_spgemm_batched_numeric_values(rtt_context c, const double *const *a_values,
+                                      const double *const *b_values, int *c_row_ptr,
+                                      int *c_col_idx, double *c_values)
+{
+    if (c == nullptr || a_values == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "batched values: NULL argument");
+    if (!c->bat_active || !c->have_symbolic)
+        return rtt::fail(RTT_ERR_STATE,
+                         "rtt_spgemm_batched_numeric_values before rtt_spgemm_batched_symbolic");
+    const int n = c->bat_count;
+    const bool with_b = b_values != nullptr;
+    if (with_b && c->bat_b_off.empty())
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "batched values: the batch has no B");
+    for (int i = 0; i < n; ++i)
+        if ((a_values[i] == nullptr && c->bat_a_off[(size_t)i + 1] > c->bat_a_off[(size_t)i]) ||
+            (with_b && b_values[i] == nullptr &&
+             c->bat_b_off[(size_t)i + 1] > c->bat_b_off[(size_t)i]))
+            return rtt::fail(RTT_ERR_INVALID_ARGUMENT,
+                             "batched values: NULL values of instance " + std::to_string(i));
+    RTT_CHECK(numeric_args_ok(c, c_row_ptr, c_col_idx, c_values));
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    Workspace &ws = c->ws;
+    cudaStream_t s = ws.stream;
+    // device table: A's value pointers [, B's], then A's entry offsets [, B's];
+    // written before the (possibly captured) device work that reads it
+    const int parts = with_b ? 2 : 1;
+    const size_t ptr_bytes = sizeof(void *) * (size_t)n * parts;
+    const size_t bytes = ptr_bytes + sizeof(int) * ((size_t)n + 1) * parts;
+    std::vector<char> host(bytes);
+    std::memcpy(host.data(), a_values, sizeof(void *) * (size_t)n);
+    if (with_b)
+        std::memcpy(host.data() + sizeof(void *) * n, b_values, sizeof(void *) * (size_t)n);
+    std::memcpy(host.data() + ptr_bytes, c->bat_a_off.data(), sizeof(int) * ((size_t)n + 1));
+    if (with_b)
+        std::memcpy(host.data() + ptr_bytes + sizeof(int) * ((size_t)n + 1), c->bat_b_off.data(),
+                    sizeof(int) * ((size_t)n + 1));
+    RTT_CHECK(c->bat_vtab.ensure(bytes, s));
+    RTT_CHECK(c->bat_big_rp.ensure(sizeof(int) * ((size_t)c->bat_rows + 1), s));
+    RTT_CUDA(cudaMemcpyAsync(c->bat_vtab.p, host.data(), bytes, cudaMemcpyHostToDevice, s));
+    const char *dt = c->bat_vtab.as<char>();
+    const double *const *a_tab = reinterpret_cast<const double *const *>(dt);
+    const double *const *b_tab = a_tab + n;
+    const int *a_off = reinterpret_cast<const int *>(dt + ptr_bytes);
+    const int *b_off = a_off + n + 1;
+    int cutoff = 0;
+    const TileBufs &TB = c->b_alias ? c->A : c->B;
+    RTT_CHECK(effective_cutoff(c, c->A.view(), TB.view(), &cutoff));
+    std::vector<long long> key{3, as_key(c_row_ptr), as_key(c_col_idx), as_key(c_values),
+                               (long long)with_b};
+    RTT_CHECK(run_phase(c, 3, key, c->cfg.fused_csr_output != 0, [&]() -> int {
+        // the instances' values into the block diagonal, then its tiles
+        RTT_CHECK(batch_values_device(ws, n, c->bat_a_max, a_tab, a_off,
+                                      c->bat_a_val.as<double>()));
+        RTT_CHECK(map_device_error(csr2tile_refill_device(ws, c->a_rp, c->a_ci,
+                                                          c->bat_a_val.as<double>(), c->A, true)));
+        if (with_b && !c->b_alias)
+        {
+            RTT_CHECK(batch_values_device(ws, n, c->bat_b_max, b_tab, b_off,
+                                          c->bat_b_val.as<double>()));
+            RTT_CHECK(map_device_error(csr2tile_refill_device(
+                ws, c->b_rp, c->b_ci, c->bat_b_val.as<double>(), c->B, true)));
+        }
+        RTT_CHECK(numeric_enqueue(c, c->bat_big_rp.as<int>(), c_col_idx, c_values, cutoff));
+        const int *meta_d = c->bat_meta.as<int>();
+        return batch_split_device(ws, n, c->bat_rows, meta_d + c->bat_rowoff_off,
+                                  meta_d + c->bat_rows_off, meta_d + c->bat_sec_off,
+                                  meta_d + c->bat_colsub_off, c->bat_big_rp.as<int>(), c_row_ptr,
+                                  c_col_idx);
     }));
     return numeric_finish(c);
 }

@@ -13,6 +13,8 @@
 // CSR (row pointers from 0, instance-local columns).
 #include "rtt_internal.cuh"
 
+#include <algorithm>
+
 namespace rtt
 {
 namespace
@@ -154,6 +156,21 @@ __global__ void k_batch_empty(int count, const int *__restrict__ rows,
         out_rp[sec_off[i]] = 0;
 }
 
+// New values of every instance into the block-diagonal value array (the
+// structure assembled by k_batch_assemble stays): blockIdx.y is the instance,
+// the x blocks stride over its entries.
+__global__ void k_batch_values(int count, const double *const *__restrict__ va_tab,
+                               const int *__restrict__ nnz_off, double *__restrict__ out_val)
+{
+    const int i = blockIdx.y;
+    if (i >= count)
+        return;
+    const int b = nnz_off[i], n = nnz_off[i + 1] - b;
+    const double *src = va_tab[i];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+        out_val[b + j] = src[j];
+}
+
 inline int warps_grid(long long warps) { return (int)((warps * 32 + 255) / 256); }
 
 } // namespace
@@ -178,6 +195,24 @@ int batch_count_device(Workspace &ws, int count, const int *row_off, const int *
     {
         k_batch_count<<<count, 256, 0, ws.stream>>>(count, row_off, rows, row_cnt, nnz);
         ws.launches++;
+        RTT_CUDA(cudaGetLastError());
+    }
+    return RTT_OK;
+}
+
+int batch_values_device(Workspace &ws, int count, int max_nnz, const double *const *va_tab,
+                        const int *nnz_off, double *out_val)
+{
+    if (count > 0 && max_nnz > 0)
+    {
+        const int xb = std::min((max_nnz + 255) / 256, 64);
+        for (int y0 = 0; y0 < count; y0 += 65535) // gridDim.y limit
+        {
+            const int ny = std::min(count - y0, 65535);
+            k_batch_values<<<dim3(xb, ny), 256, 0, ws.stream>>>(ny, va_tab + y0, nnz_off + y0,
+                                                                out_val);
+            ws.launches++;
+        }
         RTT_CUDA(cudaGetLastError());
     }
     return RTT_OK;

@@ -381,6 +381,10 @@ int batch_assemble_device(Workspace &ws, int count, int total_rows, const int *c
                           const int *nnz_off, int *out_rp, int *out_col, double *out_val);
 int batch_count_device(Workspace &ws, int count, const int *row_off, const int *rows,
                        const int *row_cnt, long long *nnz);
+// values-only update of a batch: instance i's nnz_off[i+1] - nnz_off[i]
+// values from va_tab[i] into out_val at nnz_off[i] (max_nnz: the largest)
+int batch_values_device(Workspace &ws, int count, int max_nnz, const double *const *va_tab,
+                        const int *nnz_off, double *out_val);
 int batch_split_device(Workspace &ws, int count, int total_rows, const int *row_off,
                        const int *rows, const int *sec_off, const int *col_sub, const int *big_rp,
                        int *out_rp, int *col);

@@ -437,6 +437,19 @@ class Context:
         finally:
             self._borrowed = None
 
+    def batched_numeric_values(self, a_values, b_values, rowptr, col, val):
+        """rtt_spgemm_batched_numeric_values: the last batch again with new
+        values of every A_i (device tensors, each in its CSR order) and of
+        every B_i (or None), into the same kind of outputs as
+        batched_numeric()."""
+        n = len(a_values)
+        pa = (C.c_void_p * n)(*[t.data_ptr() for t in a_values])
+        pb = (C.c_void_p * n)(*[t.data_ptr() for t in b_values]) if b_values is not None else None
+        check(lib().rtt_spgemm_batched_numeric_values(self.handle, pa, pb,
+                                                      C.c_void_p(rowptr.data_ptr()),
+                                                      C.c_void_p(col.data_ptr()),
+                                                      C.c_void_p(val.data_ptr())))
+
     def reorder_plan(self, a) -> dict:
         """Row / inner reorder plan of a device CSR tuple (rtt_reorder_plan_build,
         the reference's build_dmma_reorder_plan): counters and numpy maps."""

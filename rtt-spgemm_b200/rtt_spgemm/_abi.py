@@ -37,6 +37,7 @@ EXPORTS = [
     "rtt_csr_transpose", "rtt_early_split_policy_default", "rtt_plan_early_split",
     "rtt_reorder_plan_build", "rtt_reorder_plan_destroy", "rtt_csr_permute",
     "rtt_spgemm_numeric_values", "rtt_super16_index_build", "rtt_super16_index_destroy",
+    "rtt_spgemm_batched_numeric_values",
 ]
 
 RTT_SUPER16_A8X4 = 1
@@ -220,6 +221,8 @@ def lib() -> C.CDLL:
     L.rtt_spgemm_batched_symbolic.argtypes = [C.c_void_p, C.c_int, P(CsrView), P(CsrView),
                                               P(C.c_longlong), P(C.c_longlong)]
     L.rtt_spgemm_batched_numeric.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.rtt_spgemm_batched_numeric_values.argtypes = [C.c_void_p, P(C.c_void_p), P(C.c_void_p),
+                                                    C.c_void_p, C.c_void_p, C.c_void_p]
     L.rtt_csr_transpose.argtypes = [C.c_void_p, P(CsrView), C.c_void_p, C.c_void_p, C.c_void_p]
     L.rtt_spgemm_numeric_values.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.c_void_p]

@@ -119,3 +119,82 @@ def test_batched_rejects_bad_shapes():
         ctx.batched_symbolic([_dev(A)])
     assert ei.value.status == 3
     ctx.close()
+
+
+def _split(rp, ci, va, ms, nnz):
+    r0 = e0 = 0
+    for m, z in zip(ms, nnz):
+        yield rp[r0:r0 + m + 1], ci[e0:e0 + z], va[e0:e0 + z]
+        r0 += m + 1
+        e0 += z
+
+
+def test_batched_values_update(orc):
+    """rtt_spgemm_batched_numeric_values: new values of every instance with the
+    batch's structure kept; every instance equals a plain product with those
+    values, bit for bit, and the repeated calls replay a CUDA graph."""
+    As = _mixed()
+    d = torch.device("cuda:0")
+    views = [_dev(A) for A in As]
+    ctx = R.Context(0)
+    nnz, total = ctx.batched_symbolic(views)
+    rp = torch.empty(sum(A.m + 1 for A in As), dtype=torch.int32, device=d)
+    ci = torch.empty(max(total, 1), dtype=torch.int32, device=d)
+    va = torch.empty(max(total, 1), dtype=torch.float64, device=d)
+    ctx.batched_numeric(rp, ci, va)
+    vt = [torch.zeros(max(A.nnz, 1), dtype=torch.float64, device=d) for A in As]
+    rng = np.random.default_rng(2)
+    flags = []
+    for it in range(3):
+        new = [rng.uniform(-1, 1, A.nnz) for A in As]
+        for t, v in zip(vt, new):
+            if v.size:
+                t[:v.size].copy_(torch.from_numpy(v))
+        va.fill_(np.nan)
+        ctx.batched_numeric_values(vt, None, rp, ci, va)
+        flags.append(ctx.stats()["graph_launched"])
+        got = _split(rp.cpu().numpy(), ci.cpu().numpy(), va.cpu().numpy(), [A.m for A in As], nnz)
+        for i, (A, v, g) in enumerate(zip(As, new, got)):
+            if A.m == 0:
+                continue
+            A2 = G.CSR(A.m, A.n, A.rowptr, A.col, v)
+            prp, pci, pva = _plain(A2)
+            assert np.array_equal(g[0], prp) and np.array_equal(g[1], pci), f"{it}/{i}"
+            assert np.array_equal(g[2].view(np.int64), pva.view(np.int64)), f"{it}/{i}"
+    assert flags == [0, 1, 1], flags
+    ctx.close()
+
+
+def test_batched_values_update_general_ab(orc):
+    pairs = [(G.random_csr(40, 70, 0.05, seed=11), G.random_csr(70, 23, 0.08, seed=12)),
+             (G.random_csr(17, 5, 0.3, seed=13), G.random_csr(5, 300, 0.02, seed=14))]
+    d = torch.device("cuda:0")
+    da, db = [_dev(a) for a, _ in pairs], [_dev(b) for _, b in pairs]
+    ctx = R.Context(0)
+    nnz, total = ctx.batched_symbolic(da, db)
+    rp = torch.empty(sum(a.m + 1 for a, _ in pairs), dtype=torch.int32, device=d)
+    ci = torch.empty(max(total, 1), dtype=torch.int32, device=d)
+    va = torch.empty(max(total, 1), dtype=torch.float64, device=d)
+    ctx.batched_numeric(rp, ci, va)
+    rng = np.random.default_rng(3)
+    na = [rng.uniform(-1, 1, a.nnz) for a, _ in pairs]
+    nb = [rng.uniform(-1, 1, b.nnz) for _, b in pairs]
+    ta = [torch.from_numpy(v).to(d) for v in na]
+    tb = [torch.from_numpy(v).to(d) for v in nb]
+    ctx.batched_numeric_values(ta, tb, rp, ci, va)
+    got = _split(rp.cpu().numpy(), ci.cpu().numpy(), va.cpu().numpy(), [a.m for a, _ in pairs], nnz)
+    for i, ((A, B), g) in enumerate(zip(pairs, got)):
+        A2 = G.CSR(A.m, A.n, A.rowptr, A.col, na[i])
+        B2 = G.CSR(B.m, B.n, B.rowptr, B.col, nb[i])
+        erp, ecol, evals, eabs = orc.spgemm_csr(A2, B2)
+        assert_csr_close(g[0], g[1], g[2], erp, ecol, evals, eabs, f"pair {i}: ")
+    with pytest.raises(R.RttError):  # a batch of squares has no B to update
+        ctx2 = R.Context(0)
+        ctx2.batched_symbolic([_dev(G.laplacian_2d(8))])
+        try:
+            ctx2.batched_numeric_values([torch.zeros(1, dtype=torch.float64, device=d)],
+                                        [torch.zeros(1, dtype=torch.float64, device=d)],
+                                        rp, ci, va)
+        finally:
+            ctx2.close()
+    ctx.close()
