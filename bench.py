@@ -273,6 +273,35 @@ def run_batched(args) -> None:
     ms_b = timed(batched)
     ctx.configure(base_cfg)  # the plain arm keeps the given configuration
     ms_p = timed(plain)
+
+    # values-only update of the same batch (new values of every instance,
+    # structures kept): one context per wave keeps its batch's structure
+    upd = None
+    if not args.no_update:
+        wctx, wout = [], []
+        for w in waves:
+            c = R.Context(0, base_cfg)
+            c.set_stream(stream.cuda_stream)
+            nnz, total = c.batched_symbolic([views[i] for i in w])
+            out = (torch.empty(sum(views[i][0] + 1 for i in w), dtype=torch.int32, device=dev),
+                   torch.empty(max(total, 1), dtype=torch.int32, device=dev),
+                   torch.empty(max(total, 1), dtype=torch.float64, device=dev))
+            c.batched_numeric(*out)
+            wctx.append(c)
+            wout.append(out)
+        newvals = [v[4] * 0.5 for v in views]
+
+        def values():
+            for c, w, out in zip(wctx, waves, wout):
+                c.batched_numeric_values([newvals[i] for i in w], None, *out)
+
+        ms_u = timed(values)
+        upd = {"value": len(As) / (ms_u * 1e-3), "unit": "SpGEMMs/s", "ms_per_step": ms_u,
+               "graph_launched": wctx[0].stats()["graph_launched"],
+               "what": "same instances' structures, new values of every A_i: gathered on the "
+                       "device, tiles refilled, numeric step only (rtt_spgemm_batched_numeric_values)"}
+        for c in wctx:
+            c.close()
     n = len(As)
     line = {
         "metric": "SpGEMMs/s (batched)", "value": n / (ms_b * 1e-3), "unit": "SpGEMMs/s",
@@ -287,6 +316,7 @@ def run_batched(args) -> None:
         "plain": {"spgemms_per_s": n / (ms_p * 1e-3), "ms_per_step": ms_p,
                   "gflops": flops / (ms_p * 1e-3) / 1e9},
         "batched_over_plain": ms_p / ms_b,
+        "values_only_update": upd,
         "tuned": (list(tuner.table.get("devices", {}).values()) or [{}])[0] if tuner else None,
     }
     print(json.dumps(line), flush=True)
