@@ -131,10 +131,32 @@ __device__ __forceinline__ void flat_add(FlatSmem<ACC> &S, const Window &W, cons
 
 // The warp's products for one window: every A entry (r, k) of its rows r0, r1
 // times B's row k.  Returns the number of products when count is set.
+// first index in [lo, hi) with a[i] >= key, probing lo, lo + 1, lo + 3,
+// lo + 7, ... before a binary search: cheap when the answer is near lo
+__device__ __forceinline__ int gallop_lower_bound(const int *a, int lo, int hi, int key)
+{
+    int p = lo, d = 1;
+    while (p < hi && __ldg(a + p) < key)
+    {
+        lo = p + 1;
+        p += d;
+        d <<= 1;
+    }
+    return lower_bound(a, lo, min(p, hi), key);
+}
+
+// Cursors of a persistent worker CTA (cur != nullptr): for the first
+// CUR_CAP A entries of its task's tile row, where each B row's part in the
+// current window ended.  The task's windows follow each other in column
+// order, so the next window's part starts there: one galloping search over
+// that part instead of two binary searches over the whole row.
+constexpr int CUR_CAP = 32768;
+
 template <bool SAFE, bool CHECK, int ACC, bool NARROW>
 __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Window &W, const DevTiles &A,
                                                    const DevTiles &B, int a0, int a1, int r0,
-                                                   int r1, bool count, int4 *ent, double *enta)
+                                                   int r1, bool count, int4 *ent, double *enta,
+                                                   int *cur, int ebase, bool first)
 {
     const int lane = lane_id();
     long long n_fma = 0;
@@ -191,8 +213,22 @@ __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Windo
                 if (NARROW && CHECK && !SAFE && len > NARROW_MIN)
                 {
                     const int lo = W.Jlo * TD, hi = (W.Jlo + W.Jspan + 1) * TD;
-                    const int sb = lower_bound(B.csr_col, fs, fs + len, lo);
-                    len = lower_bound(B.csr_col, sb, fs + len, hi) - sb;
+                    const int fe = fs + len;
+                    const int ci = o_tn0 + e - ebase; // the entry's place in its tile row
+                    const bool keep = cur != nullptr && (unsigned)ci < (unsigned)CUR_CAP;
+                    int sb;
+                    if (keep && !first)
+                    {
+                        sb = min(max(cur[ci], fs), fe);
+                        if (sb < fe && __ldg(B.csr_col + sb) < lo)
+                            sb = lower_bound(B.csr_col, sb, fe, lo);
+                    }
+                    else
+                        sb = lower_bound(B.csr_col, fs, fe, lo);
+                    const int se = gallop_lower_bound(B.csr_col, sb, fe, hi);
+                    if (keep)
+                        cur[ci] = se;
+                    len = se - sb;
                     fs = sb;
                 }
             }
@@ -514,7 +550,7 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
                    double *__restrict__ c_val, const int *__restrict__ csr_rowptr,
                    int *__restrict__ csr_col, double *__restrict__ csr_val, long long *counters,
                    int *err, const uint8_t *__restrict__ heavy, const WinTask *__restrict__ tasks,
-                   WinQueue *q)
+                   WinQueue *q, int *__restrict__ cursors)
 {
     extern __shared__ __align__(128) unsigned char dyn[];
     FlatSmem<ACC> &S = *reinterpret_cast<FlatSmem<ACC> *>(dyn);
@@ -704,10 +740,19 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
             {
                 // each pair counted once: in the first tile window, in its row window
                 const bool count = S.rowwin || w0 == cs0;
+                int *cur = nullptr;
+                int ebase = 0;
+                if (WORKER && cursors != nullptr)
+                {
+                    cur = cursors + (size_t)blockIdx.x * CUR_CAP;
+                    ebase = __ldg(A.tile_nnz + a0);
+                }
                 if (W.table && nW == cs1 - cs0)
-                    n_fma += warp_products<SAFE, false, ACC, NARROW>(S, W, A, B, a0, a1, r0, r1, count, ent, enta);
+                    n_fma += warp_products<SAFE, false, ACC, NARROW>(S, W, A, B, a0, a1, r0, r1, count,
+                                                                     ent, enta, cur, ebase, w0 == wbeg);
                 else
-                    n_fma += warp_products<SAFE, true, ACC, NARROW>(S, W, A, B, a0, a1, r0, r1, count, ent, enta);
+                    n_fma += warp_products<SAFE, true, ACC, NARROW>(S, W, A, B, a0, a1, r0, r1, count,
+                                                                    ent, enta, cur, ebase, w0 == wbeg);
             }
             __syncthreads();
 
@@ -833,7 +878,7 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
             S.w_task.as<WinTask>(), cap, target, S.w_queue.as<WinQueue>(), cfg.counters);
         ws.launches++;
     }
-    auto launch = [&](auto kern, int grid, cudaStream_t st, size_t smem) -> int {
+    auto launch = [&](auto kern, int grid, cudaStream_t st, size_t smem, int *cursors) -> int {
         RTT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<grid, F_THREADS, smem, st>>>(
             A, B, S.tilem, S.nnz, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(),
@@ -842,7 +887,7 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
             cfg.write_tiles ? S.c_val.as<double>() : nullptr, fused_rowptr, cfg.csr_col,
             cfg.csr_val, cfg.counters, ws.err.as<int>(),
             split ? S.w_heavy.as<uint8_t>() : nullptr, S.w_task.as<WinTask>(),
-            S.w_queue.as<WinQueue>());
+            S.w_queue.as<WinQueue>(), cursors);
         ws.launches++;
         return RTT_OK;
     };
@@ -859,9 +904,11 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
         RTT_CUDA(cudaFuncSetAttribute(wk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         RTT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk, F_THREADS, smem));
         RTT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws.device));
+        const int grid = std::max(1, per_sm * sms);
+        RTT_CHECK(S.w_cursor.ensure(sizeof(int) * (size_t)grid * CUR_CAP, s));
         RTT_CUDA(cudaEventRecord(ws.fork_ev, s));
         RTT_CUDA(cudaStreamWaitEvent(ws.side, ws.fork_ev, 0));
-        RTT_CHECK(launch(wk, std::max(1, per_sm * sms), ws.side, smem));
+        RTT_CHECK(launch(wk, grid, ws.side, smem, S.w_cursor.as<int>()));
         RTT_CUDA(cudaEventRecord(ws.join_ev, ws.side));
     }
     auto light = cfg.conflict_safe
@@ -869,7 +916,7 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
                                        : k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, false, false>)
                      : (S.multi_window ? k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, true>
                                        : k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, false>);
-    RTT_CHECK(launch(light, S.tilem, s, smem));
+    RTT_CHECK(launch(light, S.tilem, s, smem, nullptr));
     if (split)
         RTT_CUDA(cudaStreamWaitEvent(s, ws.join_ev, 0));
     if (cfg.ev_end != nullptr)

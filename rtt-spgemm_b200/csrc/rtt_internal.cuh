@@ -304,6 +304,7 @@ struct SymbolicOut
     DevBuf tile_cnt;    // numtile ints, nnz per C tile
     // numeric split of heavy tile rows: window tasks, per-tile-row flag, queue
     DevBuf w_task, w_heavy, w_queue, w_flag;
+    DevBuf w_cursor; // per worker CTA: window cursors of its task's A entries
     // symbolic step 2: heavy tile rows (flag per tile row, list)
     DevBuf s2_heavy, s2_list;
     // symbolic step 1: tile rows with many tile pairs (list for a wide CTA)
@@ -324,7 +325,7 @@ struct SymbolicOut
                                &c_ptr,      &c_col,      &c_val,      &c_row_cnt,  &c_rowptr,
                                &c_tr_nnz,   &count_tmp,  &tile_cnt,   &w_task,     &w_heavy,
                                &w_queue,    &w_flag,     &s2_heavy,   &s2_list,
-                               &s1_list};
+                               &s1_list,    &w_cursor};
         for (const DevBuf *b : all)
             f(*b);
     }
