@@ -163,6 +163,38 @@ def cpu_baseline_port(A, flops: float, B=None) -> dict:
                       "(src/external/cusparse/spgemm_serialref_spa.h)", "seconds": dt}
 
 
+VALUE_RTOL = 1e-12  # |dC_ij| <= VALUE_RTOL * (|A||B|)_ij
+
+
+def oracle_product(A, B):
+    """The checker: the oracle's FP64 row SPA with (|A||B|)_ij per entry."""
+    import oracle
+    return oracle.Oracle().spgemm_csr(A, B, with_abs=True)
+
+
+def parity(rowptr, col, val, want, what: str) -> dict:
+    """Structure bit-exact against the oracle, values within
+    VALUE_RTOL * (|A||B|)_ij; the observed maximum errors are reported."""
+    erp, ecol, evals, eabs = want
+    rowptr = np.asarray(rowptr).astype(np.int64)
+    col = np.asarray(col)
+    same = (rowptr.shape == erp.shape and np.array_equal(rowptr, erp) and
+            col.shape == ecol.shape and np.array_equal(col, ecol))
+    out = {"checked": what, "entries": int(ecol.shape[0]), "structure_bit_exact": bool(same),
+           "bound": VALUE_RTOL}
+    if not same:
+        out.update(max_abs_err=None, max_rel_err=None, **{"pass": False})
+        return out
+    err = np.abs(np.asarray(val, dtype=np.float64) - evals)
+    pos = eabs > 0
+    rel = float((err[pos] / eabs[pos]).max()) if pos.any() else 0.0
+    if (err[~pos] > 0).any():  # an entry whose products are all zero must be exactly zero
+        rel = float("inf")
+    out.update(max_abs_err=float(err.max()) if err.size else 0.0, max_rel_err=rel,
+               **{"pass": bool(rel <= VALUE_RTOL)})
+    return out
+
+
 def run_reference(args) -> None:
     """The reference's own CPU SpGEMM (csr2tile_row_major + spgemm_cpu, compiled
     from its sources), on a bounded sample of the workload's tile rows."""
@@ -302,6 +334,23 @@ def run_batched(args) -> None:
                        "device, tiles refilled, numeric step only (rtt_spgemm_batched_numeric_values)"}
         for c in wctx:
             c.close()
+    # the checker: every instance of the first wave, batched, against the oracle
+    checks = None
+    if not args.no_parity:
+        outs = R.spgemm_batched(ctx, [views[i] for i in waves[0]])
+        torch.cuda.synchronize(dev)
+        worst = {"structure_bit_exact": True, "max_abs_err": 0.0, "max_rel_err": 0.0}
+        for i, (rp_, ci_, va_) in zip(waves[0], outs):
+            c = parity(rp_.cpu().numpy(), ci_.cpu().numpy(), va_.cpu().numpy(),
+                       oracle_product(As[i], As[i]), "")
+            worst["structure_bit_exact"] &= c["structure_bit_exact"]
+            if c["structure_bit_exact"]:
+                worst["max_abs_err"] = max(worst["max_abs_err"], c["max_abs_err"])
+                worst["max_rel_err"] = max(worst["max_rel_err"], c["max_rel_err"])
+        del outs
+        checks = {"checked": f"the {len(waves[0])} instances of the first wave, batched, vs "
+                             f"the oracle's FP64 row SPA", "bound": VALUE_RTOL, **worst,
+                  "pass": bool(worst["structure_bit_exact"] and worst["max_rel_err"] <= VALUE_RTOL)}
     n = len(As)
     line = {
         "metric": "SpGEMMs/s (batched)", "value": n / (ms_b * 1e-3), "unit": "SpGEMMs/s",
@@ -316,6 +365,7 @@ def run_batched(args) -> None:
         "plain": {"spgemms_per_s": n / (ms_p * 1e-3), "ms_per_step": ms_p,
                   "gflops": flops / (ms_p * 1e-3) / 1e9},
         "batched_over_plain": ms_p / ms_b,
+        "parity": checks,
         "values_only_update": upd,
         "tuned": (list(tuner.table.get("devices", {}).values()) or [{}])[0] if tuner else None,
     }
@@ -422,11 +472,11 @@ def run_ours(args) -> None:
         cci = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
         cva = torch.empty(max(nnz, 1), dtype=torch.float64, device=dev)
         ctx.numeric(crp, cci, cva)
-        return nnz
+        return nnz, (crp, cci, cva)
 
     nnz_c = 0
     for _ in range(args.warmup):
-        nnz_c = step()
+        nnz_c, _ = step()
     torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
@@ -444,8 +494,9 @@ def run_ours(args) -> None:
     stage = {"csr2tile_ms": [], "symbolic_ms": [], "numeric_kernel_ms": []}
     launches = 0
     ev0.record(stream)
+    last = None
     for _ in range(args.steps):
-        nnz_c = step()
+        nnz_c, last = step()
         st = ctx.stats()
         for k in stage:
             stage[k].append(st[k])
@@ -455,6 +506,10 @@ def run_ours(args) -> None:
     if dist:
         dist.barrier()
     clocks = sampler.stop()
+    # the last timed step's C, kept for the parity check below
+    got = tuple(t.cpu().numpy() for t in last)
+    got = (got[0], got[1][:nnz_c], got[2][:nnz_c])
+    del last
     ms = shards.max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
     value = shards.replica_throughput(world, flops, ms)
 
@@ -468,6 +523,7 @@ def run_ours(args) -> None:
     # repeated product with the same structure and new values (values-only
     # update, rtt_spgemm_numeric_values): no csr2tile counting, no symbolic
     upd = None
+    got_upd = None
     if not args.staging and not args.unfused and not args.no_update:
         nnz_u, _ = ctx.symbolic(a_view, None, op)
         urp = torch.empty(A.m + 1, dtype=torch.int32, device=dev)
@@ -489,11 +545,13 @@ def run_ours(args) -> None:
         upd = {"value": shards.replica_throughput(world, flops, u_ms), "unit": "GFLOP/s",
                "ms_per_step": u_ms,
                "what": "same structure, new values of A: tiles refilled, numeric step only"}
+        got_upd = (urp.cpu().numpy(), uci[:nnz_u].cpu().numpy(), uva[:nnz_u].cpu().numpy())
         del urp, uci, uva
 
     # end to end through the host-buffer C-ABI call (rtt_spgemm_csr_host):
     # H2D of A from pinned memory, the product, D2H of C into malloc'd arrays
     e2e = None
+    got_e2e = None
     if not args.no_e2e:
         pin_rp = torch.from_numpy(A.rowptr).pin_memory()
         pin_ci = torch.from_numpy(A.col).pin_memory()
@@ -513,11 +571,30 @@ def run_ours(args) -> None:
         e2e = {"value": shards.replica_throughput(world, flops, e2e_ms), "unit": "GFLOP/s",
                "h2d_bytes_per_step": 4 * (A.m + 1) + 12 * A.nnz,
                "d2h_bytes_per_step": 4 * (A.m + 1) + 12 * int(Ch.nnz), "ms_per_step": e2e_ms}
+        got_e2e = (Ch.rowptr, Ch.col, Ch.val)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_port(A, flops, A.transpose() if aat else None)
-        cpu.pop("seconds", None)
+    checks = None
+    if rank == 0:
+        B = A.transpose() if aat else A
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline_port(A, flops, B if aat else None)
+            cpu.pop("seconds", None)
+        # every result of this run against the oracle (the checker): the
+        # timed product, the values-only update and the host-buffer call
+        if not args.no_parity:
+            want = oracle_product(A, B)
+            what = "full product vs the oracle's FP64 row SPA"
+            checks = parity(*got, want, what)
+            if e2e is not None:
+                e2e["parity"] = parity(*got_e2e, want, what)
+            del want
+            if upd is not None:
+                from rtt_spgemm import generators as G
+                A2 = G.CSR(A.m, A.n, A.rowptr, A.col, A.val * 0.5)
+                want = oracle_product(A2, A2.transpose() if aat else A2)
+                upd["parity"] = parity(*got_upd, want, what + " (A values x 0.5)")
+                del want
 
     if dist:
         dist.destroy_process_group()
@@ -548,6 +625,7 @@ def run_ours(args) -> None:
         "host_syncs_per_step": st["host_syncs"],
         "gpu_launches": launches,
         "clocks": clocks,
+        "parity": checks,
         "e2e": e2e,
         "cpu_baseline": cpu,
         "values_only_update": upd,
@@ -567,6 +645,8 @@ def main() -> None:
     ap.add_argument("--unfused", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the check of the results against the oracle")
     ap.add_argument("--no-update", action="store_true",
                     help="skip the values-only update timing")
     ap.add_argument("--tune", action="store_true",

@@ -447,13 +447,14 @@ def plan_early_split(scans, matches, output_nnz, policy: dict, model: dict, sm_c
     return ch, plan
 
 
-def build(reference: bool = True) -> None:
-    """Compile liboracle.so (and the reference libraries where the reference
-    checkout exists)."""
+def build(reference_dir: str | None = None) -> None:
+    """Compile liboracle.so, and the reference's own CPU code into _ref/ when
+    reference_dir (or the environment's RTT_REFERENCE_DIR) names a reference
+    checkout that exists."""
     subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
-    if reference and Path(os.environ.get("RTT_REFERENCE_DIR", "/root/reference"), "src").is_dir():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref",
-                        "REF=" + os.environ.get("RTT_REFERENCE_DIR", "/root/reference")], check=True)
+    ref = reference_dir or os.environ.get("RTT_REFERENCE_DIR")
+    if ref and Path(ref, "src").is_dir():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", "REF=" + str(ref)], check=True)
 
 
 class Oracle(_Base):

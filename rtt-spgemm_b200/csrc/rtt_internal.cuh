@@ -338,8 +338,9 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
 
 struct NumericConfig
 {
-    int dmma_pair_cutoff = 3072;
-    bool b_staging = true;          // TMA staging of B tile rows in the numeric step
+    // the defaults of rtt_config_default: no DMMA pairs, the flat kernel
+    int dmma_pair_cutoff = 0;
+    bool b_staging = false;         // TMA staging of B tile rows in the numeric step
     int split_target = 0;           // products per window task (0 = default, < 0 = no split)
     bool write_tiles = true;
     int *csr_rowptr = nullptr;  // fused CSR output when csr_col != nullptr

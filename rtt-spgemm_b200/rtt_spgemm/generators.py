@@ -193,16 +193,25 @@ def banded_scatter(n: int, half_bw: int, p: float = 0.5, scatter_max: int = 4,
     return CSR(n, n, rp.astype(np.int32), (key % n).astype(np.int32), val)
 
 
-def batched_instances(count: int, n_lo: int = 2000, n_hi: int = 200000, seed: int = 0) -> list:
-    """The batched configuration's instances: n_i log-uniform in [n_lo, n_hi],
-    each banded (half-bandwidth uniform in 8..64, band entries kept with
-    probability 0.5) plus 0..4 random off-band entries per row, values
-    uniform in [-1, 1)."""
+def batched_shapes(count: int, n_lo: int = 2000, n_hi: int = 200000, seed: int = 0):
+    """(n_i, half-bandwidth_i) of the batched configuration's instances."""
     rng = np.random.default_rng(seed)
     ns = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), size=count)).astype(np.int64)
     hb = rng.integers(8, 65, size=count)
-    return [banded_scatter(int(n), int(h), 0.5, 4, seed=int(seed * 100003 + i))
-            for i, (n, h) in enumerate(zip(ns, hb))]
+    return ns, hb
+
+
+def batched_instances(count: int, n_lo: int = 2000, n_hi: int = 200000, seed: int = 0,
+                      which=None) -> list:
+    """The batched configuration's instances: n_i log-uniform in [n_lo, n_hi],
+    each banded (half-bandwidth uniform in 8..64, band entries kept with
+    probability 0.5) plus 0..4 random off-band entries per row, values
+    uniform in [-1, 1).  which: indices of the instances to build (all by
+    default); instance i is the same matrix either way."""
+    ns, hb = batched_shapes(count, n_lo, n_hi, seed)
+    idx = range(count) if which is None else which
+    return [banded_scatter(int(ns[i]), int(hb[i]), 0.5, 4, seed=int(seed * 100003 + i))
+            for i in idx]
 
 
 def random_csr(m: int, n: int, density: float, seed: int = 0, sort: bool = True,
