@@ -425,8 +425,14 @@ typedef struct
      * and replay that graph while those stay the same.  Off with
      * stage_timing or fused_csr_output == 0. */
     int cuda_graphs;
+    /* 64-bit products (rtt_spgemm_symbolic64): both phases run over chunks of
+     * A's tile rows holding at most chunk_tiles C tiles (0 = 2^25, about
+     * 2 GiB of C tile structure), and a chunk whose C holds more than
+     * chunk_nnz entries (0 = INT32_MAX) is halved. */
+    int chunk_tiles;
+    int chunk_nnz;
     /* Reserved, must be zero. */
-    int reserved[4];
+    int reserved[2];
 } rtt_config;
 
 RTT_API void rtt_config_default(rtt_config *config);
@@ -483,6 +489,23 @@ RTT_API int rtt_spgemm_symbolic(rtt_context ctx, const rtt_csr_view *A,
  * column. */
 RTT_API int rtt_spgemm_numeric(rtt_context ctx, int *c_row_ptr, int *c_col_idx,
                        double *c_values);
+
+/* 64-bit output (the SMatrix64 case: C with more than INT32_MAX entries).
+ * The reference stops there with WIDE_OUTPUT_UNREPRESENTABLE
+ * (src/main.cu:2203-2219; candidates capped at INT_MAX, src/dmma_spgemm.h:171-176);
+ * these two replace rtt_spgemm_symbolic / rtt_spgemm_numeric for such
+ * products (any product works through them).  Phase 1 takes the same
+ * operands and writes the exact nnz(C) as int64.  Phase 2 writes C into
+ * caller-owned device buffers: c_row_ptr (rows + 1 int64), c_col_idx (int32)
+ * and c_values (nnz_c entries each); rows sorted by column, results equal to
+ * the 32-bit path's.  The C tile structure never exists for the whole
+ * product: both phases run over chunks of A's tile rows (rtt_config
+ * chunk_tiles, chunk_nnz), and phase 2 runs steps 1-2 of each chunk again
+ * before its numeric step.  A and B stay borrowed until phase 2 returns. */
+RTT_API int rtt_spgemm_symbolic64(rtt_context ctx, const rtt_csr_view *A,
+                                  const rtt_csr_view *B, int op, long long *nnz_c);
+RTT_API int rtt_spgemm_numeric64(rtt_context ctx, long long *c_row_ptr, int *c_col_idx,
+                                 double *c_values);
 
 /* Values-only update (the reference's dynamic-B "values-only" mode,
  * src/main.cu:26-32, :1406-1453, for A and B): the same product as the last

@@ -68,6 +68,7 @@ struct rtt_context_s
     // A's structure as given to the last symbolic (values-only updates)
     const int *a_rp = nullptr;
     const int *a_ci = nullptr;
+    const double *a_va = nullptr; // A's values of the current numeric step
     bool op_aat = false;
     // page-locked staging of the host-buffer entry points (created on first use)
     void *hstage[2] = {};
@@ -88,6 +89,14 @@ struct rtt_context_s
     rtt::GraphSlot graph[4]; // numeric, values-only, batched, batched values-only
     cudaStream_t cap_stream = nullptr; // capture stream (never the legacy one)
     int cut_cached = -1; // effective DMMA cutoff of the current tiles (-1: unknown)
+    // 64-bit products: step-1 counts, per-row counts of C, its int64 row
+    // pointer, a chunk's local row pointer; chunks of A's tile rows
+    rtt::DevBuf w_cnt, w_rowcnt, w_rowptr, w_local;
+    std::vector<int> w_bounds;      // chunk c is tile rows [w_bounds[c], w_bounds[c + 1])
+    std::vector<long long> w_base;  // first entry of chunk c in C
+    rtt::DevTiles w_dA{}, w_dB{};
+    bool have_sym64 = false;
+    long long w_nnz = 0;
 };
 
 namespace
@@ -101,7 +110,8 @@ std::vector<DevBuf *> own_buffers(rtt_context c)
             &c->in_val,    &c->in2_rp,    &c->in2_col,    &c->in2_val,   &c->out_rp,
             &c->out_col,   &c->out_val,   &c->counters,   &c->maxnnz,    &c->bat_a_rp,
             &c->bat_a_col, &c->bat_a_val, &c->bat_b_rp,   &c->bat_b_col, &c->bat_b_val,
-            &c->bat_meta,  &c->bat_big_rp, &c->bat_nnz,  &c->vflags,    &c->bat_vtab};
+            &c->bat_meta,  &c->bat_big_rp, &c->bat_nnz,  &c->vflags,    &c->bat_vtab,
+            &c->w_cnt,     &c->w_rowcnt,  &c->w_rowptr,   &c->w_local};
 }
 
 std::mutex g_mutex;
@@ -589,7 +599,8 @@ void numeric_key(rtt_context c, std::vector<long long> &k)
         k.push_back(v);
     for (long long v : {as_key(c->b_rp), as_key(c->b_ci), as_key(c->b_va), c->b_nnz,
                         (long long)c->b_dups, (long long)c->b_alias, (long long)c->op_aat,
-                        as_key(c->a_rp), as_key(c->a_ci), (long long)c->cut_cached,
+                        as_key(c->a_rp), as_key(c->a_ci), as_key(c->a_va),
+                        (long long)c->cut_cached,
                         (long long)c->bat_active, (long long)c->bat_count,
                         (long long)c->bat_rows})
         k.push_back(v);
@@ -728,7 +739,12 @@ int numeric_enqueue(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_val
     dB.csr_val = c->b_va;
     dB.nnz = (int)c->b_nnz;
     nc.conflict_safe = c->b_dups;
-    RTT_CHECK(numeric_select_device(ws, c->A.view(), dB, c->S, nc));
+    // the numeric step reads A's entries from its CSR rows
+    DevTiles dA = c->A.view();
+    dA.csr_rowptr = c->a_rp;
+    dA.csr_col = c->a_ci;
+    dA.csr_val = c->a_va;
+    RTT_CHECK(numeric_select_device(ws, dA, dB, c->S, nc));
     if (!fused)
     {
         SymbolicOut &S = c->S;
@@ -775,6 +791,82 @@ int numeric_args_ok(rtt_context c, const int *c_row_ptr, const int *c_col_idx,
 }
 
 } // namespace
+
+// csr2tile of A (and B: A's own tiles for A*A, A^T's for A*A^T), B's scalar
+// CSR rows, and the device views the symbolic and numeric steps take.  The
+// shape checks of the entry points come first.  Shared by the 32-bit product
+// and the 64-bit (chunked) one.
+int prepare_operands(rtt_context c, const rtt_csr_view *A, const rtt_csr_view *B, int op,
+                     DevTiles &dA, DevTiles &dB)
+{
+    Workspace &ws = c->ws;
+    // B's row segments drive symbolic step 2: A's own when B is A
+    RTT_CHECK(map_device_error(csr2tile_device(ws, A->rows, A->cols, (int)A->nnz, A->row_ptr,
+                                               A->col_idx, A->values, c->A, true, false,
+                                               op == RTT_OP_AB && B == nullptr)));
+    c->a_rp = A->row_ptr;
+    c->a_ci = A->col_idx;
+    c->a_va = A->values;
+    c->op_aat = op == RTT_OP_AAT;
+    if (op == RTT_OP_AB && B == nullptr)
+    {
+        if (A->rows != A->cols)
+            return rtt::fail(RTT_ERR_SHAPE_MISMATCH, "A*A needs a square A");
+        c->b_alias = true;
+        c->b_rp = A->row_ptr;
+        c->b_ci = A->col_idx;
+        c->b_va = A->values;
+        c->b_nnz = A->nnz;
+        c->b_dups = c->A.dup_cols;
+    }
+    else
+    {
+        c->b_alias = false;
+        if (op == RTT_OP_AAT)
+        {
+            RTT_CHECK(c->bt_rowptr.ensure(sizeof(int) * ((size_t)A->cols + 1), ws.stream));
+            RTT_CHECK(c->bt_col.ensure(sizeof(int) * (size_t)A->nnz + 16, ws.stream));
+            RTT_CHECK(c->bt_val.ensure(sizeof(double) * (size_t)A->nnz + 16, ws.stream));
+            RTT_CHECK(csr_transpose_device(ws, A->rows, A->cols, (int)A->nnz, A->row_ptr,
+                                           A->col_idx, A->values, c->bt_rowptr.as<int>(),
+                                           c->bt_col.as<int>(), c->bt_val.as<double>()));
+            RTT_CHECK(map_device_error(csr2tile_device(ws, A->cols, A->rows, (int)A->nnz,
+                                                       c->bt_rowptr.as<int>(), c->bt_col.as<int>(),
+                                                       c->bt_val.as<double>(), c->B, true, false,
+                                                       true)));
+            c->b_rp = c->bt_rowptr.as<int>();
+            c->b_ci = c->bt_col.as<int>();
+            c->b_va = c->bt_val.as<double>();
+            c->b_nnz = A->nnz;
+        }
+        else
+        {
+            if (B->rows != A->cols)
+                return rtt::fail(RTT_ERR_SHAPE_MISMATCH, "A->cols != B->rows");
+            if (B->nnz < 0 || B->nnz > INT_MAX)
+                return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "bad B shape");
+            RTT_CHECK(map_device_error(csr2tile_device(ws, B->rows, B->cols, (int)B->nnz,
+                                                       B->row_ptr, B->col_idx, B->values, c->B,
+                                                       true, false, true)));
+            c->b_rp = B->row_ptr;
+            c->b_ci = B->col_idx;
+            c->b_va = B->values;
+            c->b_nnz = B->nnz;
+        }
+        c->b_dups = c->B.dup_cols;
+    }
+    const TileBufs &TB = c->b_alias ? c->A : c->B;
+    dB = TB.view();
+    dB.csr_rowptr = c->b_rp;
+    dB.csr_col = c->b_ci;
+    dB.csr_val = c->b_va;
+    dB.nnz = (int)c->b_nnz;
+    dA = c->A.view();
+    // A's CSR rows: step 2 walks the tile row's entries straight from them
+    dA.csr_rowptr = A->row_ptr;
+    dA.csr_col = A->col_idx;
+    return RTT_OK;
+}
 
 extern "C" {
 
@@ -911,6 +1003,8 @@ int rtt_context_set_config(rtt_context c, const rtt_config *config)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "NULL argument");
     if (config->dmma_pair_cutoff < 0)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "dmma_pair_cutoff must be >= 0");
+    if (config->chunk_tiles < 0 || config->chunk_nnz < 0)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "chunk_tiles and chunk_nnz must be >= 0");
     for (int r : config->reserved)
         if (r != 0)
             return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "reserved config fields must be zero");
@@ -1454,6 +1548,7 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "bad A shape");
     RTT_CUDA(cudaSetDevice(c->ws.device));
     c->have_symbolic = false;
+    c->have_sym64 = false;
     c->bat_active = false;
     c->cut_cached = -1;
     c->ws.launches = 0;
@@ -1463,67 +1558,11 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
     const bool timing = c->cfg.stage_timing != 0;
     if (timing)
         RTT_CUDA(cudaEventRecord(ws.ev[0], ws.stream));
-    RTT_CHECK(map_device_error(csr2tile_device(ws, A->rows, A->cols, (int)A->nnz, A->row_ptr,
-                                               A->col_idx, A->values, c->A, true, false)));
-    c->a_rp = A->row_ptr;
-    c->a_ci = A->col_idx;
-    c->op_aat = op == RTT_OP_AAT;
-    if (op == RTT_OP_AB && B == nullptr)
-    {
-        if (A->rows != A->cols)
-            return rtt::fail(RTT_ERR_SHAPE_MISMATCH, "A*A needs a square A");
-        c->b_alias = true;
-        c->b_rp = A->row_ptr;
-        c->b_ci = A->col_idx;
-        c->b_va = A->values;
-        c->b_nnz = A->nnz;
-        c->b_dups = c->A.dup_cols;
-    }
-    else
-    {
-        c->b_alias = false;
-        if (op == RTT_OP_AAT)
-        {
-            RTT_CHECK(c->bt_rowptr.ensure(sizeof(int) * ((size_t)A->cols + 1), ws.stream));
-            RTT_CHECK(c->bt_col.ensure(sizeof(int) * (size_t)A->nnz + 16, ws.stream));
-            RTT_CHECK(c->bt_val.ensure(sizeof(double) * (size_t)A->nnz + 16, ws.stream));
-            RTT_CHECK(csr_transpose_device(ws, A->rows, A->cols, (int)A->nnz, A->row_ptr,
-                                           A->col_idx, A->values, c->bt_rowptr.as<int>(),
-                                           c->bt_col.as<int>(), c->bt_val.as<double>()));
-            RTT_CHECK(map_device_error(csr2tile_device(ws, A->cols, A->rows, (int)A->nnz,
-                                                       c->bt_rowptr.as<int>(), c->bt_col.as<int>(),
-                                                       c->bt_val.as<double>(), c->B, true, false)));
-            c->b_rp = c->bt_rowptr.as<int>();
-            c->b_ci = c->bt_col.as<int>();
-            c->b_va = c->bt_val.as<double>();
-            c->b_nnz = A->nnz;
-        }
-        else
-        {
-            if (B->rows != A->cols)
-                return rtt::fail(RTT_ERR_SHAPE_MISMATCH, "A->cols != B->rows");
-            if (B->nnz < 0 || B->nnz > INT_MAX)
-                return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "bad B shape");
-            RTT_CHECK(map_device_error(csr2tile_device(ws, B->rows, B->cols, (int)B->nnz,
-                                                       B->row_ptr, B->col_idx, B->values, c->B,
-                                                       true, false)));
-            c->b_rp = B->row_ptr;
-            c->b_ci = B->col_idx;
-            c->b_va = B->values;
-            c->b_nnz = B->nnz;
-        }
-        c->b_dups = c->B.dup_cols;
-    }
+    DevTiles dA, dB;
+    RTT_CHECK(prepare_operands(c, A, B, op, dA, dB));
     const TileBufs &TB = c->b_alias ? c->A : c->B;
     if (timing)
         RTT_CUDA(cudaEventRecord(ws.ev[1], ws.stream));
-    DevTiles dB = TB.view();
-    dB.csr_rowptr = c->b_rp;
-    dB.csr_col = c->b_ci;
-    dB.csr_val = c->b_va;
-    dB.nnz = (int)c->b_nnz;
-    DevTiles dA = c->A.view();
-    dA.csr_rowptr = A->row_ptr; // A's row lengths: the symbolic step balances hub rows
     RTT_CHECK(map_device_error(symbolic_device(ws, dA, dB, c->S, !c->b_dups)));
     if (timing)
     {
@@ -1579,6 +1618,7 @@ int rtt_spgemm_numeric_values(rtt_context c, const double *a_values, const doubl
             return rtt::fail(RTT_ERR_INVALID_CSR, changed);
     }
     // B's values for the numeric step: A's (A*A), A^T's (rebuilt below) or new
+    c->a_va = a_values;
     if (c->b_alias)
         c->b_va = a_values;
     else if (c->op_aat)
@@ -1628,6 +1668,178 @@ int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_
         return numeric_enqueue(c, c_row_ptr, c_col_idx, c_values, cutoff);
     }));
     return numeric_finish(c);
+}
+
+// ------------------------------------------------------------ 64-bit products
+// C with more than INT32_MAX entries (R-MAT 2^20 A*A^T: about 9.4e9).  The
+// C tile structure of such a product does not fit beside C, so both phases
+// run over chunks of A's tile rows (tile_row_slice): the symbolic phase runs
+// steps 1-2 per chunk and keeps only the per-row counts of C (their int64
+// scan is C's row pointer); the numeric phase runs steps 1-2 of a chunk again
+// and its numeric step straight into the chunk's part of C's CSR, through a
+// chunk-local int32 row pointer.  Chunks hold at most chunk_tiles C tiles
+// (planned from step 1 over all tile rows) and fewer than chunk_nnz entries
+// (a chunk past it is halved).
+namespace
+{
+constexpr long long WIDE_CHUNK_TILES = 1ll << 25;
+
+__global__ void k_rowptr_copy(long long n, const long long *__restrict__ src,
+                              long long *__restrict__ dst)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+} // namespace
+
+int rtt_spgemm_symbolic64(rtt_context c, const rtt_csr_view *A, const rtt_csr_view *B, int op,
+                          long long *nnz_c)
+{
+    if (c == nullptr || A == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (op != RTT_OP_AB && op != RTT_OP_AAT)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "op must be RTT_OP_AB or RTT_OP_AAT");
+    if (op == RTT_OP_AAT && B != nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "RTT_OP_AAT takes B == NULL");
+    if (A->rows < 0 || A->cols < 0 || A->nnz < 0 || A->nnz > INT_MAX)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "bad A shape");
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    c->have_symbolic = false;
+    c->have_sym64 = false;
+    c->bat_active = false;
+    c->cut_cached = -1;
+    c->ws.launches = 0;
+    c->ws.syncs = 0;
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    Workspace &ws = c->ws;
+    cudaStream_t s = ws.stream;
+    DevTiles dA, dB;
+    RTT_CHECK(prepare_operands(c, A, B, op, dA, dB));
+    const int tilem = dA.tilem, m = dA.m;
+    // step 1 over every tile row: C tiles per tile row, to plan the chunks
+    std::vector<int> tcnt((size_t)tilem);
+    if (tilem > 0)
+    {
+        RTT_CHECK(c->w_cnt.ensure(sizeof(int) * (size_t)tilem, s));
+        RTT_CHECK(symbolic_tile_counts(ws, dA, dB, c->S, c->w_cnt.as<int>()));
+        RTT_CUDA(cudaMemcpyAsync(tcnt.data(), c->w_cnt.p, sizeof(int) * (size_t)tilem,
+                                 cudaMemcpyDeviceToHost, s));
+        RTT_CHECK(check_device_error(ws, "symbolic64 step 1"));
+    }
+    const long long budget = c->cfg.chunk_tiles > 0 ? c->cfg.chunk_tiles : WIDE_CHUNK_TILES;
+    const long long cap = c->cfg.chunk_nnz > 0 ? c->cfg.chunk_nnz : (long long)INT_MAX;
+    std::vector<int> bounds{0};
+    long long run = 0;
+    for (int I = 0; I < tilem; ++I)
+    {
+        if (run + tcnt[I] > budget && I > bounds.back())
+        {
+            bounds.push_back(I);
+            run = 0;
+        }
+        run += tcnt[I];
+    }
+    if (tilem > 0)
+        bounds.push_back(tilem);
+    // steps 1-2 per chunk: the per-row counts of C
+    RTT_CHECK(c->w_rowcnt.ensure(sizeof(int) * ((size_t)m + 1), s));
+    RTT_CHECK(c->w_rowptr.ensure(sizeof(long long) * ((size_t)m + 1), s));
+    std::vector<int> done{0};
+    std::vector<long long> base{0};
+    long long tiles = 0;
+    for (size_t k = 0; k + 1 < bounds.size();)
+    {
+        const int I0 = bounds[k], I1 = bounds[k + 1];
+        const DevTiles sA = tile_row_slice(dA, I0, I1);
+        int st = map_device_error(symbolic_device(ws, sA, dB, c->S, !c->b_dups));
+        if ((st == RTT_ERR_UNREPRESENTABLE || (st == RTT_OK && c->S.nnz > cap)) && I1 - I0 > 1)
+        {
+            bounds.insert(bounds.begin() + (long)k + 1, I0 + (I1 - I0) / 2); // halve it
+            continue;
+        }
+        if (st == RTT_OK && c->S.nnz > cap)
+            return rtt::fail(RTT_ERR_UNREPRESENTABLE,
+                             "one tile row of C holds more entries than a chunk may");
+        RTT_CHECK(st);
+        RTT_CUDA(cudaMemcpyAsync(c->w_rowcnt.as<int>() + (size_t)I0 * TD, c->S.c_row_cnt.p,
+                                 sizeof(int) * (size_t)sA.m, cudaMemcpyDeviceToDevice, s));
+        done.push_back(I1);
+        base.push_back(base.back() + c->S.nnz);
+        tiles += c->S.numtile;
+        ++k;
+    }
+    RTT_CHECK(scan_exclusive_i64(ws, c->w_rowcnt.as<int>(), c->w_rowptr.as<long long>(), m));
+    long long nnz = 0;
+    RTT_CHECK(read_i64_checked(ws, c->w_rowptr.as<long long>() + m, &nnz, "symbolic64"));
+    if (nnz != base.back())
+        return rtt::fail(RTT_ERR_DEVICE_CHECK, "symbolic64: chunk totals disagree with the rows");
+    c->w_bounds = done;
+    c->w_base = base;
+    c->w_dA = dA;
+    c->w_dB = dB;
+    c->w_nnz = nnz;
+    const TileBufs &TB = c->b_alias ? c->A : c->B;
+    c->stats.nnz_a = c->A.nnz;
+    c->stats.nnz_b = TB.nnz;
+    c->stats.nnz_c = nnz;
+    c->stats.tiles_a = c->A.numtile;
+    c->stats.tiles_b = TB.numtile;
+    c->stats.tiles_c = tiles;
+    c->stats.host_syncs = ws.syncs;
+    c->have_sym64 = true;
+    if (nnz_c)
+        *nnz_c = nnz;
+    return RTT_OK;
+}
+
+int rtt_spgemm_numeric64(rtt_context c, long long *c_row_ptr, int *c_col_idx, double *c_values)
+{
+    if (c == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (!c->have_sym64)
+        return rtt::fail(RTT_ERR_STATE, "rtt_spgemm_numeric64 before rtt_spgemm_symbolic64");
+    if (c_row_ptr == nullptr || (c->w_nnz > 0 && (c_col_idx == nullptr || c_values == nullptr)))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "NULL output buffer");
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    Workspace &ws = c->ws;
+    cudaStream_t s = ws.stream;
+    ws.launches = 0;
+    const DevTiles &dA = c->w_dA, &dB = c->w_dB;
+    const long long m = dA.m;
+    k_rowptr_copy<<<std::max(1, (int)std::min<long long>((m + 256) / 256, 4096)), 256, 0, s>>>(
+        m + 1, c->w_rowptr.as<long long>(), c_row_ptr);
+    ws.launches++;
+    RTT_CHECK(c->counters.ensure(sizeof(long long) * 4, s));
+    RTT_CUDA(cudaMemsetAsync(c->counters.p, 0, sizeof(long long) * 4, s));
+    for (size_t k = 0; k + 1 < c->w_bounds.size(); ++k)
+    {
+        const int I0 = c->w_bounds[k], I1 = c->w_bounds[k + 1];
+        DevTiles sA = tile_row_slice(dA, I0, I1);
+        RTT_CHECK(map_device_error(symbolic_device(ws, sA, dB, c->S, !c->b_dups)));
+        if (c->S.nnz != c->w_base[k + 1] - c->w_base[k])
+            return rtt::fail(RTT_ERR_DEVICE_CHECK, "numeric64: a chunk's size changed");
+        RTT_CHECK(c->w_local.ensure(sizeof(int) * ((size_t)sA.m + 1), s));
+        NumericConfig nc;
+        nc.counters = c->counters.as<long long>();
+        nc.split_target = c->cfg.split_target;
+        nc.write_tiles = false;
+        nc.conflict_safe = c->b_dups;
+        nc.csr_rowptr = c->w_local.as<int>();
+        nc.csr_col = c_col_idx + c->w_base[k];
+        nc.csr_val = c_values + c->w_base[k];
+        sA.csr_val = c->a_va;
+        RTT_CHECK(numeric_flat_device(ws, sA, dB, c->S, nc));
+    }
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars64 + 2, c->counters.p, sizeof(long long) * 3,
+                             cudaMemcpyDeviceToHost, s));
+    RTT_CHECK(check_device_error(ws, "numeric64"));
+    c->stats.sparse_pairs = ws.h_scalars64[3];
+    c->stats.nnz_cub = ws.h_scalars64[3];
+    c->stats.split_windows = ws.h_scalars64[4];
+    c->stats.kernel_launches = ws.launches;
+    c->stats.host_syncs = ws.syncs;
+    return RTT_OK;
 }
 
 // ------------------------------------------------------------ batched products

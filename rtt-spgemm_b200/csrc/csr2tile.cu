@@ -236,6 +236,104 @@ __global__ void __launch_bounds__(256) k_c2t_fill(int m, int tilem, const int *_
     }
 }
 
+// ------------------------------------------------------------ row segments
+// Row segments of a CSR whose rows have non-decreasing tile columns: every
+// maximal run of a row's entries inside one tile column J becomes the segment
+// (J << 16) | mask, mask bit (15 - c) for each column c of the run - the row's
+// 16-bit row mask in tile J, as csr2tile writes it into mask[].  One warp per
+// 32 consecutive rows (as k_validate_csr): each lane walks its own row when
+// the warp's rows are short; a warp holding a long row walks its rows one
+// after another, 32 entries at a time, and a segment is counted (and written)
+// by the lane that holds its first entry.
+__device__ __forceinline__ unsigned long long seg_pack(int T, unsigned mk)
+{
+    return ((unsigned long long)T << 16) | (mk & 0xFFFFu);
+}
+
+template <bool FILL>
+__global__ void __launch_bounds__(256)
+    k_row_segments(int m, const int *__restrict__ rowptr, const int *__restrict__ col,
+                   int *__restrict__ seg_cnt, const int *__restrict__ seg_ptr,
+                   unsigned long long *__restrict__ seg)
+{
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw * 32 >= m)
+        return; // whole warp
+    const int r0 = (int)(gw * 32), r = r0 + lane;
+    int b = 0, e = 0;
+    if (r < m)
+    {
+        b = rowptr[r];
+        e = rowptr[r + 1];
+    }
+    if (__reduce_max_sync(FULL, (unsigned)(e - b)) <= 256)
+    {
+        const int out = FILL && r < m ? seg_ptr[r] : 0;
+        int n = 0, T = -1;
+        unsigned mk = 0;
+        for (int j = b; j < e; ++j)
+        {
+            const int c = __ldg(col + j);
+            if ((c >> 4) != T)
+            {
+                if (T >= 0)
+                {
+                    if (FILL)
+                        seg[out + n] = seg_pack(T, mk);
+                    ++n;
+                }
+                T = c >> 4;
+                mk = 0;
+            }
+            mk |= 0x8000u >> (c & 15);
+        }
+        if (T >= 0)
+        {
+            if (FILL)
+                seg[out + n] = seg_pack(T, mk);
+            ++n;
+        }
+        if (!FILL && r < m)
+            seg_cnt[r] = n;
+        return;
+    }
+    const int rows = min(32, m - r0);
+    for (int q = 0; q < rows; ++q)
+    {
+        const int qb = __shfl_sync(FULL, b, q), qe = __shfl_sync(FULL, e, q);
+        const int out = FILL ? seg_ptr[r0 + q] : 0;
+        int n = 0;
+        for (int c0 = qb; c0 < qe; c0 += 32)
+        {
+            const int j = c0 + lane;
+            bool start = false;
+            int T = 0;
+            if (j < qe)
+            {
+                T = __ldg(col + j) >> 4;
+                start = j == qb || (__ldg(col + j - 1) >> 4) != T;
+            }
+            const unsigned st = __ballot_sync(FULL, start);
+            if (FILL && start)
+            {
+                unsigned mk = 0;
+                for (int t = j; t < qe; ++t)
+                {
+                    const int c = __ldg(col + t);
+                    if ((c >> 4) != T)
+                        break;
+                    mk |= 0x8000u >> (c & 15);
+                }
+                seg[out + n + __popc(st & ((1u << lane) - 1u))] = seg_pack(T, mk);
+            }
+            n += __popc(st);
+        }
+        if (!FILL && lane == 0)
+            seg_cnt[r0 + q] = n;
+    }
+}
+
 // ------------------------------------------------ fast path, heavy tile rows
 // A tile row holding a row with thousands of entries (an R-MAT hub) spans
 // thousands of tile columns; the half-warp above takes them one per step and
@@ -834,7 +932,8 @@ inline int grid_for(long long threads, int block) { return (int)((threads + bloc
 } // namespace
 
 int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
-                    const double *val, TileBufs &out, bool packed_col, bool sort_within_rows)
+                    const double *val, TileBufs &out, bool packed_col, bool sort_within_rows,
+                    bool segments)
 {
     if (m < 0 || n < 0 || nnz < 0)
         return fail(RTT_ERR_INVALID_ARGUMENT, "csr2tile: negative size");
@@ -842,6 +941,7 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
     out.m = m;
     out.n = n;
     out.nnz = nnz;
+    out.has_segments = false;
     out.tilem = ceil_div(m, TD);
     out.tilen = ceil_div(n, TD);
     const int tilem = out.tilem;
@@ -876,6 +976,24 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
     // rows that are unsorted may hide repeated columns too
     out.dup_cols = ws.h_scalars[6] != 0 || unsorted;
     out.generic = generic;
+    out.has_segments = false;
+    if (segments && !generic)
+    {
+        // row segments: count per row, scan, fill
+        RTT_CHECK(out.seg_cnt.ensure(sizeof(int) * ((size_t)m + 1), s));
+        RTT_CHECK(out.seg_ptr.ensure(sizeof(int) * ((size_t)m + 1), s));
+        const int grid = grid_for((long long)ceil_div(m, 32) * 32, 256);
+        k_row_segments<false><<<grid, 256, 0, s>>>(m, rowptr, col, out.seg_cnt.as<int>(), nullptr,
+                                                   nullptr);
+        ws.launches++;
+        RTT_CHECK(scan_exclusive_int(ws, out.seg_cnt.as<int>(), out.seg_ptr.as<int>(), m));
+        // at most one segment per entry: size by nnz, no host read
+        RTT_CHECK(out.seg.ensure(sizeof(unsigned long long) * ((size_t)nnz + 1), s));
+        k_row_segments<true><<<grid, 256, 0, s>>>(m, rowptr, col, nullptr, out.seg_ptr.as<int>(),
+                                                  out.seg.as<unsigned long long>());
+        ws.launches++;
+        out.has_segments = true;
+    }
 
     int *cnt = out.tmp0.as<int>();
     // heavy tile rows (a CTA each) are listed on the device; their kernels

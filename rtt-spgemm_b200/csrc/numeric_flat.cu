@@ -55,7 +55,10 @@ constexpr int ACC_SMALL = FLAT_ACC, CTAS_SMALL = 5;
 constexpr int F_SLOT_CAP = FLAT_SLOT_CAP;   // C tiles per window
 constexpr int F_CM_STRIDE = F_SLOT_CAP + 1; // row stride of cm: rows land in distinct banks
 constexpr int F_SPAN_CAP = 4096;            // tile-column span of the slot table
-constexpr int GROUP = 2;                    // B rows loaded together
+#ifndef FLAT_GROUP
+#define FLAT_GROUP 2
+#endif
+constexpr int GROUP = FLAT_GROUP;           // B rows loaded together
 static_assert(RPW == 1 || RPW == 2, "one or two rows per warp");
 
 template <int ACC>
@@ -152,14 +155,29 @@ __device__ __forceinline__ int gallop_lower_bound(const int *a, int lo, int hi, 
 // that part instead of two binary searches over the whole row.
 constexpr int CUR_CAP = 32768;
 
-template <bool SAFE, bool CHECK, int ACC, bool NARROW>
-__device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Window &W, const DevTiles &A,
-                                                   const DevTiles &B, int a0, int a1, int r0,
-                                                   int r1, bool count, int4 *ent, double *enta,
-                                                   int *cur, int ebase, bool first)
+// The warp's A entries, in batches of 32 (lane l: entry l of the batch):
+// calls fn(valid, k, a_ik, row, place) for each batch, place being the
+// entry's index inside its tile row (the same in every window).  ACSR: the
+// warp's rows are contiguous in A's CSR (the device path), entries in column
+// order; otherwise they come from A's tiles, tile by tile (the tile
+// drop-in), which is the same (K, k) order for sorted rows.
+template <bool ACSR, class F>
+__device__ __forceinline__ void warp_entries(const DevTiles &A, int a0, int a1, int r0, int r1,
+                                             int e_a, int e_m, int e_e, int ebase, F &&fn)
 {
     const int lane = lane_id();
-    long long n_fma = 0;
+    if (ACSR)
+    {
+        for (int q0 = e_a; q0 < e_e; q0 += 32)
+        {
+            const int e = q0 + lane;
+            const bool ok = e < e_e;
+            const int k = ok ? __ldg(A.csr_col + e) : 0;
+            const double a = ok ? __ldg(A.csr_val + e) : 0.0;
+            fn(ok, k, a, e < e_m ? r0 : r1, e - ebase, min(32, e_e - q0));
+        }
+        return;
+    }
     for (int t0 = a0; t0 < a1; t0 += 32)
     {
         const int t = t0 + lane;
@@ -193,14 +211,36 @@ __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Windo
             const int o_em = __shfl_sync(FULL, em, own);
             const int o_tn0 = __shfl_sync(FULL, tn0, own);
             const int o_K = __shfl_sync(FULL, K, own);
-            int fs = 0, len = 0, rq = r0;
+            const bool ok = q < total;
+            int k = 0, rq = r0, place = 0;
             double a = 0.0;
-            if (q < total)
+            if (ok)
             {
                 const int e = o_eb + (q - (o_incl - o_n));
                 rq = e < o_em ? r0 : r1;
-                const int k = o_K * TD + (A.col[o_tn0 + e] & 15);
+                k = o_K * TD + (A.col[o_tn0 + e] & 15);
                 a = __ldg(A.val + o_tn0 + e);
+                place = o_tn0 + e - ebase;
+            }
+            fn(ok, k, a, rq, place, min(32, total - q0));
+        }
+    }
+}
+
+template <bool SAFE, bool CHECK, int ACC, bool NARROW, bool ACSR>
+__device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Window &W, const DevTiles &A,
+                                                   const DevTiles &B, int a0, int a1, int r0,
+                                                   int r1, int e_a, int e_m, int e_e, bool count,
+                                                   int4 *ent, double *enta, int *cur, int ebase,
+                                                   bool first)
+{
+    const int lane = lane_id();
+    long long n_fma = 0;
+    warp_entries<ACSR>(A, a0, a1, r0, r1, e_a, e_m, e_e, ebase, [&](bool ok, int k, double a,
+                                                                    int rq, int place, int nbatch) {
+            int fs = 0, len = 0;
+            if (ok)
+            {
                 if (k < B.m)
                 {
                     fs = min(max(__ldg(B.csr_rowptr + k), 0), B.nnz);
@@ -214,7 +254,7 @@ __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Windo
                 {
                     const int lo = W.Jlo * TD, hi = (W.Jlo + W.Jspan + 1) * TD;
                     const int fe = fs + len;
-                    const int ci = o_tn0 + e - ebase; // the entry's place in its tile row
+                    const int ci = place; // the entry's place in its tile row
                     const bool keep = cur != nullptr && (unsigned)ci < (unsigned)CUR_CAP;
                     int sb;
                     if (keep && !first)
@@ -287,7 +327,7 @@ __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Windo
                     ent[lane] = make_int4(fs, len, rq * F_CM_STRIDE, 0);
                     enta[lane] = a;
                     __syncwarp();
-                    run_items(min(32, total - q0));
+                    run_items(nbatch);
                 }
             }
             else
@@ -318,8 +358,7 @@ __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Windo
                 }
             }
             __syncwarp(); // the next batch overwrites this warp's list
-        }
-    }
+        });
     return n_fma;
 }
 
@@ -541,7 +580,7 @@ __global__ void __launch_bounds__(PLAN_WARPS * 32)
 // several windows, so long sorted B rows are cut to each window's columns
 // (compiled out when every tile row fits one window: the registers are the
 // kernel's limit).
-template <bool SAFE, int ACC, int MIN_CTAS, bool WORKER, bool NARROW>
+template <bool SAFE, int ACC, int MIN_CTAS, bool WORKER, bool NARROW, bool ACSR>
 __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
     k_numeric_flat(DevTiles A, DevTiles B, int tilem, long long nnzC,
                    const int *__restrict__ c_tile_ptr, const int *__restrict__ c_tile_col,
@@ -741,18 +780,30 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
                 // each pair counted once: in the first tile window, in its row window
                 const bool count = S.rowwin || w0 == cs0;
                 int *cur = nullptr;
-                int ebase = 0;
+                // the warp's entries in A's CSR (ACSR) and the tile row's first
+                int e_a = 0, e_m = 0, e_e = 0, ebase = 0;
+                if (ACSR)
+                {
+                    const int *rp = A.csr_rowptr + (size_t)I * TD;
+                    ebase = __ldg(rp);
+                    e_a = __ldg(rp + min(r0, nrows));
+                    e_m = __ldg(rp + min(r1, nrows));
+                    e_e = __ldg(rp + min(r1 + 1, nrows));
+                }
                 if (WORKER && cursors != nullptr)
                 {
                     cur = cursors + (size_t)blockIdx.x * CUR_CAP;
-                    ebase = __ldg(A.tile_nnz + a0);
+                    if (!ACSR)
+                        ebase = __ldg(A.tile_nnz + a0);
                 }
                 if (W.table && nW == cs1 - cs0)
-                    n_fma += warp_products<SAFE, false, ACC, NARROW>(S, W, A, B, a0, a1, r0, r1, count,
-                                                                     ent, enta, cur, ebase, w0 == wbeg);
+                    n_fma += warp_products<SAFE, false, ACC, NARROW, ACSR>(
+                        S, W, A, B, a0, a1, r0, r1, e_a, e_m, e_e, count, ent, enta, cur, ebase,
+                        w0 == wbeg);
                 else
-                    n_fma += warp_products<SAFE, true, ACC, NARROW>(S, W, A, B, a0, a1, r0, r1, count,
-                                                                    ent, enta, cur, ebase, w0 == wbeg);
+                    n_fma += warp_products<SAFE, true, ACC, NARROW, ACSR>(
+                        S, W, A, B, a0, a1, r0, r1, e_a, e_m, e_e, count, ent, enta, cur, ebase,
+                        w0 == wbeg);
             }
             __syncthreads();
 
@@ -868,6 +919,9 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
     const int *fused_rowptr = cfg.csr_col ? cfg.csr_rowptr : nullptr;
     // split and narrowing only matter when some tile row has several windows
     const bool split = cfg.split_target >= 0 && S.multi_window;
+    // A's entries straight from its CSR rows when they are given (the device
+    // path), else from its tiles
+    const bool acsr = A.csr_rowptr != nullptr && A.csr_col != nullptr && A.csr_val != nullptr;
     const long long target = cfg.split_target > 0 ? cfg.split_target : SPLIT_TARGET;
     if (split)
     {
@@ -898,8 +952,10 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
         // tasks start while the tile-row CTAs run (the reference's heavy grid
         // enqueued before its light grid, src/dmma_tile_early_split.h:13-27).
         // One wave of resident CTAs; with an empty queue they exit at once.
-        auto wk = cfg.conflict_safe ? k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, true, true>
-                                    : k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, true, true>;
+        auto wk = acsr ? (cfg.conflict_safe ? k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, true, true, true>
+                                            : k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, true, true, true>)
+                       : (cfg.conflict_safe ? k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, true, true, false>
+                                            : k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, true, true, false>);
         int per_sm = 0, sms = 0;
         RTT_CUDA(cudaFuncSetAttribute(wk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         RTT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk, F_THREADS, smem));
@@ -911,11 +967,17 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
         RTT_CHECK(launch(wk, grid, ws.side, smem, S.w_cursor.as<int>()));
         RTT_CUDA(cudaEventRecord(ws.join_ev, ws.side));
     }
-    auto light = cfg.conflict_safe
-                     ? (S.multi_window ? k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, false, true>
-                                       : k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, false, false>)
-                     : (S.multi_window ? k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, true>
-                                       : k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, false>);
+    auto light =
+        acsr ? (cfg.conflict_safe
+                    ? (S.multi_window ? k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, false, true, true>
+                                      : k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, false, false, true>)
+                    : (S.multi_window ? k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, true, true>
+                                      : k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, false, true>))
+             : (cfg.conflict_safe
+                    ? (S.multi_window ? k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, false, true, false>
+                                      : k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, false, false, false>)
+                    : (S.multi_window ? k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, true, false>
+                                      : k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, false, false>));
     RTT_CHECK(launch(light, S.tilem, s, smem, nullptr));
     if (split)
         RTT_CUDA(cudaStreamWaitEvent(s, ws.join_ev, 0));

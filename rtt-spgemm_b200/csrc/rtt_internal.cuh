@@ -60,6 +60,12 @@ struct DevTiles
     const int *csr_rowptr;  // m + 1
     const int *csr_col;     // nnz
     const double *csr_val;  // nnz
+    // row segments of the scalar CSR rows (nullptr when not built): the runs
+    // of a row's entries inside one tile column, in column order, each as
+    // (tile column << 16) | 16-bit column mask (bit 15 - c) - a B row's part
+    // of every 16-bit tile row mask, listed per scalar row
+    const int *seg_ptr;               // m + 1
+    const unsigned long long *seg;    // seg_ptr[m]
 };
 
 // C tile structure produced by the symbolic phase.
@@ -236,7 +242,9 @@ struct TileBufs
     DevBuf tile_ptr, tile_col, tile_row, tile_nnz, ptr, col, val, mask;
     DevBuf csc_ptr, csc_row, csc_data, row_data;
     DevBuf tmp0, tmp1, tmp2, tmp3;
+    DevBuf seg_ptr, seg, seg_cnt; // row segments (csr2tile_device with segments = true)
     int m = 0, n = 0, tilem = 0, tilen = 0, numtile = 0, nnz = 0;
+    bool has_segments = false;
     bool dup_cols = false; // some row may repeat a column (set by csr2tile_device)
     bool generic = false;  // built by the generic (unsorted tile columns) path
     void release();
@@ -245,16 +253,20 @@ struct TileBufs
     template <class F>
     void each(F &&f) const
     {
-        const DevBuf *all[] = {&tile_ptr, &tile_col, &tile_row, &tile_nnz, &ptr, &col,
+        const DevBuf *all[] = {&tile_ptr, &tile_col, &tile_row, &tile_nnz, &ptr,  &col,
                                &val,      &mask,     &csc_ptr,  &csc_row,  &csc_data,
-                               &row_data, &tmp0,     &tmp1,     &tmp2,     &tmp3};
+                               &row_data, &tmp0,     &tmp1,     &tmp2,     &tmp3,
+                               &seg_ptr,  &seg,      &seg_cnt};
         for (const DevBuf *b : all)
             f(*b);
     }
 };
 
+// segments: also list the row segments of the CSR (seg_ptr, seg; only when
+// every row's tile columns are non-decreasing, else has_segments stays false)
 int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
-                    const double *val, TileBufs &out, bool packed_col, bool sort_within_rows);
+                    const double *val, TileBufs &out, bool packed_col, bool sort_within_rows,
+                    bool segments = false);
 // values-only update: tiles built by csr2tile_device (sort_within_rows false)
 // from a CSR of the same structure get the values val (no host round trip)
 int csr2tile_refill_device(Workspace &ws, const int *rowptr, const int *col, const double *val,
@@ -331,6 +343,12 @@ struct SymbolicOut
     }
 };
 
+// step 1 only: C tiles per tile row of A * B into cnt (A.tilem ints)
+int symbolic_tile_counts(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
+                         int *cnt);
+// tile rows [I0, I1) of a device tile matrix with its CSR rows (the 64-bit
+// products run A in such slices; B stays whole)
+DevTiles tile_row_slice(const DevTiles &A, int I0, int I1);
 // b_sorted: B's CSR rows have strictly increasing columns (lets the walk of a
 // wide tile row's windows cut long B rows to each window)
 int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,

@@ -4,6 +4,7 @@
 #include <cub/device/device_scan.cuh>
 #include <cub/iterator/transform_input_iterator.cuh>
 
+#include <algorithm>
 #include <cstdio>
 #include <mutex>
 
@@ -306,6 +307,21 @@ DevTiles TileBufs::view() const
     t.csr_rowptr = nullptr;
     t.csr_col = nullptr;
     t.csr_val = nullptr;
+    t.seg_ptr = has_segments ? seg_ptr.as<int>() : nullptr;
+    t.seg = has_segments ? seg.as<unsigned long long>() : nullptr;
+    return t;
+}
+
+DevTiles tile_row_slice(const DevTiles &A, int I0, int I1)
+{
+    DevTiles t = A;
+    t.tile_ptr = A.tile_ptr + I0;
+    t.tilem = I1 - I0;
+    t.m = std::min(A.m, I1 * TD) - I0 * TD;
+    if (A.csr_rowptr != nullptr)
+        t.csr_rowptr = A.csr_rowptr + (size_t)I0 * TD;
+    if (A.seg_ptr != nullptr)
+        t.seg_ptr = A.seg_ptr + (size_t)I0 * TD;
     return t;
 }
 

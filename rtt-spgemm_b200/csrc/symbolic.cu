@@ -59,7 +59,23 @@ struct CtaSmem2
     int4 ent[NW][32];                    // per warp: B row start, length, mask shift, mask row
     int lo, hi, nb, wend;
     int share;                           // the warps share the A entries (unbalanced rows)
+    int rp[TD + 1];                      // the tile row's A row pointers (segment walk)
 };
+
+// First segment in [lo, hi) whose tile column is >= J (a row's segments are
+// in increasing tile-column order).
+__device__ __forceinline__ int seg_lower_bound(const unsigned long long *seg, int lo, int hi, int J)
+{
+    while (lo < hi)
+    {
+        const int mid = (lo + hi) >> 1;
+        if ((long long)(__ldg(seg + mid) >> 16) < J)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
 
 // Row pairs with very different A entry counts: with NW warps, the pair
 // counts and whether one pair holds > 2.5x the mean (and > min_pair).
@@ -290,7 +306,7 @@ __global__ void __launch_bounds__(S1_WIDE_WARPS * 32)
 // single-window walk registers and issue slots).  NW warps per CTA: 8 for
 // the tile rows in order (a heavy one is skipped when heavy[] marks it), or
 // S2_HEAVY_WARPS for the heavy rows of list[] (all warps share the walk).
-template <bool NARROW, int NW>
+template <bool NARROW, int NW, bool SEGS>
 __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
     k_sym_rows(DevTiles A, DevTiles B, const int *__restrict__ c_tile_ptr,
                int *__restrict__ c_tile_col, int *__restrict__ c_tile_row,
@@ -340,10 +356,12 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
             atomicMax(&S.hi, hi);
         }
     }
+    if (SEGS && tid <= nrows)
+        S.rp[tid] = __ldg(A.csr_rowptr + I * TD + tid);
     __syncthreads();
     const int lo = S.lo, hi = S.hi;
     const bool clip = hi >= 0 && (long long)hi - lo + 1 > WBITS;
-    if (NARROW && NW == S2_WARPS)
+    if (!SEGS && NARROW && NW == S2_WARPS)
     {
         // Row pairs with very different A entry counts (an R-MAT hub row):
         // all warps share the walk.  Balanced rows keep the warp-private walk,
@@ -355,7 +373,7 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
                 S.share = skew;
         }
     }
-    if (NW != S2_WARPS && tid == 0)
+    if (!SEGS && NW != S2_WARPS && tid == 0)
         S.share = 1;
     int cbase = cbeg;
     for (long long wl = lo; hi >= 0 && wl <= hi;)
@@ -446,12 +464,83 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
                 ++slot;
             }
         }
-        for (int i = tid; i < S2_PAIRS * S2_STRIDE; i += NT)
-            S.mw[i] = 0u;
+        for (int p = warp; p < S2_PAIRS; p += NW) // the window's slots of every row pair
+            for (int i = lane; i < nb; i += 32)
+                S.mw[p * S2_STRIDE + i] = 0u;
         __syncthreads();
 
         // ---- masks
-        if ((NARROW || NW != S2_WARPS) && S.share)
+        if (SEGS)
+        {
+            // Each A entry (r, k) of the tile row ORs the row segments of B's
+            // row k - its 16-bit row masks, one per tile column - into row
+            // r's masks: one shared atomic per (entry, B tile) instead of
+            // one per (entry, B entry).  The warps share the tile row's
+            // entries, 32 at a time (masks combine by OR, in any order).  A
+            // lane walks its own entry's segments; lane l starts at segment
+            // l mod ns, since neighbouring entries of a row (k - 1, k, k + 1)
+            // list almost the same tile columns and would otherwise hit the
+            // same mask word in the same step.  Entries with more than 32
+            // segments (hub rows) are walked by the whole warp, one by one.
+            const bool cut = w > lo || wend <= hi; // a window of several
+            const int eb = S.rp[0], ee = S.rp[nrows];
+            auto mark = [&](unsigned long long sg, int r) {
+                const int d = (int)(sg >> 16) - w;
+                if ((unsigned)d < (unsigned)wlen)
+                {
+                    const int sl = S.slot8[d];
+                    if (sl != 255)
+                        atomicOr(&S.mw[(r >> 1) * S2_STRIDE + sl],
+                                 ((unsigned)sg & 0xFFFFu) << ((r & 1) * 16));
+                }
+            };
+            for (int c0 = eb + warp * 32; c0 < ee; c0 += NW * 32)
+            {
+                const int e = c0 + lane;
+                int s0 = 0, ns = 0, r = 0;
+                if (e < ee)
+                {
+                    // the entry's row: the last r with rp[r] <= e
+#pragma unroll
+                    for (int h = 8; h > 0; h >>= 1)
+                        if (r + h < nrows && S.rp[r + h] <= e)
+                            r += h;
+                    const int k = __ldg(A.csr_col + e);
+                    if (k >= 0 && k < B.m)
+                    {
+                        s0 = __ldg(B.seg_ptr + k);
+                        int s1 = __ldg(B.seg_ptr + k + 1);
+                        if (cut)
+                        {
+                            s0 = seg_lower_bound(B.seg, s0, s1, w);
+                            s1 = seg_lower_bound(B.seg, s0, s1, wend);
+                        }
+                        ns = max(s1 - s0, 0);
+                    }
+                }
+                const bool lng = ns > 32;
+                const int nsh = lng ? 0 : ns;
+                const int off = nsh > 0 ? lane % nsh : 0;
+                const int steps = __reduce_max_sync(FULL, (unsigned)nsh);
+                for (int i = 0; i < steps; ++i)
+                    if (i < nsh)
+                    {
+                        int x = off + i;
+                        x -= x >= nsh ? nsh : 0;
+                        mark(__ldg(B.seg + s0 + x), r);
+                    }
+                for (unsigned lm = __ballot_sync(FULL, lng); lm != 0u; lm &= lm - 1u)
+                {
+                    const int j = __ffs(lm) - 1;
+                    const int js0 = __shfl_sync(FULL, s0, j), jns = __shfl_sync(FULL, ns, j);
+                    const int jr = __shfl_sync(FULL, r, j);
+                    for (int t = lane; t < jns; t += 32)
+                        mark(__ldg(B.seg + js0 + t), jr);
+                }
+            }
+            __syncthreads(); // every warp's marks are in
+        }
+        else if ((NARROW || NW != S2_WARPS) && S.share)
         {
             // several windows: a hub row would leave one warp walking while
             // seven wait, so all warps share the tile row's A entries (the
@@ -656,12 +745,13 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
             run1 += warp_sum(c1);
         }
         __syncthreads();
-        // ---- outputs of the window: masks (coalesced u16), tile counts
-        for (int i = tid; i < nb * TD; i += NT)
+        // ---- outputs of the window: masks (a row pair per 32-bit word: row
+        // 2p in the low half is the lower address), tile counts
+        uint32_t *c_mask2 = reinterpret_cast<uint32_t *>(c_mask);
+        for (int i = tid; i < nb * S2_PAIRS; i += NT)
         {
-            const int sl = i >> 4, r = i & 15;
-            const uint32_t v = S.mw[(r >> 1) * S2_STRIDE + sl];
-            c_mask[(size_t)(cbase + sl) * TD + r] = (uint16_t)((v >> ((r & 1) * 16)) & 0xFFFFu);
+            const int sl = i >> 3, p = i & 7;
+            c_mask2[(size_t)(cbase + sl) * S2_PAIRS + p] = S.mw[p * S2_STRIDE + sl];
         }
         for (int sl = tid; sl < nb; sl += NT)
         {
@@ -707,20 +797,11 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
 
 } // namespace
 
-int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
-                    bool b_sorted)
+int symbolic_tile_counts(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
+                         int *cnt)
 {
     cudaStream_t s = ws.stream;
-    if (A.n != B.m)
-        return fail(RTT_ERR_SHAPE_MISMATCH, "symbolic: inner dimensions differ");
-    S.m = A.m;
-    S.n = B.n;
-    S.tilem = A.tilem;
-    S.tilen = B.tilen;
     const int tilem = A.tilem;
-    RTT_CHECK(S.count_tmp.ensure(sizeof(int) * (size_t)(tilem + 1), s));
-    RTT_CHECK(S.c_tile_ptr.ensure(sizeof(int) * (size_t)(tilem + 1), s));
-    int *cnt = S.count_tmp.as<int>();
     // flags: [0] some tile row needs several step-2 windows, [1] several
     // numeric windows, [2] heavy tile rows listed for the wide step-2 CTA
     // [3]: tile rows listed for the wide step-1 CTA
@@ -743,6 +824,24 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
             S.s1_list.as<int>(), flag + 3);
         ws.launches += 2;
     }
+    return RTT_OK;
+}
+
+int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
+                    bool b_sorted)
+{
+    cudaStream_t s = ws.stream;
+    if (A.n != B.m)
+        return fail(RTT_ERR_SHAPE_MISMATCH, "symbolic: inner dimensions differ");
+    S.m = A.m;
+    S.n = B.n;
+    S.tilem = A.tilem;
+    S.tilen = B.tilen;
+    const int tilem = A.tilem;
+    RTT_CHECK(S.count_tmp.ensure(sizeof(int) * (size_t)(tilem + 1), s));
+    RTT_CHECK(S.c_tile_ptr.ensure(sizeof(int) * (size_t)(tilem + 1), s));
+    int *cnt = S.count_tmp.as<int>();
+    RTT_CHECK(symbolic_tile_counts(ws, A, B, S, cnt));
     RTT_CHECK(scan_exclusive_int(ws, cnt, S.c_tile_ptr.as<int>(), tilem));
     RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 13, S.w_flag.p, sizeof(int) * 3,
                              cudaMemcpyDeviceToHost, s));
@@ -761,6 +860,9 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
     RTT_CHECK(S.c_rowptr.ensure(sizeof(long long) * (size_t)(tilem + 1), s));
     RTT_CHECK(S.c_tr_nnz.ensure(sizeof(int) * (size_t)(tilem + 1), s));
     RTT_CHECK(S.tile_cnt.ensure(sizeof(int) * (nt + 1), s));
+    // step 2 from B's row segments when they and A's CSR rows are at hand
+    const bool segs = B.seg_ptr != nullptr && B.seg != nullptr && A.csr_rowptr != nullptr &&
+                      A.csr_col != nullptr;
     if (tilem > 0)
     {
         if (n_heavy > 0)
@@ -769,8 +871,9 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
             // the tile-row CTAs (which skip them)
             RTT_CUDA(cudaEventRecord(ws.fork_ev, s));
             RTT_CUDA(cudaStreamWaitEvent(ws.side, ws.fork_ev, 0));
-            auto wide = b_sorted ? k_sym_rows<true, S2_HEAVY_WARPS>
-                                 : k_sym_rows<false, S2_HEAVY_WARPS>;
+            auto wide = segs ? k_sym_rows<false, S2_HEAVY_WARPS, true>
+                             : b_sorted ? k_sym_rows<true, S2_HEAVY_WARPS, false>
+                                        : k_sym_rows<false, S2_HEAVY_WARPS, false>;
             wide<<<n_heavy, S2_HEAVY_WARPS * 32, 0, ws.side>>>(
                 A, B, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(), S.c_tile_row.as<int>(),
                 S.c_mask.as<uint16_t>(), S.tile_cnt.as<int>(), S.c_row_cnt.as<int>(),
@@ -779,8 +882,9 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
             RTT_CUDA(cudaEventRecord(ws.join_ev, ws.side));
             ws.launches++;
         }
-        auto kern = b_sorted && sym_multi ? k_sym_rows<true, S2_WARPS>
-                                          : k_sym_rows<false, S2_WARPS>;
+        auto kern = segs ? k_sym_rows<false, S2_WARPS, true>
+                         : b_sorted && sym_multi ? k_sym_rows<true, S2_WARPS, false>
+                                                 : k_sym_rows<false, S2_WARPS, false>;
         kern<<<tilem, S2_THREADS, 0, s>>>(
             A, B, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(), S.c_tile_row.as<int>(),
             S.c_mask.as<uint16_t>(), S.tile_cnt.as<int>(), S.c_row_cnt.as<int>(),

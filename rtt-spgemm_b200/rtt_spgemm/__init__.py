@@ -408,6 +408,27 @@ class Context:
         finally:
             self._borrowed = None
 
+    def symbolic64(self, a, b=None, op: int = RTT_OP_AB) -> int:
+        """rtt_spgemm_symbolic64: phase 1 of a product whose C may exceed
+        INT32_MAX entries (chunked over A's tile rows).  Returns nnz(C)."""
+        va = self._view(*a)
+        vb = self._view(*b) if b is not None else None
+        nnz = C.c_longlong()
+        self._borrowed = (a, b)
+        check(lib().rtt_spgemm_symbolic64(self.handle, C.byref(va), C.byref(vb) if vb else None,
+                                          op, C.byref(nnz)))
+        return nnz.value
+
+    def numeric64(self, rowptr, col, val):
+        """rtt_spgemm_numeric64: C into device tensors rowptr (rows + 1,
+        int64), col (int32) and val (float64) of nnz(C) entries."""
+        try:
+            check(lib().rtt_spgemm_numeric64(self.handle, C.c_void_p(rowptr.data_ptr()),
+                                             C.c_void_p(col.data_ptr()),
+                                             C.c_void_p(val.data_ptr())))
+        finally:
+            self._borrowed = None
+
     def numeric_values(self, a_values, b_values, rowptr, col, val):
         """rtt_spgemm_numeric_values: the last symbolic's product with new values
         of A (device tensor in A's CSR order) and of B (or None).  The caller

@@ -37,7 +37,7 @@ EXPORTS = [
     "rtt_csr_transpose", "rtt_early_split_policy_default", "rtt_plan_early_split",
     "rtt_reorder_plan_build", "rtt_reorder_plan_destroy", "rtt_csr_permute",
     "rtt_spgemm_numeric_values", "rtt_super16_index_build", "rtt_super16_index_destroy",
-    "rtt_spgemm_batched_numeric_values",
+    "rtt_spgemm_batched_numeric_values", "rtt_spgemm_symbolic64", "rtt_spgemm_numeric64",
 ]
 
 RTT_SUPER16_A8X4 = 1
@@ -76,7 +76,8 @@ class Config(C.Structure):
     _fields_ = [("dmma_pair_cutoff", C.c_int), ("fused_csr_output", C.c_int),
                 ("keep_tiles", C.c_int), ("stage_timing", C.c_int), ("b_staging", C.c_int),
                 ("split_target", C.c_int), ("cuda_graphs", C.c_int),
-                ("reserved", C.c_int * 4)]
+                ("chunk_tiles", C.c_int), ("chunk_nnz", C.c_int),
+                ("reserved", C.c_int * 2)]
 
 
 class HybridTiles(C.Structure):
@@ -216,6 +217,9 @@ def lib() -> C.CDLL:
     L.rtt_spgemm_symbolic.argtypes = [C.c_void_p, P(CsrView), P(CsrView), C.c_int,
                                       P(C.c_longlong), P(C.c_longlong)]
     L.rtt_spgemm_numeric.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.rtt_spgemm_symbolic64.argtypes = [C.c_void_p, P(CsrView), P(CsrView), C.c_int,
+                                        P(C.c_longlong)]
+    L.rtt_spgemm_numeric64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.rtt_spgemm_tiles_view.argtypes = [C.c_void_p, P(SMatrix)]
     L.rtt_spgemm_csr_host.argtypes = [C.c_void_p, P(SMatrix), P(SMatrix), C.c_int, P(SMatrix)]
     L.rtt_spgemm_batched_symbolic.argtypes = [C.c_void_p, C.c_int, P(CsrView), P(CsrView),
