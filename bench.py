@@ -39,6 +39,8 @@ WORKLOADS = {
     "stencil27_96_brick": "3-D 27-point stencil, 96^3 grid, 2x2x4 brick ordering, C = A^2",
     "laplacian2d_256": "2-D 5-point Laplacian, 256^2 grid (n=65,536), C = A^2",
     "stencil27_80": "3-D 27-point stencil, 80^3 grid (n=512,000), C = A^2 (profiling size)",
+    "stencil27_48_brick": "3-D 27-point stencil, 48^3 grid, 2x2x4 brick ordering, C = A^2 "
+                          "(profiling size of the DMMA path)",
     "rmat16_aat": "R-MAT 2^16, 16 edges/row, (a,b,c,d)=(.57,.19,.19,.05), C = A*A^T (the R-MAT "
                   "config's generator at the largest scale whose C fits int32 offsets)",
     "rmat20_aat": "R-MAT 2^20, 16 edges/row, (a,b,c,d)=(.57,.19,.19,.05), C = A*A^T: nnz(C) past "
@@ -62,6 +64,8 @@ def make_workload(name: str, seed: int):
         return G.laplacian_2d(256)
     if name == "stencil27_80":
         return G.stencil_27(80, seed)
+    if name == "stencil27_48_brick":
+        return G.stencil_27(48, seed).permute_symmetric(G.brick_permutation(48))
     if name == "rmat16_aat":
         return G.rmat(16, 16, seed=seed + 1)
     if name == "rmat20_aat":
@@ -426,6 +430,44 @@ def run_served(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def cusparse_control(a_view, b_view, steps: int, warmup: int, flops: float, got=None) -> dict:
+    """Control: the same product through cuSPARSE's SpGEMM (torch's CSR @ CSR on
+    CUDA), timed with CUDA events on the same inputs - a library baseline on
+    the same GPU, as the reference's cuSPARSE harness measures beside its own
+    kernels.  Its structure is compared with ours."""
+    import torch
+    try:
+        rows, cols, rp, ci, va = a_view
+        A = torch.sparse_csr_tensor(rp.long(), ci.long(), va, size=(rows, cols))
+        if b_view is None:
+            B = A
+        else:
+            rows_b, cols_b, rpb, cib, vab = b_view
+            B = torch.sparse_csr_tensor(rpb.long(), cib.long(), vab, size=(rows_b, cols_b))
+        for _ in range(warmup):
+            C = A @ B
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            C = A @ B
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out = {"what": "cuSPARSE SpGEMM through torch (CSR @ CSR, float64), device-resident",
+               "ms_per_step": ms, "gflops": flops / (ms * 1e-3) / 1e9}
+        if got is not None:
+            crow = C.crow_indices().cpu().numpy()
+            ccol = C.col_indices().cpu().numpy()
+            out["same_structure"] = bool(np.array_equal(crow, np.asarray(got[0], np.int64)) and
+                                         np.array_equal(ccol, np.asarray(got[1], np.int64)))
+        del C
+        torch.cuda.empty_cache()
+        return out
+    except Exception as e:  # the control is optional: report why it did not run
+        return {"unavailable": f"{type(e).__name__}: {e}"[:300]}
+
+
 def run_wide(args) -> None:
     """A product whose C exceeds INT32_MAX entries (R-MAT 2^20 A*A^T) through
     rtt_spgemm_symbolic64 / rtt_spgemm_numeric64, one GPU.  The check samples
@@ -683,6 +725,15 @@ def run_ours(args) -> None:
                "d2h_bytes_per_step": 4 * (A.m + 1) + 12 * int(Ch.nnz), "ms_per_step": e2e_ms}
         got_e2e = (Ch.rowptr, Ch.col, Ch.val)
 
+    control = None
+    if rank == 0 and not args.no_control:
+        b_view = None
+        if aat:
+            At = A.transpose()
+            b_view = (At.m, At.n, torch.from_numpy(At.rowptr).to(dev),
+                      torch.from_numpy(At.col).to(dev), torch.from_numpy(At.val).to(dev))
+        control = cusparse_control(a_view, b_view, max(1, min(3, args.steps)), 1, flops, got)
+        del b_view
     cpu = None
     checks = None
     if rank == 0:
@@ -736,6 +787,7 @@ def run_ours(args) -> None:
         "gpu_launches": launches,
         "clocks": clocks,
         "parity": checks,
+        "cusparse_control": control,
         "e2e": e2e,
         "cpu_baseline": cpu,
         "values_only_update": upd,
@@ -757,6 +809,8 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the check of the results against the oracle")
+    ap.add_argument("--no-control", action="store_true",
+                    help="skip the cuSPARSE SpGEMM control on the same product")
     ap.add_argument("--no-update", action="store_true",
                     help="skip the values-only update timing")
     ap.add_argument("--tune", action="store_true",

@@ -507,6 +507,23 @@ RTT_API int rtt_spgemm_symbolic64(rtt_context ctx, const rtt_csr_view *A,
 RTT_API int rtt_spgemm_numeric64(rtt_context ctx, long long *c_row_ptr, int *c_col_idx,
                                  double *c_values);
 
+/* Dynamic B (the reference's B update modes, src/main.cu:26-32 and
+ * rebuild_b, :1406-1453): C = A*B for the A of the last rtt_spgemm_symbolic
+ * on ctx (op RTT_OP_AB, B or A*A) and a new B.  A's tiles are kept (A stays
+ * borrowed); B is tiled anew and the symbolic phase runs, writing nnz(C) and
+ * its tile count; rtt_spgemm_numeric follows.
+ *   - row_new_to_old == NULL: the structure mode (B_UPDATE_STRUCTURE): B is
+ *     any new matrix with B->rows == A's columns;
+ *   - otherwise the permutation mode (B_UPDATE_PERMUTATION): B's rows are
+ *     taken in the order row_new_to_old (a device array of B->rows ints,
+ *     checked to be a permutation: RTT_ERR_DEVICE_CHECK otherwise), the inner
+ *     order of an A whose columns were permuted the same way.
+ * The values mode (B_UPDATE_VALUES) is rtt_spgemm_numeric_values.
+ * RTT_ERR_STATE without such a symbolic phase (or after A*A^T or a batch). */
+RTT_API int rtt_spgemm_update_b(rtt_context ctx, const rtt_csr_view *B,
+                                const int *row_new_to_old, long long *nnz_c,
+                                long long *tiles_c);
+
 /* Values-only update (the reference's dynamic-B "values-only" mode,
  * src/main.cu:26-32, :1406-1453, for A and B): the same product as the last
  * rtt_spgemm_symbolic, with new values for A (a_values, device, A's CSR order)

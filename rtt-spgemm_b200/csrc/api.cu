@@ -18,6 +18,8 @@
 #include <mutex>
 #include <vector>
 
+#include <sys/mman.h>
+
 namespace rtt
 {
 // One captured numeric phase.  The key lists every host-side input that its
@@ -48,6 +50,7 @@ struct rtt_context_s
     rtt_config cfg;
     rtt::TileBufs A, B;
     rtt::DevBuf bt_rowptr, bt_col, bt_val; // B = A^T for RTT_OP_AAT
+    rtt::DevBuf bp_rowptr, bp_col, bp_val; // B with permuted rows (rtt_spgemm_update_b)
     rtt::DevBuf in_rp, in_col, in_val;     // host-buffer uploads
     rtt::DevBuf in2_rp, in2_col, in2_val;
     rtt::DevBuf out_rp, out_col, out_val;  // host-buffer product output
@@ -111,7 +114,8 @@ std::vector<DevBuf *> own_buffers(rtt_context c)
             &c->out_col,   &c->out_val,   &c->counters,   &c->maxnnz,    &c->bat_a_rp,
             &c->bat_a_col, &c->bat_a_val, &c->bat_b_rp,   &c->bat_b_col, &c->bat_b_val,
             &c->bat_meta,  &c->bat_big_rp, &c->bat_nnz,  &c->vflags,    &c->bat_vtab,
-            &c->w_cnt,     &c->w_rowcnt,  &c->w_rowptr,   &c->w_local};
+            &c->w_cnt,     &c->w_rowcnt,  &c->w_rowptr,   &c->w_local,   &c->bp_rowptr,
+            &c->bp_col,    &c->bp_val};
 }
 
 std::mutex g_mutex;
@@ -245,10 +249,27 @@ int upload(rtt_context c, DevBuf &b, const T *h, size_t n, cudaStream_t s)
     return RTT_OK;
 }
 
+// Host output arrays of the host-buffer entry points are malloc'd: the
+// caller frees them with free(), as with the reference.  Large ones start on
+// a 2 MiB boundary and are advised to use transparent huge pages where the
+// kernel offers them, so that their first touch (inside d2h) takes one page
+// fault per 2 MiB instead of one per 4 KiB.
+void *host_alloc(size_t bytes)
+{
+    constexpr size_t huge = size_t(2) << 20;
+    if (bytes < 2 * huge)
+        return std::malloc(bytes);
+    void *p = nullptr;
+    if (posix_memalign(&p, huge, bytes) != 0)
+        return nullptr;
+    madvise(p, bytes, MADV_HUGEPAGE); // advice only: a kernel without THP ignores it
+    return p;
+}
+
 template <typename T>
 int download(rtt_context c, T **out, const void *d, size_t n, cudaStream_t s)
 {
-    T *h = static_cast<T *>(std::malloc(sizeof(T) * (n > 0 ? n : 1)));
+    T *h = static_cast<T *>(host_alloc(sizeof(T) * (n > 0 ? n : 1)));
     if (h == nullptr)
         return fail(RTT_ERR_OUT_OF_MEMORY, "host malloc failed");
     if (n > 0)
@@ -552,8 +573,11 @@ int upload_tiles(rtt_context c, const SMatrix *M, bool col_major, TileBufs &T)
 int effective_cutoff(rtt_context c, const DevTiles &A, const DevTiles &B, int *cutoff)
 {
     *cutoff = c->cfg.dmma_pair_cutoff;
-    if (*cutoff <= 0)
+    if (*cutoff <= 0 || !A.tile_nnz || !B.tile_nnz)
+    {
+        *cutoff = 0;
         return RTT_OK;
+    }
     if (c->cut_cached >= 0)
     {
         *cutoff = c->cut_cached;
@@ -591,7 +615,8 @@ void numeric_key(rtt_context c, std::vector<long long> &k)
     for (const TileBufs *T : both)
         for (long long v : {(long long)T->m, (long long)T->n, (long long)T->tilem,
                             (long long)T->tilen, (long long)T->numtile, (long long)T->nnz,
-                            (long long)T->dup_cols, (long long)T->generic})
+                            (long long)T->dup_cols, (long long)T->generic,
+                            (long long)T->payload})
             k.push_back(v);
     const SymbolicOut &S = c->S;
     for (long long v : {(long long)S.numtile, S.nnz, (long long)S.tilem, (long long)S.tilen,
@@ -718,7 +743,8 @@ int numeric_enqueue(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_val
     NumericConfig nc;
     nc.dmma_pair_cutoff = cutoff;
     nc.counters = c->counters.as<long long>();
-    nc.b_staging = c->cfg.b_staging != 0;
+    // TMA staging reads the tile arrays: only when they were built
+    nc.b_staging = c->cfg.b_staging != 0 && c->A.payload && TB.payload;
     nc.split_target = c->cfg.split_target;
     if (c->cfg.stage_timing)
     {
@@ -800,10 +826,14 @@ int prepare_operands(rtt_context c, const rtt_csr_view *A, const rtt_csr_view *B
                      DevTiles &dA, DevTiles &dB)
 {
     Workspace &ws = c->ws;
+    // The flat numeric step reads A and B from their CSR rows, so only the
+    // tile index and B's row segments are built; the per-entry tile arrays
+    // are built for the kernels that read them (DMMA pairs, TMA staging).
+    const bool payload = c->cfg.dmma_pair_cutoff > 0 || c->cfg.b_staging != 0;
     // B's row segments drive symbolic step 2: A's own when B is A
     RTT_CHECK(map_device_error(csr2tile_device(ws, A->rows, A->cols, (int)A->nnz, A->row_ptr,
                                                A->col_idx, A->values, c->A, true, false,
-                                               op == RTT_OP_AB && B == nullptr)));
+                                               op == RTT_OP_AB && B == nullptr, payload)));
     c->a_rp = A->row_ptr;
     c->a_ci = A->col_idx;
     c->a_va = A->values;
@@ -833,7 +863,7 @@ int prepare_operands(rtt_context c, const rtt_csr_view *A, const rtt_csr_view *B
             RTT_CHECK(map_device_error(csr2tile_device(ws, A->cols, A->rows, (int)A->nnz,
                                                        c->bt_rowptr.as<int>(), c->bt_col.as<int>(),
                                                        c->bt_val.as<double>(), c->B, true, false,
-                                                       true)));
+                                                       true, payload)));
             c->b_rp = c->bt_rowptr.as<int>();
             c->b_ci = c->bt_col.as<int>();
             c->b_va = c->bt_val.as<double>();
@@ -847,7 +877,7 @@ int prepare_operands(rtt_context c, const rtt_csr_view *A, const rtt_csr_view *B
                 return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "bad B shape");
             RTT_CHECK(map_device_error(csr2tile_device(ws, B->rows, B->cols, (int)B->nnz,
                                                        B->row_ptr, B->col_idx, B->values, c->B,
-                                                       true, false, true)));
+                                                       true, false, true, payload)));
             c->b_rp = B->row_ptr;
             c->b_ci = B->col_idx;
             c->b_va = B->values;
@@ -1589,6 +1619,73 @@ int rtt_spgemm_symbolic(rtt_context c, const rtt_csr_view *A, const rtt_csr_view
     return RTT_OK;
 }
 
+int rtt_spgemm_update_b(rtt_context c, const rtt_csr_view *B, const int *row_new_to_old,
+                        long long *nnz_c, long long *tiles_c)
+{
+    if (c == nullptr || B == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "update_b: NULL argument");
+    if (!c->have_symbolic || c->bat_active || c->op_aat)
+        return rtt::fail(RTT_ERR_STATE,
+                         "rtt_spgemm_update_b needs a C = A*B (or A*A) symbolic phase first");
+    if (B->rows < 0 || B->cols < 0 || B->nnz < 0 || B->nnz > INT_MAX)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "bad B shape");
+    if (B->rows != c->A.n)
+        return rtt::fail(RTT_ERR_SHAPE_MISMATCH, "update_b: B->rows != A->cols");
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    Workspace &ws = c->ws;
+    cudaStream_t s = ws.stream;
+    c->have_symbolic = false;
+    c->cut_cached = -1;
+    ws.launches = 0;
+    ws.syncs = 0;
+    rtt_csr_view b = *B;
+    if (row_new_to_old != nullptr)
+    {
+        // permutation mode: B's rows in the given order (the map is checked
+        // to be a permutation on the device), columns as they are
+        RTT_CHECK(c->bp_rowptr.ensure(sizeof(int) * ((size_t)B->rows + 1), s));
+        RTT_CHECK(c->bp_col.ensure(sizeof(int) * (size_t)B->nnz + 16, s));
+        RTT_CHECK(c->bp_val.ensure(sizeof(double) * (size_t)B->nnz + 16, s));
+        RTT_CHECK(map_device_error(csr_permute_device(ws, *B, row_new_to_old, nullptr,
+                                                      c->bp_rowptr.as<int>(), c->bp_col.as<int>(),
+                                                      c->bp_val.as<double>())));
+        b.row_ptr = c->bp_rowptr.as<int>();
+        b.col_idx = c->bp_col.as<int>();
+        b.values = c->bp_val.as<double>();
+    }
+    // A's tiles and CSR stay as the last symbolic phase left them; B is tiled anew
+    const bool payload = c->cfg.dmma_pair_cutoff > 0 || c->cfg.b_staging != 0;
+    RTT_CHECK(map_device_error(csr2tile_device(ws, b.rows, b.cols, (int)b.nnz, b.row_ptr,
+                                               b.col_idx, b.values, c->B, true, false, true,
+                                               payload && c->A.payload)));
+    c->b_alias = false;
+    c->b_rp = b.row_ptr;
+    c->b_ci = b.col_idx;
+    c->b_va = b.values;
+    c->b_nnz = b.nnz;
+    c->b_dups = c->B.dup_cols;
+    DevTiles dB = c->B.view();
+    dB.csr_rowptr = c->b_rp;
+    dB.csr_col = c->b_ci;
+    dB.csr_val = c->b_va;
+    dB.nnz = (int)c->b_nnz;
+    DevTiles dA = c->A.view();
+    dA.csr_rowptr = c->a_rp;
+    dA.csr_col = c->a_ci;
+    RTT_CHECK(map_device_error(symbolic_device(ws, dA, dB, c->S, !c->b_dups)));
+    c->stats.nnz_b = c->B.nnz;
+    c->stats.nnz_c = c->S.nnz;
+    c->stats.tiles_b = c->B.numtile;
+    c->stats.tiles_c = c->S.numtile;
+    c->stats.host_syncs = ws.syncs;
+    if (nnz_c)
+        *nnz_c = c->S.nnz;
+    if (tiles_c)
+        *tiles_c = c->S.numtile;
+    c->have_symbolic = true;
+    return RTT_OK;
+}
+
 int rtt_spgemm_numeric_values(rtt_context c, const double *a_values, const double *b_values,
                               int *c_row_ptr, int *c_col_idx, double *c_values)
 {
@@ -1631,20 +1728,23 @@ int rtt_spgemm_numeric_values(rtt_context c, const double *a_values, const doubl
     std::vector<long long> key{1, as_key(a_values), as_key(b_values), as_key(c_row_ptr),
                                as_key(c_col_idx), as_key(c_values)};
     RTT_CHECK(run_phase(c, 1, key, c->cfg.fused_csr_output != 0, [&]() -> int {
-        // A's tiles take the new values (same structure, same tile order)
-        RTT_CHECK(map_device_error(
-            csr2tile_refill_device(ws, c->a_rp, c->a_ci, a_values, c->A, true)));
+        // A's tiles take the new values (same structure, same tile order);
+        // without tile arrays the numeric step reads the new values directly
+        if (c->A.payload)
+            RTT_CHECK(map_device_error(
+                csr2tile_refill_device(ws, c->a_rp, c->a_ci, a_values, c->A, true)));
         if (!c->b_alias && c->op_aat)
         {
             // B = A^T again, values only (its structure is unchanged)
             RTT_CHECK(csr_transpose_device(ws, c->A.m, c->A.n, c->A.nnz, c->a_rp, c->a_ci,
                                            a_values, c->bt_rowptr.as<int>(), c->bt_col.as<int>(),
                                            c->bt_val.as<double>()));
-            RTT_CHECK(map_device_error(csr2tile_refill_device(ws, c->bt_rowptr.as<int>(),
-                                                              c->bt_col.as<int>(),
-                                                              c->bt_val.as<double>(), c->B, true)));
+            if (c->B.payload)
+                RTT_CHECK(map_device_error(csr2tile_refill_device(
+                    ws, c->bt_rowptr.as<int>(), c->bt_col.as<int>(), c->bt_val.as<double>(),
+                    c->B, true)));
         }
-        else if (!c->b_alias && b_values != nullptr)
+        else if (!c->b_alias && b_values != nullptr && c->B.payload)
             RTT_CHECK(map_device_error(
                 csr2tile_refill_device(ws, c->b_rp, c->b_ci, b_values, c->B, true)));
         return numeric_enqueue(c, c_row_ptr, c_col_idx, c_values, cutoff);
@@ -2078,14 +2178,16 @@ int rtt_spgemm_batched_numeric_values(rtt_context c, const double *const *a_valu
         // the instances' values into the block diagonal, then its tiles
         RTT_CHECK(batch_values_device(ws, n, c->bat_a_max, a_tab, a_off,
                                       c->bat_a_val.as<double>()));
-        RTT_CHECK(map_device_error(csr2tile_refill_device(ws, c->a_rp, c->a_ci,
-                                                          c->bat_a_val.as<double>(), c->A, true)));
+        if (c->A.payload)
+            RTT_CHECK(map_device_error(csr2tile_refill_device(
+                ws, c->a_rp, c->a_ci, c->bat_a_val.as<double>(), c->A, true)));
         if (with_b && !c->b_alias)
         {
             RTT_CHECK(batch_values_device(ws, n, c->bat_b_max, b_tab, b_off,
                                           c->bat_b_val.as<double>()));
-            RTT_CHECK(map_device_error(csr2tile_refill_device(
-                ws, c->b_rp, c->b_ci, c->bat_b_val.as<double>(), c->B, true)));
+            if (c->B.payload)
+                RTT_CHECK(map_device_error(csr2tile_refill_device(
+                    ws, c->b_rp, c->b_ci, c->bat_b_val.as<double>(), c->B, true)));
         }
         RTT_CHECK(numeric_enqueue(c, c->bat_big_rp.as<int>(), c_col_idx, c_values, cutoff));
         const int *meta_d = c->bat_meta.as<int>();

@@ -334,6 +334,71 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// Tile structure (no per-entry payload) of a tile row from its rows'
+// segments: the tile columns are the union of the 16 rows' segment columns,
+// taken in ascending order by a half-warp (a lane per row walks its segment
+// list; the half-warp takes the minimum pending column, and the lanes holding
+// it step to their next segment).  FILL = false counts the tiles of each
+// tile row, FILL = true writes tile_col and tile_row from tile_ptr[I].  Tile
+// rows marked heavy are left to k_c2t_heavy_count / k_c2t_heavy_struct.
+template <bool FILL>
+__global__ void __launch_bounds__(256)
+    k_c2t_seg_tiles(int m, int tilem, const int *__restrict__ seg_ptr,
+                    const unsigned long long *__restrict__ seg, const int *__restrict__ tile_ptr,
+                    int *__restrict__ cnt, int *__restrict__ o_tcol, int *__restrict__ o_trow,
+                    int *err, const uint8_t *__restrict__ heavy)
+{
+    const int lane = threadIdx.x & 31, hl = lane & 15;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int I = gw * 2 + (lane >> 4);
+    const bool mine = I < tilem && !(heavy != nullptr && heavy[I]);
+    int p = 0, e = 0, t = 0, tend = 0;
+    if (mine)
+    {
+        if (I * TD + hl < m)
+        {
+            p = seg_ptr[I * TD + hl];
+            e = seg_ptr[I * TD + hl + 1];
+        }
+        if (FILL)
+        {
+            t = tile_ptr[I];
+            tend = tile_ptr[I + 1];
+        }
+    }
+    int cur = p < e ? (int)(__ldg(seg + p) >> 16) : INT_MAX;
+    int count = 0;
+    for (;;)
+    {
+        const int T = half_min(cur);
+        const bool has = T != INT_MAX;
+        if (!__any_sync(FULL, has))
+            break;
+        if (has)
+        {
+            if (FILL && hl == 0)
+            {
+                if (t < tend)
+                {
+                    o_tcol[t] = T;
+                    o_trow[t] = I;
+                }
+                else
+                    set_error(err, DERR_C2T_OVERFLOW);
+            }
+            ++t;
+            ++count;
+            if (cur == T)
+            {
+                ++p;
+                cur = p < e ? (int)(__ldg(seg + p) >> 16) : INT_MAX;
+            }
+        }
+    }
+    if (!FILL && mine && hl == 0)
+        cnt[I] = count;
+}
+
 // ------------------------------------------------ fast path, heavy tile rows
 // A tile row holding a row with thousands of entries (an R-MAT hub) spans
 // thousands of tile columns; the half-warp above takes them one per step and
@@ -488,6 +553,37 @@ __global__ void __launch_bounds__(HV_THREADS)
         if (threadIdx.x == 0)
             cnt[I] = S.count;
         __syncthreads();
+    }
+}
+
+// Structure only (no per-entry payload) of the heavy tile rows: tile
+// columns are the bitmap's set bits in order.
+__global__ void __launch_bounds__(HV_THREADS)
+    k_c2t_heavy_struct(int m, const int *__restrict__ list, const int *__restrict__ count,
+                       const int *__restrict__ rowptr, const int *__restrict__ col,
+                       const int *__restrict__ tile_ptr, int *__restrict__ o_tcol,
+                       int *__restrict__ o_trow, int *err)
+{
+    extern __shared__ __align__(16) unsigned char hv_dyn[];
+    HeavySmem &S = *reinterpret_cast<HeavySmem *>(hv_dyn);
+    const int n = *count;
+    for (int li = blockIdx.x; li < n; li += gridDim.x)
+    {
+        const int I = list[li];
+        heavy_bitmap(S, I, m, rowptr, col);
+        const int ntiles = S.count, t0 = tile_ptr[I];
+        if (t0 + ntiles != tile_ptr[I + 1])
+        {
+            if (threadIdx.x == 0)
+                set_error(err, DERR_C2T_OVERFLOW);
+        }
+        else
+            for (int k = threadIdx.x; k < ntiles; k += HV_THREADS)
+            {
+                o_tcol[t0 + k] = heavy_select(S, k);
+                o_trow[t0 + k] = I;
+            }
+        __syncthreads(); // the bitmap is rebuilt for the next tile row
     }
 }
 
@@ -933,7 +1029,7 @@ inline int grid_for(long long threads, int block) { return (int)((threads + bloc
 
 int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
                     const double *val, TileBufs &out, bool packed_col, bool sort_within_rows,
-                    bool segments)
+                    bool segments, bool payload)
 {
     if (m < 0 || n < 0 || nnz < 0)
         return fail(RTT_ERR_INVALID_ARGUMENT, "csr2tile: negative size");
@@ -942,6 +1038,7 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
     out.n = n;
     out.nnz = nnz;
     out.has_segments = false;
+    out.payload = true;
     out.tilem = ceil_div(m, TD);
     out.tilen = ceil_div(n, TD);
     const int tilem = out.tilem;
@@ -977,7 +1074,10 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
     out.dup_cols = ws.h_scalars[6] != 0 || unsorted;
     out.generic = generic;
     out.has_segments = false;
-    if (segments && !generic)
+    // the structure alone comes from the row segments, which need rows whose
+    // tile columns never decrease; otherwise the whole tile payload is built
+    const bool structure_only = !payload && !generic;
+    if ((segments || structure_only) && !generic)
     {
         // row segments: count per row, scan, fill
         RTT_CHECK(out.seg_cnt.ensure(sizeof(int) * ((size_t)m + 1), s));
@@ -1022,6 +1122,35 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
         k_c2t_heavy_count<<<hv_grid, HV_THREADS, hv_smem, s>>>(m, hv_list, hv_count, rowptr, col,
                                                                cnt);
         ws.launches++;
+    }
+    if (structure_only)
+    {
+        // tile_ptr, tile_col and tile_row only (from the row segments)
+        const int grid = grid_for((long long)ceil_div(tilem, 2) * 32, 256);
+        k_c2t_seg_tiles<false><<<grid, 256, 0, s>>>(m, tilem, out.seg_ptr.as<int>(),
+                                                     out.seg.as<unsigned long long>(), nullptr,
+                                                     cnt, nullptr, nullptr, ws.err.as<int>(),
+                                                     heavy);
+        ws.launches++;
+        RTT_CHECK(scan_exclusive_int(ws, cnt, out.tile_ptr.as<int>(), tilem));
+        int numtile = 0;
+        RTT_CHECK(read_int(ws, out.tile_ptr.as<int>() + tilem, &numtile));
+        out.numtile = numtile;
+        RTT_CHECK(out.tile_col.ensure(sizeof(int) * (size_t)numtile + 16, s));
+        RTT_CHECK(out.tile_row.ensure(sizeof(int) * (size_t)numtile + 16, s));
+        k_c2t_seg_tiles<true><<<grid, 256, 0, s>>>(m, tilem, out.seg_ptr.as<int>(),
+                                                    out.seg.as<unsigned long long>(),
+                                                    out.tile_ptr.as<int>(), nullptr,
+                                                    out.tile_col.as<int>(), out.tile_row.as<int>(),
+                                                    ws.err.as<int>(), heavy);
+        RTT_CUDA(cudaFuncSetAttribute(k_c2t_heavy_struct,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hv_smem));
+        k_c2t_heavy_struct<<<hv_grid, HV_THREADS, hv_smem, s>>>(
+            m, hv_list, hv_count, rowptr, col, out.tile_ptr.as<int>(), out.tile_col.as<int>(),
+            out.tile_row.as<int>(), ws.err.as<int>());
+        ws.launches += 2;
+        out.payload = false;
+        return RTT_OK;
     }
     if (!generic)
         k_c2t_count<<<grid_for((long long)ceil_div(tilem, 2) * 32, 256), 256, 0, s>>>(m, tilem, rowptr,

@@ -463,17 +463,29 @@ __global__ void __launch_bounds__(PLAN_WARPS * 32)
     // windows, about SPLIT_TARGET products of walking; a row whose windows all
     // fit one task keeps its own CTA and the L1 reuse of its B rows.
     long long P = 0;
-    for (int t = a0 + lane; t < a1; t += 32)
+    if (A.csr_rowptr != nullptr && A.csr_col != nullptr)
     {
-        const int e0 = __ldg(A.tile_nnz + t), e1 = __ldg(A.tile_nnz + t + 1);
-        const int K = __ldg(A.tile_col + t);
-        for (int e = e0; e < e1; ++e)
+        // the tile row's entries straight from A's CSR rows
+        const int e0 = __ldg(A.csr_rowptr + I * TD), e1 = __ldg(A.csr_rowptr + min(A.m, I * TD + TD));
+        for (int e = e0 + lane; e < e1; e += 32)
         {
-            const int k = K * TD + (A.col[e] & 15);
+            const int k = __ldg(A.csr_col + e);
             if (k < B.m)
                 P += __ldg(B.csr_rowptr + k + 1) - __ldg(B.csr_rowptr + k);
         }
     }
+    else
+        for (int t = a0 + lane; t < a1; t += 32)
+        {
+            const int e0 = __ldg(A.tile_nnz + t), e1 = __ldg(A.tile_nnz + t + 1);
+            const int K = __ldg(A.tile_col + t);
+            for (int e = e0; e < e1; ++e)
+            {
+                const int k = K * TD + (A.col[e] & 15);
+                if (k < B.m)
+                    P += __ldg(B.csr_rowptr + k + 1) - __ldg(B.csr_rowptr + k);
+            }
+        }
     P = warp_sum(P);
     const int g = (int)max(1ll, min((long long)nwin, target / max(P, 1ll)));
     const int ntask = (nwin + g - 1) / g;

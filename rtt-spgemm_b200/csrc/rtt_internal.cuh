@@ -245,6 +245,7 @@ struct TileBufs
     DevBuf seg_ptr, seg, seg_cnt; // row segments (csr2tile_device with segments = true)
     int m = 0, n = 0, tilem = 0, tilen = 0, numtile = 0, nnz = 0;
     bool has_segments = false;
+    bool payload = true;  // per-entry arrays (tile_nnz, ptr, col, val, mask) built
     bool dup_cols = false; // some row may repeat a column (set by csr2tile_device)
     bool generic = false;  // built by the generic (unsorted tile columns) path
     void release();
@@ -263,10 +264,12 @@ struct TileBufs
 };
 
 // segments: also list the row segments of the CSR (seg_ptr, seg; only when
-// every row's tile columns are non-decreasing, else has_segments stays false)
+// every row's tile columns are non-decreasing, else has_segments stays false).
+// payload = false: only the tile index (tile_ptr, tile_col, tile_row) and the
+// row segments, when the rows allow it (out.payload tells what was built)
 int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
                     const double *val, TileBufs &out, bool packed_col, bool sort_within_rows,
-                    bool segments = false);
+                    bool segments = false, bool payload = true);
 // values-only update: tiles built by csr2tile_device (sort_within_rows false)
 // from a CSR of the same structure get the values val (no host round trip)
 int csr2tile_refill_device(Workspace &ws, const int *rowptr, const int *col, const double *val,

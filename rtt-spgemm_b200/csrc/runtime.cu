@@ -295,11 +295,12 @@ DevTiles TileBufs::view() const
     t.nnz = nnz;
     t.tile_ptr = tile_ptr.as<int>();
     t.tile_col = tile_col.as<int>();
-    t.tile_nnz = tile_nnz.as<int>();
-    t.ptr = ptr.as<uint8_t>();
-    t.col = col.as<uint8_t>();
-    t.val = val.as<double>();
-    t.mask = mask.as<uint16_t>();
+    // the per-entry arrays only when built (null views otherwise)
+    t.tile_nnz = payload ? tile_nnz.as<int>() : nullptr;
+    t.ptr = payload ? ptr.as<uint8_t>() : nullptr;
+    t.col = payload ? col.as<uint8_t>() : nullptr;
+    t.val = payload ? val.as<double>() : nullptr;
+    t.mask = payload ? mask.as<uint16_t>() : nullptr;
     t.row_data = nullptr;
     t.csc_ptr = csc_ptr.as<int>();
     t.csc_row = csc_row.as<int>();

@@ -408,6 +408,20 @@ class Context:
         finally:
             self._borrowed = None
 
+    def update_b(self, b, row_new_to_old=None):
+        """rtt_spgemm_update_b: the last symbolic's A with a new B (structure
+        mode), or B's rows in the order row_new_to_old (a device int32 tensor:
+        permutation mode).  Returns (nnz, tiles) of C; numeric() follows."""
+        vb = self._view(*b)
+        nnz = C.c_longlong()
+        tiles = C.c_longlong()
+        a = self._borrowed[0] if getattr(self, "_borrowed", None) else None
+        self._borrowed = (a, b, row_new_to_old)
+        ptr = C.c_void_p(row_new_to_old.data_ptr()) if row_new_to_old is not None else None
+        check(lib().rtt_spgemm_update_b(self.handle, C.byref(vb), ptr, C.byref(nnz),
+                                        C.byref(tiles)))
+        return nnz.value, tiles.value
+
     def symbolic64(self, a, b=None, op: int = RTT_OP_AB) -> int:
         """rtt_spgemm_symbolic64: phase 1 of a product whose C may exceed
         INT32_MAX entries (chunked over A's tile rows).  Returns nnz(C)."""
