@@ -48,14 +48,23 @@ WORKLOADS = {
     "served": "Poisson request stream (2,000 req/s) of mixed A^2 / A*A^T products, n log-uniform "
               "in [4,096, n_max], 2-D/3-D stencils, R-MAT, banded+scatter, 30% reuse a resident A; "
               "120 GB pool; served (batched as they arrive) vs plain one-call FIFO",
+    "mtx": "a Matrix Market file (--mtx; e.g. a SuiteSparse matrix), C = A^2, read as the "
+           "reference's mmio_allinone reads it",
+    "mtx_aat": "a Matrix Market file (--mtx), C = A*A^T",
     "batched": "independent A_i^2: n_i log-uniform in [2,000, 200,000], banded (half-bandwidth "
                "8..64, band kept w.p. 0.5) + 0..4 random entries per row; batched form vs one "
                "call per product",
 }
 
 
+MTX = {"path": None, "value_mode": 0}
+
+
 def make_workload(name: str, seed: int):
     from rtt_spgemm import generators as G
+    if name in ("mtx", "mtx_aat"):
+        import rtt_spgemm as R
+        return R.mmio_read(MTX["path"], MTX["value_mode"])
     if name == "stencil27_96":
         return G.stencil_27(96, seed)
     if name == "stencil27_96_brick":
@@ -809,6 +818,10 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the check of the results against the oracle")
+    ap.add_argument("--mtx", default=None,
+                    help="Matrix Market file for --workload mtx / mtx_aat")
+    ap.add_argument("--mtx-ref-values", action="store_true",
+                    help="overwrite the file's values with i %% 10, as the reference's benchmark does")
     ap.add_argument("--no-control", action="store_true",
                     help="skip the cuSPARSE SpGEMM control on the same product")
     ap.add_argument("--no-update", action="store_true",
@@ -825,6 +838,10 @@ def main() -> None:
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload.startswith("mtx"):
+        if not args.mtx:
+            raise SystemExit("--workload mtx needs --mtx PATH")
+        MTX.update(path=args.mtx, value_mode=1 if args.mtx_ref_values else 0)
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "batched":

@@ -117,6 +117,20 @@ RTT_API const char *rtt_version(void);
  * the current CUDA device (device 0 unless rtt_set_device was called).
  * ------------------------------------------------------------------------ */
 
+/* Replaces mmio_allinone (src/mmio_highlevel.h:593-760), the reference's
+ * Matrix Market reader: a coordinate file (real, integer, pattern -> 1.0,
+ * complex -> real part; general, symmetric, hermitian or skew-symmetric) into
+ * a CSR SMatrix: m, n, nnz, isSymmetric and malloc'd rowpointer, columnindex,
+ * value (free them, or rtt_matrix_destroy(out, 1)).  0-based; entries neither
+ * sorted nor merged; a symmetric or hermitian file also stores each
+ * off-diagonal entry mirrored, placed as it is read - the reference's exact
+ * layout.  value_mode 1 sets entry i's value to i % 10 as the reference's
+ * benchmark does after reading (src/main.cu:1109-1110); 0 keeps the file's.
+ * Unlike the reference, indices outside the declared shape and short files
+ * are errors (RTT_ERR_INVALID_CSR); a bad banner or a missing file gives
+ * RTT_ERR_INVALID_ARGUMENT.  Host only: no GPU is needed. */
+RTT_API int rtt_mmio_read(const char *path, int value_mode, SMatrix *out);
+
 /* Select the CUDA device used by the host-buffer entry points. */
 RTT_API int rtt_set_device(int device);
 

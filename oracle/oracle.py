@@ -717,6 +717,24 @@ class Reference(_Base):
                 "exact_parent_partition")
         return ch[:n], dict(reason=reason, **{k: int(v) for k, v in zip(keys, summ)})
 
+    def mmio_allinone(self, path):
+        """The reference's Matrix Market reader: (m, n, is_symmetric, rowptr,
+        col, val) as numpy arrays."""
+        L = self.lib
+        L.ref_mmio_allinone.argtypes = [C.c_char_p] + [C.c_void_p] * 7
+        m, n, nnz, sym = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        rp, col, val = C.POINTER(C.c_int)(), C.POINTER(C.c_int)(), C.POINTER(C.c_double)()
+        st = L.ref_mmio_allinone(str(path).encode(), C.addressof(m), C.addressof(n),
+                                 C.addressof(nnz), C.addressof(sym), C.addressof(rp),
+                                 C.addressof(col), C.addressof(val))
+        if st != 0:
+            raise ValueError(f"mmio_allinone status {st}")
+        out = (m.value, n.value, sym.value, _copy(rp, m.value + 1, np.int32),
+               _copy(col, nnz.value, np.int32), _copy(val, nnz.value, np.float64))
+        for p in (rp, col, val):
+            self._free(C.cast(p, C.c_void_p))
+        return out
+
     def spgemm_serialref(self, a, b):
         rp = np.zeros(a.m + 1, dtype=np.int32)
         nnz = C.c_int(0)

@@ -12,6 +12,7 @@
  *   csr_to_hybrid_tiles                      src/dmma_tiles.h:243
  *   dmma_plan_tile_tail_queue                src/dmma_tile_tail_queue.h:190
  *   dmma_plan_tile_early_split               src/dmma_tile_early_split.h:152
+ *   mmio_allinone (Matrix Market reader)     src/mmio_highlevel.h:593
  * The output is built into oracle/_ref/ and never shipped with the product.
  */
 #include <unistd.h>
@@ -25,6 +26,7 @@
 #include "dmma_tile_tail_queue.h"
 #include "dmma_tile_early_split.h"
 #include "spgemm_serialref_spa_new.h"
+#include "mmio_highlevel.h"
 
 namespace
 {
@@ -234,6 +236,14 @@ int ref_plan_tile_early_split(int ntasks, const int *scans, const int *matches,
     summary[9] = (long long)plan.partial_workspace_bytes;
     summary[10] = plan.exact_parent_partition ? 1 : 0;
     return (int)plan.reason;
+}
+
+/* mmio_allinone (src/mmio_highlevel.h:593-760): Matrix Market file -> CSR */
+int ref_mmio_allinone(const char *path, int *m, int *n, int *nnz, int *is_sym, int **rowptr,
+                      int **col, double **val)
+{
+    QuietStdout quiet;
+    return mmio_allinone(m, n, nnz, is_sym, rowptr, col, val, const_cast<char *>(path));
 }
 
 void ref_free(void *p) { free(p); }

@@ -1646,9 +1646,8 @@ int rtt_spgemm_update_b(rtt_context c, const rtt_csr_view *B, const int *row_new
         RTT_CHECK(c->bp_rowptr.ensure(sizeof(int) * ((size_t)B->rows + 1), s));
         RTT_CHECK(c->bp_col.ensure(sizeof(int) * (size_t)B->nnz + 16, s));
         RTT_CHECK(c->bp_val.ensure(sizeof(double) * (size_t)B->nnz + 16, s));
-        RTT_CHECK(map_device_error(csr_permute_device(ws, *B, row_new_to_old, nullptr,
-                                                      c->bp_rowptr.as<int>(), c->bp_col.as<int>(),
-                                                      c->bp_val.as<double>())));
+        RTT_CHECK(csr_permute_device(ws, *B, row_new_to_old, nullptr, c->bp_rowptr.as<int>(),
+                                     c->bp_col.as<int>(), c->bp_val.as<double>()));
         b.row_ptr = c->bp_rowptr.as<int>();
         b.col_idx = c->bp_col.as<int>();
         b.values = c->bp_val.as<double>();

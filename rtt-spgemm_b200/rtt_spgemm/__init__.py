@@ -34,6 +34,7 @@ from ._abi import (EXPORTS, LIB_PATH, RTT_OP_AAT, RTT_OP_AB, RTT_SUPER16_A8X4, R
 from .generators import CSR
 
 __all__ = ["CSR", "Context", "RttError", "build", "csr2tile_col_major", "csr2tile_row_major",
+           "mmio_read",
            "generators", "lib", "spgemm_csr_host", "spgemm_tile", "tile16_to_tile8", "tile2csr",
            "tile2csr_device_noalloc", "csr_to_hybrid_tiles", "super16_index", "plan_tail_queue",
            "plan_early_split", "early_split_policy_default",
@@ -117,6 +118,19 @@ def _tiles_in(t: dict):
 
 def _destroy(s: SMatrix, owned_csr: bool = False) -> None:
     lib().rtt_matrix_destroy(C.byref(s), int(owned_csr))
+
+
+def mmio_read(path, value_mode: int = 0) -> CSR:
+    """Replacement of mmio_allinone (reference src/mmio_highlevel.h:593): a
+    Matrix Market coordinate file as CSR, the reference's layout (entries in
+    file order, symmetric files expanded); value_mode 1 = the reference
+    benchmark's value overwrite i % 10.  Returns CSR with .is_symmetric."""
+    s = SMatrix()
+    check(lib().rtt_mmio_read(str(path).encode(), int(value_mode), C.byref(s)))
+    out = CSR(s.m, s.n, _adopt(s.rowpointer, s.m + 1, np.int32),
+              _adopt(s.columnindex, s.nnz, np.int32), _adopt(s.value, s.nnz, np.float64))
+    out.is_symmetric = bool(s.isSymmetric)
+    return out
 
 
 def csr2tile_row_major(csr) -> dict:

@@ -38,7 +38,7 @@ EXPORTS = [
     "rtt_reorder_plan_build", "rtt_reorder_plan_destroy", "rtt_csr_permute",
     "rtt_spgemm_numeric_values", "rtt_super16_index_build", "rtt_super16_index_destroy",
     "rtt_spgemm_batched_numeric_values", "rtt_spgemm_symbolic64", "rtt_spgemm_numeric64",
-    "rtt_spgemm_update_b",
+    "rtt_spgemm_update_b", "rtt_mmio_read",
 ]
 
 RTT_SUPER16_A8X4 = 1
@@ -218,6 +218,7 @@ def lib() -> C.CDLL:
     L.rtt_spgemm_symbolic.argtypes = [C.c_void_p, P(CsrView), P(CsrView), C.c_int,
                                       P(C.c_longlong), P(C.c_longlong)]
     L.rtt_spgemm_numeric.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.rtt_mmio_read.argtypes = [C.c_char_p, C.c_int, P(SMatrix)]
     L.rtt_spgemm_update_b.argtypes = [C.c_void_p, P(CsrView), C.c_void_p, P(C.c_longlong),
                                       P(C.c_longlong)]
     L.rtt_spgemm_symbolic64.argtypes = [C.c_void_p, P(CsrView), P(CsrView), C.c_int,
