@@ -47,6 +47,10 @@ constexpr int S2_PAIRS = TD / 2;         // row pairs of a tile row
 constexpr int S2_HEAVY_WARPS = 32;
 constexpr int HEAVY_PAIR = 1024;
 constexpr int S2_SLOTS = 254;            // C tiles per window (slot 255 = none)
+// The segment walk shares a tile row's entries over all warps of its CTA,
+// so it needs no warp per row pair: 4-warp CTAs, twice as many per SM, hide
+// the latency of the per-tile-row set-up phases better.
+constexpr int S2_SEG_WARPS = 4;
 constexpr int S2_STRIDE = 257;           // odd stride: the pairs' mask rows in distinct banks
 
 template <int NW>
@@ -307,14 +311,16 @@ __global__ void __launch_bounds__(S1_WIDE_WARPS * 32)
 // the tile rows in order (a heavy one is skipped when heavy[] marks it), or
 // S2_HEAVY_WARPS for the heavy rows of list[] (all warps share the walk).
 template <bool NARROW, int NW, bool SEGS>
-__global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
+__global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WARPS ? 10 : 1)
     k_sym_rows(DevTiles A, DevTiles B, const int *__restrict__ c_tile_ptr,
                int *__restrict__ c_tile_col, int *__restrict__ c_tile_row,
                uint16_t *__restrict__ c_mask, int *__restrict__ c_tile_cnt,
                int *__restrict__ c_row_cnt, int *__restrict__ c_tr_nnz, int *multi, int *err,
                const uint8_t *__restrict__ heavy, const int *__restrict__ list)
 {
-    static_assert(NW == S2_WARPS || NW == S2_HEAVY_WARPS, "CTA shapes");
+    static_assert(NW == S2_WARPS || NW == S2_HEAVY_WARPS || (SEGS && NW == S2_SEG_WARPS),
+                  "CTA shapes");
+    constexpr int PPW = (S2_PAIRS + NW - 1) / NW; // row pairs each warp counts
     constexpr int NT = NW * 32;
     __shared__ CtaSmem2<NW> S;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -327,7 +333,7 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
     const int r0 = warp * 2, r1 = r0 + 1; // warp-private walk (NW == S2_WARPS) and counts
     uint32_t *mw = S.mw + min(warp, S2_PAIRS - 1) * S2_STRIDE;
     int4 *ent = S.ent[warp];
-    int run0 = 0, run1 = 0; // entries of rows r0, r1 so far
+    int run[PPW][2] = {}; // entries so far of rows 2p, 2p + 1, pair p = warp + q * NW
 
     // tile-column range reachable from the tile row
     if (tid == 0)
@@ -731,18 +737,23 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
                 }
             }
         }
-        // per-row counts of the window (warp w counts rows 2w, 2w + 1)
-        if (warp < S2_PAIRS)
+        // per-row counts of the window (pair p: rows 2p, 2p + 1)
+#pragma unroll
+        for (int q = 0; q < PPW; ++q)
         {
-            int c0 = 0, c1 = 0;
-            for (int i = lane; i < nb; i += 32)
+            const int p = warp + q * NW;
+            if (p < S2_PAIRS)
             {
-                const uint32_t v = mw[i];
-                c0 += __popc(v & 0xFFFFu);
-                c1 += __popc(v >> 16);
+                int c0 = 0, c1 = 0;
+                for (int i = lane; i < nb; i += 32)
+                {
+                    const uint32_t v = S.mw[p * S2_STRIDE + i];
+                    c0 += __popc(v & 0xFFFFu);
+                    c1 += __popc(v >> 16);
+                }
+                run[q][0] += warp_sum(c0);
+                run[q][1] += warp_sum(c1);
             }
-            run0 += warp_sum(c0);
-            run1 += warp_sum(c1);
         }
         __syncthreads();
         // ---- outputs of the window: masks (a row pair per 32-bit word: row
@@ -771,20 +782,28 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : 1)
             set_error(err, DERR_SYM_OVERFLOW);
         return;
     }
+    int mine = 0;
     if (lane == 0)
-    {
-        if (r0 < nrows)
-            c_row_cnt[I * TD + r0] = run0;
-        if (r1 < nrows)
-            c_row_cnt[I * TD + r1] = run1;
-    }
+#pragma unroll
+        for (int q = 0; q < PPW; ++q)
+        {
+            const int p = warp + q * NW;
+            if (p < S2_PAIRS)
+            {
+                if (2 * p < nrows)
+                    c_row_cnt[I * TD + 2 * p] = run[q][0];
+                if (2 * p + 1 < nrows)
+                    c_row_cnt[I * TD + 2 * p + 1] = run[q][1];
+                mine += run[q][0] + run[q][1];
+            }
+        }
     // tile row total
     __shared__ int tot;
     if (tid == 0)
         tot = 0;
     __syncthreads();
-    if (lane == 0 && warp < S2_PAIRS)
-        atomicAdd(&tot, run0 + run1);
+    if (lane == 0 && mine)
+        atomicAdd(&tot, mine);
     __syncthreads();
     if (tid == 0)
     {
@@ -882,10 +901,14 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
             RTT_CUDA(cudaEventRecord(ws.join_ev, ws.side));
             ws.launches++;
         }
-        auto kern = segs ? k_sym_rows<false, S2_WARPS, true>
-                         : b_sorted && sym_multi ? k_sym_rows<true, S2_WARPS, false>
-                                                 : k_sym_rows<false, S2_WARPS, false>;
-        kern<<<tilem, S2_THREADS, 0, s>>>(
+        // 4-warp CTAs when every tile row fits one window; a tile row with
+        // several windows walks its entries once per window, so it keeps 8
+        const bool small = segs && !sym_multi;
+        auto kern = small ? k_sym_rows<false, S2_SEG_WARPS, true>
+                          : segs ? k_sym_rows<false, S2_WARPS, true>
+                                 : b_sorted && sym_multi ? k_sym_rows<true, S2_WARPS, false>
+                                                         : k_sym_rows<false, S2_WARPS, false>;
+        kern<<<tilem, small ? S2_SEG_WARPS * 32 : S2_THREADS, 0, s>>>(
             A, B, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(), S.c_tile_row.as<int>(),
             S.c_mask.as<uint16_t>(), S.tile_cnt.as<int>(), S.c_row_cnt.as<int>(),
             S.c_tr_nnz.as<int>(), S.w_flag.as<int>() + 1, ws.err.as<int>(),

@@ -23,7 +23,7 @@ def _write_symmetric(path, A):
         f.write("%%MatrixMarket matrix coordinate real symmetric\n")
         f.write(f"{A.m} {A.n} {int(keep.sum())}\n")
         for i, j, v in zip(rows[keep], A.col[keep], A.val[keep]):
-            f.write(f"{i + 1} {j + 1} {v!r}\n")
+            f.write(f"{i + 1} {j + 1} {float(v)!r}\n")
 
 
 @pytest.mark.parametrize("value_mode", [0, 1])
