@@ -528,13 +528,23 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WAR
                 const int nsh = lng ? 0 : ns;
                 const int off = nsh > 0 ? lane % nsh : 0;
                 const int steps = __reduce_max_sync(FULL, (unsigned)nsh);
-                for (int i = 0; i < steps; ++i)
-                    if (i < nsh)
+                // four segments' loads in flight before their marks
+                constexpr int U = 4;
+                for (int i = 0; i < steps; i += U)
+                {
+                    unsigned long long sg[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
                     {
-                        int x = off + i;
+                        int x = off + i + u;
                         x -= x >= nsh ? nsh : 0;
-                        mark(__ldg(B.seg + s0 + x), r);
+                        sg[u] = i + u < nsh ? __ldg(B.seg + s0 + x) : 0ull;
                     }
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+                        if (i + u < nsh)
+                            mark(sg[u], r);
+                }
                 for (unsigned lm = __ballot_sync(FULL, lng); lm != 0u; lm &= lm - 1u)
                 {
                     const int j = __ffs(lm) - 1;

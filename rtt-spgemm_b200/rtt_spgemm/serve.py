@@ -301,7 +301,7 @@ class Server:
         if rest:
             self._run_batch_plain(ctx, stream, rest, t0)
 
-    def _run_batch_plain(self, ctx, stream, batch, t0):
+    def _run_batch_plain(self, ctx, stream, batch, t0, retry: bool = True):
         try:
             As, Bs = [], []
             for r in batch:
@@ -310,7 +310,15 @@ class Server:
                 Bs.append(b)
             outs = spgemm_batched(ctx, As, Bs)
             stream.synchronize()
-        except RttError as e:
+        except (RttError, RuntimeError) as e:
+            # device memory short: torch's cache may hold what the library
+            # needs (two allocators share the device); hand it back, once
+            oom = (isinstance(e, RttError) and e.status == 4) or "out of memory" in str(e)
+            if oom and retry:
+                del As, Bs
+                self.torch.cuda.empty_cache()
+                self._run_batch_plain(ctx, stream, batch, t0, retry=False)
+                return
             if len(batch) > 1:  # find the failing request(s): one at a time
                 for r in batch:
                     self._run_batch_plain(ctx, stream, [r], t0)
@@ -334,6 +342,10 @@ class Server:
                 r.error, r.done = str(e), r.arrival
                 continue
             r.bound = 12 * r.entries + 4 * (r.a.m + 1) + 12 * r.a.nnz + 4 * (r.a.m + 1)
+            if r.bound > self.pool:  # can never be admitted: finished on arrival
+                r.error = (f"the product's memory bound ({r.bound / 1e9:.1f} GB) exceeds the "
+                           f"device pool ({self.pool / 1e9:.1f} GB)")
+                r.done = r.arrival
         pending = deque()
         nxt = 0
         reserved = [0.0]
@@ -381,7 +393,13 @@ class Server:
                                 wait = max(0.0, requests[nxt].arrival - (time.perf_counter() - t0))
                             cv.wait(timeout=min(wait, 0.01) if wait > 0 else 0.0005)
                             batch, need = take_batch()
-                    self._run_batch(ctx, stream, batch, t0)
+                    try:
+                        self._run_batch(ctx, stream, batch, t0)
+                    except Exception as e:  # any failure finishes the batch's requests
+                        now = time.perf_counter() - t0
+                        for r in batch:
+                            if r.done < 0:
+                                r.error, r.done = f"{type(e).__name__}: {e}", now
                     with cv:
                         reserved[0] -= need
                         done[0] += len(batch)
@@ -441,10 +459,20 @@ def serve_plain(requests: list[Request], device: int = 0, config: dict | None = 
 
 
 def summarize(requests, span: float) -> dict:
-    lat = np.array([r.done - r.arrival for r in requests]) * 1e3
+    """Throughput over all requests; latency percentiles over the requests
+    that produced a result."""
+    ok = [r for r in requests if r.error is None and r.done >= 0]
+    lat = np.array([r.done - r.arrival for r in ok]) * 1e3
+    errors = {}
+    for r in requests:
+        if r.error is not None:
+            k = r.error.split(":")[0][:60]
+            errors[k] = errors.get(k, 0) + 1
     return {"requests": len(requests), "seconds": span,
             "failed": sum(r.error is not None for r in requests),
-            "spgemms_per_s": len(requests) / span if span > 0 else 0.0,
+            "errors": errors,
+            "completed": len(ok),
+            "spgemms_per_s": len(ok) / span if span > 0 else 0.0,
             "p50_ms": float(np.percentile(lat, 50)) if lat.size else 0.0,
             "p99_ms": float(np.percentile(lat, 99)) if lat.size else 0.0}
 
