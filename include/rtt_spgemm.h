@@ -445,8 +445,14 @@ typedef struct
      * chunk_nnz entries (0 = INT32_MAX) is halved. */
     int chunk_tiles;
     int chunk_nnz;
+    /* Numeric step from B's row segments (the default, 0 = on): where every
+     * tile row fits one window, B has no repeated columns and no B row has
+     * more than 16 segments, a half-warp walks a row's A entries and its
+     * lanes take the segments of each entry's B row.  1 = always the
+     * entry-per-lane walk.  Both give bitwise the same C. */
+    int no_segment_walk;
     /* Reserved, must be zero. */
-    int reserved[2];
+    int reserved[1];
 } rtt_config;
 
 RTT_API void rtt_config_default(rtt_config *config);
@@ -592,6 +598,23 @@ RTT_API int rtt_csr_transpose(rtt_context ctx, const rtt_csr_view *A, int *t_row
  * rtt_spgemm_symbolic). */
 RTT_API int rtt_reorder_plan_build(rtt_context ctx, const rtt_csr_view *A, rtt_reorder_plan *plan);
 RTT_API void rtt_reorder_plan_destroy(rtt_reorder_plan *plan);
+
+/* Replaces dump_dmma_reorder_plan (src/dmma_reorder.h:3087-3209): writes
+ * <stem>_permutations.csv (axis,old_id,new_id,new_to_old_at_new_id for every
+ * row and inner index), <stem>_unified_stats.csv (key,value: the plan's
+ * counters) and, when dump_matrix != 0, <stem>_A_reordered.mtx (A's pattern
+ * under the plan, from A's device row pointer and columns). */
+RTT_API int rtt_reorder_plan_dump(const rtt_reorder_plan *plan, const char *stem,
+                                  const int *d_row_ptr, const int *d_col_idx, int dump_matrix);
+
+/* Tile-layout heatmap (the role of export_diagnostic_heatmaps,
+ * src/super16_symbolic.cuh:2034, for this build's 16x16 tiles): the tiles of
+ * A (which = 0), B (1) or C (2) of the last symbolic phase on ctx, counted on
+ * a bins x bins grid over the tile grid (tile (I, J) -> bin (I * bins /
+ * tilem, J * bins / tilen)); hist is a host array of bins * bins counts, row
+ * major.  1 <= bins <= 4096.  After rtt_spgemm_symbolic64, C is the last
+ * chunk's. */
+RTT_API int rtt_tile_heatmap(rtt_context ctx, int which, int bins, unsigned long long *hist);
 
 /* Device CSR permutation: out row i = A row row_new_to_old[i] (NULL: i), each
  * column c replaced by col_old_to_new[c] (NULL: c) and every row sorted by

@@ -51,6 +51,7 @@ struct rtt_context_s
     rtt::TileBufs A, B;
     rtt::DevBuf bt_rowptr, bt_col, bt_val; // B = A^T for RTT_OP_AAT
     rtt::DevBuf bp_rowptr, bp_col, bp_val; // B with permuted rows (rtt_spgemm_update_b)
+    rtt::DevBuf diag_hist;                 // rtt_tile_heatmap
     rtt::DevBuf in_rp, in_col, in_val;     // host-buffer uploads
     rtt::DevBuf in2_rp, in2_col, in2_val;
     rtt::DevBuf out_rp, out_col, out_val;  // host-buffer product output
@@ -115,7 +116,7 @@ std::vector<DevBuf *> own_buffers(rtt_context c)
             &c->bat_a_col, &c->bat_a_val, &c->bat_b_rp,   &c->bat_b_col, &c->bat_b_val,
             &c->bat_meta,  &c->bat_big_rp, &c->bat_nnz,  &c->vflags,    &c->bat_vtab,
             &c->w_cnt,     &c->w_rowcnt,  &c->w_rowptr,   &c->w_local,   &c->bp_rowptr,
-            &c->bp_col,    &c->bp_val};
+            &c->bp_col,    &c->bp_val,    &c->diag_hist};
 }
 
 std::mutex g_mutex;
@@ -765,6 +766,7 @@ int numeric_enqueue(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_val
     dB.csr_val = c->b_va;
     dB.nnz = (int)c->b_nnz;
     nc.conflict_safe = c->b_dups;
+    nc.segment_walk = c->cfg.no_segment_walk == 0;
     // the numeric step reads A's entries from its CSR rows
     DevTiles dA = c->A.view();
     dA.csr_rowptr = c->a_rp;
@@ -1033,8 +1035,10 @@ int rtt_context_set_config(rtt_context c, const rtt_config *config)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "NULL argument");
     if (config->dmma_pair_cutoff < 0)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "dmma_pair_cutoff must be >= 0");
-    if (config->chunk_tiles < 0 || config->chunk_nnz < 0)
-        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "chunk_tiles and chunk_nnz must be >= 0");
+    if (config->chunk_tiles < 0 || config->chunk_nnz < 0 || config->no_segment_walk < 0 ||
+        config->no_segment_walk > 1)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT,
+                         "chunk_tiles, chunk_nnz >= 0 and no_segment_walk 0 or 1 expected");
     for (int r : config->reserved)
         if (r != 0)
             return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "reserved config fields must be zero");
@@ -1685,6 +1689,41 @@ int rtt_spgemm_update_b(rtt_context c, const rtt_csr_view *B, const int *row_new
     return RTT_OK;
 }
 
+int rtt_tile_heatmap(rtt_context c, int which, int bins, unsigned long long *hist)
+{
+    if (c == nullptr || hist == nullptr || bins < 1 || bins > 4096 || which < 0 || which > 2)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "tile_heatmap: bad arguments");
+    if (!c->have_symbolic && !c->have_sym64)
+        return rtt::fail(RTT_ERR_STATE, "tile_heatmap needs a symbolic phase first");
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    Workspace &ws = c->ws;
+    const TileBufs &TB = c->b_alias ? c->A : c->B;
+    int tilem = 0, tilen = 0;
+    const int *tp = nullptr, *tc = nullptr;
+    if (which == 2)
+    {
+        tilem = c->S.tilem;
+        tilen = c->S.tilen;
+        tp = c->S.c_tile_ptr.as<int>();
+        tc = c->S.c_tile_col.as<int>();
+    }
+    else
+    {
+        const TileBufs &T = which == 0 ? c->A : TB;
+        tilem = T.tilem;
+        tilen = T.tilen;
+        tp = T.tile_ptr.as<int>();
+        tc = T.tile_col.as<int>();
+    }
+    const size_t cells = (size_t)bins * bins;
+    RTT_CHECK(c->diag_hist.ensure(sizeof(unsigned long long) * cells, ws.stream));
+    RTT_CHECK(tile_heatmap_device(ws, tilem, tilen, tp, tc, bins,
+                                  c->diag_hist.as<unsigned long long>()));
+    RTT_CUDA(cudaMemcpyAsync(hist, c->diag_hist.p, sizeof(unsigned long long) * cells,
+                             cudaMemcpyDeviceToHost, ws.stream));
+    return check_device_error(ws, "tile_heatmap");
+}
+
 int rtt_spgemm_numeric_values(rtt_context c, const double *a_values, const double *b_values,
                               int *c_row_ptr, int *c_col_idx, double *c_values)
 {
@@ -1924,6 +1963,7 @@ int rtt_spgemm_numeric64(rtt_context c, long long *c_row_ptr, int *c_col_idx, do
         nc.split_target = c->cfg.split_target;
         nc.write_tiles = false;
         nc.conflict_safe = c->b_dups;
+        nc.segment_walk = c->cfg.no_segment_walk == 0;
         nc.csr_rowptr = c->w_local.as<int>();
         nc.csr_col = c_col_idx + c->w_base[k];
         nc.csr_val = c_values + c->w_base[k];
@@ -1981,7 +2021,8 @@ int assemble(rtt_context c, int count, const rtt_csr_view *V, const std::vector<
     // device copy of the tables: pointers first (8-byte aligned), then ints
     // (grow-only scratch: no cudaFree, which would wait for every stream)
     DevBuf &tabd = ws.tmp[0];
-    const size_t ints = (size_t)count * 4 + 2;
+    // rows, row_off (count + 1), col_add, nnz_off (count + 1), cols
+    const size_t ints = (size_t)count * 5 + 2;
     RTT_CHECK(tabd.ensure(sizeof(void *) * tab.size() + sizeof(int) * ints, s));
     char *base = tabd.as<char>();
     int *d_rows = reinterpret_cast<int *>(base + sizeof(void *) * tab.size());

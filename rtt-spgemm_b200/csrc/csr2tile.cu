@@ -294,8 +294,15 @@ __global__ void __launch_bounds__(256)
                 seg[out + n] = seg_pack(T, mk);
             ++n;
         }
-        if (!FILL && r < m)
-            seg_cnt[r] = n;
+        if (!FILL)
+        {
+            if (r < m)
+                seg_cnt[r] = n;
+            // seg_cnt[m]: the most segments of a row
+            const unsigned wmax = __reduce_max_sync(FULL, r < m ? (unsigned)n : 0u);
+            if (lane == 0 && wmax > 0)
+                atomicMax(seg_cnt + m, (int)wmax);
+        }
         return;
     }
     const int rows = min(32, m - r0);
@@ -330,7 +337,10 @@ __global__ void __launch_bounds__(256)
             n += __popc(st);
         }
         if (!FILL && lane == 0)
+        {
             seg_cnt[r0 + q] = n;
+            atomicMax(seg_cnt + m, n);
+        }
     }
 }
 
@@ -1082,6 +1092,7 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
         // row segments: count per row, scan, fill
         RTT_CHECK(out.seg_cnt.ensure(sizeof(int) * ((size_t)m + 1), s));
         RTT_CHECK(out.seg_ptr.ensure(sizeof(int) * ((size_t)m + 1), s));
+        RTT_CUDA(cudaMemsetAsync(out.seg_cnt.as<int>() + m, 0, sizeof(int), s));
         const int grid = grid_for((long long)ceil_div(m, 32) * 32, 256);
         k_row_segments<false><<<grid, 256, 0, s>>>(m, rowptr, col, out.seg_cnt.as<int>(), nullptr,
                                                    nullptr);
@@ -1134,7 +1145,11 @@ int csr2tile_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, con
         ws.launches++;
         RTT_CHECK(scan_exclusive_int(ws, cnt, out.tile_ptr.as<int>(), tilem));
         int numtile = 0;
+        // the most segments of a row comes back with the tile count (one sync)
+        RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 2, out.seg_cnt.as<int>() + m, sizeof(int),
+                                 cudaMemcpyDeviceToHost, s));
         RTT_CHECK(read_int(ws, out.tile_ptr.as<int>() + tilem, &numtile));
+        out.max_row_segs = ws.h_scalars[2];
         out.numtile = numtile;
         RTT_CHECK(out.tile_col.ensure(sizeof(int) * (size_t)numtile + 16, s));
         RTT_CHECK(out.tile_row.ensure(sizeof(int) * (size_t)numtile + 16, s));

@@ -362,6 +362,76 @@ __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Windo
     return n_fma;
 }
 
+// The warp's products from B's row segments (one window, B rows of at most
+// 16 segments, no repeated columns): half-warp h walks the A entries of its
+// row (r0 or r1) one by one, in column order, and its lanes take the
+// segments of that entry's B row - lane l the l-th segment, its tile column
+// J and 16-bit mask.  A lane finds the segment's C tile slot and the row's
+// (base, mask) word once, then adds the segment's entries (the mask's set
+// bits, in column order; their values are consecutive in B's row, from the
+// offset a half-warp scan of the masks' popcounts gives) into the row's
+// accumulator.  The lanes of one half hit distinct columns of one row, the
+// halves distinct rows; every output entry is still summed in the order of
+// its row's A entries, as in warp_products.
+template <int ACC>
+__device__ __forceinline__ long long warp_products_seg(FlatSmem<ACC> &S, const Window &W,
+                                                       const DevTiles &A, const DevTiles &B,
+                                                       int r0, int r1, int e_a, int e_m,
+                                                       int e_e, bool count)
+{
+    const int lane = lane_id(), h = lane >> 4, hl = lane & 15;
+    const int rh = h ? r1 : r0;
+    const uint32_t *cmr = S.cm + rh * F_CM_STRIDE;
+    int e = h ? e_m : e_a;
+    const int eend = h ? e_e : e_m;
+    const int steps = max(e_m - e_a, e_e - e_m);
+    long long n_fma = 0;
+    for (int st = 0; st < steps; ++st, ++e)
+    {
+        int k = -1, s0 = 0, ns = 0, fs = 0;
+        double a = 0.0;
+        if (e < eend)
+        {
+            k = __ldg(A.csr_col + e);
+            a = __ldg(A.csr_val + e);
+            if (k < B.m)
+            {
+                s0 = __ldg(B.seg_ptr + k);
+                ns = min(__ldg(B.seg_ptr + k + 1) - s0, 16);
+                fs = __ldg(B.csr_rowptr + k);
+            }
+        }
+        unsigned long long sg = 0ull;
+        if (hl < ns)
+            sg = __ldg(B.seg + s0 + hl);
+        const int pc = __popc((unsigned)sg & 0xFFFFu);
+        const int incl = half_incl_scan(pc);
+        if (count)
+            n_fma += pc;
+        if (hl < ns)
+        {
+            const int J = (int)(sg >> 16);
+            const int slot = S.slot8[min((unsigned)(J - W.Jlo), (unsigned)(F_SPAN_CAP - 1))];
+            const uint32_t w = cmr[slot];
+            const int base = (int)(w >> 16);
+            const uint32_t cmask = w & 0xFFFFu;
+            int eo = min(max(fs + incl - pc, 0), B.nnz - 1);
+            uint32_t bm = (uint32_t)sg & 0xFFFFu;
+            while (bm)
+            {
+                const int c = __clz(bm) - 16; // column in the tile, left to right
+                bm &= ~(0x8000u >> c);
+                const double b = __ldg(B.csr_val + eo);
+                eo = min(eo + 1, B.nnz - 1);
+                const int pos = min(base + __popc(cmask >> (16 - c)), ACC - 1);
+                S.acc[pos] = fma(a, b, S.acc[pos]);
+                S.ccol[pos] = J * TD + c;
+            }
+        }
+    }
+    return n_fma;
+}
+
 // ---------------------------------------------------------------------------
 // Split execution of heavy tile rows (the early split of the reference's
 // numeric step, src/dmma_tile_early_split.h:152-229, applied to C tile rows).
@@ -592,7 +662,7 @@ __global__ void __launch_bounds__(PLAN_WARPS * 32)
 // several windows, so long sorted B rows are cut to each window's columns
 // (compiled out when every tile row fits one window: the registers are the
 // kernel's limit).
-template <bool SAFE, int ACC, int MIN_CTAS, bool WORKER, bool NARROW, bool ACSR>
+template <bool SAFE, int ACC, int MIN_CTAS, bool WORKER, bool NARROW, bool ACSR, bool SEGW = false>
 __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
     k_numeric_flat(DevTiles A, DevTiles B, int tilem, long long nnzC,
                    const int *__restrict__ c_tile_ptr, const int *__restrict__ c_tile_col,
@@ -808,7 +878,9 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
                     if (!ACSR)
                         ebase = __ldg(A.tile_nnz + a0);
                 }
-                if (W.table && nW == cs1 - cs0)
+                if (SEGW && W.table && nW == cs1 - cs0)
+                    n_fma += warp_products_seg<ACC>(S, W, A, B, r0, r1, e_a, e_m, e_e, count);
+                else if (W.table && nW == cs1 - cs0)
                     n_fma += warp_products<SAFE, false, ACC, NARROW, ACSR>(
                         S, W, A, B, a0, a1, r0, r1, e_a, e_m, e_e, count, ent, enta, cur, ebase,
                         w0 == wbeg);
@@ -990,6 +1062,11 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
                                       : k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, false, false, false>)
                     : (S.multi_window ? k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, true, false>
                                       : k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, false, false>));
+    // B rows of at most 16 segments, one window per tile row, no repeated
+    // columns: the segment walk
+    if (cfg.segment_walk && acsr && !cfg.conflict_safe && !S.multi_window && B.seg_ptr != nullptr &&
+        B.seg != nullptr && B.max_row_segs > 0 && B.max_row_segs <= 16)
+        light = k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, false, true, true>;
     RTT_CHECK(launch(light, S.tilem, s, smem, nullptr));
     if (split)
         RTT_CUDA(cudaStreamWaitEvent(s, ws.join_ev, 0));

@@ -66,6 +66,7 @@ struct DevTiles
     // of every 16-bit tile row mask, listed per scalar row
     const int *seg_ptr;               // m + 1
     const unsigned long long *seg;    // seg_ptr[m]
+    int max_row_segs;                 // most segments of one row (when seg_ptr is set)
 };
 
 // C tile structure produced by the symbolic phase.
@@ -245,6 +246,7 @@ struct TileBufs
     DevBuf seg_ptr, seg, seg_cnt; // row segments (csr2tile_device with segments = true)
     int m = 0, n = 0, tilem = 0, tilen = 0, numtile = 0, nnz = 0;
     bool has_segments = false;
+    int max_row_segs = 0; // most segments of one row (structure-only builds; else 0 = unknown)
     bool payload = true;  // per-entry arrays (tile_nnz, ptr, col, val, mask) built
     bool dup_cols = false; // some row may repeat a column (set by csr2tile_device)
     bool generic = false;  // built by the generic (unsorted tile columns) path
@@ -349,6 +351,9 @@ struct SymbolicOut
 // step 1 only: C tiles per tile row of A * B into cnt (A.tilem ints)
 int symbolic_tile_counts(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
                          int *cnt);
+// tile counts of a tile grid on a bins x bins histogram (device, cleared first)
+int tile_heatmap_device(Workspace &ws, int tilem, int tilen, const int *tile_ptr,
+                        const int *tile_col, int bins, unsigned long long *d_hist);
 // tile rows [I0, I1) of a device tile matrix with its CSR rows (the 64-bit
 // products run A in such slices; B stays whole)
 DevTiles tile_row_slice(const DevTiles &A, int I0, int I1);
@@ -371,6 +376,7 @@ struct NumericConfig
     cudaEvent_t ev_begin = nullptr; // recorded around the numeric kernel when set
     cudaEvent_t ev_end = nullptr;
     bool conflict_safe = false;     // B rows may repeat a column: accumulate with shared atomics
+    bool segment_walk = true;       // the numeric step may walk B's row segments
 };
 
 // CSR row pointer of C (m + 1 ints) from the symbolic counts

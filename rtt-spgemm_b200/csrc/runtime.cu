@@ -310,6 +310,7 @@ DevTiles TileBufs::view() const
     t.csr_val = nullptr;
     t.seg_ptr = has_segments ? seg_ptr.as<int>() : nullptr;
     t.seg = has_segments ? seg.as<unsigned long long>() : nullptr;
+    t.max_row_segs = has_segments ? max_row_segs : 0;
     return t;
 }
 

@@ -499,6 +499,34 @@ class Context:
                                                       C.c_void_p(col.data_ptr()),
                                                       C.c_void_p(val.data_ptr())))
 
+    def tile_heatmap(self, which: str = "C", bins: int = 64) -> np.ndarray:
+        """rtt_tile_heatmap: tile counts of A, B or C of the last symbolic
+        phase on a bins x bins grid."""
+        h = np.zeros(bins * bins, dtype=np.uint64)
+        check(lib().rtt_tile_heatmap(self.handle, {"A": 0, "B": 1, "C": 2}[which], int(bins),
+                                     h.ctypes.data_as(C.POINTER(C.c_ulonglong))))
+        return h.reshape(bins, bins)
+
+    def reorder_plan_dump(self, a, stem: str, dump_matrix: bool = True) -> dict:
+        """Build A's reorder plan and write it as the reference's dump does
+        (rtt_reorder_plan_dump: <stem>_permutations.csv, _unified_stats.csv,
+        _A_reordered.mtx).  Returns the plan."""
+        v = self._view(*a)
+        p = ReorderPlan()
+        check(lib().rtt_reorder_plan_build(self.handle, C.byref(v), C.byref(p)))
+        try:
+            check(lib().rtt_reorder_plan_dump(C.byref(p), str(stem).encode(),
+                                              C.c_void_p(a[2].data_ptr()),
+                                              C.c_void_p(a[3].data_ptr()), int(dump_matrix)))
+            out = {k: getattr(p, k) for k, t in ReorderPlan._fields_
+                   if t is not C.POINTER(C.c_int)}
+            for k, n in (("row_old_to_new", p.rows), ("inner_old_to_new", p.cols)):
+                out[k] = np.ctypeslib.as_array(getattr(p, k), shape=(n,)).copy() if n else \
+                    np.zeros(0, np.int32)
+        finally:
+            lib().rtt_reorder_plan_destroy(C.byref(p))
+        return out
+
     def reorder_plan(self, a) -> dict:
         """Row / inner reorder plan of a device CSR tuple (rtt_reorder_plan_build,
         the reference's build_dmma_reorder_plan): counters and numpy maps."""

@@ -38,7 +38,7 @@ EXPORTS = [
     "rtt_reorder_plan_build", "rtt_reorder_plan_destroy", "rtt_csr_permute",
     "rtt_spgemm_numeric_values", "rtt_super16_index_build", "rtt_super16_index_destroy",
     "rtt_spgemm_batched_numeric_values", "rtt_spgemm_symbolic64", "rtt_spgemm_numeric64",
-    "rtt_spgemm_update_b", "rtt_mmio_read",
+    "rtt_spgemm_update_b", "rtt_mmio_read", "rtt_reorder_plan_dump", "rtt_tile_heatmap",
 ]
 
 RTT_SUPER16_A8X4 = 1
@@ -78,7 +78,7 @@ class Config(C.Structure):
                 ("keep_tiles", C.c_int), ("stage_timing", C.c_int), ("b_staging", C.c_int),
                 ("split_target", C.c_int), ("cuda_graphs", C.c_int),
                 ("chunk_tiles", C.c_int), ("chunk_nnz", C.c_int),
-                ("reserved", C.c_int * 2)]
+                ("no_segment_walk", C.c_int), ("reserved", C.c_int * 1)]
 
 
 class HybridTiles(C.Structure):
@@ -219,6 +219,9 @@ def lib() -> C.CDLL:
                                       P(C.c_longlong), P(C.c_longlong)]
     L.rtt_spgemm_numeric.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.rtt_mmio_read.argtypes = [C.c_char_p, C.c_int, P(SMatrix)]
+    L.rtt_reorder_plan_dump.argtypes = [P(ReorderPlan), C.c_char_p, C.c_void_p, C.c_void_p,
+                                        C.c_int]
+    L.rtt_tile_heatmap.argtypes = [C.c_void_p, C.c_int, C.c_int, P(C.c_ulonglong)]
     L.rtt_spgemm_update_b.argtypes = [C.c_void_p, P(CsrView), C.c_void_p, P(C.c_longlong),
                                       P(C.c_longlong)]
     L.rtt_spgemm_symbolic64.argtypes = [C.c_void_p, P(CsrView), P(CsrView), C.c_int,

@@ -61,6 +61,8 @@ class Request:
     error: str = None         # set instead of result when the product failed
     bound: int = field(default=0, repr=False)
     entries: int = field(default=0, repr=False)
+    exclusive: bool = field(default=False, repr=False)  # runs alone, nothing else in flight
+    uses: int = field(default=-1, repr=False)  # requests with its key before it (-1: not yet counted)
 
 
 def product_cub(a: CSR, op: str) -> int:
@@ -83,6 +85,10 @@ def product_cub(a: CSR, op: str) -> int:
 def product_bound(a: CSR, op: str) -> int:
     """Upper bound of C's bytes from the structure alone: nnz(C) <= nnzCub."""
     return 12 * product_cub(a, op) + 4 * (a.m + 1)
+
+
+class _OutOfMemory(Exception):
+    """A batch ran out of device memory while other work was in flight."""
 
 
 @dataclass
@@ -193,9 +199,12 @@ class Server:
         """Requests with r's reuse key before r (and count r)."""
         if r.key is None:
             return 0
+        if r.uses >= 0:  # a request queued again counts once
+            return r.uses
         with self.lock:
             n = self.uses.get(r.key, 0)
             self.uses[r.key] = n + 1
+        r.uses = n
         return n
 
     def _structure(self, r: Request):
@@ -301,7 +310,7 @@ class Server:
         if rest:
             self._run_batch_plain(ctx, stream, rest, t0)
 
-    def _run_batch_plain(self, ctx, stream, batch, t0, retry: bool = True):
+    def _run_batch_plain(self, ctx, stream, batch, t0):
         try:
             As, Bs = [], []
             for r in batch:
@@ -311,14 +320,11 @@ class Server:
             outs = spgemm_batched(ctx, As, Bs)
             stream.synchronize()
         except (RttError, RuntimeError) as e:
-            # device memory short: torch's cache may hold what the library
-            # needs (two allocators share the device); hand it back, once
+            # device memory short while other work is in flight: the worker
+            # queues the requests again, to run alone (see run())
             oom = (isinstance(e, RttError) and e.status == 4) or "out of memory" in str(e)
-            if oom and retry:
-                del As, Bs
-                self.torch.cuda.empty_cache()
-                self._run_batch_plain(ctx, stream, batch, t0, retry=False)
-                return
+            if oom and not all(r.exclusive for r in batch):
+                raise _OutOfMemory() from e
             if len(batch) > 1:  # find the failing request(s): one at a time
                 for r in batch:
                     self._run_batch_plain(ctx, stream, [r], t0)
@@ -342,10 +348,6 @@ class Server:
                 r.error, r.done = str(e), r.arrival
                 continue
             r.bound = 12 * r.entries + 4 * (r.a.m + 1) + 12 * r.a.nnz + 4 * (r.a.m + 1)
-            if r.bound > self.pool:  # can never be admitted: finished on arrival
-                r.error = (f"the product's memory bound ({r.bound / 1e9:.1f} GB) exceeds the "
-                           f"device pool ({self.pool / 1e9:.1f} GB)")
-                r.done = r.arrival
         pending = deque()
         nxt = 0
         reserved = [0.0]
@@ -363,8 +365,18 @@ class Server:
                     pending.append(requests[nxt])
                 nxt += 1
             batch, need, entries = [], 0.0, 0
+            if pending and pending[0].exclusive:
+                # a request that ran out of memory beside other work runs
+                # alone once everything else has finished
+                if reserved[0] > 0:
+                    return [], 0.0
+                batch = [pending.popleft()]
+                reserved[0] += self.pool
+                return batch, self.pool
             while pending and len(batch) < self.max_batch:
                 r = pending[0]
+                if r.exclusive:
+                    break
                 if batch and reserved[0] + need + r.bound > self.pool:
                     break
                 if batch and entries + r.entries > INT32_MAX:
@@ -393,14 +405,24 @@ class Server:
                                 wait = max(0.0, requests[nxt].arrival - (time.perf_counter() - t0))
                             cv.wait(timeout=min(wait, 0.01) if wait > 0 else 0.0005)
                             batch, need = take_batch()
+                    retry = []
                     try:
+                        if batch[0].exclusive:
+                            torch.cuda.empty_cache()  # what torch caches, back to the device
                         self._run_batch(ctx, stream, batch, t0)
-                    except Exception as e:  # any failure finishes the batch's requests
+                    except _OutOfMemory:
+                        retry = [r for r in batch if r.done < 0]
+                        for r in retry:
+                            r.exclusive = True
+                    except Exception as e:  # any other failure finishes the batch's requests
                         now = time.perf_counter() - t0
                         for r in batch:
                             if r.done < 0:
                                 r.error, r.done = f"{type(e).__name__}: {e}", now
                     with cv:
+                        for r in reversed(retry):
+                            pending.appendleft(r)
+                        done[0] -= len(retry)
                         reserved[0] -= need
                         done[0] += len(batch)
                         cv.notify_all()

@@ -203,3 +203,29 @@ def test_kat_2d_laplacian_closed_form():
              np.where(dx + dy == 1, -8.0,
              np.where((dx == 1) & (dy == 1), 2.0, 1.0)))
     assert np.array_equal(C.val, expect)
+
+
+SEGWALK_CASES = {
+    "stencil27_12": lambda: G.stencil_27(12, 3),
+    "lap2d_256": lambda: G.laplacian_2d(256),
+    "banded": lambda: G.banded_scatter(3000, 12, seed=9),
+    "ragged": lambda: G.laplacian_2d(37, 11),
+    "rect": lambda: G.random_csr(300, 300, 0.02, seed=8),
+}
+
+
+@pytest.mark.parametrize("case", list(SEGWALK_CASES))
+def test_segment_walk_equals_entry_walk(case, orc):
+    """The numeric step over B's row segments (default, where it applies)
+    and the entry-per-lane walk sum every output in the same order: bitwise
+    the same C, and the oracle's within the bound."""
+    A = SEGWALK_CASES[case]()
+    got = {}
+    for off in (0, 1):
+        ctx = R.Context(0, dict(no_segment_walk=off))
+        rp, ci, va, nnz, _ = _run(ctx, A)
+        got[off] = (rp, ci, va)
+        ctx.close()
+    assert np.array_equal(got[0][0], got[1][0]) and np.array_equal(got[0][1], got[1][1])
+    assert np.array_equal(got[0][2].view(np.int64), got[1][2].view(np.int64))
+    assert_csr_close(*got[0], *orc.spgemm_csr(A, A), f"{case} segment walk: ")
