@@ -445,12 +445,15 @@ typedef struct
      * chunk_nnz entries (0 = INT32_MAX) is halved. */
     int chunk_tiles;
     int chunk_nnz;
-    /* Numeric step from B's row segments (the default, 0 = on): where every
-     * tile row fits one window, B has no repeated columns and no B row has
-     * more than 16 segments, a half-warp walks a row's A entries and its
-     * lanes take the segments of each entry's B row.  1 = always the
-     * entry-per-lane walk.  Both give bitwise the same C. */
-    int no_segment_walk;
+    /* Numeric step from B's row segments when nonzero (default 0: the
+     * entry-per-lane walk): where every tile row fits one window, B has no
+     * repeated columns and no B row has more than 32 segments, a half-warp
+     * walks a row's A entries and its lanes take the segments of each
+     * entry's B row.  Both give bitwise the same C; on B200 the segment walk
+     * measured slower on the 27-point stencil (numeric 4.18 against 2.29 ms
+     * at 96^3: one A entry per half-warp in flight leaves the walk
+     * latency-bound), so it is opt-in. */
+    int segment_walk;
     /* Reserved, must be zero. */
     int reserved[1];
 } rtt_config;
@@ -491,6 +494,13 @@ typedef struct
  * not be used by two host threads at once. */
 RTT_API int rtt_context_create(rtt_context *ctx, int device);
 RTT_API void rtt_context_destroy(rtt_context ctx);
+/* Releases every device buffer the context has grown (tiles, C structure,
+ * workspace) and its captured graphs; the context stays usable (stream and
+ * configuration kept) and the next product grows them again.  The state of
+ * the last symbolic phase is dropped.  For long-running callers under memory
+ * pressure (the serving loop calls it before a product that ran out of
+ * memory is tried alone).  No counterpart in the reference. */
+RTT_API int rtt_context_trim(rtt_context ctx);
 /* stream is a cudaStream_t (NULL = legacy default stream). */
 RTT_API int rtt_context_set_stream(rtt_context ctx, void *stream);
 RTT_API int rtt_context_set_config(rtt_context ctx, const rtt_config *config);

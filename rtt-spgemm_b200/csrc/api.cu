@@ -766,7 +766,7 @@ int numeric_enqueue(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_val
     dB.csr_val = c->b_va;
     dB.nnz = (int)c->b_nnz;
     nc.conflict_safe = c->b_dups;
-    nc.segment_walk = c->cfg.no_segment_walk == 0;
+    nc.segment_walk = c->cfg.segment_walk != 0;
     // the numeric step reads A's entries from its CSR rows
     DevTiles dA = c->A.view();
     dA.csr_rowptr = c->a_rp;
@@ -1018,6 +1018,35 @@ void rtt_context_destroy(rtt_context c)
     cudaGetLastError();
 }
 
+int rtt_context_trim(rtt_context c)
+{
+    if (c == nullptr)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    RTT_CUDA(cudaSetDevice(c->ws.device));
+    RTT_CUDA(cudaStreamSynchronize(c->ws.stream));
+    if (c->ws.side != nullptr)
+        RTT_CUDA(cudaStreamSynchronize(c->ws.side));
+    for (rtt::GraphSlot &g : c->graph)
+        g.reset();
+    c->A.release();
+    c->B.release();
+    c->S.release();
+    for (rtt::DevBuf *b : own_buffers(c))
+        b->release();
+    c->ws.scan_tmp.release();
+    for (rtt::DevBuf &b : c->ws.tmp)
+        b.release();
+    c->have_symbolic = false;
+    c->have_sym64 = false;
+    c->bat_active = false;
+    c->cut_cached = -1;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, c->ws.device) == cudaSuccess)
+        cudaMemPoolTrimTo(pool, 0);
+    cudaGetLastError();
+    return RTT_OK;
+}
+
 int rtt_context_set_stream(rtt_context c, void *stream)
 {
     if (c == nullptr)
@@ -1035,10 +1064,10 @@ int rtt_context_set_config(rtt_context c, const rtt_config *config)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "NULL argument");
     if (config->dmma_pair_cutoff < 0)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "dmma_pair_cutoff must be >= 0");
-    if (config->chunk_tiles < 0 || config->chunk_nnz < 0 || config->no_segment_walk < 0 ||
-        config->no_segment_walk > 1)
+    if (config->chunk_tiles < 0 || config->chunk_nnz < 0 || config->segment_walk < 0 ||
+        config->segment_walk > 1)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT,
-                         "chunk_tiles, chunk_nnz >= 0 and no_segment_walk 0 or 1 expected");
+                         "chunk_tiles, chunk_nnz >= 0 and segment_walk 0 or 1 expected");
     for (int r : config->reserved)
         if (r != 0)
             return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "reserved config fields must be zero");
@@ -1963,7 +1992,7 @@ int rtt_spgemm_numeric64(rtt_context c, long long *c_row_ptr, int *c_col_idx, do
         nc.split_target = c->cfg.split_target;
         nc.write_tiles = false;
         nc.conflict_safe = c->b_dups;
-        nc.segment_walk = c->cfg.no_segment_walk == 0;
+        nc.segment_walk = c->cfg.segment_walk != 0;
         nc.csr_rowptr = c->w_local.as<int>();
         nc.csr_col = c_col_idx + c->w_base[k];
         nc.csr_val = c_values + c->w_base[k];

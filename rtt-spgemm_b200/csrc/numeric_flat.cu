@@ -363,16 +363,18 @@ __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Windo
 }
 
 // The warp's products from B's row segments (one window, B rows of at most
-// 16 segments, no repeated columns): half-warp h walks the A entries of its
-// row (r0 or r1) one by one, in column order, and its lanes take the
-// segments of that entry's B row - lane l the l-th segment, its tile column
-// J and 16-bit mask.  A lane finds the segment's C tile slot and the row's
+// SEGW_MAX segments, no repeated columns): half-warp h walks the A entries of
+// its row (r0 or r1) one by one, in column order, and its lanes take the
+// segments of that entry's B row - lane l the segments l, l + 16, ..., each
+// with its tile column J and 16-bit mask.  A lane finds the segment's C tile slot and the row's
 // (base, mask) word once, then adds the segment's entries (the mask's set
 // bits, in column order; their values are consecutive in B's row, from the
 // offset a half-warp scan of the masks' popcounts gives) into the row's
 // accumulator.  The lanes of one half hit distinct columns of one row, the
 // halves distinct rows; every output entry is still summed in the order of
 // its row's A entries, as in warp_products.
+constexpr int SEGW_MAX = 32; // segments of a B row the segment walk takes (two rounds)
+
 template <int ACC>
 __device__ __forceinline__ long long warp_products_seg(FlatSmem<ACC> &S, const Window &W,
                                                        const DevTiles &A, const DevTiles &B,
@@ -397,36 +399,45 @@ __device__ __forceinline__ long long warp_products_seg(FlatSmem<ACC> &S, const W
             if (k < B.m)
             {
                 s0 = __ldg(B.seg_ptr + k);
-                ns = min(__ldg(B.seg_ptr + k + 1) - s0, 16);
+                ns = min(__ldg(B.seg_ptr + k + 1) - s0, SEGW_MAX);
                 fs = __ldg(B.csr_rowptr + k);
             }
         }
-        unsigned long long sg = 0ull;
-        if (hl < ns)
-            sg = __ldg(B.seg + s0 + hl);
-        const int pc = __popc((unsigned)sg & 0xFFFFu);
-        const int incl = half_incl_scan(pc);
-        if (count)
-            n_fma += pc;
-        if (hl < ns)
+        // up to SEGW_MAX segments: lane hl takes segments hl, hl + 16, ...
+        const int rounds = (int)(__reduce_max_sync(FULL, (unsigned)ns) + 15) >> 4;
+        int before = 0; // entries of the B row in the earlier rounds' segments
+        for (int rd = 0; rd < rounds; ++rd)
         {
-            const int J = (int)(sg >> 16);
-            const int slot = S.slot8[min((unsigned)(J - W.Jlo), (unsigned)(F_SPAN_CAP - 1))];
-            const uint32_t w = cmr[slot];
-            const int base = (int)(w >> 16);
-            const uint32_t cmask = w & 0xFFFFu;
-            int eo = min(max(fs + incl - pc, 0), B.nnz - 1);
-            uint32_t bm = (uint32_t)sg & 0xFFFFu;
-            while (bm)
+            const int sl = rd * 16 + hl;
+            unsigned long long sg = 0ull;
+            if (sl < ns)
+                sg = __ldg(B.seg + s0 + sl);
+            const int pc = __popc((unsigned)sg & 0xFFFFu);
+            const int incl = half_incl_scan(pc);
+            const int round_total = __shfl_sync(FULL, incl, (lane & 16) | 15);
+            if (count)
+                n_fma += pc;
+            if (sl < ns)
             {
-                const int c = __clz(bm) - 16; // column in the tile, left to right
-                bm &= ~(0x8000u >> c);
-                const double b = __ldg(B.csr_val + eo);
-                eo = min(eo + 1, B.nnz - 1);
-                const int pos = min(base + __popc(cmask >> (16 - c)), ACC - 1);
-                S.acc[pos] = fma(a, b, S.acc[pos]);
-                S.ccol[pos] = J * TD + c;
+                const int J = (int)(sg >> 16);
+                const int slot = S.slot8[min((unsigned)(J - W.Jlo), (unsigned)(F_SPAN_CAP - 1))];
+                const uint32_t w = cmr[slot];
+                const int base = (int)(w >> 16);
+                const uint32_t cmask = w & 0xFFFFu;
+                int eo = min(max(fs + before + incl - pc, 0), B.nnz - 1);
+                uint32_t bm = (uint32_t)sg & 0xFFFFu;
+                while (bm)
+                {
+                    const int c = __clz(bm) - 16; // column in the tile, left to right
+                    bm &= ~(0x8000u >> c);
+                    const double b = __ldg(B.csr_val + eo);
+                    eo = min(eo + 1, B.nnz - 1);
+                    const int pos = min(base + __popc(cmask >> (16 - c)), ACC - 1);
+                    S.acc[pos] = fma(a, b, S.acc[pos]);
+                    S.ccol[pos] = J * TD + c;
+                }
             }
+            before += round_total;
         }
     }
     return n_fma;
@@ -1062,10 +1073,10 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
                                       : k_numeric_flat<true, ACC_SMALL, CTAS_SMALL, false, false, false>)
                     : (S.multi_window ? k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, true, false>
                                       : k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, false, false>));
-    // B rows of at most 16 segments, one window per tile row, no repeated
-    // columns: the segment walk
+    // B rows of at most SEGW_MAX segments, one window per tile row, no
+    // repeated columns: the segment walk
     if (cfg.segment_walk && acsr && !cfg.conflict_safe && !S.multi_window && B.seg_ptr != nullptr &&
-        B.seg != nullptr && B.max_row_segs > 0 && B.max_row_segs <= 16)
+        B.seg != nullptr && B.max_row_segs > 0 && B.max_row_segs <= SEGW_MAX)
         light = k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, false, true, true>;
     RTT_CHECK(launch(light, S.tilem, s, smem, nullptr));
     if (split)

@@ -376,7 +376,7 @@ struct NumericConfig
     cudaEvent_t ev_begin = nullptr; // recorded around the numeric kernel when set
     cudaEvent_t ev_end = nullptr;
     bool conflict_safe = false;     // B rows may repeat a column: accumulate with shared atomics
-    bool segment_walk = true;       // the numeric step may walk B's row segments
+    bool segment_walk = false;      // the numeric step may walk B's row segments
 };
 
 // CSR row pointer of C (m + 1 ints) from the symbolic counts

@@ -393,6 +393,10 @@ class Context:
         except Exception:
             pass
 
+    def trim(self):
+        """rtt_context_trim: release the context's grown device buffers."""
+        check(lib().rtt_context_trim(self.handle))
+
     def set_stream(self, stream_ptr: int):
         check(lib().rtt_context_set_stream(self.handle, C.c_void_p(stream_ptr)))
 

@@ -39,6 +39,7 @@ EXPORTS = [
     "rtt_spgemm_numeric_values", "rtt_super16_index_build", "rtt_super16_index_destroy",
     "rtt_spgemm_batched_numeric_values", "rtt_spgemm_symbolic64", "rtt_spgemm_numeric64",
     "rtt_spgemm_update_b", "rtt_mmio_read", "rtt_reorder_plan_dump", "rtt_tile_heatmap",
+    "rtt_context_trim",
 ]
 
 RTT_SUPER16_A8X4 = 1
@@ -78,7 +79,7 @@ class Config(C.Structure):
                 ("keep_tiles", C.c_int), ("stage_timing", C.c_int), ("b_staging", C.c_int),
                 ("split_target", C.c_int), ("cuda_graphs", C.c_int),
                 ("chunk_tiles", C.c_int), ("chunk_nnz", C.c_int),
-                ("no_segment_walk", C.c_int), ("reserved", C.c_int * 1)]
+                ("segment_walk", C.c_int), ("reserved", C.c_int * 1)]
 
 
 class HybridTiles(C.Structure):
@@ -213,6 +214,7 @@ def lib() -> C.CDLL:
     L.rtt_context_destroy.argtypes = [C.c_void_p]
     L.rtt_context_destroy.restype = None
     L.rtt_context_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.rtt_context_trim.argtypes = [C.c_void_p]
     L.rtt_context_set_config.argtypes = [C.c_void_p, P(Config)]
     L.rtt_context_get_stats.argtypes = [C.c_void_p, P(Stats)]
     L.rtt_spgemm_symbolic.argtypes = [C.c_void_p, P(CsrView), P(CsrView), C.c_int,

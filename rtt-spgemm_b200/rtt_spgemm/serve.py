@@ -118,7 +118,9 @@ class Server:
         self.config = config
         self.nworkers = workers
         self.keep_results = keep_results
+        # reuse key -> device operands (LRU, bounded by bytes; counted against the pool)
         self.resident: OrderedDict = OrderedDict()
+        self.resident_bytes = pool_bytes / 8
         self.lock = threading.Lock()
         # reuse key -> _Structure (LRU), bounded by count and by the bytes of
         # their products' bounds
@@ -192,6 +194,15 @@ class Server:
         if r.key is not None:
             with self.lock:
                 self.resident[r.key] = (a, at, src)
+                self.resident.move_to_end(r.key)
+                # least recently used operands leave first (a batch in flight
+                # keeps its own references)
+                nbytes = lambda e: sum(t.numel() * t.element_size()
+                                       for x in (e[0], e[1]) if x is not None for t in x[2:5])
+                total = sum(nbytes(e) for e in self.resident.values())
+                while len(self.resident) > 1 and total > self.resident_bytes:
+                    _, old = self.resident.popitem(last=False)
+                    total -= nbytes(old)
         return a, (at if r.op == "AAT" else a)
 
     # -- resident tile structures -----------------------------------------
@@ -337,6 +348,23 @@ class Server:
             r.done = t
             r.result = o if self.keep_results else None
 
+    def _release_memory(self):
+        """Before a request that ran out of memory runs alone (nothing else
+        in flight): drop the resident structures, spare contexts and operands,
+        shrink the workers' grown buffers, and hand torch's cache back."""
+        with self.lock:
+            structs = list(self.structures.values())
+            self.structures.clear()
+            spare, self._spare = self._spare, []
+            self.resident.clear()
+        for st in structs:
+            st.ctx.close()
+        for ctx in spare:
+            ctx.close()
+        for _, ctx in self._slots:
+            ctx.trim()
+        self.torch.cuda.empty_cache()
+
     # -- the loop ---------------------------------------------------------
     def run(self, requests: list[Request]) -> dict:
         """Serve requests (sorted by arrival) in real time; returns latency
@@ -408,7 +436,7 @@ class Server:
                     retry = []
                     try:
                         if batch[0].exclusive:
-                            torch.cuda.empty_cache()  # what torch caches, back to the device
+                            self._release_memory()
                         self._run_batch(ctx, stream, batch, t0)
                     except _OutOfMemory:
                         retry = [r for r in batch if r.done < 0]

@@ -216,13 +216,13 @@ SEGWALK_CASES = {
 
 @pytest.mark.parametrize("case", list(SEGWALK_CASES))
 def test_segment_walk_equals_entry_walk(case, orc):
-    """The numeric step over B's row segments (default, where it applies)
+    """The numeric step over B's row segments (segment_walk, where it applies)
     and the entry-per-lane walk sum every output in the same order: bitwise
     the same C, and the oracle's within the bound."""
     A = SEGWALK_CASES[case]()
     got = {}
     for off in (0, 1):
-        ctx = R.Context(0, dict(no_segment_walk=off))
+        ctx = R.Context(0, dict(segment_walk=1 - off))
         rp, ci, va, nnz, _ = _run(ctx, A)
         got[off] = (rp, ci, va)
         ctx.close()

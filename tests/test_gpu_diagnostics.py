@@ -56,16 +56,19 @@ def test_tile_heatmaps(orc, bins):
     da = _dev(A)
     nnz, tiles = ctx.symbolic(da)
     ta = orc.csr2tile_row_major(A)
-    c = orc.spgemm_csr(A, A, with_abs=False)
-    C = G.CSR(A.m, A.n, c[0].astype(np.int32), c[1], c[2])
-    tc = orc.csr2tile_row_major(C)
-    for which, t in (("A", ta), ("B", ta), ("C", tc)):
+    tm, tn = ta["tilem"], ta["tilen"]
+    I = np.repeat(np.arange(tm), np.diff(ta["tile_ptr"]))
+    J = ta["tile_columnidx"]
+    # C's tiles: the tile-level product of A's tile pattern with B's (= A's),
+    # as step 1 forms it (a tile whose entries all cancel structurally stays)
+    TA = np.zeros((tm, tn), bool)
+    TA[I, J] = True
+    TC = (TA.astype(np.int64) @ TA.astype(np.int64)) > 0
+    CI, CJ = np.nonzero(TC)
+    for which, (ii, jj) in (("A", (I, J)), ("B", (I, J)), ("C", (CI, CJ))):
         h = ctx.tile_heatmap(which, bins)
-        tm, tn = t["tilem"], t["tilen"]
-        I = np.repeat(np.arange(tm), np.diff(t["tile_ptr"]))
-        J = t["tile_columnidx"]
         want = np.zeros((bins, bins), np.uint64)
-        np.add.at(want, (I * bins // tm, J * bins // tn), 1)
+        np.add.at(want, (ii * bins // tm, jj * bins // tn), 1)
         assert np.array_equal(h, want), which
     assert int(ctx.tile_heatmap("C", bins).sum()) == tiles
     ctx.close()
