@@ -284,7 +284,8 @@ def run_batched(args) -> None:
     if cur:
         waves.append(cur)
     ctx = R.Context(0, {"stage_timing": 0, "dmma_pair_cutoff": args.dmma_cutoff,
-                        "b_staging": 1 if args.staging else 0})
+                        "b_staging": 1 if args.staging else 0,
+                        "persistent_rows": 1 if args.persistent_rows else 0})
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
 
@@ -318,7 +319,8 @@ def run_batched(args) -> None:
         return e0.elapsed_time(e1) / args.steps
 
     base_cfg = {"stage_timing": 0, "dmma_pair_cutoff": args.dmma_cutoff,
-                "b_staging": 1 if args.staging else 0}
+                "b_staging": 1 if args.staging else 0,
+                "persistent_rows": 1 if args.persistent_rows else 0}
     ms_b = timed(batched)
     ctx.configure(base_cfg)  # the plain arm keeps the given configuration
     ms_p = timed(plain)
@@ -669,7 +671,8 @@ def run_ours(args) -> None:
     ctx = R.Context(local, {"stage_timing": 1, "dmma_pair_cutoff": args.dmma_cutoff,
                             "fused_csr_output": 0 if args.unfused else 1,
                             "b_staging": 1 if args.staging else 0,
-                            "segment_walk": 1 if args.segment_walk else 0})
+                            "segment_walk": 1 if args.segment_walk else 0,
+                            "persistent_rows": 1 if args.persistent_rows else 0})
     ctx.set_stream(stream.cuda_stream)
     rp = torch.from_numpy(A.rowptr).to(dev)
     ci = torch.from_numpy(A.col).to(dev)
@@ -903,6 +906,8 @@ def main() -> None:
     ap.add_argument("--serve-repeats", type=int, default=3,
                     help="served: timed runs of each arm (median and spread reported)")
     ap.add_argument("--wave-rows", type=int, default=4_000_000)
+    ap.add_argument("--persistent-rows", action="store_true",
+                    help="numeric step: one resident wave of tile-row CTAs over a device queue")
     ap.add_argument("--segment-walk", action="store_true",
                     help="numeric step: walk B's row segments where that applies")
     ap.add_argument("--staging", action="store_true",

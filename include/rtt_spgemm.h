@@ -454,8 +454,11 @@ typedef struct
      * at 96^3: one A entry per half-warp in flight leaves the walk
      * latency-bound), so it is opt-in. */
     int segment_walk;
-    /* Reserved, must be zero. */
-    int reserved[1];
+    /* Numeric step's tile-row CTAs as one resident wave taking tile rows
+     * from a device queue (nonzero) instead of one CTA per tile row (0, the
+     * default).  For a batch the queue spans every instance's tile rows.
+     * Both give bitwise the same C. */
+    int persistent_rows;
 } rtt_config;
 
 RTT_API void rtt_config_default(rtt_config *config);

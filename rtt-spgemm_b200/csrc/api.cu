@@ -767,6 +767,7 @@ int numeric_enqueue(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_val
     dB.nnz = (int)c->b_nnz;
     nc.conflict_safe = c->b_dups;
     nc.segment_walk = c->cfg.segment_walk != 0;
+    nc.persistent_rows = c->cfg.persistent_rows != 0;
     // the numeric step reads A's entries from its CSR rows
     DevTiles dA = c->A.view();
     dA.csr_rowptr = c->a_rp;
@@ -1065,12 +1066,9 @@ int rtt_context_set_config(rtt_context c, const rtt_config *config)
     if (config->dmma_pair_cutoff < 0)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "dmma_pair_cutoff must be >= 0");
     if (config->chunk_tiles < 0 || config->chunk_nnz < 0 || config->segment_walk < 0 ||
-        config->segment_walk > 1)
+        config->segment_walk > 1 || config->persistent_rows < 0 || config->persistent_rows > 1)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT,
-                         "chunk_tiles, chunk_nnz >= 0 and segment_walk 0 or 1 expected");
-    for (int r : config->reserved)
-        if (r != 0)
-            return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "reserved config fields must be zero");
+                         "chunk_tiles, chunk_nnz >= 0, segment_walk and persistent_rows 0 or 1");
     c->cfg = *config;
     c->cut_cached = -1;
     return RTT_OK;
@@ -1993,6 +1991,7 @@ int rtt_spgemm_numeric64(rtt_context c, long long *c_row_ptr, int *c_col_idx, do
         nc.write_tiles = false;
         nc.conflict_safe = c->b_dups;
         nc.segment_walk = c->cfg.segment_walk != 0;
+        nc.persistent_rows = c->cfg.persistent_rows != 0;
         nc.csr_rowptr = c->w_local.as<int>();
         nc.csr_col = c_col_idx + c->w_base[k];
         nc.csr_val = c_values + c->w_base[k];

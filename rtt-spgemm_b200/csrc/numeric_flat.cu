@@ -470,7 +470,7 @@ struct WinQueue
     int count;    // tasks written by the plan
     int head;     // next task to take
     int overflow; // some heavy tile row found no room and kept its own CTA
-    int pad;
+    int next;     // next tile row for the persistent tile-row CTAs
 };
 
 constexpr int PLAN_WARPS = 8;
@@ -673,7 +673,8 @@ __global__ void __launch_bounds__(PLAN_WARPS * 32)
 // several windows, so long sorted B rows are cut to each window's columns
 // (compiled out when every tile row fits one window: the registers are the
 // kernel's limit).
-template <bool SAFE, int ACC, int MIN_CTAS, bool WORKER, bool NARROW, bool ACSR, bool SEGW = false>
+template <bool SAFE, int ACC, int MIN_CTAS, bool WORKER, bool NARROW, bool ACSR, bool SEGW = false,
+          bool PERSIST = false>
 __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
     k_numeric_flat(DevTiles A, DevTiles B, int tilem, long long nnzC,
                    const int *__restrict__ c_tile_ptr, const int *__restrict__ c_tile_col,
@@ -712,6 +713,20 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
             if (I < 0 || I >= tilem)
                 break; // not a task of this product (uniform)
         }
+        else if (PERSIST)
+        {
+            // persistent tile-row CTAs: the next tile row from the queue
+            // (every instance of a batch: its block diagonal's tile rows)
+            __syncthreads(); // the previous tile row is done with shared memory
+            if (tid == 0)
+                S.task = atomicAdd(&q->next, 1);
+            __syncthreads();
+            I = S.task;
+            if (I >= tilem)
+                break;
+            if (heavy != nullptr && heavy[I])
+                continue; // a split row: the workers take its windows
+        }
         else
         {
             I = blockIdx.x;
@@ -721,7 +736,11 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
         const int a0 = __ldg(A.tile_ptr + I), a1 = __ldg(A.tile_ptr + I + 1);
         const int cs0 = __ldg(c_tile_ptr + I), cs1 = __ldg(c_tile_ptr + I + 1);
         if (cs0 == cs1 || a0 == a1)
+        {
+            if (PERSIST)
+                continue;
             break; // no C tiles in this tile row (uniform)
+        }
         if (!worker)
         {
             wbeg = cs0;
@@ -973,7 +992,7 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
             else
                 w0 = w1;
         }
-        if (!worker)
+        if (!worker && !PERSIST)
             break;
     }
     if (counters != nullptr)
@@ -1078,7 +1097,24 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
     if (cfg.segment_walk && acsr && !cfg.conflict_safe && !S.multi_window && B.seg_ptr != nullptr &&
         B.seg != nullptr && B.max_row_segs > 0 && B.max_row_segs <= SEGW_MAX)
         light = k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, false, true, true>;
-    RTT_CHECK(launch(light, S.tilem, s, smem, nullptr));
+    int light_grid = S.tilem;
+    if (cfg.persistent_rows && !cfg.conflict_safe && acsr && light == (S.multi_window
+            ? k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, true, true>
+            : k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, false, true>))
+    {
+        // one wave of resident CTAs taking tile rows from a device queue
+        light = S.multi_window
+                    ? k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, true, true, false, true>
+                    : k_numeric_flat<false, ACC_SMALL, CTAS_SMALL, false, false, true, false, true>;
+        int per_sm = 0, sms = 0;
+        RTT_CUDA(cudaFuncSetAttribute(light, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        RTT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, light, F_THREADS, smem));
+        RTT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws.device));
+        light_grid = std::max(1, std::min(per_sm * sms, S.tilem));
+        if (!split)
+            RTT_CUDA(cudaMemsetAsync(S.w_queue.p, 0, sizeof(WinQueue), s));
+    }
+    RTT_CHECK(launch(light, light_grid, s, smem, nullptr));
     if (split)
         RTT_CUDA(cudaStreamWaitEvent(s, ws.join_ev, 0));
     if (cfg.ev_end != nullptr)

@@ -377,6 +377,7 @@ struct NumericConfig
     cudaEvent_t ev_end = nullptr;
     bool conflict_safe = false;     // B rows may repeat a column: accumulate with shared atomics
     bool segment_walk = false;      // the numeric step may walk B's row segments
+    bool persistent_rows = false;   // tile-row CTAs as one resident wave over a device queue
 };
 
 // CSR row pointer of C (m + 1 ints) from the symbolic counts

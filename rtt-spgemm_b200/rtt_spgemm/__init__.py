@@ -380,7 +380,7 @@ class Context:
         for k, v in (config or {}).items():
             setattr(cfg, k, int(v))
         check(lib().rtt_context_set_config(self.handle, C.byref(cfg)))
-        self.config = {k: getattr(cfg, k) for k, _ in Config._fields_ if k != "reserved"}
+        self.config = {k: getattr(cfg, k) for k, _ in Config._fields_}
 
     def close(self):
         if self.handle:

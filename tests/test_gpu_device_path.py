@@ -229,3 +229,19 @@ def test_segment_walk_equals_entry_walk(case, orc):
     assert np.array_equal(got[0][0], got[1][0]) and np.array_equal(got[0][1], got[1][1])
     assert np.array_equal(got[0][2].view(np.int64), got[1][2].view(np.int64))
     assert_csr_close(*got[0], *orc.spgemm_csr(A, A), f"{case} segment walk: ")
+
+
+@pytest.mark.parametrize("case", ["stencil27_12", "banded", "rmat_12", "lap2d_ragged"])
+def test_persistent_rows_equal_per_row_ctas(case, orc):
+    """Tile-row CTAs as one resident wave over a device queue (with the split
+    workers beside them for multi-window rows): bitwise the one-CTA-per-row C."""
+    A = CASES[case]()
+    got = {}
+    for pers in (0, 1):
+        ctx = R.Context(0, dict(persistent_rows=pers))
+        rp, ci, va, nnz, _ = _run(ctx, A)
+        got[pers] = (rp, ci, va)
+        ctx.close()
+    assert np.array_equal(got[0][0], got[1][0]) and np.array_equal(got[0][1], got[1][1])
+    assert np.array_equal(got[0][2].view(np.int64), got[1][2].view(np.int64))
+    assert_csr_close(*got[1], *orc.spgemm_csr(A, A), f"{case} persistent: ")
