@@ -189,9 +189,9 @@ RTT_API int rtt_tile2csr_restore_rows(SMatrix *matrix, const int *row_new_to_old
  * Limits: m <= 33,554,432 rows (larger m returns RTT_ERR_INVALID_ARGUMENT
  * with a message naming the limit); its working memory is a 1 MiB static
  * device array per device.  The first call on a device looks that array up
- * (cudaGetSymbolAddress) and may load the module: make it before any stream
- * capture.  Calls that overlapped on one device would share the array and
- * race, so calls through this process are serialised by a lock. */
+ * (cudaGetSymbolAddress) and may load the module.  Calls that overlapped on
+ * one device would share the array and race, so calls through this process
+ * are serialised by a lock. */
 RTT_API int rtt_tile2csr_device_noalloc(const SMatrix *matrix, int tile_dim, int canonical,
                                         long long out_capacity, long long *out_nnz,
                                         void *stream);
@@ -490,6 +490,9 @@ typedef struct
     /* 1 when the last numeric phase ran as a launch of a captured CUDA graph
      * (cuda_graphs), else 0. */
     int graph_launched;
+    /* Window tasks of the last numeric step that hold two or more windows
+     * (a worker keeps per-entry cursors from one window to the next). */
+    long long split_multi_window_tasks;
 } rtt_stats;
 
 /* A context owns a CUDA stream handle (borrowed), workspace and the state

@@ -733,7 +733,7 @@ int run_phase(rtt_context c, int slot, const std::vector<long long> &head, bool 
 }
 
 // Device work of the numeric step into C's CSR (c_row_ptr, c_col_idx,
-// c_values), counters copied to ws.h_scalars64[2..4]; no host reads unless
+// c_values), counters copied to ws.h_scalars64[2..5]; no host reads unless
 // fused_csr_output == 0 (tile2csr sizes its output on the host).
 int numeric_enqueue(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_values, int cutoff)
 {
@@ -784,7 +784,7 @@ int numeric_enqueue(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_val
                                        S.tilem, TD, nullptr, -1, c_row_ptr, c_col_idx, c_values,
                                        false));
     }
-    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars64 + 2, c->counters.p, sizeof(long long) * 3,
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars64 + 2, c->counters.p, sizeof(long long) * 4,
                              cudaMemcpyDeviceToHost, ws.stream));
     return RTT_OK;
 }
@@ -806,6 +806,7 @@ int numeric_finish(rtt_context c)
     // entries of nnz(B(k, :)), the reference's nnzCub
     c->stats.nnz_cub = ws.h_scalars64[3];
     c->stats.split_windows = ws.h_scalars64[4];
+    c->stats.split_multi_window_tasks = ws.h_scalars64[5];
     c->stats.kernel_launches = ws.launches;
     c->stats.host_syncs = ws.syncs;
     return RTT_OK;
@@ -1998,12 +1999,13 @@ int rtt_spgemm_numeric64(rtt_context c, long long *c_row_ptr, int *c_col_idx, do
         sA.csr_val = c->a_va;
         RTT_CHECK(numeric_flat_device(ws, sA, dB, c->S, nc));
     }
-    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars64 + 2, c->counters.p, sizeof(long long) * 3,
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars64 + 2, c->counters.p, sizeof(long long) * 4,
                              cudaMemcpyDeviceToHost, s));
     RTT_CHECK(check_device_error(ws, "numeric64"));
     c->stats.sparse_pairs = ws.h_scalars64[3];
     c->stats.nnz_cub = ws.h_scalars64[3];
     c->stats.split_windows = ws.h_scalars64[4];
+    c->stats.split_multi_window_tasks = ws.h_scalars64[5];
     c->stats.kernel_launches = ws.launches;
     c->stats.host_syncs = ws.syncs;
     return RTT_OK;

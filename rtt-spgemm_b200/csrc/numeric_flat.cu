@@ -590,7 +590,14 @@ __global__ void __launch_bounds__(PLAN_WARPS * 32)
         if (base < 0)
             q->overflow = 1;
         else if (counters != nullptr)
+        {
             atomicAdd((unsigned long long *)&counters[2], (unsigned long long)ntask);
+            // tasks of two or more windows (the last task holds the remainder)
+            const int last = nwin - (ntask - 1) * g;
+            const int multi_tasks = g >= 2 ? ntask - (last < 2 ? 1 : 0) : 0;
+            if (multi_tasks > 0)
+                atomicAdd((unsigned long long *)&counters[3], (unsigned long long)multi_tasks);
+        }
     }
     base = __shfl_sync(FULL, base, 0);
     if (lane == 0)

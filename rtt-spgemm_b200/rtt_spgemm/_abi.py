@@ -155,7 +155,7 @@ class Stats(C.Structure):
                 ("kernel_launches", C.c_int), ("host_syncs", C.c_int),
                 ("csr2tile_ms", C.c_double), ("symbolic_ms", C.c_double),
                 ("numeric_kernel_ms", C.c_double), ("split_windows", C.c_longlong),
-                ("graph_launched", C.c_int)]
+                ("graph_launched", C.c_int), ("split_multi_window_tasks", C.c_longlong)]
 
 
 def build(verbose: bool = False) -> Path:

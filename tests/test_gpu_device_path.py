@@ -146,6 +146,10 @@ def test_many_window_rows_fused_equals_tiles(case, orc):
             assert ctx.stats()["split_windows"] > 0, name
         if "nosplit" in name:
             assert ctx.stats()["split_windows"] == 0, name
+        # a 2^16 target groups banded_20k's windows: tasks of several windows,
+        # whose workers carry per-entry cursors from one window to the next
+        if name == "fused_split64k" and case == "banded_20k":
+            assert ctx.stats()["split_multi_window_tasks"] > 0, name
         ctx.close()
     fused = runs["fused"]
     for name, other in runs.items():
@@ -153,6 +157,37 @@ def test_many_window_rows_fused_equals_tiles(case, orc):
         assert np.array_equal(fused[2].view(np.int64), other[2].view(np.int64)), name
     erp, ecol, evals, eabs = orc.spgemm_csr(A, A)
     assert_csr_close(fused[0], fused[1], fused[2], erp, ecol, evals, eabs, f"{case}: ")
+
+
+def test_split_cursors_past_the_cap(orc):
+    """Tile rows of 40,000 A entries (2,500 per row) against B rows of two
+    scattered entries: about 40 windows per tile row, grouped 13 to a task by
+    the default split target, so a worker's window cursors cover only the
+    first 32,768 entries of the row and the rest take the binary search.
+    Bitwise equal to the unsplit run and to the tile output, within the bar
+    of the oracle."""
+    rng = np.random.default_rng(81)
+    m, k, n = 48, 40000, 100000
+    rows = np.repeat(np.arange(m), 2500)
+    cols = np.concatenate([rng.choice(k, 2500, replace=False) for _ in range(m)])
+    A = G.from_coo(m, k, rows, cols, rng.uniform(-1, 1, rows.size))
+    brows = np.repeat(np.arange(k), 2)
+    B = G.from_coo(k, n, brows, rng.integers(0, n, brows.size), rng.uniform(-1, 1, brows.size))
+    runs = {}
+    for name, cfg in (("split", dict(fused_csr_output=1)),
+                      ("nosplit", dict(fused_csr_output=1, split_target=-1)),
+                      ("tiled", dict(fused_csr_output=0))):
+        ctx = R.Context(0, cfg)
+        runs[name] = _run(ctx, A, B)
+        st = ctx.stats()
+        if name == "split":
+            assert st["split_windows"] > 0 and st["split_multi_window_tasks"] > 0, st
+        ctx.close()
+    ref = runs["split"]
+    for name, other in runs.items():
+        assert np.array_equal(ref[0], other[0]) and np.array_equal(ref[1], other[1]), name
+        assert np.array_equal(ref[2].view(np.int64), other[2].view(np.int64)), name
+    assert_csr_close(ref[0], ref[1], ref[2], *orc.spgemm_csr(A, B), "cursors past the cap: ")
 
 
 def test_deterministic_and_reusable(orc):
