@@ -285,7 +285,8 @@ def run_batched(args) -> None:
         waves.append(cur)
     ctx = R.Context(0, {"stage_timing": 0, "dmma_pair_cutoff": args.dmma_cutoff,
                         "b_staging": 1 if args.staging else 0,
-                        "persistent_rows": 1 if args.persistent_rows else 0})
+                        "persistent_rows": 1 if args.persistent_rows else 0,
+                "sym_window_slots": args.sym_window_slots})
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
 
@@ -320,7 +321,8 @@ def run_batched(args) -> None:
 
     base_cfg = {"stage_timing": 0, "dmma_pair_cutoff": args.dmma_cutoff,
                 "b_staging": 1 if args.staging else 0,
-                "persistent_rows": 1 if args.persistent_rows else 0}
+                "persistent_rows": 1 if args.persistent_rows else 0,
+                "sym_window_slots": args.sym_window_slots}
     ms_b = timed(batched)
     ctx.configure(base_cfg)  # the plain arm keeps the given configuration
     ms_p = timed(plain)
@@ -556,7 +558,7 @@ def run_wide(args) -> None:
     cub = nnz_cub(A, True)
     flops = 2.0 * cub
     stream = torch.cuda.current_stream(dev)
-    ctx = R.Context(0, {"stage_timing": 0})
+    ctx = R.Context(0, {"stage_timing": 0, "sym_window_slots": args.sym_window_slots})
     ctx.set_stream(stream.cuda_stream)
     a_view = (A.m, A.n, torch.from_numpy(A.rowptr).to(dev), torch.from_numpy(A.col).to(dev),
               torch.from_numpy(A.val).to(dev))
@@ -672,7 +674,8 @@ def run_ours(args) -> None:
                             "fused_csr_output": 0 if args.unfused else 1,
                             "b_staging": 1 if args.staging else 0,
                             "segment_walk": 1 if args.segment_walk else 0,
-                            "persistent_rows": 1 if args.persistent_rows else 0})
+                            "persistent_rows": 1 if args.persistent_rows else 0,
+                "sym_window_slots": args.sym_window_slots})
     ctx.set_stream(stream.cuda_stream)
     rp = torch.from_numpy(A.rowptr).to(dev)
     ci = torch.from_numpy(A.col).to(dev)
@@ -906,6 +909,9 @@ def main() -> None:
     ap.add_argument("--serve-repeats", type=int, default=3,
                     help="served: timed runs of each arm (median and spread reported)")
     ap.add_argument("--wave-rows", type=int, default=4_000_000)
+    ap.add_argument("--sym-window-slots", type=int, default=0,
+                    help="symbolic step 2: C tiles per window of the wide-window CTAs "
+                         "(0 = default, -1 = off)")
     ap.add_argument("--persistent-rows", action="store_true",
                     help="numeric step: one resident wave of tile-row CTAs over a device queue")
     ap.add_argument("--segment-walk", action="store_true",

@@ -459,6 +459,12 @@ typedef struct
      * default).  For a batch the queue spans every instance's tile rows.
      * Both give bitwise the same C. */
     int persistent_rows;
+    /* Symbolic step 2 of C tile rows with more C tiles than 254 (R-MAT
+     * rows): every window of C tiles walks the tile row's A entries again,
+     * so such rows run in CTAs whose windows hold up to sym_window_slots C
+     * tiles (0 = the default, 2045; 255..6000 to choose; -1 = off, every
+     * row in windows of 254).  Every setting gives bitwise the same C. */
+    int sym_window_slots;
 } rtt_config;
 
 RTT_API void rtt_config_default(rtt_config *config);

@@ -1070,7 +1070,12 @@ int rtt_context_set_config(rtt_context c, const rtt_config *config)
         config->segment_walk > 1 || config->persistent_rows < 0 || config->persistent_rows > 1)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT,
                          "chunk_tiles, chunk_nnz >= 0, segment_walk and persistent_rows 0 or 1");
+    if (config->sym_window_slots < -1 ||
+        (config->sym_window_slots > 0 &&
+         (config->sym_window_slots < 255 || config->sym_window_slots > 6000)))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "sym_window_slots must be -1, 0 or 255..6000");
     c->cfg = *config;
+    c->S.sym_window_slots = config->sym_window_slots;
     c->cut_cached = -1;
     return RTT_OK;
 }

@@ -149,11 +149,16 @@ __device__ __forceinline__ int gallop_lower_bound(const int *a, int lo, int hi, 
 }
 
 // Cursors of a persistent worker CTA (cur != nullptr): for the first
-// CUR_CAP A entries of its task's tile row, where each B row's part in the
-// current window ended.  The task's windows follow each other in column
+// cursor_cap(A) A entries of its task's tile row, where each B row's part in
+// the current window ended.  The task's windows follow each other in column
 // order, so the next window's part starts there: one galloping search over
-// that part instead of two binary searches over the whole row.
+// that part instead of two binary searches over the whole row.  A tile row
+// holds at most A.nnz entries, so a CTA's cursor array needs no more.
 constexpr int CUR_CAP = 32768;
+__host__ __device__ __forceinline__ int cursor_cap(const DevTiles &A)
+{
+    return A.nnz < CUR_CAP ? (A.nnz > 1 ? A.nnz : 1) : CUR_CAP;
+}
 
 // The warp's A entries, in batches of 32 (lane l: entry l of the batch):
 // calls fn(valid, k, a_ik, row, place) for each batch, place being the
@@ -255,7 +260,7 @@ __device__ __forceinline__ long long warp_products(FlatSmem<ACC> &S, const Windo
                     const int lo = W.Jlo * TD, hi = (W.Jlo + W.Jspan + 1) * TD;
                     const int fe = fs + len;
                     const int ci = place; // the entry's place in its tile row
-                    const bool keep = cur != nullptr && (unsigned)ci < (unsigned)CUR_CAP;
+                    const bool keep = cur != nullptr && (unsigned)ci < (unsigned)cursor_cap(A);
                     int sb;
                     if (keep && !first)
                     {
@@ -911,7 +916,7 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
                 }
                 if (WORKER && cursors != nullptr)
                 {
-                    cur = cursors + (size_t)blockIdx.x * CUR_CAP;
+                    cur = cursors + (size_t)blockIdx.x * cursor_cap(A);
                     if (!ACSR)
                         ebase = __ldg(A.tile_nnz + a0);
                 }
@@ -1082,7 +1087,7 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
         RTT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk, F_THREADS, smem));
         RTT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws.device));
         const int grid = std::max(1, per_sm * sms);
-        RTT_CHECK(S.w_cursor.ensure(sizeof(int) * (size_t)grid * CUR_CAP, s));
+        RTT_CHECK(S.w_cursor.ensure(sizeof(int) * (size_t)grid * cursor_cap(A), s));
         RTT_CUDA(cudaEventRecord(ws.fork_ev, s));
         RTT_CUDA(cudaStreamWaitEvent(ws.side, ws.fork_ev, 0));
         RTT_CHECK(launch(wk, grid, ws.side, smem, S.w_cursor.as<int>()));

@@ -208,7 +208,7 @@ struct Workspace
     DevBuf err;        // int device error word
     DevBuf scan_tmp;   // CUB temp storage
     DevBuf tmp[4];     // grow-only scratch of the transpose and the batch tables
-    int *h_scalars = nullptr; // pinned, 16 ints
+    int *h_scalars = nullptr; // pinned, 32 ints
     long long *h_scalars64 = nullptr; // pinned, 8 long long
     int launches = 0;
     int syncs = 0;
@@ -322,13 +322,17 @@ struct SymbolicOut
     // numeric split of heavy tile rows: window tasks, per-tile-row flag, queue
     DevBuf w_task, w_heavy, w_queue, w_flag;
     DevBuf w_cursor; // per worker CTA: window cursors of its task's A entries
-    // symbolic step 2: heavy tile rows (flag per tile row, list)
-    DevBuf s2_heavy, s2_list;
+    // symbolic step 2: heavy tile rows (flag per tile row, list) and the
+    // list of tile rows for the wide-window CTAs
+    DevBuf s2_heavy, s2_list, s2_wlist;
     // symbolic step 1: tile rows with many tile pairs (list for a wide CTA)
     DevBuf s1_list;
     // some C tile row needs more than one window of the flat numeric kernel
     // (set by the symbolic step; true when unknown)
     bool multi_window = true;
+    // C tiles per window of the wide-window step-2 CTAs (0: the default,
+    // -1: tile rows with many C tiles stay in the 254-slot CTAs)
+    int sym_window_slots = 0;
     int numtile = 0;
     long long nnz = 0;
     int tilem = 0, tilen = 0, m = 0, n = 0;
@@ -342,7 +346,7 @@ struct SymbolicOut
                                &c_ptr,      &c_col,      &c_val,      &c_row_cnt,  &c_rowptr,
                                &c_tr_nnz,   &count_tmp,  &tile_cnt,   &w_task,     &w_heavy,
                                &w_queue,    &w_flag,     &s2_heavy,   &s2_list,
-                               &s1_list,    &w_cursor};
+                               &s2_wlist,   &s1_list,    &w_cursor};
         for (const DevBuf *b : all)
             f(*b);
     }

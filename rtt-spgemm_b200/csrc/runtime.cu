@@ -133,7 +133,7 @@ int Workspace::init(int dev)
     RTT_CUDA(cudaMemset(err.p, 0, sizeof(int) * 4));
     if (h_scalars == nullptr)
     {
-        RTT_CUDA(cudaMallocHost(&h_scalars, sizeof(int) * 16));
+        RTT_CUDA(cudaMallocHost(&h_scalars, sizeof(int) * 32));
         RTT_CUDA(cudaMallocHost(&h_scalars64, sizeof(long long) * 8));
     }
     for (cudaEvent_t &e : ev)

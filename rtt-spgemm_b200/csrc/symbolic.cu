@@ -21,6 +21,7 @@
 #include "rtt_internal.cuh"
 
 #include <climits>
+#include <type_traits>
 
 namespace rtt
 {
@@ -52,19 +53,36 @@ constexpr int S2_SLOTS = 254;            // C tiles per window (slot 255 = none)
 // the latency of the per-tile-row set-up phases better.
 constexpr int S2_SEG_WARPS = 4;
 constexpr int S2_STRIDE = 257;           // odd stride: the pairs' mask rows in distinct banks
+// Wide windows: tile rows with more C tiles than S2_SLOTS (an R-MAT row's
+// tens of thousands) walk their A entries once per window, so the tile rows
+// step 1 lists as such run in CTAs whose slot table holds u16 slots, up to
+// S2_WIDE_MAX C tiles per window (rtt_config.sym_window_slots; the mask rows
+// after the fixed part of dynamic shared memory).
+constexpr int S2_WIDE_DEFAULT = 2045;
+constexpr int S2_WIDE_MAX = 6000; // the 32-warp CTA's mask rows within 227 KB
 
-template <int NW>
+// Shared memory of a step-2 CTA; the mask rows (S2_PAIRS rows of `stride`
+// words: per slot, row 2p in the low 16 bits and 2p + 1 in the high 16)
+// follow it.
+template <int NW, bool WIDE>
 struct CtaSmem2
 {
+    using Slot = typename std::conditional<WIDE, uint16_t, uint8_t>::type;
+    static constexpr int NONE = WIDE ? 0xFFFF : 0xFF;
     uint32_t bitmap[WWORDS];
     int wordpre[WWORDS];
-    uint8_t slot8[WBITS];                // window column -> slot
-    uint32_t mw[S2_PAIRS * S2_STRIDE];   // per row pair and slot: row 2p (low 16), 2p+1 (high 16)
     int4 ent[NW][32];                    // per warp: B row start, length, mask shift, mask row
+    Slot slot[WBITS];                    // window column -> slot
     int lo, hi, nb, wend;
     int share;                           // the warps share the A entries (unbalanced rows)
     int rp[TD + 1];                      // the tile row's A row pointers (segment walk)
 };
+
+template <int NW, bool WIDE>
+constexpr size_t smem2_bytes(int stride)
+{
+    return (sizeof(CtaSmem2<NW, WIDE>) + 15) / 16 * 16 + sizeof(uint32_t) * S2_PAIRS * (size_t)stride;
+}
 
 // First segment in [lo, hi) whose tile column is >= J (a row's segments are
 // in increasing tile-column order).
@@ -172,16 +190,19 @@ constexpr long long S1_WIDE_PAIRS = 1 << 16;
 constexpr int S1_WIDE_WARPS = 16;
 
 // Step-1 outcome of tile row I: C tiles, the step-2 window flag and the
-// step-2 heavy list.
+// step-2 lists: heavy rows (heavy[I] = 1) and rows with more C tiles than
+// one 254-slot window (heavy[I] = 2, for the wide-window CTAs).
 __device__ __forceinline__ void step1_out(const DevTiles &A, int I, int count, int lo, int hi,
                                           int lane, int *cnt, int *multi, uint8_t *heavy,
-                                          int *list, int *list_count)
+                                          int *list, int *list_count, int *wlist,
+                                          int *wlist_count)
 {
     // step 2 will need more than one window for this tile row; with an
     // unbalanced row pair it becomes a heavy row (a wide CTA of its own)
     const bool multi_win = count > S2_SLOTS || (hi >= 0 && (long long)hi - lo + 1 > WBITS);
     const bool hv = multi_win && heavy != nullptr &&
                     skewed_pairs(A, I, min(TD, A.m - I * TD), lane, HEAVY_PAIR);
+    const bool wide = !hv && count > S2_SLOTS && wlist != nullptr;
     if (lane == 0)
     {
         cnt[I] = count;
@@ -189,16 +210,18 @@ __device__ __forceinline__ void step1_out(const DevTiles &A, int I, int count, i
             atomicOr(multi, 1);
         if (heavy != nullptr)
         {
-            heavy[I] = hv;
+            heavy[I] = hv ? 1 : wide ? 2 : 0;
             if (hv)
                 list[atomicAdd(list_count, 1)] = I;
+            else if (wide)
+                wlist[atomicAdd(wlist_count, 1)] = I;
         }
     }
 }
 
 __global__ void __launch_bounds__(SYM_WARPS * 32)
     k_sym_count(DevTiles A, DevTiles B, int *cnt, int *multi, uint8_t *heavy, int *list,
-                int *list_count, int *wide, int *wide_count)
+                int *list_count, int *wide, int *wide_count, int *wlist, int *wlist_count)
 {
     __shared__ WarpSmem1 sm[SYM_WARPS];
     const int lane = lane_id(), wi = threadIdx.x >> 5;
@@ -235,7 +258,7 @@ __global__ void __launch_bounds__(SYM_WARPS * 32)
             __syncwarp();
         }
     }
-    step1_out(A, I, count, lo, hi, lane, cnt, multi, heavy, list, list_count);
+    step1_out(A, I, count, lo, hi, lane, cnt, multi, heavy, list, list_count, wlist, wlist_count);
 }
 
 // Step 1 of the tile rows k_sym_count listed as wide: one CTA of
@@ -243,7 +266,8 @@ __global__ void __launch_bounds__(SYM_WARPS * 32)
 // warps splitting its A tiles and OR-ing into one shared bitmap per window.
 __global__ void __launch_bounds__(S1_WIDE_WARPS * 32)
     k_sym_count_wide(DevTiles A, DevTiles B, int *cnt, int *multi, uint8_t *heavy, int *list,
-                     int *list_count, const int *wide, const int *wide_count)
+                     int *list_count, const int *wide, const int *wide_count, int *wlist,
+                     int *wlist_count)
 {
     __shared__ uint32_t bitmap[WWORDS];
     __shared__ int s_start[S1_WIDE_WARPS][32], s_pre[S1_WIDE_WARPS][32];
@@ -298,7 +322,8 @@ __global__ void __launch_bounds__(S1_WIDE_WARPS * 32)
             }
         }
         if (wi == 0)
-            step1_out(A, I, s_count, lo, hi, lane, cnt, multi, heavy, list, list_count);
+            step1_out(A, I, s_count, lo, hi, lane, cnt, multi, heavy, list, list_count, wlist,
+                      wlist_count);
         __syncthreads(); // s_* are reset for the next tile row
     }
 }
@@ -310,19 +335,27 @@ __global__ void __launch_bounds__(S1_WIDE_WARPS * 32)
 // single-window walk registers and issue slots).  NW warps per CTA: 8 for
 // the tile rows in order (a heavy one is skipped when heavy[] marks it), or
 // S2_HEAVY_WARPS for the heavy rows of list[] (all warps share the walk).
-template <bool NARROW, int NW, bool SEGS>
-__global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WARPS ? 10 : 1)
+template <bool NARROW, int NW, bool SEGS, bool WIDE = false>
+__global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? (WIDE ? 2 : 5) : NW == S2_SEG_WARPS ? 10 : 1)
     k_sym_rows(DevTiles A, DevTiles B, const int *__restrict__ c_tile_ptr,
                int *__restrict__ c_tile_col, int *__restrict__ c_tile_row,
                uint16_t *__restrict__ c_mask, int *__restrict__ c_tile_cnt,
                int *__restrict__ c_row_cnt, int *__restrict__ c_tr_nnz, int *multi, int *err,
-               const uint8_t *__restrict__ heavy, const int *__restrict__ list)
+               const uint8_t *__restrict__ heavy, const int *__restrict__ list, int wide_slots)
 {
     static_assert(NW == S2_WARPS || NW == S2_HEAVY_WARPS || (SEGS && NW == S2_SEG_WARPS),
                   "CTA shapes");
     constexpr int PPW = (S2_PAIRS + NW - 1) / NW; // row pairs each warp counts
     constexpr int NT = NW * 32;
-    __shared__ CtaSmem2<NW> S;
+    using Smem = CtaSmem2<NW, WIDE>;
+    using Slot = typename Smem::Slot;
+    constexpr int NONE = Smem::NONE;
+    // slots per window and the odd stride of the mask rows
+    const int NSLOT = WIDE ? wide_slots : S2_SLOTS;
+    const int STRIDE = WIDE ? (wide_slots + 2) | 1 : S2_STRIDE;
+    extern __shared__ __align__(16) unsigned char s2_raw[];
+    Smem &S = *reinterpret_cast<Smem *>(s2_raw);
+    uint32_t *const MW = reinterpret_cast<uint32_t *>(s2_raw + (sizeof(Smem) + 15) / 16 * 16);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int I = list != nullptr ? list[blockIdx.x] : (int)blockIdx.x;
     if (I >= A.tilem || (list == nullptr && heavy != nullptr && heavy[I]))
@@ -331,7 +364,7 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WAR
     const int cbeg = __ldg(c_tile_ptr + I), cend = __ldg(c_tile_ptr + I + 1);
     const int nrows = min(TD, A.m - I * TD);
     const int r0 = warp * 2, r1 = r0 + 1; // warp-private walk (NW == S2_WARPS) and counts
-    uint32_t *mw = S.mw + min(warp, S2_PAIRS - 1) * S2_STRIDE;
+    uint32_t *mw = MW + min(warp, S2_PAIRS - 1) * STRIDE;
     int4 *ent = S.ent[warp];
     int run[PPW][2] = {}; // entries so far of rows 2p, 2p + 1, pair p = warp + q * NW
 
@@ -421,17 +454,17 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WAR
             if (lane == 0)
             {
                 int nb = run, we = wend;
-                if (nb > S2_SLOTS)
+                if (nb > NSLOT)
                 {
-                    // cut the window after its S2_SLOTS-th tile column
+                    // cut the window after its NSLOT-th tile column
                     int q = 0;
-                    while (S.wordpre[q] + __popc(S.bitmap[q]) < S2_SLOTS)
+                    while (S.wordpre[q] + __popc(S.bitmap[q]) < NSLOT)
                         ++q;
                     uint32_t bits = S.bitmap[q];
-                    for (int k = S.wordpre[q]; k < S2_SLOTS - 1; ++k)
+                    for (int k = S.wordpre[q]; k < NSLOT - 1; ++k)
                         bits &= bits - 1;
                     we = w + q * 32 + __ffs(bits); // one past the last kept column
-                    nb = S2_SLOTS;
+                    nb = NSLOT;
                 }
                 S.nb = nb;
                 S.wend = we;
@@ -449,8 +482,9 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WAR
                 set_error(err, DERR_SYM_OVERFLOW);
             return;
         }
-        for (int i = tid; i < (wlen + 3) / 4; i += NT)
-            reinterpret_cast<uint32_t *>(S.slot8)[i] = 0xFFFFFFFFu;
+        constexpr int SPW = 4 / sizeof(Slot); // slots per 32-bit word
+        for (int i = tid; i < (wlen + SPW - 1) / SPW; i += NT)
+            reinterpret_cast<uint32_t *>(S.slot)[i] = 0xFFFFFFFFu;
         __syncthreads();
         for (int q = tid; q < nwords; q += NT)
         {
@@ -463,7 +497,7 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WAR
                 const int d = q * 32 + b;
                 if (d < wlen)
                 {
-                    S.slot8[d] = (uint8_t)slot;
+                    S.slot[d] = (Slot)slot;
                     c_tile_col[cbase + slot] = w + d;
                     c_tile_row[cbase + slot] = I;
                 }
@@ -472,7 +506,7 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WAR
         }
         for (int p = warp; p < S2_PAIRS; p += NW) // the window's slots of every row pair
             for (int i = lane; i < nb; i += 32)
-                S.mw[p * S2_STRIDE + i] = 0u;
+                MW[p * STRIDE + i] = 0u;
         __syncthreads();
 
         // ---- masks
@@ -494,9 +528,9 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WAR
                 const int d = (int)(sg >> 16) - w;
                 if ((unsigned)d < (unsigned)wlen)
                 {
-                    const int sl = S.slot8[d];
-                    if (sl != 255)
-                        atomicOr(&S.mw[(r >> 1) * S2_STRIDE + sl],
+                    const int sl = S.slot[d];
+                    if (sl != NONE)
+                        atomicOr(&MW[(r >> 1) * STRIDE + sl],
                                  ((unsigned)sg & 0xFFFFu) << ((r & 1) * 16));
                 }
             };
@@ -603,7 +637,7 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WAR
                                 fs = sb;
                             }
                             sh = (r & 1) * 16;
-                            rb = (r >> 1) * S2_STRIDE;
+                            rb = (r >> 1) * STRIDE;
                         }
                     }
                     int nbat = min(32, total - q0);
@@ -622,9 +656,9 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WAR
                         const int d = (col >> 4) - w;
                         if ((unsigned)d < (unsigned)wlen)
                         {
-                            const int sl = S.slot8[d];
-                            if (sl != 255)
-                                atomicOr(&S.mw[rb + sl], (0x8000u >> (col & 15)) << sh);
+                            const int sl = S.slot[d];
+                            if (sl != NONE)
+                                atomicOr(&MW[rb + sl], (0x8000u >> (col & 15)) << sh);
                         }
                     };
                     for (int j = 0; j < nbat; j += 2)
@@ -720,8 +754,8 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WAR
                         const int d = (col >> 4) - w;
                         if ((unsigned)d < (unsigned)wlen)
                         {
-                            const int sl = S.slot8[d];
-                            if (sl != 255)
+                            const int sl = S.slot[d];
+                            if (sl != NONE)
                                 atomicOr(&mw[sl], (0x8000u >> (col & 15)) << sh);
                         }
                     };
@@ -757,7 +791,7 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WAR
                 int c0 = 0, c1 = 0;
                 for (int i = lane; i < nb; i += 32)
                 {
-                    const uint32_t v = S.mw[p * S2_STRIDE + i];
+                    const uint32_t v = MW[p * STRIDE + i];
                     c0 += __popc(v & 0xFFFFu);
                     c1 += __popc(v >> 16);
                 }
@@ -772,14 +806,14 @@ __global__ void __launch_bounds__(NW * 32, NW == S2_WARPS ? 5 : NW == S2_SEG_WAR
         for (int i = tid; i < nb * S2_PAIRS; i += NT)
         {
             const int sl = i >> 3, p = i & 7;
-            c_mask2[(size_t)(cbase + sl) * S2_PAIRS + p] = S.mw[p * S2_STRIDE + sl];
+            c_mask2[(size_t)(cbase + sl) * S2_PAIRS + p] = MW[p * STRIDE + sl];
         }
         for (int sl = tid; sl < nb; sl += NT)
         {
             int c = 0;
 #pragma unroll
             for (int wv = 0; wv < S2_PAIRS; ++wv)
-                c += __popc(S.mw[wv * S2_STRIDE + sl]);
+                c += __popc(MW[wv * STRIDE + sl]);
             c_tile_cnt[cbase + sl] = c;
         }
         __syncthreads();
@@ -832,25 +866,30 @@ int symbolic_tile_counts(Workspace &ws, const DevTiles &A, const DevTiles &B, Sy
     cudaStream_t s = ws.stream;
     const int tilem = A.tilem;
     // flags: [0] some tile row needs several step-2 windows, [1] several
-    // numeric windows, [2] heavy tile rows listed for the wide step-2 CTA
-    // [3]: tile rows listed for the wide step-1 CTA
-    RTT_CHECK(S.w_flag.ensure(sizeof(int) * 4, s));
-    RTT_CUDA(cudaMemsetAsync(S.w_flag.p, 0, sizeof(int) * 4, s));
+    // numeric windows, [2] heavy tile rows listed for the wide step-2 CTA,
+    // [3] tile rows listed for the wide step-1 CTA, [4] tile rows listed for
+    // the wide-window step-2 CTAs
+    RTT_CHECK(S.w_flag.ensure(sizeof(int) * 8, s));
+    RTT_CUDA(cudaMemsetAsync(S.w_flag.p, 0, sizeof(int) * 8, s));
     RTT_CHECK(S.s2_heavy.ensure((size_t)tilem + 16, s));
     RTT_CHECK(S.s2_list.ensure(sizeof(int) * (size_t)tilem + 16, s));
     RTT_CHECK(S.s1_list.ensure(sizeof(int) * (size_t)tilem + 16, s));
+    const bool wide = S.sym_window_slots >= 0;
+    if (wide)
+        RTT_CHECK(S.s2_wlist.ensure(sizeof(int) * (size_t)tilem + 16, s));
     if (tilem > 0)
     {
         int *flag = S.w_flag.as<int>();
+        int *wlist = wide ? S.s2_wlist.as<int>() : nullptr;
         k_sym_count<<<ceil_div(tilem, SYM_WARPS), SYM_WARPS * 32, 0, s>>>(
             A, B, cnt, flag, S.s2_heavy.as<uint8_t>(), S.s2_list.as<int>(), flag + 2,
-            S.s1_list.as<int>(), flag + 3);
+            S.s1_list.as<int>(), flag + 3, wlist, flag + 4);
         int sms = 0;
         RTT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws.device));
         // persistent CTAs over the wide list (empty: they exit at once)
         k_sym_count_wide<<<std::min(tilem, 2 * sms), S1_WIDE_WARPS * 32, 0, s>>>(
             A, B, cnt, flag, S.s2_heavy.as<uint8_t>(), S.s2_list.as<int>(), flag + 2,
-            S.s1_list.as<int>(), flag + 3);
+            S.s1_list.as<int>(), flag + 3, wlist, flag + 4);
         ws.launches += 2;
     }
     return RTT_OK;
@@ -872,12 +911,15 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
     int *cnt = S.count_tmp.as<int>();
     RTT_CHECK(symbolic_tile_counts(ws, A, B, S, cnt));
     RTT_CHECK(scan_exclusive_int(ws, cnt, S.c_tile_ptr.as<int>(), tilem));
-    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 13, S.w_flag.p, sizeof(int) * 3,
+    RTT_CUDA(cudaMemcpyAsync(ws.h_scalars + 16, S.w_flag.p, sizeof(int) * 5,
                              cudaMemcpyDeviceToHost, s));
     int numtile = 0;
     RTT_CHECK(read_int_checked(ws, S.c_tile_ptr.as<int>() + tilem, &numtile, "symbolic step 1"));
-    const bool sym_multi = ws.h_scalars[13] != 0;
-    const int n_heavy = ws.h_scalars[15];
+    const bool sym_multi = ws.h_scalars[16] != 0;
+    const int n_heavy = ws.h_scalars[18];
+    const int n_wide = S.sym_window_slots >= 0 ? ws.h_scalars[20] : 0;
+    const int wslots = S.sym_window_slots > 0 ? S.sym_window_slots : S2_WIDE_DEFAULT;
+    const int wstride = (wslots + 2) | 1;
     S.numtile = numtile;
     const size_t nt = (size_t)numtile;
     RTT_CHECK(S.c_tile_col.ensure(sizeof(int) * nt, s));
@@ -894,37 +936,70 @@ int symbolic_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Symboli
                       A.csr_col != nullptr;
     if (tilem > 0)
     {
-        if (n_heavy > 0)
-        {
-            // heavy rows: one wide CTA each, on the side stream, alongside
-            // the tile-row CTAs (which skip them)
-            RTT_CUDA(cudaEventRecord(ws.fork_ev, s));
-            RTT_CUDA(cudaStreamWaitEvent(ws.side, ws.fork_ev, 0));
-            auto wide = segs ? k_sym_rows<false, S2_HEAVY_WARPS, true>
-                             : b_sorted ? k_sym_rows<true, S2_HEAVY_WARPS, false>
-                                        : k_sym_rows<false, S2_HEAVY_WARPS, false>;
-            wide<<<n_heavy, S2_HEAVY_WARPS * 32, 0, ws.side>>>(
+        auto go = [&](auto kern, int grid, int threads, size_t smem, cudaStream_t st,
+                      const uint8_t *heavy, const int *list, int slots) -> int {
+            if (smem > 48 * 1024)
+                RTT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem));
+            kern<<<grid, threads, smem, st>>>(
                 A, B, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(), S.c_tile_row.as<int>(),
                 S.c_mask.as<uint16_t>(), S.tile_cnt.as<int>(), S.c_row_cnt.as<int>(),
-                S.c_tr_nnz.as<int>(), S.w_flag.as<int>() + 1, ws.err.as<int>(), nullptr,
-                S.s2_list.as<int>());
-            RTT_CUDA(cudaEventRecord(ws.join_ev, ws.side));
+                S.c_tr_nnz.as<int>(), S.w_flag.as<int>() + 1, ws.err.as<int>(), heavy, list,
+                slots);
             ws.launches++;
+            return RTT_OK;
+        };
+        if (n_heavy > 0 || n_wide > 0)
+        {
+            // heavy rows (one 32-warp CTA each) and rows with many C tiles
+            // (wide-window CTAs) on the side stream, alongside the tile-row
+            // CTAs (which skip them)
+            RTT_CUDA(cudaEventRecord(ws.fork_ev, s));
+            RTT_CUDA(cudaStreamWaitEvent(ws.side, ws.fork_ev, 0));
         }
+        if (n_heavy > 0 && S.sym_window_slots >= 0)
+        {
+            auto hk = segs ? k_sym_rows<false, S2_HEAVY_WARPS, true, true>
+                           : b_sorted ? k_sym_rows<true, S2_HEAVY_WARPS, false, true>
+                                      : k_sym_rows<false, S2_HEAVY_WARPS, false, true>;
+            RTT_CHECK(go(hk, n_heavy, S2_HEAVY_WARPS * 32, smem2_bytes<S2_HEAVY_WARPS, true>(wstride),
+                         ws.side, nullptr, S.s2_list.as<int>(), wslots));
+        }
+        else if (n_heavy > 0)
+        {
+            auto hk = segs ? k_sym_rows<false, S2_HEAVY_WARPS, true>
+                           : b_sorted ? k_sym_rows<true, S2_HEAVY_WARPS, false>
+                                      : k_sym_rows<false, S2_HEAVY_WARPS, false>;
+            RTT_CHECK(go(hk, n_heavy, S2_HEAVY_WARPS * 32,
+                         smem2_bytes<S2_HEAVY_WARPS, false>(S2_STRIDE), ws.side, nullptr,
+                         S.s2_list.as<int>(), 0));
+        }
+        if (n_wide > 0)
+        {
+            auto wk = segs ? k_sym_rows<false, S2_WARPS, true, true>
+                           : b_sorted ? k_sym_rows<true, S2_WARPS, false, true>
+                                      : k_sym_rows<false, S2_WARPS, false, true>;
+            RTT_CHECK(go(wk, n_wide, S2_THREADS, smem2_bytes<S2_WARPS, true>(wstride), ws.side,
+                         nullptr, S.s2_wlist.as<int>(), wslots));
+        }
+        if (n_heavy > 0 || n_wide > 0)
+            RTT_CUDA(cudaEventRecord(ws.join_ev, ws.side));
         // 4-warp CTAs when every tile row fits one window; a tile row with
         // several windows walks its entries once per window, so it keeps 8
         const bool small = segs && !sym_multi;
-        auto kern = small ? k_sym_rows<false, S2_SEG_WARPS, true>
-                          : segs ? k_sym_rows<false, S2_WARPS, true>
-                                 : b_sorted && sym_multi ? k_sym_rows<true, S2_WARPS, false>
-                                                         : k_sym_rows<false, S2_WARPS, false>;
-        kern<<<tilem, small ? S2_SEG_WARPS * 32 : S2_THREADS, 0, s>>>(
-            A, B, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(), S.c_tile_row.as<int>(),
-            S.c_mask.as<uint16_t>(), S.tile_cnt.as<int>(), S.c_row_cnt.as<int>(),
-            S.c_tr_nnz.as<int>(), S.w_flag.as<int>() + 1, ws.err.as<int>(),
-            n_heavy > 0 ? S.s2_heavy.as<uint8_t>() : nullptr, nullptr);
-        ws.launches++;
-        if (n_heavy > 0)
+        const uint8_t *skip = n_heavy > 0 || n_wide > 0 ? S.s2_heavy.as<uint8_t>() : nullptr;
+        if (small)
+            RTT_CHECK(go(k_sym_rows<false, S2_SEG_WARPS, true>, tilem, S2_SEG_WARPS * 32,
+                         smem2_bytes<S2_SEG_WARPS, false>(S2_STRIDE), s, skip, nullptr, 0));
+        else
+        {
+            auto kern = segs ? k_sym_rows<false, S2_WARPS, true>
+                             : b_sorted && sym_multi ? k_sym_rows<true, S2_WARPS, false>
+                                                     : k_sym_rows<false, S2_WARPS, false>;
+            RTT_CHECK(go(kern, tilem, S2_THREADS, smem2_bytes<S2_WARPS, false>(S2_STRIDE), s, skip,
+                         nullptr, 0));
+        }
+        if (n_heavy > 0 || n_wide > 0)
             RTT_CUDA(cudaStreamWaitEvent(s, ws.join_ev, 0));
     }
     // read with nnz(C) below (one synchronisation for both)

@@ -25,7 +25,11 @@ runs, its operands plus the exact upper bound of the symbolic phase for C
 (nnzCub entries of 12 bytes: C cannot have more entries than products) plus
 its row pointer, against a fixed pool.  Operands that a request marks with a
 reuse key stay resident on the device (with A^T for A*A^T requests) and are
-not copied again.
+not copied again.  Each context's own workspace (tile index, symbolic
+structure, the window cursors of the numeric step's persistent workers:
+4 bytes per A entry up to 32,768 per worker CTA) sits outside this
+accounting, so pool_bytes should leave room for it below the device's
+memory.
 
 A batch's product is one CSR with int32 offsets, so a batch also keeps the
 sum of its requests' entry bounds (nnzCub) within 2^31 - 1.  A request whose
@@ -132,6 +136,13 @@ class Server:
         # one (stream, context) per worker, kept across run() calls: their
         # grow-only device buffers stay sized for the traffic seen so far
         self._slots = []
+        self.events: dict = {}   # what the last run() did (counts and seconds)
+
+    def _event(self, name: str, seconds: float = 0.0, n: int = 1):
+        with self.lock:
+            e = self.events.setdefault(name, [0, 0.0])
+            e[0] += n
+            e[1] += seconds
 
     def _slot(self, i):
         torch = self.torch
@@ -236,6 +247,10 @@ class Server:
         r.done = time.perf_counter() - t0
         r.result = (out[0], out[1][:nnz], out[2][:nnz]) if self.keep_results else None
 
+    @staticmethod
+    def _is_oom(e: Exception) -> bool:
+        return (isinstance(e, RttError) and e.status == 4) or "out of memory" in str(e)
+
     def _run_resident(self, st: _Structure, stream, r: Request, t0: float):
         """Numeric step only, on the key's resident structure."""
         with st.lock:
@@ -251,7 +266,9 @@ class Server:
                     # the tiles (and, for A*A, B's values) now come from vals
                     st.vals, st.cur = vals, r.a
                 stream.synchronize()
-            except RttError as e:
+            except (RttError, RuntimeError) as e:
+                if self._is_oom(e):  # the output did not fit beside other work
+                    raise _OutOfMemory() from e
                 r.error, r.done = str(e), time.perf_counter() - t0
                 return
         self._finish(r, out, st.nnz, t0)
@@ -278,9 +295,12 @@ class Server:
             out = self._outputs(r.a.m, nnz)
             ctx.numeric(*out)
             stream.synchronize()
-        except RttError as e:
+        except (RttError, RuntimeError) as e:
+            ctx.trim()
             with self.lock:
                 self._spare.append(ctx)
+            if self._is_oom(e):  # queued again, to run alone in the plain batch path
+                raise _OutOfMemory() from e
             r.error, r.done = str(e), time.perf_counter() - t0
             return
         self._finish(r, out, nnz, t0)
@@ -311,15 +331,27 @@ class Server:
         rest = []
         for r in batch:
             uses = self._count(r)
-            st = self._structure(r)
+            # a request that ran out of memory beside other work runs alone,
+            # in the plain batch path, after every structure was released
+            st = None if r.exclusive else self._structure(r)
+            t1 = time.perf_counter()
             if st is not None:
                 self._run_resident(st, stream, r, t0)
-            elif uses >= 2 and self.max_structures > 0 and r.bound <= self.structure_bytes:
+                self._event("resident_numeric", time.perf_counter() - t1)
+            elif (uses >= 2 and not r.exclusive and self.max_structures > 0
+                  and r.bound <= self.structure_bytes / 4):
+                # a structure is kept only when at least four of its size
+                # fit the structure budget, so that keys are not evicted by
+                # every large newcomer
                 self._build_resident(stream, r, t0)
+                self._event("resident_build", time.perf_counter() - t1)
             else:
                 rest.append(r)
         if rest:
+            t1 = time.perf_counter()
             self._run_batch_plain(ctx, stream, rest, t0)
+            self._event("batch" if len(rest) > 1 else "batch_of_one", time.perf_counter() - t1)
+            self._event("batched_requests", n=len(rest))
 
     def _run_batch_plain(self, ctx, stream, batch, t0):
         try:
@@ -333,7 +365,7 @@ class Server:
         except (RttError, RuntimeError) as e:
             # device memory short while other work is in flight: the worker
             # queues the requests again, to run alone (see run())
-            oom = (isinstance(e, RttError) and e.status == 4) or "out of memory" in str(e)
+            oom = self._is_oom(e)
             if oom and not all(r.exclusive for r in batch):
                 raise _OutOfMemory() from e
             if len(batch) > 1:  # find the failing request(s): one at a time
@@ -357,6 +389,7 @@ class Server:
             self.structures.clear()
             spare, self._spare = self._spare, []
             self.resident.clear()
+        t1 = time.perf_counter()
         for st in structs:
             st.ctx.close()
         for ctx in spare:
@@ -364,6 +397,7 @@ class Server:
         for _, ctx in self._slots:
             ctx.trim()
         self.torch.cuda.empty_cache()
+        self._event("release_memory", time.perf_counter() - t1)
 
     # -- the loop ---------------------------------------------------------
     def run(self, requests: list[Request]) -> dict:
@@ -376,6 +410,7 @@ class Server:
                 r.error, r.done = str(e), r.arrival
                 continue
             r.bound = 12 * r.entries + 4 * (r.a.m + 1) + 12 * r.a.nnz + 4 * (r.a.m + 1)
+        self.events = {}
         pending = deque()
         nxt = 0
         reserved = [0.0]
@@ -442,6 +477,7 @@ class Server:
                         retry = [r for r in batch if r.done < 0]
                         for r in retry:
                             r.exclusive = True
+                        self._event("out_of_memory_requeued", n=len(retry))
                     except Exception as e:  # any other failure finishes the batch's requests
                         now = time.perf_counter() - t0
                         for r in batch:
@@ -461,7 +497,10 @@ class Server:
         for th in threads:
             th.join()
         span = max(r.done for r in requests) if requests else 0.0
-        return summarize(requests, span)
+        out = summarize(requests, span)
+        out["events"] = {k: {"count": v[0], "seconds": round(v[1], 4)}
+                         for k, v in sorted(self.events.items())}
+        return out
 
 
 def serve_plain(requests: list[Request], device: int = 0, config: dict | None = None,

@@ -86,7 +86,8 @@ def test_bad_arguments_rejected_before_device_work():
     assert cfg.dmma_pair_cutoff == 0 and cfg.fused_csr_output == 1  # DMMA opt-in
     assert cfg.split_target == 0  # heavy tile rows split at the default target
     assert cfg.cuda_graphs == 1  # repeated numeric phases replay a CUDA graph
-    assert C.sizeof(R.Config) == 11 * 4
+    assert cfg.sym_window_slots == 0  # wide step-2 windows at their default size
+    assert C.sizeof(R.Config) == 12 * 4
 
 
 def test_generators_shapes():

@@ -280,3 +280,40 @@ def test_persistent_rows_equal_per_row_ctas(case, orc):
     assert np.array_equal(got[0][0], got[1][0]) and np.array_equal(got[0][1], got[1][1])
     assert np.array_equal(got[0][2].view(np.int64), got[1][2].view(np.int64))
     assert_csr_close(*got[1], *orc.spgemm_csr(A, A), f"{case} persistent: ")
+
+
+WIDE_WINDOW_CASES = {
+    "banded": (MANY_WINDOW_CASES["banded"], R.RTT_OP_AB),
+    "rmat_12_aat": (MANY_WINDOW_CASES["rmat_12"], R.RTT_OP_AAT),
+    "banded_20k": (MANY_WINDOW_CASES["banded_20k"], R.RTT_OP_AB),
+    "unsorted_wide": (MANY_WINDOW_CASES["unsorted_wide"], R.RTT_OP_AB),
+    "rmat_14": (MANY_WINDOW_CASES["rmat_14"], R.RTT_OP_AB),
+}
+
+
+@pytest.mark.parametrize("case", list(WIDE_WINDOW_CASES))
+def test_sym_window_slots_equal(case, orc):
+    """Symbolic step 2 of tile rows with more than 254 C tiles in 254-slot
+    windows (-1), in the wide-window CTAs at the default (0), the smallest
+    (255) and the largest (6000) window: bitwise the same C, which matches
+    the oracle."""
+    make, op = WIDE_WINDOW_CASES[case]
+    A = make()
+    got = {}
+    for slots in (-1, 0, 255, 6000):
+        ctx = R.Context(0, dict(sym_window_slots=slots))
+        got[slots] = _run(ctx, A, None, op)
+        ctx.close()
+    ref = got[-1]
+    for slots, g in got.items():
+        assert np.array_equal(ref[0], g[0]) and np.array_equal(ref[1], g[1]), slots
+        assert np.array_equal(ref[2].view(np.int64), g[2].view(np.int64)), slots
+    B = A.transpose() if op == R.RTT_OP_AAT else A
+    assert_csr_close(*ref[:3], *orc.spgemm_csr(A, B), f"{case} windows: ")
+
+
+def test_sym_window_slots_checked():
+    for bad in (-2, 1, 254, 6001):
+        with pytest.raises(R.RttError) as e:
+            R.Context(0, dict(sym_window_slots=bad))
+        assert e.value.status == 1  # RTT_ERR_INVALID_ARGUMENT
