@@ -136,7 +136,13 @@ class ClockSampler:
                 cmd += ["-i", self.uuid]
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(cmd, stdout=self.fh, stderr=subprocess.DEVNULL)
-            time.sleep(0.3)
+            # wait until the sampler has written its first samples: its start-up
+            # (driver queries) then lies before the warm-up steps, not in them
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < 5.0:
+                time.sleep(0.05)
+                if self.path.stat().st_size > 0 and self.path.read_text().count("\n") >= 2:
+                    break
         except Exception:
             self.proc = None
 
@@ -865,7 +871,7 @@ def run_ours(args) -> None:
                      "step_frac": step_frac},
         "stages_ms": {k: statistics.mean(v) for k, v in stage.items()},
         "step_ms": {"min": min(step_ms), "median": statistics.median(step_ms),
-                    "max": max(step_ms)},
+                    "max": max(step_ms), "each": [round(x, 3) for x in step_ms]},
         "dmma_pairs": st["dmma_pairs"], "sparse_pairs": st["sparse_pairs"],
         "host_syncs_per_step": st["host_syncs"],
         "gpu_launches": launches,
