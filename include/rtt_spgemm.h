@@ -353,14 +353,25 @@ typedef struct
     int rows, cols, nnz;
     int active_rows, active_inner; /* rows / columns reached by the traversal */
     int components, levels;        /* components traversed, traversal levels */
-    int accepted;                  /* 1: the proposal has fewer 8x4 A tiles and is the plan;
-                                      0: the plan is the identity */
+    int accepted;                  /* 1: the coarse proposal has fewer 8x4 A tiles and was
+                                      taken; 0: the coarse stage left A's order */
     long long tiles_before;        /* distinct 8x4 tiles of A as given */
-    long long tiles_after;         /* ... under the plan (never more than tiles_before) */
-    long long proposal_tiles;      /* ... under the traversal's proposal */
+    long long tiles_after;         /* ... under the plan (never more than tiles_before,
+                                      except in RTT_REORDER_UNGUARDED) */
+    long long proposal_tiles;      /* ... under the coarse traversal's proposal */
     long long moved_rows, moved_inner;
     int *row_old_to_new, *row_new_to_old;
     int *inner_old_to_new, *inner_new_to_old;
+    int variant;                   /* RTT_REORDER_* the plan was built with */
+    /* Fine passes: windows of 32 rows (4 groups of 8) and of 16 inner
+     * indices (4 groups of 4), and the windows whose packing was committed. */
+    int row_windows, accepted_row_windows;
+    int inner_windows, accepted_inner_windows;
+    long long row_tile_reduction, inner_tile_reduction; /* 8x4 tiles the committed windows removed */
+    /* Fan-out proxy: over the windows' groups (8 rows, or 4 inner indices),
+     * the span of the opposite axis's tiles they touch, before and after. */
+    long long row_fanout_before, row_fanout_after;
+    long long inner_fanout_before, inner_fanout_after;
 } rtt_reorder_plan;
 
 /* Frees the arrays of a hybrid tile matrix and zeroes it (the reference's
@@ -609,16 +620,41 @@ RTT_API int rtt_spgemm_batched_symbolic(rtt_context ctx, int count, const rtt_cs
 RTT_API int rtt_csr_transpose(rtt_context ctx, const rtt_csr_view *A, int *t_row_ptr,
                               int *t_col_idx, double *t_values);
 
+/* Stages of a reorder plan: the reference's DmmaReorderVariant ablations
+ * (src/dmma_reorder.h:63-71, resolved as at :123-137). */
+enum
+{
+    RTT_REORDER_FULL = 0,         /* coarse traversal, then the row and inner fine passes */
+    RTT_REORDER_COARSE = 1,       /* the coarse traversal only */
+    RTT_REORDER_FINE = 2,         /* the fine passes only, from A's own order */
+    RTT_REORDER_COARSE_ROW = 3,   /* coarse, then the row fine pass */
+    RTT_REORDER_COARSE_INNER = 4, /* coarse, then the inner fine pass */
+    RTT_REORDER_UNGUARDED = 5     /* every stage's proposal taken without the exact rule */
+};
+
 /* Replaces build_dmma_reorder_plan (src/dmma_reorder.h:2651) for a device CSR
- * A: a bipartite Cuthill-McKee traversal of A's rows and columns proposes a
- * joint row / K order, committed only if it cuts A's distinct 8x4 tiles (the
- * reference's exact commit rule, :1671-1727), else the identity.  The
- * reference's fine passes that pack 8x4 tensor-core groups are not
- * performed, so its permutations are not reproduced; the commit guarantee
- * is.  With A' = P A Q^T and B' = Q B, C' = A' B' = P C.  Uses the context's
- * tile buffers as scratch (a following product starts with
- * rtt_spgemm_symbolic). */
+ * A, in the stages of RTT_REORDER_FULL:
+ *  1. coarse: a bipartite Cuthill-McKee traversal of A's rows and columns
+ *     proposes a joint row / K order, committed only if it cuts A's distinct
+ *     8x4 tiles (the exact commit rule, :1671-1727);
+ *  2. row fine pass (:2865-2920): in each window of 32 consecutive rows,
+ *     rows are packed into groups of 8 - an anchor (most entries, widest
+ *     fingerprint of 4-column panels, leftmost panel...), then the rows
+ *     adding the fewest new panel bits to the group's fingerprint - and a
+ *     window's packing is committed only if it has fewer 8x4 tiles, or as
+ *     many and a smaller fan-out (:1841-1887);
+ *  3. inner fine pass (:2922-2990): the same over windows of 16 inner
+ *     indices in groups of 4, against 8-row panels.
+ * Every committed step keeps or cuts the tile count, so the plan never has
+ * more 8x4 tiles than A.  The traversal's permutations are this build's
+ * (not BGRF-v1's); the fine passes follow the reference's rules with this
+ * build's fingerprint hash.  With A' = P A Q^T and B' = Q B, C' = A' B' =
+ * P C.  Uses the context's tile buffers as scratch (a following product
+ * starts with rtt_spgemm_symbolic). */
 RTT_API int rtt_reorder_plan_build(rtt_context ctx, const rtt_csr_view *A, rtt_reorder_plan *plan);
+/* The same with the stages of variant (RTT_REORDER_*). */
+RTT_API int rtt_reorder_plan_build_variant(rtt_context ctx, const rtt_csr_view *A, int variant,
+                                           rtt_reorder_plan *plan);
 RTT_API void rtt_reorder_plan_destroy(rtt_reorder_plan *plan);
 
 /* Replaces dump_dmma_reorder_plan (src/dmma_reorder.h:3087-3209): writes

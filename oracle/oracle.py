@@ -347,6 +347,186 @@ def reorder_cm(a, max_components: int = 256):
     return pos[0], pos[1], comps, levels
 
 
+M64 = (1 << 64) - 1
+
+
+def _ro_mix(k: int) -> int:
+    """MurmurHash3's 64-bit finaliser (the fine passes' fingerprint mixer)."""
+    k ^= k >> 33
+    k = (k * 0xFF51AFD7ED558CCD) & M64
+    k ^= k >> 33
+    k = (k * 0xC4CEB9FE1A85EC53) & M64
+    k ^= k >> 33
+    return k
+
+
+def _axis_profile(idx, other_positions, panel):
+    """Profile of one index of an axis: entry count, soft bucket (log2 / 2),
+    panel range and span, the two fingerprint words, their occupancy."""
+    deg = len(other_positions)
+    if deg == 0:
+        return dict(id=idx, degree=0, bucket=-1, occ=0, pmin=-1, pmax=-1, span=0, f0=0, f1=0)
+    f0 = f1 = 0
+    ps = [int(p) // panel for p in other_positions]
+    for p in ps:
+        f0 |= 1 << (_ro_mix(2 * p + 1) & 63)
+        f1 |= 1 << (_ro_mix(2 * p + 2) & 63)
+    lo, hi = min(ps), max(ps)
+    return dict(id=idx, degree=deg, bucket=(deg.bit_length() - 1) // 2,
+                occ=bin(f0).count("1") + bin(f1).count("1"), pmin=lo, pmax=hi,
+                span=hi - lo + 1, f0=f0, f1=f1)
+
+
+def _coarse_key(q):
+    """The coarse profile order (src/dmma_reorder.h:1287-1311), least first."""
+    return (q["degree"] == 0, -q["bucket"], -q["occ"], q["pmin"], q["span"], -q["degree"],
+            q["f0"], q["f1"], q["id"])
+
+
+def _pack_window(profs, group):
+    """Greedy packing of one window (src/dmma_reorder.h:1511-1608): an anchor,
+    the least unused profile in the coarse order, then the unused profile of
+    best score against the group (:1386-1416) until the group is full.
+    Returns the window's old ids in their new order."""
+    from fractions import Fraction
+
+    unused = list(range(len(profs)))
+    out = []
+    while unused:
+        a = min(unused, key=lambda i: _coarse_key(profs[i]))
+        unused.remove(a)
+        A = profs[a]
+        out.append(A["id"])
+        g0, g1, gmin, gmax = A["f0"], A["f1"], A["pmin"], A["pmax"]
+        for _ in range(1, group):
+            if not unused:
+                break
+
+            def score(i):
+                q = profs[i]
+                overlap = bin(g0 & q["f0"]).count("1") + bin(g1 & q["f1"]).count("1")
+                adds = (bin(~g0 & M64 & q["f0"]).count("1") +
+                        bin(~g1 & M64 & q["f1"]).count("1"))
+                uni = max(bin(g0 | q["f0"]).count("1") + bin(g1 | q["f1"]).count("1"), 1)
+                nmin, nmax = gmin, gmax
+                if q["pmin"] >= 0:
+                    nmin = q["pmin"] if gmin < 0 else min(gmin, q["pmin"])
+                    nmax = max(gmax, q["pmax"])
+                cur = 0 if gmin < 0 else gmax - gmin + 1
+                nxt = 0 if nmin < 0 else nmax - nmin + 1
+                return (abs(A["bucket"] - q["bucket"]), adds, -Fraction(overlap, uni), -overlap,
+                        nxt - cur, abs(A["degree"] - q["degree"]), q["id"])
+            b = min(unused, key=score)
+            unused.remove(b)
+            B = profs[b]
+            out.append(B["id"])
+            if B["pmin"] >= 0:
+                gmin = B["pmin"] if gmin < 0 else min(gmin, B["pmin"])
+                gmax = max(gmax, B["pmax"])
+            g0 |= B["f0"]
+            g1 |= B["f1"]
+    return out
+
+
+def reorder_fine_pass(a, row_o2n, col_o2n, rows: bool, guarded: bool = True):
+    """One fine pass of the reorder (src/dmma_reorder.h:2865-2990) on top of
+    the maps: rows in windows of 32 and groups of 8 against 4-column panels,
+    or (rows=False) columns in windows of 16 and groups of 4 against 8-row
+    panels.  A window's packing replaces its order only if it has fewer 8x4
+    tiles, or as many and a smaller fan-out (the sum over its groups of the
+    span of the opposite tiles), :1841-1887.  Returns (row_o2n, col_o2n,
+    stats: windows, accepted, tile reduction, fan-out before / after)."""
+    W, G, panel = (32, 8, 4) if rows else (16, 4, 8)
+    row_o2n = np.asarray(row_o2n, np.int64).copy()
+    col_o2n = np.asarray(col_o2n, np.int64).copy()
+    rp = np.asarray(a.rowptr, np.int64)
+    col = np.asarray(a.col, np.int64)
+    ent_r = np.repeat(np.arange(a.m), np.diff(rp))
+    if rows:
+        count, mine, other = a.m, row_o2n, col_o2n
+        adj = [col[rp[i]:rp[i + 1]] for i in range(a.m)]
+    else:
+        count, mine, other = a.n, col_o2n, row_o2n
+        order = np.lexsort((ent_r, col))
+        tp = np.zeros(a.n + 1, np.int64)
+        tp[1:] = np.cumsum(np.bincount(col, minlength=a.n))
+        adj = [ent_r[order][tp[j]:tp[j + 1]] for j in range(a.n)]
+    n2o = np.empty(count, np.int64)
+    n2o[mine] = np.arange(count)
+    prop = n2o.copy()
+    windows = (count + W - 1) // W
+    for w in range(windows):
+        ids = n2o[w * W:(w + 1) * W]
+        profs = [_axis_profile(int(i), other[adj[i]], panel) for i in ids]
+        prop[w * W:w * W + len(ids)] = _pack_window(profs, G)
+    prop_o2n = np.empty(count, np.int64)
+    prop_o2n[prop] = np.arange(count)
+    # tiles and fan-out per window under the current order and the proposal
+    opp_tiles = (a.n + 3) // 4 if rows else (a.m + 7) // 8
+
+    def per_window(pos_of):
+        tiles = [set() for _ in range(windows)]
+        spans = [[None] * (W // G) for _ in range(windows)]
+        for r, c in zip(ent_r, col):
+            R, Cc = int(row_o2n[r]), int(col_o2n[c])
+            pos = int(pos_of[r]) if rows else int(pos_of[c])
+            opp = Cc // 4 if rows else R // 8
+            w, g = pos // W, (pos % W) // G
+            tiles[w].add((g, opp))
+            s = spans[w][g]
+            spans[w][g] = (opp, opp) if s is None else (min(s[0], opp), max(s[1], opp))
+        fan = [sum(s[1] - s[0] + 1 for s in sp if s is not None) for sp in spans]
+        return [len(t) for t in tiles], fan
+
+    cur_t, cur_f = per_window(mine)
+    prop_t, prop_f = per_window(prop_o2n)
+    new_n2o = n2o.copy()
+    acc = red = fb = fa = 0
+    for w in range(windows):
+        ok = (not guarded) or prop_t[w] < cur_t[w] or (prop_t[w] == cur_t[w] and
+                                                       prop_f[w] < cur_f[w])
+        fb += cur_f[w]
+        fa += prop_f[w] if ok else cur_f[w]
+        if ok:
+            new_n2o[w * W:(w + 1) * W] = prop[w * W:(w + 1) * W]
+            acc += 1
+            red += max(cur_t[w] - prop_t[w], 0)
+    new_o2n = np.empty(count, np.int64)
+    new_o2n[new_n2o] = np.arange(count)
+    if rows:
+        row_o2n = new_o2n
+    else:
+        col_o2n = new_o2n
+    return row_o2n, col_o2n, dict(windows=windows, accepted=acc, reduction=red,
+                                  fanout_before=fb, fanout_after=fa)
+
+
+def reorder_plan(a, variant: int = 0):
+    """Restatement of rtt_reorder_plan_build_variant: the coarse traversal of
+    reorder_cm under the exact commit rule, then the row and inner fine
+    passes, as the variant selects (0 full, 1 coarse, 2 fine, 3 coarse+row,
+    4 coarse+inner, 5 unguarded).  Returns (row_o2n, col_o2n, info)."""
+    coarse = variant != 2
+    row_fine = variant not in (1, 4)
+    inner_fine = variant not in (1, 3)
+    guarded = variant != 5
+    r, c = np.arange(a.m), np.arange(a.n)
+    info = {"tiles_before": tiles_8x4(a), "accepted": 0}
+    info["proposal_tiles"] = info["tiles_before"]
+    if coarse:
+        pr, pc, comps, levels = reorder_cm(a)
+        info.update(components=comps, levels=levels, proposal_tiles=tiles_8x4(a, pr, pc))
+        if (not guarded) or info["proposal_tiles"] < info["tiles_before"]:
+            r, c = pr, pc
+            info["accepted"] = 1
+    if row_fine:
+        r, c, info["row"] = reorder_fine_pass(a, r, c, True, guarded)
+    if inner_fine:
+        r, c, info["inner"] = reorder_fine_pass(a, r, c, False, guarded)
+    info["tiles_after"] = tiles_8x4(a, r, c)
+    return r, c, info
+
+
 def plan_tail_queue(scans, matches, output_nnz, policy: dict, model: dict):
     """Restatement of dmma_plan_tile_tail_queue (src/dmma_tile_tail_queue.h:190-291)
     with the chunk rule of :148-176 in numpy float32 (round-to-nearest, no

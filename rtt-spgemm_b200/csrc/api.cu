@@ -2276,14 +2276,22 @@ int rtt_spgemm_batched_numeric_values(rtt_context c, const double *const *a_valu
 
 int rtt_reorder_plan_build(rtt_context c, const rtt_csr_view *A, rtt_reorder_plan *plan)
 {
+    return rtt_reorder_plan_build_variant(c, A, RTT_REORDER_FULL, plan);
+}
+
+int rtt_reorder_plan_build_variant(rtt_context c, const rtt_csr_view *A, int variant,
+                                   rtt_reorder_plan *plan)
+{
     if (c == nullptr || A == nullptr || plan == nullptr || !view_ok(*A))
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "reorder_plan_build: bad arguments");
+    if (variant < RTT_REORDER_FULL || variant > RTT_REORDER_UNGUARDED)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "reorder_plan_build: unknown variant");
     RTT_CUDA(cudaSetDevice(c->ws.device));
     // the traversal trusts A's structure: validate it like csr2tile does
     RTT_CHECK(map_device_error(csr2tile_device(c->ws, A->rows, A->cols, (int)A->nnz, A->row_ptr,
                                                A->col_idx, A->values, c->A, true, false)));
     c->have_symbolic = false; // the context's A tiles were reused as scratch
-    return rtt::reorder_plan_device(c->ws, *A, plan);
+    return rtt::reorder_plan_device(c->ws, *A, variant, plan);
 }
 
 void rtt_reorder_plan_destroy(rtt_reorder_plan *plan)

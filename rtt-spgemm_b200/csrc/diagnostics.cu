@@ -93,8 +93,10 @@ int rtt_reorder_plan_dump(const rtt_reorder_plan *plan, const char *stem, const 
     f = std::fopen((prefix + "_unified_stats.csv").c_str(), "w");
     if (f == nullptr)
         return fail(RTT_ERR_INVALID_ARGUMENT, "reorder_plan_dump: cannot write stats");
-    std::fprintf(f, "key,value\nalgorithm,%s\n",
-                 plan->accepted ? "bipartite_cm_coarse" : "identity_baseline");
+    static const char *const variants[] = {"full", "coarse", "fine", "coarse-row",
+                                           "coarse-inner", "unguarded"};
+    const int vi = plan->variant >= 0 && plan->variant <= 5 ? plan->variant : 0;
+    std::fprintf(f, "key,value\nalgorithm,bipartite_cm+fine\nvariant,%s\n", variants[vi]);
     std::fprintf(f,
                  "rows,%d\ncols,%d\nnnz,%d\nactive_rows,%d\nactive_inner,%d\n"
                  "moved_rows,%lld\nmoved_inner,%lld\ncoarse_components,%d\ncoarse_levels,%d\n"
@@ -103,7 +105,16 @@ int rtt_reorder_plan_dump(const rtt_reorder_plan *plan, const char *stem, const 
                  plan->rows, plan->cols, plan->nnz, plan->active_rows, plan->active_inner,
                  plan->moved_rows, plan->moved_inner, plan->components, plan->levels,
                  plan->accepted, plan->tiles_before, plan->tiles_after, plan->proposal_tiles,
-                 plan->tiles_before - plan->tiles_after);
+                 plan->accepted ? plan->tiles_before - plan->proposal_tiles : 0ll);
+    std::fprintf(f,
+                 "row_windows,%d\naccepted_row_windows,%d\nrow_tile_reduction,%lld\n"
+                 "row_fanout_before,%lld\nrow_fanout_after,%lld\n"
+                 "inner_windows,%d\naccepted_inner_windows,%d\ninner_tile_reduction,%lld\n"
+                 "inner_fanout_before,%lld\ninner_fanout_after,%lld\n",
+                 plan->row_windows, plan->accepted_row_windows, plan->row_tile_reduction,
+                 plan->row_fanout_before, plan->row_fanout_after, plan->inner_windows,
+                 plan->accepted_inner_windows, plan->inner_tile_reduction,
+                 plan->inner_fanout_before, plan->inner_fanout_after);
     if (std::fclose(f) != 0)
         return fail(RTT_ERR_INVALID_ARGUMENT, "reorder_plan_dump: write failed");
     if (!dump_matrix)

@@ -288,7 +288,7 @@ int build_tile_csc(Workspace &ws, TileBufs &t);
 int tiles_to_col_major(Workspace &ws, const TileBufs &rowmajor, TileBufs &out);
 // CSR transpose on the device
 // bipartite Cuthill-McKee reorder plan of a device CSR (host maps malloc'd)
-int reorder_plan_device(Workspace &ws, const rtt_csr_view &A, rtt_reorder_plan *plan);
+int reorder_plan_device(Workspace &ws, const rtt_csr_view &A, int variant, rtt_reorder_plan *plan);
 // device CSR with permuted rows and remapped (then sorted) columns
 int csr_permute_device(Workspace &ws, const rtt_csr_view &A, const int *row_new_to_old,
                        const int *col_old_to_new, int *out_rp, int *out_col, double *out_val);

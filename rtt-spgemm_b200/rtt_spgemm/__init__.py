@@ -28,6 +28,8 @@ import numpy as np
 
 from . import generators
 from ._abi import (EXPORTS, LIB_PATH, RTT_OP_AAT, RTT_OP_AB, RTT_SUPER16_A8X4, RTT_SUPER16_B4X8,
+                   RTT_REORDER_FULL, RTT_REORDER_COARSE, RTT_REORDER_FINE, RTT_REORDER_COARSE_ROW,
+                   RTT_REORDER_COARSE_INNER, RTT_REORDER_UNGUARDED,
                    Super16Index, Config, CsrView, EarlySplitPlan,
                    HybridTiles, ReorderPlan, RttError, SMatrix, Stats, TailCostModel, TailPlan,
                    TailPolicy, build, check, lib)
@@ -39,7 +41,9 @@ __all__ = ["CSR", "Context", "RttError", "build", "csr2tile_col_major", "csr2til
            "tile2csr_device_noalloc", "csr_to_hybrid_tiles", "super16_index", "plan_tail_queue",
            "plan_early_split", "early_split_policy_default",
            "TAIL_POLICY_DEFAULT", "TAIL_MODEL_DEFAULT", "spgemm_batched",
-           "EXPORTS", "LIB_PATH", "RTT_OP_AB", "RTT_OP_AAT"]
+           "EXPORTS", "LIB_PATH", "RTT_OP_AB", "RTT_OP_AAT", "RTT_REORDER_FULL",
+           "RTT_REORDER_COARSE", "RTT_REORDER_FINE", "RTT_REORDER_COARSE_ROW",
+           "RTT_REORDER_COARSE_INNER", "RTT_REORDER_UNGUARDED"]
 
 TD = 16
 
@@ -531,12 +535,14 @@ class Context:
             lib().rtt_reorder_plan_destroy(C.byref(p))
         return out
 
-    def reorder_plan(self, a) -> dict:
+    def reorder_plan(self, a, variant: int = 0) -> dict:
         """Row / inner reorder plan of a device CSR tuple (rtt_reorder_plan_build,
-        the reference's build_dmma_reorder_plan): counters and numpy maps."""
+        the reference's build_dmma_reorder_plan), with the stages of variant
+        (RTT_REORDER_*; 0 = all): counters and numpy maps."""
         v = self._view(*a)
         p = ReorderPlan()
-        check(lib().rtt_reorder_plan_build(self.handle, C.byref(v), C.byref(p)))
+        check(lib().rtt_reorder_plan_build_variant(self.handle, C.byref(v), int(variant),
+                                                   C.byref(p)))
         out = {k: getattr(p, k) for k, t in ReorderPlan._fields_ if t is not C.POINTER(C.c_int)}
         for k, n in (("row_old_to_new", p.rows), ("row_new_to_old", p.rows),
                      ("inner_old_to_new", p.cols), ("inner_new_to_old", p.cols)):

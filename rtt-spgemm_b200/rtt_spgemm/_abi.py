@@ -17,6 +17,9 @@ LIB_PATH = PKG_ROOT / "librtt_spgemm.so"
 RTT_OK = 0
 RTT_OP_AB = 0
 RTT_OP_AAT = 1
+# reorder plan stages (rtt_reorder_plan_build_variant)
+RTT_REORDER_FULL, RTT_REORDER_COARSE, RTT_REORDER_FINE = 0, 1, 2
+RTT_REORDER_COARSE_ROW, RTT_REORDER_COARSE_INNER, RTT_REORDER_UNGUARDED = 3, 4, 5
 STATUS = {
     0: "RTT_OK", 1: "RTT_ERR_INVALID_ARGUMENT", 2: "RTT_ERR_INVALID_CSR",
     3: "RTT_ERR_SHAPE_MISMATCH", 4: "RTT_ERR_OUT_OF_MEMORY", 5: "RTT_ERR_CUDA",
@@ -35,7 +38,8 @@ EXPORTS = [
     "rtt_tile2csr_device_noalloc", "rtt_csr_to_hybrid_tiles", "rtt_hybrid_tiles_destroy",
     "rtt_plan_tail_queue", "rtt_spgemm_batched_symbolic", "rtt_spgemm_batched_numeric",
     "rtt_csr_transpose", "rtt_early_split_policy_default", "rtt_plan_early_split",
-    "rtt_reorder_plan_build", "rtt_reorder_plan_destroy", "rtt_csr_permute",
+    "rtt_reorder_plan_build", "rtt_reorder_plan_build_variant", "rtt_reorder_plan_destroy",
+    "rtt_csr_permute",
     "rtt_spgemm_numeric_values", "rtt_super16_index_build", "rtt_super16_index_destroy",
     "rtt_spgemm_batched_numeric_values", "rtt_spgemm_symbolic64", "rtt_spgemm_numeric64",
     "rtt_spgemm_update_b", "rtt_mmio_read", "rtt_reorder_plan_dump", "rtt_tile_heatmap",
@@ -145,7 +149,12 @@ class ReorderPlan(C.Structure):
         (k, C.c_longlong) for k in ("tiles_before", "tiles_after", "proposal_tiles",
                                     "moved_rows", "moved_inner")] + [
         (k, C.POINTER(C.c_int)) for k in ("row_old_to_new", "row_new_to_old", "inner_old_to_new",
-                                          "inner_new_to_old")]
+                                          "inner_new_to_old")] + [
+        (k, C.c_int) for k in ("variant", "row_windows", "accepted_row_windows",
+                               "inner_windows", "accepted_inner_windows")] + [
+        (k, C.c_longlong) for k in ("row_tile_reduction", "inner_tile_reduction",
+                                    "row_fanout_before", "row_fanout_after",
+                                    "inner_fanout_before", "inner_fanout_after")]
 
 
 class Stats(C.Structure):
@@ -241,6 +250,7 @@ def lib() -> C.CDLL:
     L.rtt_spgemm_numeric_values.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.c_void_p]
     L.rtt_reorder_plan_build.argtypes = [C.c_void_p, P(CsrView), P(ReorderPlan)]
+    L.rtt_reorder_plan_build_variant.argtypes = [C.c_void_p, P(CsrView), C.c_int, P(ReorderPlan)]
     L.rtt_reorder_plan_destroy.argtypes = [P(ReorderPlan)]
     L.rtt_reorder_plan_destroy.restype = None
     L.rtt_csr_permute.argtypes = [C.c_void_p, P(CsrView), C.c_void_p, C.c_void_p, C.c_void_p,

@@ -1,9 +1,9 @@
 """GPU parity of the reorder (rtt_reorder_plan_build, the reference's
-build_dmma_reorder_plan reduced to its traversal and exact commit rule) and of
-rtt_csr_permute: the maps equal the CPU restatement's, the tile counts equal
-the oracle's, a plan never has more 8x4 A tiles than the identity, and a
-product through reordered operands gives the same C once its rows are
-restored."""
+build_dmma_reorder_plan: coarse traversal under the exact commit rule, then
+the row and inner fine passes) and of rtt_csr_permute: the maps and counters
+of every variant equal the CPU restatement's, the tile counts equal the
+oracle's, a guarded plan never has more 8x4 A tiles than A, and a product
+through reordered operands gives the same C once its rows are restored."""
 from __future__ import annotations
 
 import numpy as np
@@ -44,9 +44,11 @@ CASES = {
 
 @pytest.mark.parametrize("case", list(CASES))
 def test_reorder_plan_matches_restatement(case):
+    """The coarse stage alone (RTT_REORDER_COARSE): the traversal's maps and
+    the commit rule against the CPU restatement."""
     A = CASES[case]()
     ctx = R.Context(0)
-    plan = ctx.reorder_plan(_dev(A))
+    plan = ctx.reorder_plan(_dev(A), R.RTT_REORDER_COARSE)
     ctx.close()
     r, c, comps, levels = O.reorder_cm(A)
     assert plan["tiles_before"] == O.tiles_8x4(A)
@@ -63,6 +65,51 @@ def test_reorder_plan_matches_restatement(case):
         assert np.array_equal(plan["inner_old_to_new"], np.arange(A.n))
     assert np.array_equal(plan["row_new_to_old"][plan["row_old_to_new"]], np.arange(A.m))
     assert np.array_equal(plan["inner_new_to_old"][plan["inner_old_to_new"]], np.arange(A.n))
+
+
+@pytest.mark.parametrize("variant", [R.RTT_REORDER_FULL, R.RTT_REORDER_FINE,
+                                     R.RTT_REORDER_COARSE_ROW, R.RTT_REORDER_COARSE_INNER,
+                                     R.RTT_REORDER_UNGUARDED])
+@pytest.mark.parametrize("case", list(CASES))
+def test_reorder_fine_passes_match_restatement(case, variant):
+    """Every stage of every variant - the coarse traversal under the commit
+    rule, the row pass (windows of 32, groups of 8) and the inner pass
+    (windows of 16, groups of 4), each window committed by its exact tile
+    count and fan-out - gives the maps and counters of the CPU restatement
+    (oracle.reorder_plan), bit for bit."""
+    A = CASES[case]()
+    ctx = R.Context(0)
+    plan = ctx.reorder_plan(_dev(A), variant)
+    ctx.close()
+    r, c, info = O.reorder_plan(A, variant)
+    assert np.array_equal(plan["row_old_to_new"], r)
+    assert np.array_equal(plan["inner_old_to_new"], c)
+    assert np.array_equal(plan["row_new_to_old"][plan["row_old_to_new"]], np.arange(A.m))
+    assert np.array_equal(plan["inner_new_to_old"][plan["inner_old_to_new"]], np.arange(A.n))
+    assert plan["variant"] == variant
+    assert plan["tiles_before"] == info["tiles_before"]
+    assert plan["tiles_after"] == info["tiles_after"] == O.tiles_8x4(A, r, c)
+    assert plan["accepted"] == info["accepted"]
+    for axis in ("row", "inner"):
+        if axis in info:
+            st = info[axis]
+            assert plan[f"{axis}_windows"] == st["windows"]
+            assert plan[f"accepted_{axis}_windows"] == st["accepted"]
+            assert plan[f"{axis}_tile_reduction"] == st["reduction"]
+            assert plan[f"{axis}_fanout_before"] == st["fanout_before"]
+            assert plan[f"{axis}_fanout_after"] == st["fanout_after"]
+        else:
+            assert plan[f"{axis}_windows"] == 0
+    if variant != R.RTT_REORDER_UNGUARDED:
+        assert plan["tiles_after"] <= plan["tiles_before"]
+
+
+def test_reorder_variant_checked():
+    ctx = R.Context(0)
+    with pytest.raises(R.RttError) as e:
+        ctx.reorder_plan(_dev(G.laplacian_2d(8)), 6)
+    assert e.value.status == 1
+    ctx.close()
 
 
 @pytest.mark.parametrize("case", ["scrambled_band", "scrambled_band_2k", "rmat_10"])
