@@ -10,7 +10,12 @@ The knobs (rtt_config fields):
   streamed through a TMA stage ring (the one that also runs DMMA pairs);
 * ``split_target`` - the tile-row bucket threshold of the early split: tile
   rows whose windows walk more products than this are cut into window tasks
-  (0: the library default, negative: never).
+  (0: the library default, negative: never);
+* ``sym_window_slots`` - the tile-row bucket threshold of symbolic step 2:
+  tile rows with more C tiles than 254 run in wide-window CTAs of this many
+  slots (0: 2045, -1: never);
+* ``persistent_rows`` - tile-row CTAs as one resident wave over a device
+  queue instead of one CTA per tile row.
 
 A shape class is the operation (A*A, A*A^T, A*B), and the base-2 buckets of
 the row count, the mean entries per row and the row-length skew (longest row
@@ -38,6 +43,9 @@ CANDIDATES = [
     {"dmma_pair_cutoff": 0, "b_staging": 0, "split_target": -1},
     {"dmma_pair_cutoff": 3072, "b_staging": 0, "split_target": 0},
     {"dmma_pair_cutoff": 0, "b_staging": 1, "split_target": 0},
+    {"dmma_pair_cutoff": 0, "b_staging": 0, "split_target": 0, "sym_window_slots": -1},
+    {"dmma_pair_cutoff": 0, "b_staging": 0, "split_target": 0, "sym_window_slots": 4093},
+    {"dmma_pair_cutoff": 0, "b_staging": 0, "split_target": 0, "persistent_rows": 1},
 ]
 
 OPS = {0: "AB", 1: "AAT"}
