@@ -31,6 +31,14 @@ structure, the window cursors of the numeric step's persistent workers:
 accounting, so pool_bytes should leave room for it below the device's
 memory.
 
+A request whose bound exceeds a quarter of the pool (exclusive_share) runs
+alone once nothing else is in flight, and a batch of one request runs
+through the plain path (no block-diagonal assembly); a batch that runs out
+of device memory beside other work is queued again, its requests to run
+alone, and a request alone that still runs out of memory releases what the
+server keeps (resident structures and operands, grown buffers) and tries
+once more.
+
 A batch's product is one CSR with int32 offsets, so a batch also keeps the
 sum of its requests' entry bounds (nnzCub) within 2^31 - 1.  A request whose
 own result cannot be represented, or any other failing request, is finished
@@ -112,12 +120,15 @@ class _Structure:
 class Server:
     def __init__(self, device: int = 0, pool_bytes: float = 120e9, max_batch: int = 512,
                  workers: int = 2, config: dict | None = None, keep_results: bool = True,
-                 max_structures: int = 16, structure_bytes: float | None = None):
+                 max_structures: int = 16, structure_bytes: float | None = None,
+                 exclusive_share: float = 0.25):
         import torch
 
         self.torch = torch
         self.device = torch.device("cuda", device)
         self.pool = float(pool_bytes)
+        # a request whose bound exceeds this share of the pool runs alone
+        self.exclusive_share = exclusive_share
         self.max_batch = max_batch
         self.config = config
         self.nworkers = workers
@@ -183,10 +194,12 @@ class Server:
               t.from_numpy(a.val).to(d, non_blocking=True))
         return va
 
-    def _operands(self, r: Request, ctx: Context):
+    def _operands(self, r: Request, ctx: Context, need_at: bool = True):
         """Device operands of a request.  A reuse key names a structure: a
         request whose host operand is another object than the resident one
-        brings new values, which replace the resident values (and A^T)."""
+        brings new values, which replace the resident values (and A^T).
+        need_at=False leaves A^T out (the single-request path multiplies
+        with RTT_OP_AAT)."""
         with self.lock:
             hit = self.resident.get(r.key) if r.key is not None else None
             if hit is not None:
@@ -200,7 +213,7 @@ class Server:
         elif hit is None:
             hit = (self._upload(r.a, ctx), None, r.a)
         a, at, src = hit
-        if r.op == "AAT" and at is None:
+        if r.op == "AAT" and at is None and need_at:
             at = ctx.transpose(a)
         if r.key is not None:
             with self.lock:
@@ -353,7 +366,30 @@ class Server:
             self._event("batch" if len(rest) > 1 else "batch_of_one", time.perf_counter() - t1)
             self._event("batched_requests", n=len(rest))
 
+    def _run_single(self, ctx, stream, r: Request, t0: float, retried: bool = False):
+        """One request through the plain path on the worker's context (no
+        block-diagonal assembly, A*A^T as RTT_OP_AAT)."""
+        try:
+            a, _ = self._operands(r, ctx, need_at=False)
+            nnz, _ = ctx.symbolic(a, None, 1 if r.op == "AAT" else 0)
+            out = self._outputs(r.a.m, nnz)
+            ctx.numeric(*out)
+            stream.synchronize()
+        except (RttError, RuntimeError) as e:
+            if self._is_oom(e):
+                if not r.exclusive:  # queued again, to run alone
+                    raise _OutOfMemory() from e
+                if not retried:  # alone and still short: release what is kept, once
+                    out = None
+                    self._release_memory()
+                    return self._run_single(ctx, stream, r, t0, True)
+            r.error, r.done = str(e), time.perf_counter() - t0
+            return
+        self._finish(r, out, nnz, t0)
+
     def _run_batch_plain(self, ctx, stream, batch, t0):
+        if len(batch) == 1:
+            return self._run_single(ctx, stream, batch[0], t0)
         try:
             As, Bs = [], []
             for r in batch:
@@ -410,6 +446,9 @@ class Server:
                 r.error, r.done = str(e), r.arrival
                 continue
             r.bound = 12 * r.entries + 4 * (r.a.m + 1) + 12 * r.a.nnz + 4 * (r.a.m + 1)
+            # a product this large would crowd the others out of the pool:
+            # it runs alone, when nothing else is in flight
+            r.exclusive = r.bound > self.pool * self.exclusive_share
         self.events = {}
         pending = deque()
         nxt = 0
@@ -470,8 +509,6 @@ class Server:
                             batch, need = take_batch()
                     retry = []
                     try:
-                        if batch[0].exclusive:
-                            self._release_memory()
                         self._run_batch(ctx, stream, batch, t0)
                     except _OutOfMemory:
                         retry = [r for r in batch if r.done < 0]
