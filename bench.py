@@ -430,14 +430,17 @@ def run_served(args) -> None:
         # the same requests (same matrices, arrivals and keys), results cleared
         return [serve.Request(r.a, r.op, r.key, r.arrival) for r in stream0]
 
+    # every run is the stream once: its 30 % of requests that repeat an
+    # earlier A reuse that request's operands (and, from a key's third use
+    # on, its tile structure); nothing carries over from one run to the next
     server = serve.Server(pool_bytes=120e9, keep_results=False)
     server.run(fresh())
-    server.resident.clear()
+    server.reset_reuse()
     settle()
     served_runs = []
     for _ in range(max(1, args.serve_repeats)):
         served_runs.append(server.run(fresh()))
-        server.resident.clear()
+        server.reset_reuse()
         settle()
     server.close()
     settle()

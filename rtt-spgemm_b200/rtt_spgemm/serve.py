@@ -165,6 +165,23 @@ class Server:
                 self._slots.append((stream, ctx))
             return self._slots[i]
 
+    def reset_reuse(self):
+        """Forget every reuse key: use counts, resident operands and resident
+        structures (their contexts are kept as spares, up to four).  A new
+        request stream starts from here."""
+        with self.lock:
+            structs = list(self.structures.values())
+            self.structures.clear()
+            self.resident.clear()
+            self.uses.clear()
+        for st in structs:
+            with st.lock:
+                with self.lock:
+                    if len(self._spare) < 4:
+                        self._spare.append(st.ctx)
+                        continue
+                st.ctx.close()
+
     def close(self):
         """Release the workers' contexts, the resident structures and operands."""
         for _, ctx in self._slots:
