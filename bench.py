@@ -292,7 +292,7 @@ def run_batched(args) -> None:
     ctx = R.Context(0, {"stage_timing": 0, "dmma_pair_cutoff": args.dmma_cutoff,
                         "b_staging": 1 if args.staging else 0,
                         "persistent_rows": 1 if args.persistent_rows else 0,
-                "sym_window_slots": args.sym_window_slots})
+                "sym_window_slots": args.sym_window_slots, "leaf_dmma": 1 if args.leaf_dmma else 0})
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
 
@@ -328,7 +328,7 @@ def run_batched(args) -> None:
     base_cfg = {"stage_timing": 0, "dmma_pair_cutoff": args.dmma_cutoff,
                 "b_staging": 1 if args.staging else 0,
                 "persistent_rows": 1 if args.persistent_rows else 0,
-                "sym_window_slots": args.sym_window_slots}
+                "sym_window_slots": args.sym_window_slots, "leaf_dmma": 1 if args.leaf_dmma else 0}
     ms_b = timed(batched)
     ctx.configure(base_cfg)  # the plain arm keeps the given configuration
     ms_p = timed(plain)
@@ -567,7 +567,7 @@ def run_wide(args) -> None:
     cub = nnz_cub(A, True)
     flops = 2.0 * cub
     stream = torch.cuda.current_stream(dev)
-    ctx = R.Context(0, {"stage_timing": 0, "sym_window_slots": args.sym_window_slots})
+    ctx = R.Context(0, {"stage_timing": 0, "sym_window_slots": args.sym_window_slots, "leaf_dmma": 1 if args.leaf_dmma else 0})
     ctx.set_stream(stream.cuda_stream)
     a_view = (A.m, A.n, torch.from_numpy(A.rowptr).to(dev), torch.from_numpy(A.col).to(dev),
               torch.from_numpy(A.val).to(dev))
@@ -684,7 +684,7 @@ def run_ours(args) -> None:
                             "b_staging": 1 if args.staging else 0,
                             "segment_walk": 1 if args.segment_walk else 0,
                             "persistent_rows": 1 if args.persistent_rows else 0,
-                "sym_window_slots": args.sym_window_slots})
+                "sym_window_slots": args.sym_window_slots, "leaf_dmma": 1 if args.leaf_dmma else 0})
     ctx.set_stream(stream.cuda_stream)
     rp = torch.from_numpy(A.rowptr).to(dev)
     ci = torch.from_numpy(A.col).to(dev)
@@ -763,7 +763,8 @@ def run_ours(args) -> None:
     abytes = alg_bytes(A.m, A.nnz, A.nnz, nnz_c)
     num_ms = statistics.mean(stage["numeric_kernel_ms"])
     achieved = abytes / (num_ms * 1e-3) / 1e9
-    traffic = None if args.staging or args.unfused else load_traffic(args.workload)
+    traffic = (None if args.staging or args.unfused or args.leaf_dmma
+               else load_traffic(args.workload))
 
     # repeated product with the same structure and new values (values-only
     # update, rtt_spgemm_numeric_values): no csr2tile counting, no symbolic
@@ -869,6 +870,8 @@ def run_ours(args) -> None:
                    "b_staging": bool(args.staging)},
         "roofline": {"bound": "hbm",
                      "kernel": ("k_numeric_rows (TMA-staged numeric + fused tile2csr)" if args.staging
+                                else "k_numeric_leaf (FP64 DMMA from hybrid leaves; the leaf "
+                                     "build and tile2csr outside the kernel time)" if args.leaf_dmma
                                 else "k_numeric_flat (numeric + fused tile2csr)"),
                      "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
@@ -925,6 +928,8 @@ def main() -> None:
                          "(0 = default, -1 = off)")
     ap.add_argument("--persistent-rows", action="store_true",
                     help="numeric step: one resident wave of tile-row CTAs over a device queue")
+    ap.add_argument("--leaf-dmma", action="store_true",
+                    help="numeric step: FP64 DMMA straight from 8x4 / 4x8 hybrid leaves")
     ap.add_argument("--segment-walk", action="store_true",
                     help="numeric step: walk B's row segments where that applies")
     ap.add_argument("--staging", action="store_true",

@@ -476,6 +476,14 @@ typedef struct
      * tiles (0 = the default, 2045; 255..6000 to choose; -1 = off, every
      * row in windows of 254).  Every setting gives bitwise the same C. */
     int sym_window_slots;
+    /* Numeric step on the FP64 tensor cores straight from hybrid leaf tiles
+     * when nonzero (the reference's dmma_numeric_kernel path): A and B are
+     * cut into 8x4 / 4x8 leaves (dense when they hold >= 24 of 32 entries),
+     * each 8x8 quadrant of a C tile is a sum of mma.sync.m8n8k4.f64 over
+     * the matching K blocks, and tile2csr writes the CSR.  Same structure;
+     * values within the FP64 bound (other summation order).  Default 0: the
+     * scalar kernel is faster on every workload measured. */
+    int leaf_dmma;
 } rtt_config;
 
 RTT_API void rtt_config_default(rtt_config *config);

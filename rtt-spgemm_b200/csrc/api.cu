@@ -101,6 +101,8 @@ struct rtt_context_s
     rtt::DevTiles w_dA{}, w_dB{};
     bool have_sym64 = false;
     long long w_nnz = 0;
+    // hybrid leaves of A and B for the leaf DMMA numeric step (leaf_dmma)
+    rtt::HybridDev leaf_a, leaf_b;
 };
 
 namespace
@@ -648,6 +650,13 @@ void numeric_key(rtt_context c, std::vector<long long> &k)
         k.push_back(v);
 }
 
+// The numeric phase can be captured: CSR written by the numeric kernel, and
+// no leaf DMMA step (its leaf build reads sizes on the host).
+bool graphs_allowed(rtt_context c)
+{
+    return c->cfg.fused_csr_output != 0 && c->cfg.leaf_dmma == 0;
+}
+
 // Runs enqueue (device work on ws.stream, with no host read and no sync)
 // either eagerly or as a CUDA graph: the second call in a row with the same
 // key captures it (on a private stream: the legacy default stream cannot
@@ -752,7 +761,9 @@ int numeric_enqueue(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_val
         nc.ev_begin = ws.ev[3];
         nc.ev_end = ws.ev[4];
     }
-    const bool fused = c->cfg.fused_csr_output != 0;
+    // the leaf DMMA step writes C's tiles; tile2csr makes the CSR
+    const bool leaf = c->cfg.leaf_dmma != 0;
+    const bool fused = c->cfg.fused_csr_output != 0 && !leaf;
     nc.write_tiles = !fused || c->cfg.keep_tiles != 0;
     if (fused)
     {
@@ -773,7 +784,10 @@ int numeric_enqueue(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_val
     dA.csr_rowptr = c->a_rp;
     dA.csr_col = c->a_ci;
     dA.csr_val = c->a_va;
-    RTT_CHECK(numeric_select_device(ws, dA, dB, c->S, nc));
+    if (leaf)
+        RTT_CHECK(numeric_leaf_device(ws, dA, dB, c->leaf_a, c->leaf_b, c->S, nc));
+    else
+        RTT_CHECK(numeric_select_device(ws, dA, dB, c->S, nc));
     if (!fused)
     {
         SymbolicOut &S = c->S;
@@ -1001,6 +1015,8 @@ void rtt_context_destroy(rtt_context c)
     c->A.release();
     c->B.release();
     c->S.release();
+    c->leaf_a.release();
+    c->leaf_b.release();
     for (rtt::DevBuf *b : own_buffers(c))
         b->release();
     for (int b = 0; b < 2; ++b)
@@ -1033,6 +1049,8 @@ int rtt_context_trim(rtt_context c)
     c->A.release();
     c->B.release();
     c->S.release();
+    c->leaf_a.release();
+    c->leaf_b.release();
     for (rtt::DevBuf *b : own_buffers(c))
         b->release();
     c->ws.scan_tmp.release();
@@ -1070,6 +1088,8 @@ int rtt_context_set_config(rtt_context c, const rtt_config *config)
         config->segment_walk > 1 || config->persistent_rows < 0 || config->persistent_rows > 1)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT,
                          "chunk_tiles, chunk_nnz >= 0, segment_walk and persistent_rows 0 or 1");
+    if (config->leaf_dmma < 0 || config->leaf_dmma > 1)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "leaf_dmma must be 0 or 1");
     if (config->sym_window_slots < -1 ||
         (config->sym_window_slots > 0 &&
          (config->sym_window_slots < 255 || config->sym_window_slots > 6000)))
@@ -1798,7 +1818,7 @@ int rtt_spgemm_numeric_values(rtt_context c, const double *a_values, const doubl
     RTT_CHECK(effective_cutoff(c, c->A.view(), TB.view(), &cutoff));
     std::vector<long long> key{1, as_key(a_values), as_key(b_values), as_key(c_row_ptr),
                                as_key(c_col_idx), as_key(c_values)};
-    RTT_CHECK(run_phase(c, 1, key, c->cfg.fused_csr_output != 0, [&]() -> int {
+    RTT_CHECK(run_phase(c, 1, key, graphs_allowed(c), [&]() -> int {
         // A's tiles take the new values (same structure, same tile order);
         // without tile arrays the numeric step reads the new values directly
         if (c->A.payload)
@@ -1835,7 +1855,7 @@ int rtt_spgemm_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_
     const TileBufs &TB = c->b_alias ? c->A : c->B;
     RTT_CHECK(effective_cutoff(c, c->A.view(), TB.view(), &cutoff));
     std::vector<long long> key{0, as_key(c_row_ptr), as_key(c_col_idx), as_key(c_values)};
-    RTT_CHECK(run_phase(c, 0, key, c->cfg.fused_csr_output != 0, [&]() -> int {
+    RTT_CHECK(run_phase(c, 0, key, graphs_allowed(c), [&]() -> int {
         return numeric_enqueue(c, c_row_ptr, c_col_idx, c_values, cutoff);
     }));
     return numeric_finish(c);
@@ -2189,7 +2209,7 @@ int rtt_spgemm_batched_numeric(rtt_context c, int *c_row_ptr, int *c_col_idx, do
                                (long long)c->bat_rowoff_off,
                                (long long)c->bat_sec_off,
                                (long long)c->bat_colsub_off};
-    RTT_CHECK(run_phase(c, 2, key, c->cfg.fused_csr_output != 0, [&]() -> int {
+    RTT_CHECK(run_phase(c, 2, key, graphs_allowed(c), [&]() -> int {
         RTT_CHECK(numeric_enqueue(c, c->bat_big_rp.as<int>(), c_col_idx, c_values, cutoff));
         const int *meta_d = c->bat_meta.as<int>();
         return batch_split_device(c->ws, c->bat_count, c->bat_rows, meta_d + c->bat_rowoff_off,
@@ -2249,7 +2269,7 @@ int rtt_spgemm_batched_numeric_values(rtt_context c, const double *const *a_valu
     RTT_CHECK(effective_cutoff(c, c->A.view(), TB.view(), &cutoff));
     std::vector<long long> key{3, as_key(c_row_ptr), as_key(c_col_idx), as_key(c_values),
                                (long long)with_b};
-    RTT_CHECK(run_phase(c, 3, key, c->cfg.fused_csr_output != 0, [&]() -> int {
+    RTT_CHECK(run_phase(c, 3, key, graphs_allowed(c), [&]() -> int {
         // the instances' values into the block diagonal, then its tiles
         RTT_CHECK(batch_values_device(ws, n, c->bat_a_max, a_tab, a_off,
                                       c->bat_a_val.as<double>()));

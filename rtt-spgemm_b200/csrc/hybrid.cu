@@ -222,46 +222,39 @@ int to_host(T **out, const T *d, size_t n, cudaStream_t s)
 
 } // namespace
 
-int csr_to_hybrid_host(Workspace &ws, const SMatrix *M, int tr, int tc, int col_major, int thr,
-                       int build_csc, rtt_hybrid_tiles *out)
+int csr_to_hybrid_device(Workspace &ws, int m, int n, int nnz, const int *rp, const int *ci,
+                         const double *va, int tr, int tc, int col_major, int thr, int build_csc,
+                         HybridDev &H)
 {
     cudaStream_t s = ws.stream;
-    const int m = M->m, n = M->n, nnz = M->nnz;
-    DevArrays D;
-    int *rp = nullptr, *ci = nullptr;
-    double *va = nullptr;
-    RTT_CHECK(D.get(&rp, (size_t)m + 1));
-    RTT_CHECK(D.get(&ci, (size_t)nnz));
-    RTT_CHECK(D.get(&va, (size_t)nnz));
-    RTT_CUDA(cudaMemcpyAsync(rp, M->rowpointer, sizeof(int) * ((size_t)m + 1), cudaMemcpyHostToDevice, s));
-    if (nnz > 0)
-    {
-        RTT_CUDA(cudaMemcpyAsync(ci, M->columnindex, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, s));
-        RTT_CUDA(cudaMemcpyAsync(va, M->value, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice, s));
-    }
     RTT_CUDA(cudaMemsetAsync(ws.err.p, 0, sizeof(int), s));
     k_hyb_validate<<<blocks(std::max(m + 1, nnz), 256), 256, 0, s>>>(m, n, nnz, rp, ci, ws.err.as<int>());
+    ws.launches++;
     RTT_CHECK(check_device_error(ws, "hybrid tiles: CSR"));
 
     const int trc = m / tr + (m % tr != 0), tcc = n / tc + (n % tc != 0);
-    rtt_hybrid_tiles r{};
-    r.rows = m;
-    r.cols = n;
-    r.tile_rows = tr;
-    r.tile_cols = tc;
-    r.tile_row_count = trc;
-    r.tile_col_count = tcc;
-
-    unsigned long long *keys = nullptr, *skeys = nullptr;
-    double *svals = nullptr;
-    int *chead = nullptr, *thead = nullptr, *cid = nullptr, *tid = nullptr;
-    RTT_CHECK(D.get(&keys, (size_t)nnz));
-    RTT_CHECK(D.get(&skeys, (size_t)nnz));
-    RTT_CHECK(D.get(&svals, (size_t)nnz));
-    RTT_CHECK(D.get(&chead, (size_t)nnz + 1));
-    RTT_CHECK(D.get(&thead, (size_t)nnz + 1));
-    RTT_CHECK(D.get(&cid, (size_t)nnz + 1));
-    RTT_CHECK(D.get(&tid, (size_t)nnz + 1));
+    H.rows = m;
+    H.cols = n;
+    H.tr = tr;
+    H.tc = tc;
+    H.trc = trc;
+    H.tcc = tcc;
+    H.col_major = col_major;
+    H.has_csc = build_csc != 0;
+    // grow-only scratch: entry level, coordinate level, tile level
+    auto get = [&](DevBuf &b, size_t bytes) { return b.ensure(bytes > 0 ? bytes : 16, s); };
+    const size_t E = (size_t)nnz;
+    RTT_CHECK(get(H.tmp[0], 8 * E));       // keys
+    RTT_CHECK(get(H.tmp[1], 8 * E));       // sorted keys
+    RTT_CHECK(get(H.tmp[2], 8 * E));       // sorted values
+    RTT_CHECK(get(H.tmp[3], 4 * (E + 1))); // coordinate heads
+    RTT_CHECK(get(H.tmp[4], 4 * (E + 1))); // tile heads
+    RTT_CHECK(get(H.tmp[5], 4 * (E + 1))); // coordinate ids
+    RTT_CHECK(get(H.tmp[6], 4 * (E + 1))); // tile ids
+    auto *keys = H.tmp[0].as<unsigned long long>(), *skeys = H.tmp[1].as<unsigned long long>();
+    double *svals = H.tmp[2].as<double>();
+    int *chead = H.tmp[3].as<int>(), *thead = H.tmp[4].as<int>(), *cid = H.tmp[5].as<int>(),
+        *tid = H.tmp[6].as<int>();
     int ncoord = 0, ntiles = 0;
     if (nnz > 0)
     {
@@ -280,35 +273,37 @@ int csr_to_hybrid_host(Workspace &ws, const SMatrix *M, int tr, int tc, int col_
         RTT_CUDA(cub::DeviceRadixSort::SortPairs(ws.scan_tmp.p, bytes, keys, skeys, va, svals, nnz,
                                                  0, hibit, s));
         k_hyb_heads<<<blocks(nnz, 256), 256, 0, s>>>(nnz, skeys, chead, thead);
+        ws.launches += 4;
         // inclusive scans: coordinate / tile id of every entry
         RTT_CHECK(scan_into(ws, chead, cid, nnz)); // cid[i + 1] = inclusive count
         RTT_CHECK(scan_into(ws, thead, tid, nnz));
         RTT_CHECK(read_int(ws, cid + nnz, &ncoord));
         RTT_CHECK(read_int(ws, tid + nnz, &ntiles));
     }
-    // per coordinate / per tile arrays
-    double *cval = nullptr;
-    unsigned char *cphys = nullptr;
-    int *ctile = nullptr, *tcount = nullptr, *tcol = nullptr, *trow = nullptr, *tfirst = nullptr,
-        *tsize = nullptr, *toff = nullptr, *row_hist = nullptr, *rowptr = nullptr, *ndense = nullptr;
-    unsigned int *mask = nullptr;
-    double *values = nullptr;
-    RTT_CHECK(D.get(&cval, (size_t)ncoord));
-    RTT_CHECK(D.get(&cphys, (size_t)ncoord));
-    RTT_CHECK(D.get(&ctile, (size_t)ncoord));
-    RTT_CHECK(D.get(&tcount, (size_t)ntiles));
-    RTT_CHECK(D.get(&tcol, (size_t)ntiles));
-    RTT_CHECK(D.get(&trow, (size_t)ntiles));
-    RTT_CHECK(D.get(&tfirst, (size_t)ntiles));
-    RTT_CHECK(D.get(&tsize, (size_t)ntiles));
-    RTT_CHECK(D.get(&toff, (size_t)ntiles + 1));
-    RTT_CHECK(D.get(&row_hist, (size_t)trc + 1));
-    RTT_CHECK(D.get(&rowptr, (size_t)trc + 1));
-    RTT_CHECK(D.get(&ndense, 1));
-    RTT_CHECK(D.get(&mask, (size_t)ntiles));
-    RTT_CUDA(cudaMemsetAsync(mask, 0, sizeof(unsigned) * (size_t)std::max(ntiles, 1), s));
-    RTT_CUDA(cudaMemsetAsync(tcount, 0, sizeof(int) * (size_t)std::max(ntiles, 1), s));
-    RTT_CUDA(cudaMemsetAsync(row_hist, 0, sizeof(int) * ((size_t)trc + 1), s));
+    const size_t NC = (size_t)ncoord, NT = (size_t)ntiles;
+    RTT_CHECK(get(H.tmp[7], 8 * NC));      // coordinate values
+    RTT_CHECK(get(H.tmp[8], NC));          // coordinate physical index
+    RTT_CHECK(get(H.tmp[9], 4 * NC));      // coordinate tile
+    RTT_CHECK(get(H.tmp[10], 4 * NT));     // tile counts
+    RTT_CHECK(get(H.tmp[11], 4 * NT));     // tile rows
+    RTT_CHECK(get(H.tmp[12], 4 * NT));     // tile first coordinate
+    RTT_CHECK(get(H.tmp[13], 4 * NT));     // tile payload sizes
+    RTT_CHECK(get(H.tmp[14], 4 * ((size_t)std::max(trc, tcc) + 1))); // row / column histogram
+    RTT_CHECK(get(H.tmp[15], 16));         // dense count
+    RTT_CHECK(get(H.row_ptr, 4 * ((size_t)trc + 1)));
+    RTT_CHECK(get(H.col_idx, 4 * NT));
+    RTT_CHECK(get(H.value_off, 4 * (NT + 1)));
+    RTT_CHECK(get(H.mask, 4 * NT));
+    double *cval = H.tmp[7].as<double>();
+    unsigned char *cphys = H.tmp[8].as<unsigned char>();
+    int *ctile = H.tmp[9].as<int>(), *tcount = H.tmp[10].as<int>(), *trow = H.tmp[11].as<int>(),
+        *tfirst = H.tmp[12].as<int>(), *tsize = H.tmp[13].as<int>(), *hist = H.tmp[14].as<int>(),
+        *ndense = H.tmp[15].as<int>();
+    int *tcol = H.col_idx.as<int>(), *toff = H.value_off.as<int>(), *rowptr = H.row_ptr.as<int>();
+    unsigned int *mask = H.mask.as<unsigned int>();
+    RTT_CUDA(cudaMemsetAsync(mask, 0, sizeof(unsigned) * std::max(NT, (size_t)1), s));
+    RTT_CUDA(cudaMemsetAsync(tcount, 0, sizeof(int) * std::max(NT, (size_t)1), s));
+    RTT_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * ((size_t)trc + 1), s));
     RTT_CUDA(cudaMemsetAsync(ndense, 0, sizeof(int), s));
     int payload = 0, ndense_h = 0;
     if (nnz > 0)
@@ -316,8 +311,9 @@ int csr_to_hybrid_host(Workspace &ws, const SMatrix *M, int tr, int tc, int col_
         k_hyb_tiles<<<blocks(nnz, 256), 256, 0, s>>>(nnz, skeys, svals, chead, cid + 1, tid + 1,
                                                      cval, cphys, ctile, mask, tcount, tcol, trow,
                                                      tfirst);
-        k_hyb_sizes<<<blocks(ntiles, 256), 256, 0, s>>>(ntiles, tcount, thr, tsize, row_hist, trow,
+        k_hyb_sizes<<<blocks(ntiles, 256), 256, 0, s>>>(ntiles, tcount, thr, tsize, hist, trow,
                                                        ndense);
+        ws.launches += 2;
         RTT_CHECK(scan_into(ws, tsize, toff, ntiles));
         RTT_CHECK(read_int(ws, toff + ntiles, &payload));
         RTT_CHECK(read_int(ws, ndense, &ndense_h));
@@ -326,27 +322,30 @@ int csr_to_hybrid_host(Workspace &ws, const SMatrix *M, int tr, int tc, int col_
     {
         RTT_CUDA(cudaMemsetAsync(toff, 0, sizeof(int), s));
     }
-    RTT_CHECK(scan_into(ws, row_hist, rowptr, trc));
-    RTT_CHECK(D.get(&values, (size_t)payload));
+    RTT_CHECK(scan_into(ws, hist, rowptr, trc));
+    RTT_CHECK(get(H.values, 8 * (size_t)payload));
+    double *values = H.values.as<double>();
     RTT_CUDA(cudaMemsetAsync(values, 0, sizeof(double) * (size_t)std::max(payload, 1), s));
     if (ncoord > 0)
+    {
         k_hyb_values<<<blocks(ncoord, 256), 256, 0, s>>>(ncoord, cval, cphys, ctile, tfirst, toff,
                                                          tcount, thr, values);
-    r.num_tiles = ntiles;
-    r.payload_size = payload;
-    r.dense_tiles = ndense_h;
-    r.sparse_tiles = ntiles - ndense_h;
+        ws.launches++;
+    }
+    H.ntiles = ntiles;
+    H.payload = payload;
+    H.ndense = ndense_h;
 
-    int *csc_ptr = nullptr, *csc_row = nullptr, *csc_ids = nullptr;
     if (build_csc)
     {
-        int *col_hist = nullptr, *iota = nullptr, *skey = nullptr;
-        RTT_CHECK(D.get(&col_hist, (size_t)tcc + 1));
-        RTT_CHECK(D.get(&csc_ptr, (size_t)tcc + 1));
-        RTT_CHECK(D.get(&iota, (size_t)ntiles));
-        RTT_CHECK(D.get(&skey, (size_t)ntiles));
-        RTT_CHECK(D.get(&csc_ids, (size_t)ntiles));
-        RTT_CHECK(D.get(&csc_row, (size_t)ntiles));
+        RTT_CHECK(get(H.csc_ptr, 4 * ((size_t)tcc + 1)));
+        RTT_CHECK(get(H.csc_row, 4 * NT));
+        RTT_CHECK(get(H.csc_ids, 4 * NT));
+        RTT_CHECK(get(H.tmp[16], 4 * NT)); // iota
+        RTT_CHECK(get(H.tmp[17], 4 * NT)); // sorted column keys
+        int *iota = H.tmp[16].as<int>(), *skey = H.tmp[17].as<int>();
+        int *csc_ptr = H.csc_ptr.as<int>(), *csc_row = H.csc_row.as<int>(),
+            *csc_ids = H.csc_ids.as<int>();
         if (ntiles > 0)
         {
             // stable sort of tile ids by tile column keeps tile-row order per column
@@ -361,36 +360,82 @@ int csr_to_hybrid_host(Workspace &ws, const SMatrix *M, int tr, int tc, int col_
             RTT_CUDA(cub::DeviceRadixSort::SortPairs(ws.scan_tmp.p, bytes, tcol, skey, iota,
                                                      csc_ids, ntiles, 0, cbits, s));
             k_hyb_gather<<<blocks(ntiles, 256), 256, 0, s>>>(ntiles, csc_ids, trow, csc_row);
+            ws.launches += 4;
         }
         // column pointer: scan of the tiles per tile column
-        RTT_CUDA(cudaMemsetAsync(col_hist, 0, sizeof(int) * ((size_t)tcc + 1), s));
+        RTT_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * ((size_t)tcc + 1), s));
         if (ntiles > 0)
-            k_hyb_hist<<<blocks(ntiles, 256), 256, 0, s>>>(ntiles, tcol, col_hist);
-        RTT_CHECK(scan_into(ws, col_hist, csc_ptr, tcc));
+        {
+            k_hyb_hist<<<blocks(ntiles, 256), 256, 0, s>>>(ntiles, tcol, hist);
+            ws.launches++;
+        }
+        RTT_CHECK(scan_into(ws, hist, csc_ptr, tcc));
     }
-    RTT_CHECK(check_device_error(ws, "hybrid tiles"));
+    return check_device_error(ws, "hybrid tiles");
+}
 
+void HybridDev::release()
+{
+    DevBuf *all[] = {&row_ptr, &col_idx, &value_off, &mask, &values, &csc_ptr, &csc_row, &csc_ids};
+    for (DevBuf *b : all)
+        b->release();
+    for (DevBuf &b : tmp)
+        b.release();
+}
+
+int csr_to_hybrid_host(Workspace &ws, const SMatrix *M, int tr, int tc, int col_major, int thr,
+                       int build_csc, rtt_hybrid_tiles *out)
+{
+    cudaStream_t s = ws.stream;
+    const int m = M->m, n = M->n, nnz = M->nnz;
+    DevArrays D;
+    int *rp = nullptr, *ci = nullptr;
+    double *va = nullptr;
+    RTT_CHECK(D.get(&rp, (size_t)m + 1));
+    RTT_CHECK(D.get(&ci, (size_t)nnz));
+    RTT_CHECK(D.get(&va, (size_t)nnz));
+    RTT_CUDA(cudaMemcpyAsync(rp, M->rowpointer, sizeof(int) * ((size_t)m + 1), cudaMemcpyHostToDevice, s));
+    if (nnz > 0)
+    {
+        RTT_CUDA(cudaMemcpyAsync(ci, M->columnindex, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, s));
+        RTT_CUDA(cudaMemcpyAsync(va, M->value, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice, s));
+    }
+    HybridDev H;
+    int st = csr_to_hybrid_device(ws, m, n, nnz, rp, ci, va, tr, tc, col_major, thr, build_csc, H);
     // host copies (malloc'd, caller frees with rtt_hybrid_tiles_destroy)
-    rtt_hybrid_tiles h = r;
-    int st = RTT_OK;
+    rtt_hybrid_tiles h{};
     if (st == RTT_OK)
-        st = to_host(&h.tile_row_ptr, rowptr, (size_t)trc + 1, s);
+    {
+        h.rows = m;
+        h.cols = n;
+        h.tile_rows = tr;
+        h.tile_cols = tc;
+        h.tile_row_count = H.trc;
+        h.tile_col_count = H.tcc;
+        h.num_tiles = H.ntiles;
+        h.payload_size = H.payload;
+        h.dense_tiles = H.ndense;
+        h.sparse_tiles = H.ntiles - H.ndense;
+        st = to_host(&h.tile_row_ptr, H.row_ptr.as<int>(), (size_t)H.trc + 1, s);
+    }
     if (st == RTT_OK)
-        st = to_host(&h.tile_col_idx, tcol, (size_t)ntiles, s);
+        st = to_host(&h.tile_col_idx, H.col_idx.as<int>(), (size_t)H.ntiles, s);
     if (st == RTT_OK)
-        st = to_host(&h.value_offsets, toff, (size_t)ntiles + 1, s);
+        st = to_host(&h.value_offsets, H.value_off.as<int>(), (size_t)H.ntiles + 1, s);
     if (st == RTT_OK)
-        st = to_host(&h.masks, mask, (size_t)ntiles, s);
+        st = to_host(&h.masks, H.mask.as<unsigned int>(), (size_t)H.ntiles, s);
     if (st == RTT_OK)
-        st = to_host(&h.values, values, (size_t)payload, s);
+        st = to_host(&h.values, H.values.as<double>(), (size_t)H.payload, s);
     if (st == RTT_OK && build_csc)
     {
-        st = to_host(&h.tile_col_ptr, csc_ptr, (size_t)tcc + 1, s);
+        st = to_host(&h.tile_col_ptr, H.csc_ptr.as<int>(), (size_t)H.tcc + 1, s);
         if (st == RTT_OK)
-            st = to_host(&h.tile_row_idx, csc_row, (size_t)ntiles, s);
+            st = to_host(&h.tile_row_idx, H.csc_row.as<int>(), (size_t)H.ntiles, s);
         if (st == RTT_OK)
-            st = to_host(&h.csc_tile_ids, csc_ids, (size_t)ntiles, s);
+            st = to_host(&h.csc_tile_ids, H.csc_ids.as<int>(), (size_t)H.ntiles, s);
     }
+    cudaStreamSynchronize(s);
+    H.release();
     if (st != RTT_OK)
     {
         rtt_hybrid_tiles_destroy(&h);

@@ -392,6 +392,11 @@ int numeric_rows_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
 // numeric step without a copy pipeline: warp-private Gustavson per row pair
 int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
                         const NumericConfig &cfg);
+struct HybridDev;
+// numeric step on the FP64 tensor cores from hybrid leaves of A's and B's CSR
+// (A.csr_*, B.csr_*; the leaves are built into LA / LB): C's 16x16 tiles
+int numeric_leaf_device(Workspace &ws, const DevTiles &A, const DevTiles &B, HybridDev &LA,
+                        HybridDev &LB, SymbolicOut &S, const NumericConfig &cfg);
 // the flat kernel unless DMMA pairs exist or TMA staging of B is asked for
 int numeric_select_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
                           const NumericConfig &cfg);
@@ -426,6 +431,27 @@ int batch_split_device(Workspace &ws, int count, int total_rows, const int *row_
 int plan_tail_queue_device(Workspace &ws, int n, const int *d_scans, const int *d_matches,
                            const int *d_out, const rtt_tail_policy &policy,
                            const rtt_tail_cost_model &model, int *d_chunks, rtt_tail_plan *plan);
+// Hybrid leaf tiles on the device (the reference's HybridTileMatrix as
+// DmmaDeviceTiles, src/dmma_tiles.h:29-62, src/dmma_spgemm.h:178-221): CSR
+// over leaf rows (row_ptr, col_idx), value_off (a tile is dense exactly when
+// its span is 32), u32 masks, values, and the optional CSC (csc_ptr over leaf
+// columns, csc_row, csc_ids = CSR tile ids).  Buffers grow only.
+struct HybridDev
+{
+    int rows = 0, cols = 0, tr = 0, tc = 0, trc = 0, tcc = 0;
+    int ntiles = 0, payload = 0, ndense = 0, col_major = 0;
+    bool has_csc = false;
+    DevBuf row_ptr, col_idx, value_off, mask, values, csc_ptr, csc_row, csc_ids;
+    DevBuf tmp[18]; // build scratch
+    void release();
+};
+// device CSR -> hybrid leaf tiles of tile_rows x tile_cols (32 elements) in H
+int csr_to_hybrid_device(Workspace &ws, int m, int n, int nnz, const int *rowptr, const int *col,
+                         const double *val, int tile_rows, int tile_cols, int col_major,
+                         int dense_threshold, int build_csc, HybridDev &H);
+// Leaves with at least this many of their 32 entries are stored dense (the
+// reference's default dense threshold).
+constexpr int LEAF_DENSE_THRESHOLD = 24;
 // CSR (host arrays) -> hybrid leaf tiles on the device, results malloc'd into out
 int csr_to_hybrid_host(Workspace &ws, const SMatrix *M, int tile_rows, int tile_cols,
                        int col_major, int dense_threshold, int build_csc, rtt_hybrid_tiles *out);

@@ -87,7 +87,8 @@ def test_bad_arguments_rejected_before_device_work():
     assert cfg.split_target == 0  # heavy tile rows split at the default target
     assert cfg.cuda_graphs == 1  # repeated numeric phases replay a CUDA graph
     assert cfg.sym_window_slots == 0  # wide step-2 windows at their default size
-    assert C.sizeof(R.Config) == 12 * 4
+    assert cfg.leaf_dmma == 0  # the scalar numeric kernel by default
+    assert C.sizeof(R.Config) == 13 * 4
 
 
 def test_generators_shapes():

@@ -56,6 +56,8 @@ CONFIGS = {
     "flat": dict(fused_csr_output=1, dmma_pair_cutoff=0, b_staging=0),
     "flat_unfused": dict(fused_csr_output=0, dmma_pair_cutoff=0, b_staging=0),
     "staged": dict(fused_csr_output=1, dmma_pair_cutoff=0, b_staging=1),
+    # FP64 DMMA straight from 8x4 / 4x8 hybrid leaves
+    "leaf": dict(leaf_dmma=1),
 }
 
 
@@ -76,6 +78,8 @@ def test_a_squared(case, cfg, orc):
         assert st["dmma_pairs"] > 0
     if cfg in ("fused_nodmma", "flat", "flat_unfused", "staged"):
         assert st["dmma_pairs"] == 0
+    if cfg == "leaf" and nnz > 0:
+        assert st["dmma_pairs"] > 0  # leaf pairs multiplied on the tensor cores
     ctx.close()
 
 
@@ -317,3 +321,51 @@ def test_sym_window_slots_checked():
         with pytest.raises(R.RttError) as e:
             R.Context(0, dict(sym_window_slots=bad))
         assert e.value.status == 1  # RTT_ERR_INVALID_ARGUMENT
+
+
+def test_leaf_dmma_forms(orc):
+    """The leaf DMMA numeric step in the other forms: A*A^T, general A*B, a
+    values-only update and a batch, each against the oracle (structure
+    bit-exact, values within the bound)."""
+    cfg = dict(leaf_dmma=1)
+    A = G.rmat(11, 8, seed=4)
+    ctx = R.Context(0, cfg)
+    rp, ci, va, nnz, _ = _run(ctx, A, None, R.RTT_OP_AAT)
+    assert_csr_close(rp, ci, va, *orc.spgemm_csr(A, A.transpose()), "leaf AAT: ")
+    assert ctx.stats()["nnz_cub"] == orc.nnzcub(A, A.transpose())
+    ctx.close()
+    A2 = G.random_csr(500, 300, 0.02, seed=31)
+    B2 = G.random_csr(300, 700, 0.015, seed=32)
+    ctx = R.Context(0, cfg)
+    rp, ci, va, nnz, _ = _run(ctx, A2, B2)
+    assert_csr_close(rp, ci, va, *orc.spgemm_csr(A2, B2), "leaf A*B: ")
+    ctx.close()
+    # a values-only update
+    S = G.stencil_27(12, 2)
+    ctx = R.Context(0, cfg)
+    d = torch.device("cuda:0")
+    da = (S.m, S.n, torch.from_numpy(S.rowptr).to(d), torch.from_numpy(S.col).to(d),
+          torch.from_numpy(S.val).to(d))
+    nnz, _ = ctx.symbolic(da)
+    out = (torch.empty(S.m + 1, dtype=torch.int32, device=d),
+           torch.empty(nnz, dtype=torch.int32, device=d),
+           torch.empty(nnz, dtype=torch.float64, device=d))
+    ctx.numeric(*out)
+    nv = da[4] * -0.5 + 0.25
+    ctx.numeric_values(nv, None, *out)
+    torch.cuda.synchronize()
+    S2 = G.CSR(S.m, S.n, S.rowptr, S.col, nv.cpu().numpy())
+    assert_csr_close(out[0].cpu().numpy(), out[1].cpu().numpy(), out[2].cpu().numpy(),
+                     *orc.spgemm_csr(S2, S2), "leaf values-only: ")
+    ctx.close()
+    # a batch
+    As = [G.banded_scatter(300 + 97 * i, 5, seed=i) for i in range(5)]
+    ctx = R.Context(0, cfg)
+    outs = R.spgemm_batched(ctx, [(X.m, X.n, torch.from_numpy(X.rowptr).to(d),
+                                   torch.from_numpy(X.col).to(d), torch.from_numpy(X.val).to(d))
+                                  for X in As])
+    torch.cuda.synchronize()
+    for X, (orp, oci, ova) in zip(As, outs):
+        assert_csr_close(orp.cpu().numpy(), oci.cpu().numpy(), ova.cpu().numpy(),
+                         *orc.spgemm_csr(X, X), "leaf batch: ")
+    ctx.close()
