@@ -609,6 +609,17 @@ RTT_API int rtt_spgemm_tiles_view(rtt_context ctx, SMatrix *c_tiles_device);
 RTT_API int rtt_spgemm_csr_host(rtt_context ctx, const SMatrix *A, const SMatrix *B,
                         int op, SMatrix *C);
 
+/* The same product into caller-owned host arrays, for callers that keep
+ * their output buffers from one product to the next (a serving loop): C's
+ * row pointer (A->m + 1 ints) always, its columns and values when nnz(C) <=
+ * capacity.  Page-locked arrays receive the DMA directly; pageable ones go
+ * through the context's staging buffers.  *nnz_c receives nnz(C); when it
+ * exceeds capacity nothing else is written and the call returns
+ * RTT_ERR_INVALID_ARGUMENT (grow the arrays to *nnz_c and call again). */
+RTT_API int rtt_spgemm_csr_host_into(rtt_context ctx, const SMatrix *A, const SMatrix *B, int op,
+                                     int *c_row_ptr, int *c_col_idx, double *c_values,
+                                     long long capacity, long long *nnz_c);
+
 /* Batched form (no single reference function: it batches the device path
  * above over independent products, many SpGEMMs of uneven sizes in one
  * pipeline run).  count products C_i = A_i * B_i (B == NULL: C_i =

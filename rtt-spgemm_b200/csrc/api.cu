@@ -2380,10 +2380,13 @@ int rtt_spgemm_tiles_view(rtt_context c, SMatrix *out)
     return RTT_OK;
 }
 
-int rtt_spgemm_csr_host(rtt_context c, const SMatrix *A, const SMatrix *B, int op, SMatrix *C)
+namespace
 {
-    if (c == nullptr || !csr_args_ok(A) || C == nullptr || (B != nullptr && !csr_args_ok(B)))
-        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "spgemm_csr_host: bad arguments");
+// The host-buffer product up to C on the device (c->out_*): uploads, both
+// phases; m, n and nnz of C come back.
+int csr_host_product(rtt_context c, const SMatrix *A, const SMatrix *B, int op, int *m_out,
+                     int *n_out, long long *nnz_out)
+{
     RTT_CUDA(cudaSetDevice(c->ws.device));
     cudaStream_t s = c->ws.stream;
     RTT_CHECK(upload(c, c->in_rp, A->rowpointer, (size_t)A->m + 1, s));
@@ -2403,12 +2406,26 @@ int rtt_spgemm_csr_host(rtt_context c, const SMatrix *A, const SMatrix *B, int o
     long long nnz = 0, tiles = 0;
     RTT_CHECK(rtt_spgemm_symbolic(c, &va, B ? &vb : nullptr, op, &nnz, &tiles));
     const int m = A->m;
-    const int n = op == RTT_OP_AAT ? A->m : (B ? B->n : A->n);
     RTT_CHECK(c->out_rp.ensure(sizeof(int) * ((size_t)m + 1), s));
     RTT_CHECK(c->out_col.ensure(sizeof(int) * (size_t)nnz + 16, s));
     RTT_CHECK(c->out_val.ensure(sizeof(double) * (size_t)nnz + 16, s));
     RTT_CHECK(rtt_spgemm_numeric(c, c->out_rp.as<int>(), c->out_col.as<int>(),
                                  c->out_val.as<double>()));
+    *m_out = m;
+    *n_out = op == RTT_OP_AAT ? A->m : (B ? B->n : A->n);
+    *nnz_out = nnz;
+    return RTT_OK;
+}
+} // namespace
+
+int rtt_spgemm_csr_host(rtt_context c, const SMatrix *A, const SMatrix *B, int op, SMatrix *C)
+{
+    if (c == nullptr || !csr_args_ok(A) || C == nullptr || (B != nullptr && !csr_args_ok(B)))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "spgemm_csr_host: bad arguments");
+    int m = 0, n = 0;
+    long long nnz = 0;
+    RTT_CHECK(csr_host_product(c, A, B, op, &m, &n, &nnz));
+    cudaStream_t s = c->ws.stream;
     HostArrays h;
     int **rp = h.slot<int>(), **ci = h.slot<int>();
     double **v = h.slot<double>();
@@ -2423,6 +2440,33 @@ int rtt_spgemm_csr_host(rtt_context c, const SMatrix *A, const SMatrix *B, int o
     C->columnindex = *ci;
     C->value = *v;
     h.committed = true;
+    return RTT_OK;
+}
+
+int rtt_spgemm_csr_host_into(rtt_context c, const SMatrix *A, const SMatrix *B, int op,
+                             int *c_row_ptr, int *c_col_idx, double *c_values,
+                             long long capacity, long long *nnz_c)
+{
+    if (c == nullptr || !csr_args_ok(A) || (B != nullptr && !csr_args_ok(B)) ||
+        c_row_ptr == nullptr || nnz_c == nullptr || capacity < 0 ||
+        (capacity > 0 && (c_col_idx == nullptr || c_values == nullptr)))
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "spgemm_csr_host_into: bad arguments");
+    int m = 0, n = 0;
+    long long nnz = 0;
+    RTT_CHECK(csr_host_product(c, A, B, op, &m, &n, &nnz));
+    *nnz_c = nnz;
+    if (nnz > capacity)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT,
+                         "spgemm_csr_host_into: nnz(C) = " + std::to_string(nnz) +
+                             " exceeds the capacity of the output arrays (nnz_c holds the size)");
+    cudaStream_t s = c->ws.stream;
+    RTT_CHECK(d2h(c, c_row_ptr, c->out_rp.p, sizeof(int) * ((size_t)m + 1), s));
+    if (nnz > 0)
+    {
+        RTT_CHECK(d2h(c, c_col_idx, c->out_col.p, sizeof(int) * (size_t)nnz, s));
+        RTT_CHECK(d2h(c, c_values, c->out_val.p, sizeof(double) * (size_t)nnz, s));
+    }
+    RTT_CUDA(cudaStreamSynchronize(s));
     return RTT_OK;
 }
 

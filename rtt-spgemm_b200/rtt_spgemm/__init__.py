@@ -598,6 +598,26 @@ class Context:
         return CSR(sc.m, sc.n, _adopt(sc.rowpointer, sc.m + 1, np.int32),
                    _adopt(sc.columnindex, sc.nnz, np.int32), _adopt(sc.value, sc.nnz, np.float64))
 
+    def spgemm_csr_host_into(self, a, out, b=None, op: int = RTT_OP_AB) -> int:
+        """Host CSR in -> C into the caller's host arrays out = (rowptr, col,
+        val) (numpy; page-locked ones take the DMA directly), reused from call
+        to call (rtt_spgemm_csr_host_into).  Returns nnz(C); raises RttError
+        when col / val are shorter than nnz(C) (the error says the size)."""
+        sa, ka = _csr_smatrix(a)
+        sb, kb = _csr_smatrix(b) if b is not None else (None, None)
+        rp, col, val = out
+        if rp.dtype != np.int32 or col.dtype != np.int32 or val.dtype != np.float64:
+            raise TypeError("out arrays must be int32, int32, float64")
+        if rp.size < a.m + 1:
+            raise ValueError("out rowptr must hold m + 1 entries")
+        cap = min(col.size, val.size)
+        nnz = C.c_longlong(0)
+        check(lib().rtt_spgemm_csr_host_into(
+            self.handle, C.byref(sa), C.byref(sb) if sb is not None else None, op,
+            C.c_void_p(rp.ctypes.data), C.c_void_p(col.ctypes.data) if cap else None,
+            C.c_void_p(val.ctypes.data) if cap else None, cap, C.byref(nnz)))
+        return int(nnz.value)
+
 
 def spgemm_batched(ctx: "Context", As, Bs=None, tuner=None):
     """C_i = A_i * B_i (or A_i^2) for a list of device CSR tuples, through one

@@ -35,6 +35,7 @@ EXPORTS = [
     "rtt_config_default", "rtt_context_create", "rtt_context_destroy", "rtt_context_set_stream",
     "rtt_context_set_config", "rtt_context_get_stats", "rtt_spgemm_symbolic",
     "rtt_spgemm_numeric", "rtt_spgemm_tiles_view", "rtt_spgemm_csr_host",
+    "rtt_spgemm_csr_host_into",
     "rtt_tile2csr_device_noalloc", "rtt_csr_to_hybrid_tiles", "rtt_hybrid_tiles_destroy",
     "rtt_plan_tail_queue", "rtt_spgemm_batched_symbolic", "rtt_spgemm_batched_numeric",
     "rtt_csr_transpose", "rtt_early_split_policy_default", "rtt_plan_early_split",
@@ -241,6 +242,9 @@ def lib() -> C.CDLL:
     L.rtt_spgemm_numeric64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.rtt_spgemm_tiles_view.argtypes = [C.c_void_p, P(SMatrix)]
     L.rtt_spgemm_csr_host.argtypes = [C.c_void_p, P(SMatrix), P(SMatrix), C.c_int, P(SMatrix)]
+    L.rtt_spgemm_csr_host_into.argtypes = [C.c_void_p, P(SMatrix), P(SMatrix), C.c_int,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong,
+                                           P(C.c_longlong)]
     L.rtt_spgemm_batched_symbolic.argtypes = [C.c_void_p, C.c_int, P(CsrView), P(CsrView),
                                               P(C.c_longlong), P(C.c_longlong)]
     L.rtt_spgemm_batched_numeric.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]

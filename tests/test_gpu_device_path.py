@@ -369,3 +369,28 @@ def test_leaf_dmma_forms(orc):
         assert_csr_close(orp.cpu().numpy(), oci.cpu().numpy(), ova.cpu().numpy(),
                          *orc.spgemm_csr(X, X), "leaf batch: ")
     ctx.close()
+
+
+def test_host_into_caller_buffers(orc):
+    """rtt_spgemm_csr_host_into: C into the caller's host arrays, page-locked
+    or pageable, reused across calls; too-small arrays get a clean error with
+    the size, and the result equals the malloc'd-output call's bit for bit."""
+    A = G.stencil_27(24, 1)  # C's values above the 4 MB of the staged copies
+    ctx = R.Context(0)
+    want = ctx.spgemm_csr_host(A)
+    small = (np.zeros(A.m + 1, np.int32), np.zeros(10, np.int32), np.zeros(10))
+    with pytest.raises(R.RttError) as e:
+        ctx.spgemm_csr_host_into(A, small)
+    assert e.value.status == 1 and str(want.col.size) in str(e.value)
+    nnz = want.col.size
+    pinned = tuple(torch.empty(n, dtype=t).pin_memory().numpy()
+                   for n, t in ((A.m + 1, torch.int32), (nnz + 5, torch.int32),
+                                (nnz + 5, torch.float64)))
+    pageable = (np.zeros(A.m + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz))
+    for out in (pinned, pageable, pinned):
+        got = ctx.spgemm_csr_host_into(A, out)
+        assert got == nnz
+        assert np.array_equal(out[0], want.rowptr) and np.array_equal(out[1][:nnz], want.col)
+        assert np.array_equal(out[2][:nnz].view(np.int64), want.val.view(np.int64))
+    ctx.close()
+    assert_csr_close(pageable[0], pageable[1], pageable[2], *orc.spgemm_csr(A, A), "into: ")
