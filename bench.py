@@ -292,7 +292,7 @@ def run_batched(args) -> None:
     ctx = R.Context(0, {"stage_timing": 0, "dmma_pair_cutoff": args.dmma_cutoff,
                         "b_staging": 1 if args.staging else 0,
                         "persistent_rows": 1 if args.persistent_rows else 0,
-                "sym_window_slots": args.sym_window_slots, "leaf_dmma": 1 if args.leaf_dmma else 0})
+                "sym_window_slots": args.sym_window_slots, "leaf_dmma": 1 if args.leaf_dmma else 0, "global_rows": args.global_rows})
     stream = torch.cuda.current_stream(dev)
     ctx.set_stream(stream.cuda_stream)
 
@@ -328,7 +328,7 @@ def run_batched(args) -> None:
     base_cfg = {"stage_timing": 0, "dmma_pair_cutoff": args.dmma_cutoff,
                 "b_staging": 1 if args.staging else 0,
                 "persistent_rows": 1 if args.persistent_rows else 0,
-                "sym_window_slots": args.sym_window_slots, "leaf_dmma": 1 if args.leaf_dmma else 0}
+                "sym_window_slots": args.sym_window_slots, "leaf_dmma": 1 if args.leaf_dmma else 0, "global_rows": args.global_rows}
     ms_b = timed(batched)
     ctx.configure(base_cfg)  # the plain arm keeps the given configuration
     ms_p = timed(plain)
@@ -567,7 +567,7 @@ def run_wide(args) -> None:
     cub = nnz_cub(A, True)
     flops = 2.0 * cub
     stream = torch.cuda.current_stream(dev)
-    ctx = R.Context(0, {"stage_timing": 0, "sym_window_slots": args.sym_window_slots, "leaf_dmma": 1 if args.leaf_dmma else 0})
+    ctx = R.Context(0, {"stage_timing": 0, "sym_window_slots": args.sym_window_slots, "leaf_dmma": 1 if args.leaf_dmma else 0, "global_rows": args.global_rows})
     ctx.set_stream(stream.cuda_stream)
     a_view = (A.m, A.n, torch.from_numpy(A.rowptr).to(dev), torch.from_numpy(A.col).to(dev),
               torch.from_numpy(A.val).to(dev))
@@ -684,7 +684,7 @@ def run_ours(args) -> None:
                             "b_staging": 1 if args.staging else 0,
                             "segment_walk": 1 if args.segment_walk else 0,
                             "persistent_rows": 1 if args.persistent_rows else 0,
-                "sym_window_slots": args.sym_window_slots, "leaf_dmma": 1 if args.leaf_dmma else 0})
+                "sym_window_slots": args.sym_window_slots, "leaf_dmma": 1 if args.leaf_dmma else 0, "global_rows": args.global_rows})
     ctx.set_stream(stream.cuda_stream)
     rp = torch.from_numpy(A.rowptr).to(dev)
     ci = torch.from_numpy(A.col).to(dev)
@@ -948,6 +948,9 @@ def main() -> None:
                          "(0 = default, -1 = off)")
     ap.add_argument("--persistent-rows", action="store_true",
                     help="numeric step: one resident wave of tile-row CTAs over a device queue")
+    ap.add_argument("--global-rows", type=int, default=0,
+                    help="heavy tile rows accumulated in C's values in device memory "
+                         "(1 read-modify-write, 2 atomic adds)")
     ap.add_argument("--leaf-dmma", action="store_true",
                     help="numeric step: FP64 DMMA straight from 8x4 / 4x8 hybrid leaves")
     ap.add_argument("--segment-walk", action="store_true",

@@ -484,6 +484,15 @@ typedef struct
      * values within the FP64 bound (other summation order).  Default 0: the
      * scalar kernel is faster on every workload measured. */
     int leaf_dmma;
+    /* C tile rows that need several shared-memory windows (R-MAT rows) are
+     * cut into tasks of about 8192 C entries that accumulate straight into
+     * C's CSR values in device memory, so each A entry is walked once per
+     * task instead of once per window: 0 = off, 1 = read-modify-write in
+     * each row's (K, k) order (bitwise the same C), 2 = atomic adds of the
+     * products (values within the FP64 bound).  Only with the fused CSR
+     * output, sorted B rows without repeated columns and at most 2^20 tile
+     * columns; otherwise the windows. */
+    int global_rows;
 } rtt_config;
 
 RTT_API void rtt_config_default(rtt_config *config);

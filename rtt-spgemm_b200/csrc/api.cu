@@ -779,6 +779,7 @@ int numeric_enqueue(rtt_context c, int *c_row_ptr, int *c_col_idx, double *c_val
     nc.conflict_safe = c->b_dups;
     nc.segment_walk = c->cfg.segment_walk != 0;
     nc.persistent_rows = c->cfg.persistent_rows != 0;
+    nc.global_rows = c->cfg.global_rows;
     // the numeric step reads A's entries from its CSR rows
     DevTiles dA = c->A.view();
     dA.csr_rowptr = c->a_rp;
@@ -1090,6 +1091,8 @@ int rtt_context_set_config(rtt_context c, const rtt_config *config)
                          "chunk_tiles, chunk_nnz >= 0, segment_walk and persistent_rows 0 or 1");
     if (config->leaf_dmma < 0 || config->leaf_dmma > 1)
         return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "leaf_dmma must be 0 or 1");
+    if (config->global_rows < 0 || config->global_rows > 2)
+        return rtt::fail(RTT_ERR_INVALID_ARGUMENT, "global_rows must be 0, 1 or 2");
     if (config->sym_window_slots < -1 ||
         (config->sym_window_slots > 0 &&
          (config->sym_window_slots < 255 || config->sym_window_slots > 6000)))
@@ -2018,6 +2021,7 @@ int rtt_spgemm_numeric64(rtt_context c, long long *c_row_ptr, int *c_col_idx, do
         nc.conflict_safe = c->b_dups;
         nc.segment_walk = c->cfg.segment_walk != 0;
         nc.persistent_rows = c->cfg.persistent_rows != 0;
+    nc.global_rows = c->cfg.global_rows;
         nc.csr_rowptr = c->w_local.as<int>();
         nc.csr_col = c_col_idx + c->w_base[k];
         nc.csr_val = c_values + c->w_base[k];

@@ -499,9 +499,24 @@ __device__ __forceinline__ bool win_cut(const int *c_tile_nnz, int cs0, int cs1,
     return (__ldg(c_tile_nnz + t) - P0) / H != (__ldg(c_tile_nnz + t - 1) - P0) / H;
 }
 
+// Global accumulation of heavy tile rows (NumericConfig::global_rows): a task
+// is a run of consecutive C tiles of a heavy row holding about GLOB_H
+// entries (at most GLOB_H + 255), with no cap on its tiles: its products
+// accumulate in C's own value array, so no shared-memory window bounds it.
+constexpr int GLOB_H = 8192;
+constexpr int GLOB_RELCAP = GLOB_H + 256; // C tiles of one task, at most
+__device__ __forceinline__ bool glob_cut(const int *c_tile_nnz, int cs0, int cs1, int P0, int t)
+{
+    if (t >= cs1)
+        return false;
+    if (t == cs0)
+        return true;
+    return (__ldg(c_tile_nnz + t) - P0) / GLOB_H != (__ldg(c_tile_nnz + t - 1) - P0) / GLOB_H;
+}
+
 // One warp per C tile row: decide heavy or not, and queue the windows of a
 // heavy one.  heavy[I] = 1 tells the numeric kernel's CTA for I to exit.
-template <int ACC>
+template <int ACC, bool GLOB = false>
 __global__ void __launch_bounds__(PLAN_WARPS * 32)
     k_win_plan(int tilem, int m, DevTiles A, DevTiles B,
                const int *__restrict__ c_tile_ptr, const int *__restrict__ c_tile_nnz,
@@ -540,16 +555,21 @@ __global__ void __launch_bounds__(PLAN_WARPS * 32)
         return;
     }
     const int P0 = __ldg(c_tile_nnz + cs0);
+    auto cuts = [&](int t) {
+        return GLOB ? glob_cut(c_tile_nnz, cs0, cs1, P0, t) : win_cut<ACC>(c_tile_nnz, cs0, cs1, P0, t);
+    };
     int nwin = 0;
     for (int t0 = cs0; t0 < cs1; t0 += 32)
-        nwin += __popc(__ballot_sync(FULL, win_cut<ACC>(c_tile_nnz, cs0, cs1, P0, t0 + lane)));
+        nwin += __popc(__ballot_sync(FULL, cuts(t0 + lane)));
     // Cost of one window: the tile row's products, since every window walks
     // all of them (the cost model of the reference's tail queue, products
     // standing in for its scan/match terms).  A task takes g consecutive
     // windows, about SPLIT_TARGET products of walking; a row whose windows all
     // fit one task keeps its own CTA and the L1 reuse of its B rows.
     long long P = 0;
-    if (A.csr_rowptr != nullptr && A.csr_col != nullptr)
+    if (GLOB)
+        ; // one task per run of GLOB_H entries: no grouping of windows
+    else if (A.csr_rowptr != nullptr && A.csr_col != nullptr)
     {
         // the tile row's entries straight from A's CSR rows
         const int e0 = __ldg(A.csr_rowptr + I * TD), e1 = __ldg(A.csr_rowptr + min(A.m, I * TD + TD));
@@ -573,10 +593,12 @@ __global__ void __launch_bounds__(PLAN_WARPS * 32)
             }
         }
     P = warp_sum(P);
-    const int g = (int)max(1ll, min((long long)nwin, target / max(P, 1ll)));
+    const int g = GLOB ? 1 : (int)max(1ll, min((long long)nwin, target / max(P, 1ll)));
     const int ntask = (nwin + g - 1) / g;
     int base = -1;
-    if (ntask >= 2 && lane == 0)
+    // globally accumulated rows are queued even as a single task: their CTA
+    // would walk the entries once per shared-memory window
+    if ((GLOB ? ntask >= 1 : ntask >= 2) && lane == 0)
     {
         // room for all the tasks, or none at all (then the row keeps its own CTA)
         int old = *(volatile int *)&q->count;
@@ -618,7 +640,7 @@ __global__ void __launch_bounds__(PLAN_WARPS * 32)
     for (int t0 = cs0; t0 < cs1; t0 += 32)
     {
         const int t = t0 + lane;
-        const bool cut = win_cut<ACC>(c_tile_nnz, cs0, cs1, P0, t);
+        const bool cut = cuts(t);
         const unsigned wbal = __ballot_sync(FULL, cut);
         // a task starts at every g-th window
         const bool start = cut && (nw + __popc(wbal & ((1u << lane) - 1u))) % g == 0;
@@ -1016,6 +1038,197 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
     }
 }
 
+
+// Workers of globally accumulated heavy tile rows (NumericConfig::global_rows):
+// persistent CTAs take the tasks k_win_plan<..., true> queued - runs of
+// consecutive C tiles of a heavy row - and accumulate their products in C's
+// CSR value array itself.  Per task, in the CTA's slice of the scratch
+// arrays: the tile column -> task tile table, and per (task tile, row) the
+// row's entries before that tile (a scan of the masks' popcounts, from the
+// task's own per-row start); the task's entries get their columns and a zero
+// value.  Then each warp walks its two rows' A entries in column order, each
+// B row cut to the task's columns by two binary searches, and adds every
+// product at position row start + entries before the tile + entries before
+// the column in the tile.  A row belongs to one warp and the warp takes its
+// entries in order, with __syncwarp between entries (memory order among its
+// lanes): every output is summed in the (K, k) order of the shared-memory
+// kernel.  RED = false: read-modify-write with fma, bitwise that kernel's
+// result; RED = true: atomic adds of the rounded product (no wait on the
+// value), the same sums in the last bits' rounding.  Four entries' address
+// loads are issued ahead of their adds.
+template <bool RED>
+__global__ void __launch_bounds__(F_THREADS)
+    k_numeric_glob(DevTiles A, DevTiles B, int tilem, long long nnzC,
+                   const int *__restrict__ c_tile_col, const uint16_t *__restrict__ c_mask,
+                   const int *__restrict__ csr_rowptr, int *__restrict__ csr_col,
+                   double *__restrict__ csr_val, const WinTask *__restrict__ tasks, WinQueue *q,
+                   int cap, int tilen, int *__restrict__ slot_all, int *__restrict__ rel_all,
+                   int *err)
+{
+    __shared__ int s_tk, s_I, s_w0, s_w1;
+    __shared__ int s_run[TD], s_rp[TD + 1], s_ea[TD + 1];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int *slot = slot_all + (size_t)blockIdx.x * tilen;
+    int *rel = rel_all + (size_t)blockIdx.x * GLOB_RELCAP * TD;
+    const int ntasks = min(*(volatile int *)&q->count, cap);
+    for (;;)
+    {
+        __syncthreads(); // the previous task is done with the scratch arrays
+        if (tid == 0)
+            s_tk = atomicAdd(&q->head, 1);
+        __syncthreads();
+        const int tk = s_tk;
+        if (tk >= ntasks)
+            break;
+        if (tid == 0)
+        {
+            s_I = __ldg(&tasks[tk].I);
+            s_w0 = __ldg(&tasks[tk].w0);
+            s_w1 = __ldg(&tasks[tk].w1);
+        }
+        if (tid < TD)
+            s_run[tid] = __ldg(&tasks[tk].run[tid]);
+        __syncthreads();
+        const int I = s_I, w0 = s_w0, w1 = s_w1, nt = w1 - w0;
+        if (I < 0 || I >= tilem || nt <= 0 || nt > GLOB_RELCAP)
+        {
+            if (tid == 0)
+                set_error(err, DERR_WINDOW);
+            break; // uniform
+        }
+        const int nrows = min(TD, A.m - I * TD);
+        if (tid <= nrows)
+        {
+            s_rp[tid] = __ldg(csr_rowptr + I * TD + tid);
+            s_ea[tid] = __ldg(A.csr_rowptr + I * TD + tid);
+        }
+        for (int i = tid; i < nt; i += F_THREADS)
+        {
+            const int J = __ldg(c_tile_col + w0 + i);
+            if ((unsigned)J < (unsigned)tilen)
+                slot[J] = i;
+        }
+        __syncthreads();
+        // per (task tile, row): entries of the row before the tile; the task's
+        // entries get their columns and a zero value (warp w: rows 2w, 2w + 1)
+        for (int rr = 0; rr < RPW; ++rr)
+        {
+            const int r = warp * RPW + rr;
+            if (r >= nrows)
+                break; // warp-uniform
+            int carry = s_run[r];
+            for (int c0 = 0; c0 < nt; c0 += 32)
+            {
+                const int i = c0 + lane;
+                const uint32_t m = i < nt ? (uint32_t)__ldg(c_mask + (size_t)(w0 + i) * TD + r) : 0u;
+                const int pc = __popc(m);
+                const int incl = warp_incl_scan(pc);
+                const int off = carry + incl - pc;
+                if (i < nt)
+                {
+                    rel[i * TD + r] = off;
+                    const int J = __ldg(c_tile_col + w0 + i);
+                    const long long pos = (long long)s_rp[r] + off;
+                    uint32_t mm = m;
+                    for (int k = 0; mm != 0u; ++k)
+                    {
+                        const int c = __clz(mm) - 16;
+                        mm &= ~(0x8000u >> c);
+                        if (pos + k >= nnzC)
+                        {
+                            set_error(err, DERR_NUM_BOUNDS);
+                            break;
+                        }
+                        csr_col[pos + k] = J * TD + c;
+                        csr_val[pos + k] = 0.0;
+                    }
+                }
+                carry += __shfl_sync(FULL, incl, 31);
+            }
+        }
+        __syncthreads();
+        // products: the warp's rows, entries in column order
+        const int r0 = warp * RPW, r1 = r0 + RPW - 1;
+        if (r0 < nrows)
+        {
+            const int lo = __ldg(c_tile_col + w0) * TD, hi = (__ldg(c_tile_col + w1 - 1) + 1) * TD;
+            const int e_a = s_ea[r0], e_m = s_ea[min(r0 + 1, nrows)], e_e = s_ea[min(r1 + 1, nrows)];
+            for (int q0 = e_a; q0 < e_e; q0 += 32)
+            {
+                const int e = q0 + lane;
+                int fs = 0, len = 0, rq = r0;
+                double a = 0.0;
+                if (e < e_e)
+                {
+                    const int k = __ldg(A.csr_col + e);
+                    a = __ldg(A.csr_val + e);
+                    rq = e < e_m ? r0 : r1;
+                    if (k >= 0 && k < B.m)
+                    {
+                        const int f0 = min(max(__ldg(B.csr_rowptr + k), 0), B.nnz);
+                        const int f1 = min(max(__ldg(B.csr_rowptr + k + 1), f0), B.nnz);
+                        fs = lower_bound(B.csr_col, f0, f1, lo);
+                        len = lower_bound(B.csr_col, fs, f1, hi) - fs;
+                    }
+                }
+                // items of at most 32 products: entry j's B row in pieces of 32
+                const unsigned live = __ballot_sync(FULL, len > 0);
+                for (unsigned lv = live; lv != 0u; lv &= lv - 1u)
+                {
+                    const int j = __ffs(lv) - 1;
+                    const int jfs = __shfl_sync(FULL, fs, j), jlen = __shfl_sync(FULL, len, j);
+                    const int jr = __shfl_sync(FULL, rq, j);
+                    const double ja = __shfl_sync(FULL, a, j);
+                    const long long rbase = s_rp[jr];
+                    for (int f0 = 0; f0 < jlen; f0 += 4 * 32)
+                    {
+                        long long pos[4];
+                        double prod[4];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                        {
+                            pos[u] = -1;
+                            prod[u] = 0.0;
+                            const int f = f0 + u * 32 + lane;
+                            if (f < jlen)
+                            {
+                                const int col = __ldg(B.csr_col + jfs + f);
+                                const double b = __ldg(B.csr_val + jfs + f);
+                                const int J = col >> 4, c = col & 15;
+                                const int sl = (unsigned)J < (unsigned)tilen ? slot[J] : -1;
+                                if ((unsigned)sl < (unsigned)nt)
+                                {
+                                    const uint32_t w = __ldg(c_mask + (size_t)(w0 + sl) * TD + jr);
+                                    if (w & (0x8000u >> c))
+                                    {
+                                        pos[u] = rbase + rel[sl * TD + jr] + __popc(w >> (16 - c));
+                                        prod[u] = b;
+                                    }
+                                }
+                                if (pos[u] < 0 || pos[u] >= nnzC)
+                                {
+                                    set_error(err, DERR_NUM_BOUNDS);
+                                    pos[u] = -1;
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            if (pos[u] >= 0)
+                            {
+                                if (RED)
+                                    atomicAdd(csr_val + pos[u], ja * prod[u]);
+                                else
+                                    __stcg(csr_val + pos[u], fma(ja, prod[u], __ldcg(csr_val + pos[u])));
+                            }
+                    }
+                    __syncwarp(); // this entry's adds before the next entry's
+                }
+            }
+        }
+    }
+}
+
 } // namespace
 
 int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
@@ -1049,10 +1262,16 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
     // path), else from its tiles
     const bool acsr = A.csr_rowptr != nullptr && A.csr_col != nullptr && A.csr_val != nullptr;
     const long long target = cfg.split_target > 0 ? cfg.split_target : SPLIT_TARGET;
+    // heavy tile rows in global memory: fused CSR output, sorted B rows
+    // without repeated columns, A from its CSR rows
+    // (the per-CTA tile-column table limits it to at most 2^20 tile columns)
+    const bool glob = split && cfg.global_rows > 0 && acsr && !cfg.conflict_safe &&
+                      cfg.csr_col != nullptr && !cfg.write_tiles && S.tilen <= (1 << 20);
     if (split)
     {
         RTT_CUDA(cudaMemsetAsync(S.w_queue.p, 0, sizeof(WinQueue), s));
-        k_win_plan<ACC_SMALL><<<(S.tilem + PLAN_WARPS - 1) / PLAN_WARPS, PLAN_WARPS * 32, 0, s>>>(
+        auto plan = glob ? k_win_plan<ACC_SMALL, true> : k_win_plan<ACC_SMALL, false>;
+        plan<<<(S.tilem + PLAN_WARPS - 1) / PLAN_WARPS, PLAN_WARPS * 32, 0, s>>>(
             S.tilem, S.m, A, B, S.c_tile_ptr.as<int>(), S.c_tile_nnz.as<int>(),
             S.c_mask.as<uint16_t>(), fused_rowptr, S.w_heavy.as<uint8_t>(),
             S.w_task.as<WinTask>(), cap, target, S.w_queue.as<WinQueue>(), cfg.counters);
@@ -1072,7 +1291,28 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
         return RTT_OK;
     };
     const size_t smem = sizeof(FlatSmem<ACC_SMALL>);
-    if (split)
+    if (glob)
+    {
+        // the global-row workers, on the side stream beside the tile-row CTAs
+        auto gk = cfg.global_rows == 2 ? k_numeric_glob<true> : k_numeric_glob<false>;
+        int per_sm = 0, sms = 0;
+        RTT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gk, F_THREADS, 0));
+        RTT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws.device));
+        const int grid = std::max(1, per_sm * sms);
+        const int tilen = std::max(S.tilen, 1);
+        RTT_CHECK(S.g_slot.ensure(sizeof(int) * (size_t)grid * tilen, s));
+        RTT_CHECK(S.g_rel.ensure(sizeof(int) * (size_t)grid * GLOB_RELCAP * TD, s));
+        RTT_CUDA(cudaEventRecord(ws.fork_ev, s));
+        RTT_CUDA(cudaStreamWaitEvent(ws.side, ws.fork_ev, 0));
+        gk<<<grid, F_THREADS, 0, ws.side>>>(A, B, S.tilem, S.nnz, S.c_tile_col.as<int>(),
+                                            S.c_mask.as<uint16_t>(), fused_rowptr, cfg.csr_col,
+                                            cfg.csr_val, S.w_task.as<WinTask>(),
+                                            S.w_queue.as<WinQueue>(), cap, tilen,
+                                            S.g_slot.as<int>(), S.g_rel.as<int>(), ws.err.as<int>());
+        ws.launches++;
+        RTT_CUDA(cudaEventRecord(ws.join_ev, ws.side));
+    }
+    else if (split)
     {
         // The workers go first, on the side stream, so that the split rows'
         // tasks start while the tile-row CTAs run (the reference's heavy grid

@@ -322,6 +322,7 @@ struct SymbolicOut
     // numeric split of heavy tile rows: window tasks, per-tile-row flag, queue
     DevBuf w_task, w_heavy, w_queue, w_flag;
     DevBuf w_cursor; // per worker CTA: window cursors of its task's A entries
+    DevBuf g_slot, g_rel; // per global-row worker CTA: tile column table, row offsets
     // symbolic step 2: heavy tile rows (flag per tile row, list) and the
     // list of tile rows for the wide-window CTAs
     DevBuf s2_heavy, s2_list, s2_wlist;
@@ -346,7 +347,8 @@ struct SymbolicOut
                                &c_ptr,      &c_col,      &c_val,      &c_row_cnt,  &c_rowptr,
                                &c_tr_nnz,   &count_tmp,  &tile_cnt,   &w_task,     &w_heavy,
                                &w_queue,    &w_flag,     &s2_heavy,   &s2_list,
-                               &s2_wlist,   &s1_list,    &w_cursor};
+                               &s2_wlist,   &s1_list,    &w_cursor,   &g_slot,
+                               &g_rel};
         for (const DevBuf *b : all)
             f(*b);
     }
@@ -382,6 +384,9 @@ struct NumericConfig
     bool conflict_safe = false;     // B rows may repeat a column: accumulate with shared atomics
     bool segment_walk = false;      // the numeric step may walk B's row segments
     bool persistent_rows = false;   // tile-row CTAs as one resident wave over a device queue
+    // heavy tile rows accumulated in C's CSR values in global memory: 0 off,
+    // 1 read-modify-write (bitwise the shared-memory result), 2 atomic adds
+    int global_rows = 0;
 };
 
 // CSR row pointer of C (m + 1 ints) from the symbolic counts

@@ -85,7 +85,7 @@ class Config(C.Structure):
                 ("split_target", C.c_int), ("cuda_graphs", C.c_int),
                 ("chunk_tiles", C.c_int), ("chunk_nnz", C.c_int),
                 ("segment_walk", C.c_int), ("persistent_rows", C.c_int),
-                ("sym_window_slots", C.c_int), ("leaf_dmma", C.c_int)]
+                ("sym_window_slots", C.c_int), ("leaf_dmma", C.c_int), ("global_rows", C.c_int)]
 
 
 class HybridTiles(C.Structure):

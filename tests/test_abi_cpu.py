@@ -88,7 +88,8 @@ def test_bad_arguments_rejected_before_device_work():
     assert cfg.cuda_graphs == 1  # repeated numeric phases replay a CUDA graph
     assert cfg.sym_window_slots == 0  # wide step-2 windows at their default size
     assert cfg.leaf_dmma == 0  # the scalar numeric kernel by default
-    assert C.sizeof(R.Config) == 13 * 4
+    assert cfg.global_rows == 0
+    assert C.sizeof(R.Config) == 14 * 4
 
 
 def test_generators_shapes():

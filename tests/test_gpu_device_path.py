@@ -142,7 +142,9 @@ def test_many_window_rows_fused_equals_tiles(case, orc):
                       ("fused_split1", dict(fused_csr_output=1, split_target=1)),
                       ("tiled_split1", dict(fused_csr_output=0, split_target=1)),
                       ("fused_split64k", dict(fused_csr_output=1, split_target=1 << 16)),
-                      ("fused_nosplit", dict(fused_csr_output=1, split_target=-1))):
+                      ("fused_nosplit", dict(fused_csr_output=1, split_target=-1)),
+                      # heavy rows accumulated in C's values in device memory
+                      ("fused_global", dict(fused_csr_output=1, global_rows=1))):
         ctx = R.Context(0, cfg)
         runs[name] = _run(ctx, A)
         # split_target 1: every multi-window row becomes one task per window
@@ -163,6 +165,27 @@ def test_many_window_rows_fused_equals_tiles(case, orc):
     assert_csr_close(fused[0], fused[1], fused[2], erp, ecol, evals, eabs, f"{case}: ")
 
 
+@pytest.mark.parametrize("case", list(MANY_WINDOW_CASES))
+def test_global_rows_atomic_adds(case, orc):
+    """Heavy tile rows accumulated with atomic adds (global_rows = 2): the
+    structure of the shared-memory result, values within the bound of the
+    oracle; the products of one output still come in the row's entry order,
+    so two runs agree bit for bit."""
+    A = MANY_WINDOW_CASES[case]()
+    runs = []
+    for _ in range(2):
+        ctx = R.Context(0, dict(global_rows=2))
+        runs.append(_run(ctx, A))
+        assert ctx.stats()["split_windows"] > 0 or case == "unsorted_wide"
+        ctx.close()
+    ctx = R.Context(0)
+    ref = _run(ctx, A)
+    ctx.close()
+    assert np.array_equal(runs[0][0], ref[0]) and np.array_equal(runs[0][1], ref[1])
+    assert np.array_equal(runs[0][2].view(np.int64), runs[1][2].view(np.int64))
+    assert_csr_close(*runs[0][:3], *orc.spgemm_csr(A, A), f"{case} global atomics: ")
+
+
 def test_split_cursors_past_the_cap(orc):
     """Tile rows of 40,000 A entries (2,500 per row) against B rows of two
     scattered entries: about 40 windows per tile row, grouped 13 to a task by
@@ -180,6 +203,7 @@ def test_split_cursors_past_the_cap(orc):
     runs = {}
     for name, cfg in (("split", dict(fused_csr_output=1)),
                       ("nosplit", dict(fused_csr_output=1, split_target=-1)),
+                      ("global", dict(fused_csr_output=1, global_rows=1)),
                       ("tiled", dict(fused_csr_output=0))):
         ctx = R.Context(0, cfg)
         runs[name] = _run(ctx, A, B)
