@@ -505,6 +505,18 @@ __device__ __forceinline__ bool win_cut(const int *c_tile_nnz, int cs0, int cs1,
 // accumulate in C's own value array, so no shared-memory window bounds it.
 constexpr int GLOB_H = 8192;
 constexpr int GLOB_RELCAP = GLOB_H + 256; // C tiles of one task, at most
+// The atomic form keeps a task's tile table and (row offset, mask) words in
+// shared memory: a task holds at most GNT C tiles whose tile columns lie in
+// one aligned block of GSPAN (the cuts fall on multiples of both).
+constexpr int GNT = 512, GSPAN = 4096;
+__device__ __forceinline__ bool glob2_cut(const int *c_tile_col, int cs0, int cs1, int t)
+{
+    if (t >= cs1)
+        return false;
+    if (t == cs0 || (t - cs0) % GNT == 0)
+        return true;
+    return __ldg(c_tile_col + t) / GSPAN != __ldg(c_tile_col + t - 1) / GSPAN;
+}
 __device__ __forceinline__ bool glob_cut(const int *c_tile_nnz, int cs0, int cs1, int P0, int t)
 {
     if (t >= cs1)
@@ -516,10 +528,11 @@ __device__ __forceinline__ bool glob_cut(const int *c_tile_nnz, int cs0, int cs1
 
 // One warp per C tile row: decide heavy or not, and queue the windows of a
 // heavy one.  heavy[I] = 1 tells the numeric kernel's CTA for I to exit.
-template <int ACC, bool GLOB = false>
+template <int ACC, int GMODE = 0>
 __global__ void __launch_bounds__(PLAN_WARPS * 32)
     k_win_plan(int tilem, int m, DevTiles A, DevTiles B,
-               const int *__restrict__ c_tile_ptr, const int *__restrict__ c_tile_nnz,
+               const int *__restrict__ c_tile_ptr, const int *__restrict__ c_tile_col,
+               const int *__restrict__ c_tile_nnz,
                const uint16_t *__restrict__ c_mask, const int *__restrict__ csr_rowptr,
                uint8_t *__restrict__ heavy, WinTask *__restrict__ tasks, int cap,
                long long target, WinQueue *q, long long *counters)
@@ -555,8 +568,11 @@ __global__ void __launch_bounds__(PLAN_WARPS * 32)
         return;
     }
     const int P0 = __ldg(c_tile_nnz + cs0);
+    constexpr bool GLOB = GMODE != 0;
     auto cuts = [&](int t) {
-        return GLOB ? glob_cut(c_tile_nnz, cs0, cs1, P0, t) : win_cut<ACC>(c_tile_nnz, cs0, cs1, P0, t);
+        return GMODE == 2   ? glob2_cut(c_tile_col, cs0, cs1, t)
+               : GMODE == 1 ? glob_cut(c_tile_nnz, cs0, cs1, P0, t)
+                            : win_cut<ACC>(c_tile_nnz, cs0, cs1, P0, t);
     };
     int nwin = 0;
     for (int t0 = cs0; t0 < cs1; t0 += 32)
@@ -1229,6 +1245,164 @@ __global__ void __launch_bounds__(F_THREADS)
     }
 }
 
+
+// The atomic form of the global-row workers (global_rows = 2): a task's
+// tile column -> tile table (u16 over its GSPAN block) and per (tile, row)
+// word (entries of the row before the tile within the task << 16 | row mask)
+// live in shared memory, so a product costs two shared loads and one atomic
+// add into C's value array.  The task's A entries are shared by all warps
+// (32 at a time, each entry's row found among the 16 row starts), so a hub
+// row does not leave seven warps waiting; products of one output then come
+// from several warps in no fixed order, and the values agree with the other
+// kernels to the FP64 bound, not bit for bit.
+__global__ void __launch_bounds__(F_THREADS)
+    k_numeric_glob2(DevTiles A, DevTiles B, int tilem, long long nnzC,
+                    const int *__restrict__ c_tile_col, const uint16_t *__restrict__ c_mask,
+                    const int *__restrict__ csr_rowptr, int *__restrict__ csr_col,
+                    double *__restrict__ csr_val, const WinTask *__restrict__ tasks, WinQueue *q,
+                    int cap, int *err)
+{
+    extern __shared__ __align__(16) unsigned char g2_raw[];
+    uint32_t *s_cm = reinterpret_cast<uint32_t *>(g2_raw);          // GNT * TD words
+    uint16_t *s_slot = reinterpret_cast<uint16_t *>(s_cm + GNT * TD); // GSPAN
+    __shared__ int s_tk, s_I, s_w0, s_w1, s_jlo;
+    __shared__ int s_run[TD], s_rp[TD + 1], s_ea[TD + 1];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ntasks = min(*(volatile int *)&q->count, cap);
+    for (;;)
+    {
+        __syncthreads(); // the previous task is done with shared memory
+        if (tid == 0)
+            s_tk = atomicAdd(&q->head, 1);
+        __syncthreads();
+        const int tk = s_tk;
+        if (tk >= ntasks)
+            break;
+        if (tid == 0)
+        {
+            s_I = __ldg(&tasks[tk].I);
+            s_w0 = __ldg(&tasks[tk].w0);
+            s_w1 = __ldg(&tasks[tk].w1);
+            s_jlo = __ldg(c_tile_col + s_w0);
+        }
+        if (tid < TD)
+            s_run[tid] = __ldg(&tasks[tk].run[tid]);
+        __syncthreads();
+        const int I = s_I, w0 = s_w0, w1 = s_w1, nt = w1 - w0, jlo = s_jlo;
+        const int jspan = nt > 0 ? __ldg(c_tile_col + w1 - 1) - jlo + 1 : 0;
+        if (I < 0 || I >= tilem || nt <= 0 || nt > GNT || jspan > GSPAN)
+        {
+            if (tid == 0)
+                set_error(err, DERR_WINDOW);
+            break; // uniform
+        }
+        const int nrows = min(TD, A.m - I * TD);
+        if (tid <= nrows)
+        {
+            s_rp[tid] = __ldg(csr_rowptr + I * TD + tid);
+            s_ea[tid] = __ldg(A.csr_rowptr + I * TD + tid);
+        }
+        for (int i = tid; i < nt; i += F_THREADS)
+            s_slot[__ldg(c_tile_col + w0 + i) - jlo] = (uint16_t)i;
+        // per (tile, row): entries before the tile in the task, row mask; the
+        // task's entries get their columns and a zero value
+        for (int rr = 0; rr < RPW; ++rr)
+        {
+            const int r = warp * RPW + rr;
+            if (r >= nrows)
+                break; // warp-uniform
+            int carry = 0;
+            for (int c0 = 0; c0 < nt; c0 += 32)
+            {
+                const int i = c0 + lane;
+                const uint32_t m = i < nt ? (uint32_t)__ldg(c_mask + (size_t)(w0 + i) * TD + r) : 0u;
+                const int pc = __popc(m);
+                const int incl = warp_incl_scan(pc);
+                const int off = carry + incl - pc;
+                if (i < nt)
+                {
+                    s_cm[i * TD + r] = ((uint32_t)off << 16) | m;
+                    const int J = __ldg(c_tile_col + w0 + i);
+                    const long long pos = (long long)__ldg(csr_rowptr + I * TD + r) + s_run[r] + off;
+                    uint32_t mm = m;
+                    for (int k = 0; mm != 0u; ++k)
+                    {
+                        const int c = __clz(mm) - 16;
+                        mm &= ~(0x8000u >> c);
+                        if (pos + k >= nnzC)
+                        {
+                            set_error(err, DERR_NUM_BOUNDS);
+                            break;
+                        }
+                        csr_col[pos + k] = J * TD + c;
+                        csr_val[pos + k] = 0.0;
+                    }
+                }
+                carry += __shfl_sync(FULL, incl, 31);
+            }
+        }
+        __syncthreads();
+        // products: the task's A entries, 32 per warp at a time
+        const int lo = jlo * TD, hi = (jlo + jspan) * TD;
+        const int ea = s_ea[0], ee = s_ea[nrows];
+        for (int q0 = ea + warp * 32; q0 < ee; q0 += F_THREADS)
+        {
+            const int e = q0 + lane;
+            int fs = 0, len = 0, r = 0;
+            double a = 0.0;
+            if (e < ee)
+            {
+#pragma unroll
+                for (int h = 8; h > 0; h >>= 1)
+                    if (r + h < nrows && s_ea[r + h] <= e)
+                        r += h;
+                const int k = __ldg(A.csr_col + e);
+                a = __ldg(A.csr_val + e);
+                if (k >= 0 && k < B.m)
+                {
+                    const int f0 = min(max(__ldg(B.csr_rowptr + k), 0), B.nnz);
+                    const int f1 = min(max(__ldg(B.csr_rowptr + k + 1), f0), B.nnz);
+                    fs = lower_bound(B.csr_col, f0, f1, lo);
+                    len = lower_bound(B.csr_col, fs, f1, hi) - fs;
+                }
+            }
+            for (unsigned lv = __ballot_sync(FULL, len > 0); lv != 0u; lv &= lv - 1u)
+            {
+                const int j = __ffs(lv) - 1;
+                const int jfs = __shfl_sync(FULL, fs, j), jlen = __shfl_sync(FULL, len, j);
+                const int jr = __shfl_sync(FULL, r, j);
+                const double ja = __shfl_sync(FULL, a, j);
+                const long long rbase = (long long)s_rp[jr] + s_run[jr];
+                for (int f = lane; f < jlen; f += 32)
+                {
+                    const int col = __ldg(B.csr_col + jfs + f);
+                    const double b = __ldg(B.csr_val + jfs + f);
+                    const int d = (col >> 4) - jlo, c = col & 15;
+                    if ((unsigned)d >= (unsigned)GSPAN)
+                    {
+                        set_error(err, DERR_NUM_BOUNDS);
+                        continue;
+                    }
+                    const int sl = s_slot[d];
+                    if (sl >= nt) // a tile column of no task tile: cannot happen
+                    {
+                        set_error(err, DERR_NUM_BOUNDS);
+                        continue;
+                    }
+                    const uint32_t w = s_cm[sl * TD + jr];
+                    const long long pos = rbase + (w >> 16) + __popc((w & 0xFFFFu) >> (16 - c));
+                    if ((w & (0x8000u >> c)) == 0u || pos >= nnzC)
+                    {
+                        set_error(err, DERR_NUM_BOUNDS);
+                        continue;
+                    }
+                    atomicAdd(csr_val + pos, ja * b);
+                }
+            }
+        }
+    }
+}
+
 } // namespace
 
 int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, SymbolicOut &S,
@@ -1266,13 +1440,17 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
     // without repeated columns, A from its CSR rows
     // (the per-CTA tile-column table limits it to at most 2^20 tile columns)
     const bool glob = split && cfg.global_rows > 0 && acsr && !cfg.conflict_safe &&
-                      cfg.csr_col != nullptr && !cfg.write_tiles && S.tilen <= (1 << 20);
+                      cfg.csr_col != nullptr && !cfg.write_tiles &&
+                      (cfg.global_rows == 2 || S.tilen <= (1 << 20));
     if (split)
     {
         RTT_CUDA(cudaMemsetAsync(S.w_queue.p, 0, sizeof(WinQueue), s));
-        auto plan = glob ? k_win_plan<ACC_SMALL, true> : k_win_plan<ACC_SMALL, false>;
+        auto plan = !glob                  ? k_win_plan<ACC_SMALL, 0>
+                    : cfg.global_rows == 2 ? k_win_plan<ACC_SMALL, 2>
+                                           : k_win_plan<ACC_SMALL, 1>;
         plan<<<(S.tilem + PLAN_WARPS - 1) / PLAN_WARPS, PLAN_WARPS * 32, 0, s>>>(
-            S.tilem, S.m, A, B, S.c_tile_ptr.as<int>(), S.c_tile_nnz.as<int>(),
+            S.tilem, S.m, A, B, S.c_tile_ptr.as<int>(), S.c_tile_col.as<int>(),
+            S.c_tile_nnz.as<int>(),
             S.c_mask.as<uint16_t>(), fused_rowptr, S.w_heavy.as<uint8_t>(),
             S.w_task.as<WinTask>(), cap, target, S.w_queue.as<WinQueue>(), cfg.counters);
         ws.launches++;
@@ -1294,21 +1472,38 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
     if (glob)
     {
         // the global-row workers, on the side stream beside the tile-row CTAs
-        auto gk = cfg.global_rows == 2 ? k_numeric_glob<true> : k_numeric_glob<false>;
         int per_sm = 0, sms = 0;
-        RTT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gk, F_THREADS, 0));
         RTT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ws.device));
-        const int grid = std::max(1, per_sm * sms);
-        const int tilen = std::max(S.tilen, 1);
-        RTT_CHECK(S.g_slot.ensure(sizeof(int) * (size_t)grid * tilen, s));
-        RTT_CHECK(S.g_rel.ensure(sizeof(int) * (size_t)grid * GLOB_RELCAP * TD, s));
         RTT_CUDA(cudaEventRecord(ws.fork_ev, s));
         RTT_CUDA(cudaStreamWaitEvent(ws.side, ws.fork_ev, 0));
-        gk<<<grid, F_THREADS, 0, ws.side>>>(A, B, S.tilem, S.nnz, S.c_tile_col.as<int>(),
-                                            S.c_mask.as<uint16_t>(), fused_rowptr, cfg.csr_col,
-                                            cfg.csr_val, S.w_task.as<WinTask>(),
-                                            S.w_queue.as<WinQueue>(), cap, tilen,
-                                            S.g_slot.as<int>(), S.g_rel.as<int>(), ws.err.as<int>());
+        if (cfg.global_rows == 2)
+        {
+            const size_t gsm = sizeof(uint32_t) * GNT * TD + sizeof(uint16_t) * GSPAN;
+            RTT_CUDA(cudaFuncSetAttribute(k_numeric_glob2,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
+            RTT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_numeric_glob2,
+                                                                   F_THREADS, gsm));
+            const int grid = std::max(1, per_sm * sms);
+            k_numeric_glob2<<<grid, F_THREADS, gsm, ws.side>>>(
+                A, B, S.tilem, S.nnz, S.c_tile_col.as<int>(), S.c_mask.as<uint16_t>(),
+                fused_rowptr, cfg.csr_col, cfg.csr_val, S.w_task.as<WinTask>(),
+                S.w_queue.as<WinQueue>(), cap, ws.err.as<int>());
+        }
+        else
+        {
+            auto gk = k_numeric_glob<false>;
+            RTT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gk, F_THREADS, 0));
+            const int grid = std::max(1, per_sm * sms);
+            const int tilen = std::max(S.tilen, 1);
+            RTT_CHECK(S.g_slot.ensure(sizeof(int) * (size_t)grid * tilen, s));
+            RTT_CHECK(S.g_rel.ensure(sizeof(int) * (size_t)grid * GLOB_RELCAP * TD, s));
+            gk<<<grid, F_THREADS, 0, ws.side>>>(A, B, S.tilem, S.nnz, S.c_tile_col.as<int>(),
+                                                S.c_mask.as<uint16_t>(), fused_rowptr, cfg.csr_col,
+                                                cfg.csr_val, S.w_task.as<WinTask>(),
+                                                S.w_queue.as<WinQueue>(), cap, tilen,
+                                                S.g_slot.as<int>(), S.g_rel.as<int>(),
+                                                ws.err.as<int>());
+        }
         ws.launches++;
         RTT_CUDA(cudaEventRecord(ws.join_ev, ws.side));
     }

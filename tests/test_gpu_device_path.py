@@ -167,23 +167,20 @@ def test_many_window_rows_fused_equals_tiles(case, orc):
 
 @pytest.mark.parametrize("case", list(MANY_WINDOW_CASES))
 def test_global_rows_atomic_adds(case, orc):
-    """Heavy tile rows accumulated with atomic adds (global_rows = 2): the
+    """Heavy tile rows accumulated with atomic adds (global_rows = 2, the
+    task's tables in shared memory, its entries shared by all warps): the
     structure of the shared-memory result, values within the bound of the
-    oracle; the products of one output still come in the row's entry order,
-    so two runs agree bit for bit."""
+    oracle (the order of the adds is not fixed)."""
     A = MANY_WINDOW_CASES[case]()
-    runs = []
-    for _ in range(2):
-        ctx = R.Context(0, dict(global_rows=2))
-        runs.append(_run(ctx, A))
-        assert ctx.stats()["split_windows"] > 0 or case == "unsorted_wide"
-        ctx.close()
+    ctx = R.Context(0, dict(global_rows=2))
+    got = _run(ctx, A)
+    assert ctx.stats()["split_windows"] > 0 or case == "unsorted_wide"
+    ctx.close()
     ctx = R.Context(0)
     ref = _run(ctx, A)
     ctx.close()
-    assert np.array_equal(runs[0][0], ref[0]) and np.array_equal(runs[0][1], ref[1])
-    assert np.array_equal(runs[0][2].view(np.int64), runs[1][2].view(np.int64))
-    assert_csr_close(*runs[0][:3], *orc.spgemm_csr(A, A), f"{case} global atomics: ")
+    assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+    assert_csr_close(*got[:3], *orc.spgemm_csr(A, A), f"{case} global atomics: ")
 
 
 def test_split_cursors_past_the_cap(orc):
