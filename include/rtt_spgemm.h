@@ -487,11 +487,15 @@ typedef struct
     /* C tile rows that need several shared-memory windows (R-MAT rows) are
      * cut into tasks of about 8192 C entries that accumulate straight into
      * C's CSR values in device memory, so each A entry is walked once per
-     * task instead of once per window: 0 = off, 1 = read-modify-write in
-     * each row's (K, k) order (bitwise the same C), 2 = atomic adds of the
-     * products (values within the FP64 bound).  Only with the fused CSR
-     * output, sorted B rows without repeated columns and at most 2^20 tile
-     * columns; otherwise the windows. */
+     * task instead of once per window: 0 = off (the default), 1 =
+     * read-modify-write in each row's (K, k) order (bitwise the same C, but
+     * slower than the windows: a warp per row leaves the others waiting on
+     * hub rows), 2 = atomic adds, the task's tables in shared memory and its
+     * entries shared by all warps (R-MAT 2^16 A*A^T numeric 21.0 -> 14.0 ms
+     * on B200; values within the FP64 bound, their last bits depending on
+     * the order of the adds).  Only with the fused CSR output and sorted B
+     * rows without repeated columns (1: at most 2^20 tile columns);
+     * otherwise the windows. */
     int global_rows;
 } rtt_config;
 

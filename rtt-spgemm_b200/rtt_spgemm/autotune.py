@@ -15,7 +15,10 @@ The knobs (rtt_config fields):
   tile rows with more C tiles than 254 run in wide-window CTAs of this many
   slots (0: 2045, -1: never);
 * ``persistent_rows`` - tile-row CTAs as one resident wave over a device
-  queue instead of one CTA per tile row.
+  queue instead of one CTA per tile row;
+* ``global_rows`` - tile rows that need several shared-memory windows
+  accumulate in C's values in device memory (2: atomic adds, the values to
+  the FP64 bound but not bit for bit).
 
 A shape class is the operation (A*A, A*A^T, A*B), and the base-2 buckets of
 the row count, the mean entries per row and the row-length skew (longest row
@@ -46,6 +49,7 @@ CANDIDATES = [
     {"dmma_pair_cutoff": 0, "b_staging": 0, "split_target": 0, "sym_window_slots": -1},
     {"dmma_pair_cutoff": 0, "b_staging": 0, "split_target": 0, "sym_window_slots": 4093},
     {"dmma_pair_cutoff": 0, "b_staging": 0, "split_target": 0, "persistent_rows": 1},
+    {"dmma_pair_cutoff": 0, "b_staging": 0, "split_target": 0, "global_rows": 2},
 ]
 
 OPS = {0: "AB", 1: "AAT"}
