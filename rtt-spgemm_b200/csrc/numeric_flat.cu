@@ -508,7 +508,7 @@ constexpr int GLOB_RELCAP = GLOB_H + 256; // C tiles of one task, at most
 // The atomic form keeps a task's tile table and (row offset, mask) words in
 // shared memory: a task holds at most GNT C tiles whose tile columns lie in
 // one aligned block of GSPAN (the cuts fall on multiples of both).
-constexpr int GNT = 512, GSPAN = 4096;
+constexpr int GNT = 256, GSPAN = 4096;
 __device__ __forceinline__ bool glob2_cut(const int *c_tile_col, int cs0, int cs1, int t)
 {
     if (t >= cs1)
