@@ -1068,11 +1068,9 @@ __global__ void __launch_bounds__(F_THREADS, MIN_CTAS)
 // the column in the tile.  A row belongs to one warp and the warp takes its
 // entries in order, with __syncwarp between entries (memory order among its
 // lanes): every output is summed in the (K, k) order of the shared-memory
-// kernel.  RED = false: read-modify-write with fma, bitwise that kernel's
-// result; RED = true: atomic adds of the rounded product (no wait on the
-// value), the same sums in the last bits' rounding.  Four entries' address
-// loads are issued ahead of their adds.
-template <bool RED>
+// kernel, by read-modify-write with fma, bitwise that kernel's result.
+// Four pieces of an entry's B row have their addresses loaded ahead of their
+// adds.
 __global__ void __launch_bounds__(F_THREADS)
     k_numeric_glob(DevTiles A, DevTiles B, int tilem, long long nnzC,
                    const int *__restrict__ c_tile_col, const uint16_t *__restrict__ c_mask,
@@ -1231,12 +1229,7 @@ __global__ void __launch_bounds__(F_THREADS)
 #pragma unroll
                         for (int u = 0; u < 4; ++u)
                             if (pos[u] >= 0)
-                            {
-                                if (RED)
-                                    atomicAdd(csr_val + pos[u], ja * prod[u]);
-                                else
-                                    __stcg(csr_val + pos[u], fma(ja, prod[u], __ldcg(csr_val + pos[u])));
-                            }
+                                __stcg(csr_val + pos[u], fma(ja, prod[u], __ldcg(csr_val + pos[u])));
                     }
                     __syncwarp(); // this entry's adds before the next entry's
                 }
@@ -1491,7 +1484,7 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
         }
         else
         {
-            auto gk = k_numeric_glob<false>;
+            auto gk = k_numeric_glob;
             RTT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gk, F_THREADS, 0));
             const int grid = std::max(1, per_sm * sms);
             const int tilen = std::max(S.tilen, 1);
