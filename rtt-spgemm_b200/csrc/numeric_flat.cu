@@ -505,17 +505,18 @@ __device__ __forceinline__ bool win_cut(const int *c_tile_nnz, int cs0, int cs1,
 // accumulate in C's own value array, so no shared-memory window bounds it.
 constexpr int GLOB_H = 8192;
 constexpr int GLOB_RELCAP = GLOB_H + 256; // C tiles of one task, at most
-// The atomic form keeps a task's tile table and (row offset, mask) words in
-// shared memory: a task holds at most GNT C tiles whose tile columns lie in
-// one aligned block of GSPAN (the cuts fall on multiples of both).
-constexpr int GNT = 256, GSPAN = 4096;
+// The atomic form keeps a task's tile table (an open-addressing hash of its
+// tile columns: a task's tiles may lie anywhere in the row) and (row offset,
+// mask) words in shared memory: a task holds at most GNT C tiles.
+constexpr int GNT = 256, GHASH = 2 * GNT;
 __device__ __forceinline__ bool glob2_cut(const int *c_tile_col, int cs0, int cs1, int t)
 {
-    if (t >= cs1)
-        return false;
-    if (t == cs0 || (t - cs0) % GNT == 0)
-        return true;
-    return __ldg(c_tile_col + t) / GSPAN != __ldg(c_tile_col + t - 1) / GSPAN;
+    (void)c_tile_col;
+    return t < cs1 && (t == cs0 || (t - cs0) % GNT == 0);
+}
+__device__ __forceinline__ int glob2_hash(int J)
+{
+    return (int)(((unsigned)J * 0x9E3779B1u) >> 23) & (GHASH - 1); // 9 bits
 }
 __device__ __forceinline__ bool glob_cut(const int *c_tile_nnz, int cs0, int cs1, int P0, int t)
 {
@@ -1240,7 +1241,7 @@ __global__ void __launch_bounds__(F_THREADS)
 
 
 // The atomic form of the global-row workers (global_rows = 2): a task's
-// tile column -> tile table (u16 over its GSPAN block) and per (tile, row)
+// tile column -> tile table (a shared-memory hash) and per (tile, row)
 // word (entries of the row before the tile within the task << 16 | row mask)
 // live in shared memory, so a product costs two shared loads and one atomic
 // add into C's value array.  The task's A entries are shared by all warps
@@ -1256,8 +1257,9 @@ __global__ void __launch_bounds__(F_THREADS)
                     int cap, int *err)
 {
     extern __shared__ __align__(16) unsigned char g2_raw[];
-    uint32_t *s_cm = reinterpret_cast<uint32_t *>(g2_raw);          // GNT * TD words
-    uint16_t *s_slot = reinterpret_cast<uint16_t *>(s_cm + GNT * TD); // GSPAN
+    uint32_t *s_cm = reinterpret_cast<uint32_t *>(g2_raw);  // GNT * TD words
+    int *s_hk = reinterpret_cast<int *>(s_cm + GNT * TD);   // GHASH tile columns (-1: empty)
+    uint16_t *s_hv = reinterpret_cast<uint16_t *>(s_hk + GHASH); // their task tiles
     __shared__ int s_tk, s_I, s_w0, s_w1, s_jlo;
     __shared__ int s_run[TD], s_rp[TD + 1], s_ea[TD + 1];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1283,7 +1285,7 @@ __global__ void __launch_bounds__(F_THREADS)
         __syncthreads();
         const int I = s_I, w0 = s_w0, w1 = s_w1, nt = w1 - w0, jlo = s_jlo;
         const int jspan = nt > 0 ? __ldg(c_tile_col + w1 - 1) - jlo + 1 : 0;
-        if (I < 0 || I >= tilem || nt <= 0 || nt > GNT || jspan > GSPAN)
+        if (I < 0 || I >= tilem || nt <= 0 || nt > GNT)
         {
             if (tid == 0)
                 set_error(err, DERR_WINDOW);
@@ -1295,8 +1297,21 @@ __global__ void __launch_bounds__(F_THREADS)
             s_rp[tid] = __ldg(csr_rowptr + I * TD + tid);
             s_ea[tid] = __ldg(A.csr_rowptr + I * TD + tid);
         }
+        for (int i = tid; i < GHASH; i += F_THREADS)
+            s_hk[i] = -1;
+        __syncthreads();
         for (int i = tid; i < nt; i += F_THREADS)
-            s_slot[__ldg(c_tile_col + w0 + i) - jlo] = (uint16_t)i;
+        {
+            // the task's tile columns are distinct: linear probing finds a free slot
+            const int J = __ldg(c_tile_col + w0 + i);
+            int h = glob2_hash(J);
+            for (int p = 0; p < GHASH; ++p, h = (h + 1) & (GHASH - 1))
+                if (atomicCAS(&s_hk[h], -1, J) == -1)
+                {
+                    s_hv[h] = (uint16_t)i;
+                    break;
+                }
+        }
         // per (tile, row): entries before the tile in the task, row mask; the
         // task's entries get their columns and a zero value
         for (int rr = 0; rr < RPW; ++rr)
@@ -1370,14 +1385,21 @@ __global__ void __launch_bounds__(F_THREADS)
                 {
                     const int col = __ldg(B.csr_col + jfs + f);
                     const double b = __ldg(B.csr_val + jfs + f);
-                    const int d = (col >> 4) - jlo, c = col & 15;
-                    if ((unsigned)d >= (unsigned)GSPAN)
+                    const int J = col >> 4, c = col & 15;
+                    int sl = -1;
+                    int h = glob2_hash(J);
+                    for (int p = 0; p < GHASH; ++p, h = (h + 1) & (GHASH - 1))
                     {
-                        set_error(err, DERR_NUM_BOUNDS);
-                        continue;
+                        const int key = s_hk[h];
+                        if (key == J)
+                        {
+                            sl = s_hv[h];
+                            break;
+                        }
+                        if (key < 0)
+                            break;
                     }
-                    const int sl = s_slot[d];
-                    if (sl >= nt) // a tile column of no task tile: cannot happen
+                    if ((unsigned)sl >= (unsigned)nt) // a column of no task tile: cannot happen
                     {
                         set_error(err, DERR_NUM_BOUNDS);
                         continue;
@@ -1471,7 +1493,8 @@ int numeric_flat_device(Workspace &ws, const DevTiles &A, const DevTiles &B, Sym
         RTT_CUDA(cudaStreamWaitEvent(ws.side, ws.fork_ev, 0));
         if (cfg.global_rows == 2)
         {
-            const size_t gsm = sizeof(uint32_t) * GNT * TD + sizeof(uint16_t) * GSPAN;
+            const size_t gsm = sizeof(uint32_t) * GNT * TD + sizeof(int) * GHASH +
+                               sizeof(uint16_t) * GHASH;
             RTT_CUDA(cudaFuncSetAttribute(k_numeric_glob2,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsm));
             RTT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_numeric_glob2,
