@@ -509,6 +509,8 @@ constexpr int GLOB_RELCAP = GLOB_H + 256; // C tiles of one task, at most
 // tile columns: a task's tiles may lie anywhere in the row) and (row offset,
 // mask) words in shared memory: a task holds at most GNT C tiles.
 constexpr int GNT = 256, GHASH = 2 * GNT;
+// rows of fewer shared-memory windows than this stay with the windows
+constexpr int GLOB_MIN_WINDOWS = 4;
 __device__ __forceinline__ bool glob2_cut(const int *c_tile_col, int cs0, int cs1, int t)
 {
     (void)c_tile_col;
@@ -578,6 +580,21 @@ __global__ void __launch_bounds__(PLAN_WARPS * 32)
     int nwin = 0;
     for (int t0 = cs0; t0 < cs1; t0 += 32)
         nwin += __popc(__ballot_sync(FULL, cuts(t0 + lane)));
+    if (GMODE == 2)
+    {
+        // only rows that the shared-memory kernel would walk in many windows
+        // go to device memory: a row of a few windows keeps its CTA (the
+        // atomic adds cost more than its re-walks)
+        int nstd = 0;
+        for (int t0 = cs0; t0 < cs1; t0 += 32)
+            nstd += __popc(__ballot_sync(FULL, win_cut<ACC>(c_tile_nnz, cs0, cs1, P0, t0 + lane)));
+        if (nstd < GLOB_MIN_WINDOWS)
+        {
+            if (lane == 0)
+                heavy[I] = 0;
+            return;
+        }
+    }
     // Cost of one window: the tile row's products, since every window walks
     // all of them (the cost model of the reference's tail queue, products
     // standing in for its scan/match terms).  A task takes g consecutive

@@ -174,7 +174,8 @@ def test_global_rows_atomic_adds(case, orc):
     A = MANY_WINDOW_CASES[case]()
     ctx = R.Context(0, dict(global_rows=2))
     got = _run(ctx, A)
-    assert ctx.stats()["split_windows"] > 0 or case == "unsorted_wide"
+    if case.startswith("rmat"):  # rows of many windows: tasks in device memory
+        assert ctx.stats()["split_windows"] > 0
     ctx.close()
     ctx = R.Context(0)
     ref = _run(ctx, A)
