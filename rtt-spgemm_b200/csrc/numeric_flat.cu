@@ -1329,8 +1329,8 @@ __global__ void __launch_bounds__(F_THREADS)
                     break;
                 }
         }
-        // per (tile, row): entries before the tile in the task, row mask; the
-        // task's entries get their columns and a zero value
+        // per (tile, row): entries before the tile in the task and the row
+        // mask (a scan per row, warp w: rows 2w, 2w + 1) ...
         for (int rr = 0; rr < RPW; ++rr)
         {
             const int r = warp * RPW + rr;
@@ -1343,27 +1343,36 @@ __global__ void __launch_bounds__(F_THREADS)
                 const uint32_t m = i < nt ? (uint32_t)__ldg(c_mask + (size_t)(w0 + i) * TD + r) : 0u;
                 const int pc = __popc(m);
                 const int incl = warp_incl_scan(pc);
-                const int off = carry + incl - pc;
                 if (i < nt)
-                {
-                    s_cm[i * TD + r] = ((uint32_t)off << 16) | m;
-                    const int J = __ldg(c_tile_col + w0 + i);
-                    const long long pos = (long long)__ldg(csr_rowptr + I * TD + r) + s_run[r] + off;
-                    uint32_t mm = m;
-                    for (int k = 0; mm != 0u; ++k)
-                    {
-                        const int c = __clz(mm) - 16;
-                        mm &= ~(0x8000u >> c);
-                        if (pos + k >= nnzC)
-                        {
-                            set_error(err, DERR_NUM_BOUNDS);
-                            break;
-                        }
-                        csr_col[pos + k] = J * TD + c;
-                        csr_val[pos + k] = 0.0;
-                    }
-                }
+                    s_cm[i * TD + r] = ((uint32_t)(carry + incl - pc) << 16) | m;
                 carry += __shfl_sync(FULL, incl, 31);
+            }
+        }
+        __syncthreads();
+        // ... then the task's entries get their columns and a zero value,
+        // all threads over the (tile, row) pairs (a hub row is shared out)
+        for (int x = tid; x < nt * TD; x += F_THREADS)
+        {
+            const int i = x >> 4, r = x & 15;
+            if (r >= nrows)
+                continue;
+            const uint32_t w = s_cm[i * TD + r];
+            uint32_t mm = w & 0xFFFFu;
+            if (mm == 0u)
+                continue;
+            const int J = __ldg(c_tile_col + w0 + i);
+            const long long pos = (long long)s_rp[r] + s_run[r] + (w >> 16);
+            for (int k = 0; mm != 0u; ++k)
+            {
+                const int c = __clz(mm) - 16;
+                mm &= ~(0x8000u >> c);
+                if (pos + k >= nnzC)
+                {
+                    set_error(err, DERR_NUM_BOUNDS);
+                    break;
+                }
+                csr_col[pos + k] = J * TD + c;
+                csr_val[pos + k] = 0.0;
             }
         }
         __syncthreads();
