@@ -492,7 +492,7 @@ typedef struct
      * slower than the windows: a warp per row leaves the others waiting on
      * hub rows), 2 = atomic adds for rows of at least 4 windows, the task's
      * tables in shared memory and its entries shared by all warps (rows of
-     * fewer windows keep them; R-MAT 2^16 A*A^T numeric 21.0 -> 14.0 ms
+     * fewer windows keep them; R-MAT 2^16 A*A^T numeric 21.0 -> 13.0 ms
      * on B200; values within the FP64 bound, their last bits depending on
      * the order of the adds).  Only with the fused CSR output and sorted B
      * rows without repeated columns (1: at most 2^20 tile columns);
